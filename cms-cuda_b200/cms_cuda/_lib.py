@@ -1,0 +1,266 @@
+"""
+ctypes binding of ``libcms_b200.so`` (C ABI in ``include/cms_b200.h``).
+
+The library is built in-tree (``cms-cuda_b200/build.py``) and loaded from
+this directory.  There is no CPU fallback: if the library or a GPU is
+missing, calls fail loudly.
+"""
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcms_b200.so")
+
+CMS_HOST, CMS_DEVICE = 0, 1
+OK, ERR_ARG, ERR_CUDA, ERR_STATE, ERR_COINCIDENT, ERR_EMPTY, ERR_CAPACITY = 0, -1, -2, -3, -4, -5, -6
+ST_COINCIDENT, ST_EMPTY, ST_OVERFLOW, ST_NEAR_OVERFLOW = 1, 2, 4, 8
+SC_FIELDS, SC_SIDE_FIELDS = 5, 7
+
+# every symbol the header declares
+EXPORTED = (
+    "cms_ctx_create", "cms_ctx_destroy", "cms_set_settings", "cms_get_settings", "cms_load_batch",
+    "cms_generate_surfaces", "cms_contact_ms", "cms_max_contact_ms", "cms_shape_complementarity",
+    "cms_complex_info_get", "cms_export_atoms", "cms_export_neighbors", "cms_export_toroid",
+    "cms_export_probes", "cms_export_dots", "cms_export_trimmed", "cms_run_graph", "cms_kernel_launches",
+    "cms_last_error", "cms_version", "cms_device_count",
+)
+
+
+class Settings(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in
+                ("rp", "density", "band", "sep", "weight", "binwidth_dist", "binwidth_norm")]
+
+
+class ComplexInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_atoms", ctypes.c_int64), ("n_binder", ctypes.c_int64),
+        ("nb_entries", ctypes.c_int64), ("bu_entries", ctypes.c_int64),
+        ("max_nb", ctypes.c_int64), ("max_bu", ctypes.c_int64),
+        ("n_toroid", ctypes.c_int64), ("n_probes", ctypes.c_int64),
+        ("n_probes_plus", ctypes.c_int64 * 2), ("n_probes_minus", ctypes.c_int64 * 2),
+        ("n_dots", ctypes.c_int64 * 2), ("n_trimmed", ctypes.c_int64 * 2),
+        ("convex", ctypes.c_int64), ("toroidal", ctypes.c_int64), ("concave", ctypes.c_int64),
+        ("status", ctypes.c_int32), ("coincident_i", ctypes.c_int32), ("coincident_j", ctypes.c_int32),
+        ("radmax", ctypes.c_double),
+    ]
+
+
+class CmsError(RuntimeError):
+    """Error reported by the CUDA library."""
+
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+_lib = None
+_lock = threading.Lock()
+
+_VP = ctypes.c_void_p
+_I32 = ctypes.c_int32
+_PI64 = ctypes.POINTER(ctypes.c_int64)
+
+
+def load():
+    """Load the CUDA library once; raises OSError when it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing: build it with `python cms-cuda_b200/build.py`")
+        lib = ctypes.CDLL(LIB_PATH)
+        sig = {
+            "cms_ctx_create": [ctypes.POINTER(_VP), ctypes.c_int, _VP],
+            "cms_ctx_destroy": [_VP],
+            "cms_set_settings": [_VP, ctypes.POINTER(Settings)],
+            "cms_get_settings": [_VP, ctypes.POINTER(Settings)],
+            "cms_load_batch": [_VP, _I32, _PI64, _PI64, _VP, _VP, _VP, _I32],
+            "cms_generate_surfaces": [_VP, _I32],
+            "cms_contact_ms": [_VP, _VP, _VP, _I32],
+            "cms_max_contact_ms": [_VP, _VP, _VP, _I32],
+            "cms_shape_complementarity": [_VP, _VP, _VP, _I32],
+            "cms_complex_info_get": [_VP, _I32, ctypes.POINTER(ComplexInfo)],
+            "cms_export_atoms": [_VP, _I32, _VP, _VP, _VP, _VP],
+            "cms_export_neighbors": [_VP, _I32, _VP, _VP, _VP, _VP],
+            "cms_export_toroid": [_VP, _I32, _VP, _VP, _VP, _VP, _VP, _VP],
+            "cms_export_probes": [_VP, _I32, _VP, _VP, _VP, _VP, _VP, _VP],
+            "cms_export_dots": [_VP, _I32, _I32, _VP, _VP, _VP, _VP, _VP, _VP],
+            "cms_export_trimmed": [_VP, _I32, _I32, _VP],
+            "cms_run_graph": [_VP],
+        }
+        for name, args in sig.items():
+            f = getattr(lib, name)
+            f.argtypes = args
+            f.restype = ctypes.c_int32
+        lib.cms_kernel_launches.argtypes = [_VP]
+        lib.cms_kernel_launches.restype = ctypes.c_int64
+        lib.cms_last_error.argtypes = [_VP]
+        lib.cms_last_error.restype = ctypes.c_char_p
+        lib.cms_version.argtypes = []
+        lib.cms_version.restype = ctypes.c_char_p
+        lib.cms_device_count.argtypes = []
+        lib.cms_device_count.restype = ctypes.c_int32
+        _lib = lib
+        return lib
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+class Context:
+    """One device context (one CUDA stream) of the library; not thread-safe."""
+
+    def __init__(self, device=0, stream=None):
+        self.lib = load()
+        h = ctypes.c_void_p()
+        st = self.lib.cms_ctx_create(ctypes.byref(h), int(device), ctypes.c_void_p(stream) if stream else None)
+        self.h = h
+        self._check(st)
+        self.B = 0
+        self.N = 0
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) and self.h.value:
+                self.lib.cms_ctx_destroy(self.h)
+                self.h = ctypes.c_void_p()
+        except Exception:
+            pass
+
+    def close(self):
+        self.__del__()
+
+    def _check(self, status):
+        if status != OK:
+            msg = self.lib.cms_last_error(self.h).decode() if self.h.value else "context creation failed"
+            raise CmsError(status, msg)
+
+    # -- settings / inputs ----------------------------------------------------
+    def set_settings(self, s):
+        v = Settings(float(s.rp), float(s.density), float(s.band), float(s.sep), float(s.weight),
+                     float(s.binwidth_dist), float(s.binwidth_norm))
+        self._check(self.lib.cms_set_settings(self.h, ctypes.byref(v)))
+
+    def load_batch(self, atom_off, n_binder, xyz, radius, density=None):
+        atom_off = np.ascontiguousarray(atom_off, dtype=np.int64)
+        n_binder = np.ascontiguousarray(n_binder, dtype=np.int64)
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        radius = np.ascontiguousarray(radius, dtype=np.float64)
+        if density is not None:
+            density = np.ascontiguousarray(density, dtype=np.float64)
+        B = len(n_binder)
+        if len(atom_off) != B + 1 or atom_off[-1] != len(radius) or len(xyz) != len(radius):
+            raise ValueError("inconsistent batch arrays")
+        self._check(self.lib.cms_load_batch(self.h, B, atom_off.ctypes.data_as(_PI64),
+                                            n_binder.ctypes.data_as(_PI64), _ptr(xyz), _ptr(radius),
+                                            _ptr(density), CMS_HOST))
+        self.B, self.N = B, int(atom_off[-1])
+
+    def load_batch_device(self, atom_off, n_binder, xyz_ptr, radius_ptr, density_ptr=None):
+        """Device-pointer variant (e.g. torch tensors' data_ptr())."""
+        atom_off = np.ascontiguousarray(atom_off, dtype=np.int64)
+        n_binder = np.ascontiguousarray(n_binder, dtype=np.int64)
+        self._check(self.lib.cms_load_batch(self.h, len(n_binder), atom_off.ctypes.data_as(_PI64),
+                                            n_binder.ctypes.data_as(_PI64), ctypes.c_void_p(xyz_ptr),
+                                            ctypes.c_void_p(radius_ptr),
+                                            ctypes.c_void_p(density_ptr) if density_ptr else None, CMS_DEVICE))
+        self.B, self.N = len(n_binder), int(atom_off[-1])
+
+    # -- pipeline -------------------------------------------------------------
+    def generate(self, all_atoms=False):
+        self._check(self.lib.cms_generate_surfaces(self.h, 1 if all_atoms else 0))
+
+    def run_graph(self):
+        self._check(self.lib.cms_run_graph(self.h))
+
+    def kernel_launches(self):
+        return int(self.lib.cms_kernel_launches(self.h))
+
+    def contact_ms(self):
+        per_atom = np.empty(self.N, dtype=np.float64)
+        totals = np.empty(2 * self.B, dtype=np.float64)
+        self._check(self.lib.cms_contact_ms(self.h, _ptr(per_atom), _ptr(totals), CMS_HOST))
+        return per_atom, totals.reshape(self.B, 2)
+
+    def max_contact_ms(self):
+        per_atom = np.empty(self.N, dtype=np.float64)
+        totals = np.empty(self.B, dtype=np.float64)
+        self._check(self.lib.cms_max_contact_ms(self.h, _ptr(per_atom), _ptr(totals), CMS_HOST))
+        return per_atom, totals
+
+    def shape_complementarity(self):
+        sc = np.empty(self.B * SC_FIELDS, dtype=np.float64)
+        sides = np.empty(self.B * 2 * SC_SIDE_FIELDS, dtype=np.float64)
+        self._check(self.lib.cms_shape_complementarity(self.h, _ptr(sc), _ptr(sides), CMS_HOST))
+        return sc.reshape(self.B, SC_FIELDS), sides.reshape(self.B, 2, SC_SIDE_FIELDS)
+
+    # -- exports --------------------------------------------------------------
+    def info(self, c):
+        i = ComplexInfo()
+        self._check(self.lib.cms_complex_info_get(self.h, int(c), ctypes.byref(i)))
+        return i
+
+    def export_atoms(self, c, n):
+        atten = np.empty(n, np.int8); access = np.empty(n, np.int8)
+        nn = np.empty(n, np.int32); nb = np.empty(n, np.int32)
+        self._check(self.lib.cms_export_atoms(self.h, int(c), _ptr(atten), _ptr(access), _ptr(nn), _ptr(nb)))
+        return atten, access, nn, nb
+
+    def export_neighbors(self, c, n, info):
+        nb_off = np.empty(n + 1, np.int64); nb_id = np.empty(max(info.nb_entries, 1), np.int32)
+        bu_off = np.empty(n + 1, np.int64); bu_id = np.empty(max(info.bu_entries, 1), np.int32)
+        self._check(self.lib.cms_export_neighbors(self.h, int(c), _ptr(nb_off), _ptr(nb_id), _ptr(bu_off),
+                                                  _ptr(bu_id)))
+        return nb_off, nb_id[:info.nb_entries], bu_off, bu_id[:info.bu_entries]
+
+    def export_toroid(self, c, info):
+        n = info.n_toroid
+        a1 = np.empty(max(n, 1), np.int32); a2 = np.empty(max(n, 1), np.int32)
+        uij = np.empty((max(n, 1), 3)); tij = np.empty((max(n, 1), 3)); rij = np.empty(max(n, 1))
+        bet = np.empty(max(n, 1), np.int8)
+        self._check(self.lib.cms_export_toroid(self.h, int(c), _ptr(a1), _ptr(a2), _ptr(uij), _ptr(tij), _ptr(rij),
+                                               _ptr(bet)))
+        return a1[:n], a2[:n], uij[:n], tij[:n], rij[:n], bet[:n].astype(bool)
+
+    def export_probes(self, c, info):
+        n = max(info.n_probes, 1)
+        a0 = np.empty(n, np.int32); a1 = np.empty(n, np.int32); a2 = np.empty(n, np.int32)
+        h = np.empty(n); pt = np.empty((n, 3)); alt = np.empty((n, 3))
+        self._check(self.lib.cms_export_probes(self.h, int(c), _ptr(a0), _ptr(a1), _ptr(a2), _ptr(h), _ptr(pt),
+                                               _ptr(alt)))
+        k = info.n_probes
+        return a0[:k], a1[:k], a2[:k], h[:k], pt[:k], alt[:k]
+
+    def export_dots(self, c, m, info):
+        n = max(info.n_dots[m], 1)
+        coor = np.empty((n, 3)); nml = np.empty((n, 3)); area = np.empty(n)
+        bur = np.empty(n, np.int8); typ = np.empty(n, np.int8); atom = np.empty(n, np.int32)
+        self._check(self.lib.cms_export_dots(self.h, int(c), int(m), _ptr(coor), _ptr(nml), _ptr(area), _ptr(bur),
+                                             _ptr(typ), _ptr(atom)))
+        k = info.n_dots[m]
+        return coor[:k], nml[:k], area[:k], bur[:k], typ[:k], atom[:k]
+
+    def export_trimmed(self, c, m, info):
+        n = max(info.n_trimmed[m], 1)
+        idx = np.empty(n, np.int32)
+        self._check(self.lib.cms_export_trimmed(self.h, int(c), int(m), _ptr(idx)))
+        return idx[:info.n_trimmed[m]]
+
+
+def device_count():
+    try:
+        return int(load().cms_device_count())
+    except OSError:
+        return 0
+
+
+def version():
+    return load().cms_version().decode()

@@ -1,0 +1,978 @@
+// C ABI of libcms_b200.so: context, device workspace, pipeline orchestration
+// (stage-synchronised sizing path and CUDA-graph path) and exports.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cms_b200.h"
+#include "cms_readout.cuh"
+
+using namespace cms;
+
+namespace {
+
+struct DBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+__global__ void k_pack_atoms(long long N, const double* xyz, const double* rad, const double* dens_in, double dens,
+                             double4* xyzr, double* dens_out)
+{
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < N; g += (long long)gridDim.x * blockDim.x) {
+        xyzr[g] = make_double4(xyz[3 * g], xyz[3 * g + 1], xyz[3 * g + 2], rad[g]);
+        dens_out[g] = dens_in ? dens_in[g] : dens;
+    }
+}
+
+__global__ void k_fill_d(double* p, long long n, double v)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = v;
+}
+
+__global__ void k_fill_i(int* p, long long n, int v)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = v;
+}
+
+// totals the host needs after a run: cells, neighbour / buried entries,
+// toroid pairs, probes, dots, buried dots, trimmed dots
+__global__ void k_summary(Dev d, Rd r, long long* out)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        out[0] = d.ncell_scan[d.B];
+        out[1] = d.nb_off[d.N];
+        out[2] = d.bu_off[d.N];
+        out[3] = d.tor_off[d.N];
+        out[4] = d.plus_off[d.N] + d.minus_off[d.N];
+        out[5] = d.dot_off[2LL * d.B];
+    }
+}
+
+// toroid queue geometry for export (second_loop formulas, _core.py:1372-1416)
+__global__ void k_export_toroid(Dev d, long long q0, long long n, double* out)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const long long q = q0 + k;
+        const int i = d.tor_i[q], j = d.tor_j[q];
+        const double rp = d.st.rp;
+        double4 a = d.xyzr[i], b = d.xyzr[j];
+        V3 xi = v3(a.x, a.y, a.z), xj = v3(b.x, b.y, b.z);
+        V3 diff = xj - xi;
+        double dij_sq = sq_alt(diff);
+        double dij = sqrt(dij_sq);
+        double eri = a.w + rp, erj = b.w + rp;
+        double asymm = (eri * eri - erj * erj) / dij;
+        V3 uij = diff / dij;
+        V3 tij = ((xi + xj) * 0.5) + uij * (asymm * 0.5);
+        double far_sq = (eri + erj) * (eri + erj) - dij_sq;
+        double rd = a.w - b.w;
+        double cont_sq = dij_sq - rd * rd;
+        double rij = ((0.5 * sqrt(far_sq)) * sqrt(cont_sq)) / dij;
+        double* o = out + 8 * k;
+        o[0] = uij.x; o[1] = uij.y; o[2] = uij.z;
+        o[3] = tij.x; o[4] = tij.y; o[5] = tij.z;
+        o[6] = rij;
+        o[7] = fabs(asymm) < dij ? 1.0 : 0.0;
+    }
+}
+
+}  // namespace
+
+struct cms_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cms_settings st{1.7, 15.0, 1.5, 8.0, 0.5, 0.02, 0.02};
+    int B = 0;
+    long long N = 0;
+    std::vector<int64_t> h_off, h_n0;
+    std::vector<DBuf> bufs;
+    Dev d{};
+    Rd r{};
+    long long cap_cells = 0, cap_nb = 0, cap_bu = 0, cap_tor = 0, cap_probe = 0, cap_dot = 0;
+    long long tot[8] = {0};
+    bool have_batch = false, surf_ok = false, cms_ok = false, sc_ok = false, max_ok = false;
+    int surf_all_atoms = -1;
+    long long* pinned = nullptr;
+    // per-complex host mirrors (valid after generation)
+    std::vector<long long> h_nb_off_b, h_plus, h_minus, h_dot_off, h_tor_off_b;
+    std::vector<int> h_status;
+    std::vector<unsigned long long> h_coin;
+    std::vector<Seg> h_seg;
+    std::vector<double> h_radmax;
+    // graph
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+    long long graph_key[3] = {-1, -1, -1};
+    long long launches = -1;
+    std::string err;
+
+    // named buffer slots
+    enum Slot {
+        S_IN_XYZ, S_IN_RAD, S_IN_DENS, S_ATOM_OFF, S_N0, S_XYZR, S_DENS, S_CPLX, S_MOL, S_ATTEN, S_ACCESS, S_CELL_OF,
+        S_CX, S_NCELL, S_NCELL_SCAN, S_STATUS, S_COIN, S_CELL_CNT, S_CELL_START, S_CELL_FILL, S_CELL_ATOM,
+        S_NNB, S_NB_OFF, S_NBUR, S_BU_OFF, S_NB_ID, S_NB_D2, S_NB_TMP, S_BU_ID,
+        S_NTOR, S_TOR_OFF, S_TOR_I, S_TOR_J,
+        S_NPLUS, S_PLUS_OFF, S_NMINUS, S_MINUS_OFF, S_PA0, S_PA1, S_PA2, S_PH, S_PXYZ, S_PALT, S_PLOW_FLAG, S_PLOW_OFF,
+        S_PLOW_LIST,
+        S_CONV_CNT, S_CONV_OFF, S_TOR1_CNT, S_TOR1_OFF, S_TOR2_CNT, S_TOR2_OFF, S_TOR_HAS, S_CONC_CNT, S_CONC_OFF,
+        S_SEG, S_DOT_OFF, S_DXYZ, S_DNML, S_DAREA, S_DBUR, S_DTYPE, S_DATOM, S_DUNIT, S_DSUB, S_TOR_LAST1, S_TOR_LAST2,
+        S_R_FLAG, S_R_BUR_SCAN, S_R_BUR_IDX, S_R_BUR_F4, S_R_BUR_CM, S_R_ACC_IDX, S_R_ACC_F4, S_R_KEEP, S_R_TRIM_SCAN,
+        S_R_TRIM_IDX, S_R_TRIM_F4, S_R_NN_D2, S_R_NN_IDX, S_R_VAL, S_R_OWN, S_R_ACNT, S_R_AFILL, S_R_AOFF, S_R_ASLOT,
+        S_CM_TMP, S_SCAN_TMP, S_PER_ATOM_CMS, S_TOT_CMS, S_PER_ATOM_MAX, S_TOT_MAX, S_SC_SIDE, S_SC_OUT, S_TASKS,
+        S_TILE_CNT, S_TILE_OFF, S_SUMMARY, S_EXPORT, S_COUNT
+    };
+
+    cms_ctx() : bufs(S_COUNT) {}
+
+    template <class T>
+    T* ensure(int slot, long long count)
+    {
+        size_t need = (size_t)std::max<long long>(count, 1) * sizeof(T);
+        DBuf& b = bufs[slot];
+        if (b.bytes < need) {
+            if (b.p) cudaFree(b.p);
+            size_t alloc = need + need / 4;
+            b.p = nullptr;
+            b.bytes = 0;
+            if (cudaMalloc(&b.p, alloc) != cudaSuccess) {
+                b.p = nullptr;
+                throw std::string("device allocation failed");
+            }
+            b.bytes = alloc;
+        }
+        return (T*)b.p;
+    }
+    template <class T>
+    T* get(int slot) { return (T*)bufs[slot].p; }
+};
+
+namespace {
+
+struct Fail {
+    cms_status code;
+    std::string msg;
+};
+
+void ck(cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess) throw Fail{CMS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+long long read_ll(cms_ctx* x, const long long* dev)
+{
+    ck(cudaMemcpyAsync(x->pinned, dev, sizeof(long long), cudaMemcpyDeviceToHost, x->stream), "readback");
+    ck(cudaStreamSynchronize(x->stream), "sync");
+    return x->pinned[0];
+}
+
+unsigned grid1(long long n) { long long b = (n + 255) / 256; return (unsigned)std::max(1LL, std::min(b, 148LL * 16)); }
+
+// (re)bind every per-atom / per-complex buffer for the current batch
+void bind_batch(cms_ctx* x)
+{
+    const long long N = x->N, B = x->B;
+    Dev& d = x->d;
+    d.B = x->B;
+    d.N = N;
+    d.atom_off = x->ensure<int>(cms_ctx::S_ATOM_OFF, B + 1);
+    d.n0 = x->ensure<int>(cms_ctx::S_N0, B);
+    d.xyzr = x->ensure<double4>(cms_ctx::S_XYZR, N);
+    d.dens = x->ensure<double>(cms_ctx::S_DENS, N);
+    d.cplx = x->ensure<int>(cms_ctx::S_CPLX, N);
+    d.mol = x->ensure<int8_t>(cms_ctx::S_MOL, N);
+    d.atten = x->ensure<int8_t>(cms_ctx::S_ATTEN, N);
+    d.access = x->ensure<int8_t>(cms_ctx::S_ACCESS, N);
+    d.cell_of = x->ensure<int>(cms_ctx::S_CELL_OF, N);
+    d.cx = x->ensure<Cplx>(cms_ctx::S_CX, B);
+    d.ncell = x->ensure<int>(cms_ctx::S_NCELL, B);
+    d.ncell_scan = x->ensure<long long>(cms_ctx::S_NCELL_SCAN, B + 1);
+    d.status = x->ensure<int>(cms_ctx::S_STATUS, B);
+    d.coin = x->ensure<unsigned long long>(cms_ctx::S_COIN, B);
+    d.cell_atom = x->ensure<int>(cms_ctx::S_CELL_ATOM, N);
+    d.nnb = x->ensure<int>(cms_ctx::S_NNB, N);
+    d.nb_off = x->ensure<long long>(cms_ctx::S_NB_OFF, N + 1);
+    d.nbur = x->ensure<int>(cms_ctx::S_NBUR, N);
+    d.bu_off = x->ensure<long long>(cms_ctx::S_BU_OFF, N + 1);
+    d.ntor = x->ensure<int>(cms_ctx::S_NTOR, N);
+    d.tor_off = x->ensure<long long>(cms_ctx::S_TOR_OFF, N + 1);
+    d.nplus = x->ensure<int>(cms_ctx::S_NPLUS, N);
+    d.plus_off = x->ensure<long long>(cms_ctx::S_PLUS_OFF, N + 1);
+    d.nminus = x->ensure<int>(cms_ctx::S_NMINUS, N);
+    d.minus_off = x->ensure<long long>(cms_ctx::S_MINUS_OFF, N + 1);
+    d.conv_cnt = x->ensure<int>(cms_ctx::S_CONV_CNT, N);
+    d.conv_off = x->ensure<long long>(cms_ctx::S_CONV_OFF, N + 1);
+    d.seg = x->ensure<Seg>(cms_ctx::S_SEG, 8 * B);
+    d.dot_off = x->ensure<long long>(cms_ctx::S_DOT_OFF, 2 * B + 1);
+    d.tor_last1 = x->ensure<unsigned long long>(cms_ctx::S_TOR_LAST1, N);
+    d.tor_last2 = x->ensure<unsigned long long>(cms_ctx::S_TOR_LAST2, N);
+    Rd& r = x->r;
+    r.acnt = x->ensure<int>(cms_ctx::S_R_ACNT, N);
+    r.afill = x->ensure<int>(cms_ctx::S_R_AFILL, N);
+    r.aoff = x->ensure<long long>(cms_ctx::S_R_AOFF, N + 1);
+    x->ensure<int>(cms_ctx::S_CM_TMP, 2 * B + 2);
+    x->ensure<double>(cms_ctx::S_PER_ATOM_CMS, N);
+    x->ensure<double>(cms_ctx::S_TOT_CMS, 2 * B);
+    x->ensure<double>(cms_ctx::S_PER_ATOM_MAX, N);
+    x->ensure<double>(cms_ctx::S_TOT_MAX, 2 * B);
+    x->ensure<double>(cms_ctx::S_SC_SIDE, 2 * B * SC_SIDE_FIELDS);
+    x->ensure<double>(cms_ctx::S_SC_OUT, B * SC_FIELDS);
+    x->ensure<NNTask>(cms_ctx::S_TASKS, 3 * 2 * B);
+    x->ensure<int>(cms_ctx::S_TILE_CNT, 2 * B);
+    x->ensure<long long>(cms_ctx::S_TILE_OFF, 2 * B + 1);
+    x->ensure<long long>(cms_ctx::S_SUMMARY, 8);
+}
+
+void bind_caps(cms_ctx* x)
+{
+    Dev& d = x->d;
+    Rd& r = x->r;
+    d.cells_cap = x->cap_cells;
+    d.cell_cnt = x->ensure<int>(cms_ctx::S_CELL_CNT, x->cap_cells);
+    d.cell_fill = x->ensure<int>(cms_ctx::S_CELL_FILL, x->cap_cells);
+    d.cell_start = x->ensure<long long>(cms_ctx::S_CELL_START, x->cap_cells + 1);
+    d.nb_cap = x->cap_nb;
+    d.bu_cap = x->cap_bu;
+    d.nb_id = x->ensure<int>(cms_ctx::S_NB_ID, x->cap_nb);
+    d.nb_tmp = x->ensure<int>(cms_ctx::S_NB_TMP, x->cap_nb);
+    d.nb_d2 = x->ensure<double>(cms_ctx::S_NB_D2, x->cap_nb);
+    d.bu_id = x->ensure<int>(cms_ctx::S_BU_ID, x->cap_bu);
+    d.tor_cap = x->cap_tor;
+    d.tor_i = x->ensure<int>(cms_ctx::S_TOR_I, x->cap_tor);
+    d.tor_j = x->ensure<int>(cms_ctx::S_TOR_J, x->cap_tor);
+    d.tor1_cnt = x->ensure<int>(cms_ctx::S_TOR1_CNT, x->cap_tor);
+    d.tor2_cnt = x->ensure<int>(cms_ctx::S_TOR2_CNT, x->cap_tor);
+    d.tor1_off = x->ensure<long long>(cms_ctx::S_TOR1_OFF, x->cap_tor + 1);
+    d.tor2_off = x->ensure<long long>(cms_ctx::S_TOR2_OFF, x->cap_tor + 1);
+    d.tor_has = x->ensure<int8_t>(cms_ctx::S_TOR_HAS, x->cap_tor);
+    d.probe_cap = x->cap_probe;
+    d.pa0 = x->ensure<int>(cms_ctx::S_PA0, x->cap_probe);
+    d.pa1 = x->ensure<int>(cms_ctx::S_PA1, x->cap_probe);
+    d.pa2 = x->ensure<int>(cms_ctx::S_PA2, x->cap_probe);
+    d.ph = x->ensure<double>(cms_ctx::S_PH, x->cap_probe);
+    d.pxyz = x->ensure<double>(cms_ctx::S_PXYZ, 3 * x->cap_probe);
+    d.palt = x->ensure<double>(cms_ctx::S_PALT, 3 * x->cap_probe);
+    d.plow_flag = x->ensure<int>(cms_ctx::S_PLOW_FLAG, x->cap_probe);
+    d.plow_off = x->ensure<long long>(cms_ctx::S_PLOW_OFF, x->cap_probe + 1);
+    d.plow_list = x->ensure<int>(cms_ctx::S_PLOW_LIST, x->cap_probe);
+    d.conc_cnt = x->ensure<int>(cms_ctx::S_CONC_CNT, x->cap_probe);
+    d.conc_off = x->ensure<long long>(cms_ctx::S_CONC_OFF, x->cap_probe + 1);
+    d.dot_cap = x->cap_dot;
+    const long long D = x->cap_dot;
+    d.dxyz = x->ensure<double>(cms_ctx::S_DXYZ, 3 * D);
+    d.dnml = x->ensure<double>(cms_ctx::S_DNML, 3 * D);
+    d.darea = x->ensure<double>(cms_ctx::S_DAREA, D);
+    d.dbur = x->ensure<int8_t>(cms_ctx::S_DBUR, D);
+    d.dtype = x->ensure<int8_t>(cms_ctx::S_DTYPE, D);
+    d.datom = x->ensure<int>(cms_ctx::S_DATOM, D);
+    d.dunit = x->ensure<int>(cms_ctx::S_DUNIT, D);
+    d.dsub = x->ensure<int>(cms_ctx::S_DSUB, D);
+    r.flag = x->ensure<int>(cms_ctx::S_R_FLAG, D);
+    r.bur_scan = x->ensure<long long>(cms_ctx::S_R_BUR_SCAN, D + 1);
+    r.bur_idx = x->ensure<int>(cms_ctx::S_R_BUR_IDX, D);
+    r.bur_f4 = x->ensure<float4>(cms_ctx::S_R_BUR_F4, D);
+    r.bur_cm = x->ensure<int>(cms_ctx::S_R_BUR_CM, D);
+    r.acc_idx = x->ensure<int>(cms_ctx::S_R_ACC_IDX, D);
+    r.acc_f4 = x->ensure<float4>(cms_ctx::S_R_ACC_F4, D);
+    r.keep = x->ensure<int>(cms_ctx::S_R_KEEP, D);
+    r.trim_scan = x->ensure<long long>(cms_ctx::S_R_TRIM_SCAN, D + 1);
+    r.trim_idx = x->ensure<int>(cms_ctx::S_R_TRIM_IDX, D);
+    r.trim_f4 = x->ensure<float4>(cms_ctx::S_R_TRIM_F4, D);
+    r.nn_d2 = x->ensure<double>(cms_ctx::S_R_NN_D2, D);
+    r.nn_idx = x->ensure<int>(cms_ctx::S_R_NN_IDX, D);
+    r.val = x->ensure<double>(cms_ctx::S_R_VAL, D);
+    r.own = x->ensure<int>(cms_ctx::S_R_OWN, D);
+    r.aslot = x->ensure<int>(cms_ctx::S_R_ASLOT, D);
+    long long mx = std::max({x->N + 1, x->cap_cells + 1, x->cap_tor + 1, x->cap_probe + 1, D + 1, 2LL * x->B + 2});
+    x->ensure<long long>(cms_ctx::S_SCAN_TMP, scan_tmp_elems(mx) + 8);
+}
+
+void set_settings_dev(cms_ctx* x)
+{
+    x->d.st.rp = x->st.rp; x->d.st.density = x->st.density; x->d.st.band = x->st.band; x->d.st.sep = x->st.sep;
+    x->d.st.weight = x->st.weight; x->d.st.bw_dist = x->st.binwidth_dist; x->d.st.bw_norm = x->st.binwidth_norm;
+}
+
+long long* scan_tmp(cms_ctx* x) { return x->get<long long>(cms_ctx::S_SCAN_TMP); }
+
+// ---------------------------------------------------------------------------
+// the pipeline.  sized = true: read each stage's total back and grow the
+// buffers to fit (host syncs between stages); sized = false: enqueue every
+// stage with the current capacities (capturable in a CUDA graph).
+// ---------------------------------------------------------------------------
+void grow(long long& cap, long long need)
+{
+    if (need > cap) cap = need + need / 8 + 64;
+}
+
+void enqueue_surface(cms_ctx* x, bool sized)
+{
+    Dev& d = x->d;
+    cudaStream_t s = x->stream;
+    long long* tmp = scan_tmp(x);
+    ck(cudaMemsetAsync(d.status, 0, sizeof(int) * x->B, s), "memset");
+    launch_setup(d, s);
+    scan_counts(d.ncell, d.ncell_scan, d.B, tmp, s);
+    if (sized) {
+        long long nc = read_ll(x, d.ncell_scan + d.B);
+        grow(x->cap_cells, nc);
+        bind_caps(x);
+        tmp = scan_tmp(x);
+    }
+    launch_cells(d, x->cap_cells, tmp, s);
+    launch_attention(d, s);
+    launch_neighbor_count(d, s);
+    scan_counts(d.nnb, d.nb_off, d.N, tmp, s);
+    scan_counts(d.nbur, d.bu_off, d.N, tmp, s);
+    if (sized) {
+        grow(x->cap_nb, read_ll(x, d.nb_off + d.N));
+        grow(x->cap_bu, read_ll(x, d.bu_off + d.N));
+        bind_caps(x);
+        tmp = scan_tmp(x);
+    }
+    launch_neighbor_emit(d, s);
+    launch_pairs(d, false, s);
+    scan_counts(d.ntor, d.tor_off, d.N, tmp, s);
+    if (sized) {
+        grow(x->cap_tor, read_ll(x, d.tor_off + d.N));
+        bind_caps(x);
+        tmp = scan_tmp(x);
+    }
+    launch_pairs(d, true, s);
+    launch_triples(d, false, s);
+    scan_counts(d.nplus, d.plus_off, d.N, tmp, s);
+    scan_counts(d.nminus, d.minus_off, d.N, tmp, s);
+    if (sized) {
+        grow(x->cap_probe, read_ll(x, d.plus_off + d.N) + read_ll(x, d.minus_off + d.N));
+        bind_caps(x);
+        tmp = scan_tmp(x);
+    }
+    launch_triples(d, true, s);
+    launch_low_probes(d, x->cap_probe, tmp, s);
+    ck(cudaMemsetAsync(d.tor1_cnt, 0, sizeof(int) * x->cap_tor, s), "memset");
+    ck(cudaMemsetAsync(d.tor2_cnt, 0, sizeof(int) * x->cap_tor, s), "memset");
+    ck(cudaMemsetAsync(d.conc_cnt, 0, sizeof(int) * x->cap_probe, s), "memset");
+    launch_convex(d, false, s);
+    launch_toroidal(d, x->cap_tor, false, s);
+    launch_concave(d, x->cap_probe, false, s);
+    scan_counts(d.conv_cnt, d.conv_off, d.N, tmp, s);
+    scan_counts(d.tor1_cnt, d.tor1_off, x->cap_tor, tmp, s);
+    scan_counts(d.tor2_cnt, d.tor2_off, x->cap_tor, tmp, s);
+    scan_counts(d.conc_cnt, d.conc_off, x->cap_probe, tmp, s);
+    launch_layout(d, (long long*)x->get<int>(cms_ctx::S_CM_TMP), tmp, s);
+    if (sized) {
+        grow(x->cap_dot, read_ll(x, d.dot_off + 2LL * d.B));
+        bind_caps(x);
+        tmp = scan_tmp(x);
+    }
+    launch_convex(d, true, s);
+    launch_toroidal(d, x->cap_tor, true, s);
+    launch_concave(d, x->cap_probe, true, s);
+    launch_tor_access(d, x->cap_tor, s);
+}
+
+NNArgs nn_args(cms_ctx* x, int kind)
+{
+    NNArgs a{};
+    a.task = x->get<NNTask>(cms_ctx::S_TASKS) + kind * 2 * x->B;
+    a.ntask = 2 * x->B;
+    a.tile_cnt = x->get<int>(cms_ctx::S_TILE_CNT);
+    a.tile_off = x->get<long long>(cms_ctx::S_TILE_OFF);
+    return a;
+}
+
+long long tile_cap(cms_ctx* x) { return x->cap_dot / 256 + 2LL * x->B + 1; }
+
+void enqueue_cms(cms_ctx* x)
+{
+    Dev& d = x->d;
+    Rd& r = x->r;
+    cudaStream_t s = x->stream;
+    long long* tmp = scan_tmp(x);
+    NNTask* task = x->get<NNTask>(cms_ctx::S_TASKS);
+    launch_tasks(d, r, 0, task, s);
+    k_fill_d<<<grid1(x->cap_dot), 256, 0, s>>>(r.nn_d2, x->cap_dot, INFINITY);
+    NNArgs a = nn_args(x, 0);
+    a.q_f4 = r.bur_f4; a.q_idx = r.bur_idx; a.r_f4 = r.bur_f4; a.r_idx = r.bur_idx;
+    a.out_d2 = r.nn_d2;
+    launch_nn(d, a, NN_MIN, tile_cap(x), tmp, s);
+    launch_cms_weights(d, r, x->cap_dot, s);
+    launch_per_atom_sum(d, r, x->cap_dot, x->get<double>(cms_ctx::S_PER_ATOM_CMS), tmp, s);
+    launch_atom_totals(d, x->get<double>(cms_ctx::S_PER_ATOM_CMS), x->get<double>(cms_ctx::S_TOT_CMS), s);
+}
+
+void enqueue_sc(cms_ctx* x)
+{
+    Dev& d = x->d;
+    Rd& r = x->r;
+    cudaStream_t s = x->stream;
+    long long* tmp = scan_tmp(x);
+    NNTask* task = x->get<NNTask>(cms_ctx::S_TASKS);
+    launch_tasks(d, r, 1, task + 2 * x->B, s);
+    NNArgs a = nn_args(x, 1);
+    a.q_f4 = r.bur_f4; a.q_idx = r.bur_idx; a.r_f4 = r.acc_f4; a.r_idx = r.acc_idx;
+    a.out_flag = r.keep;
+    a.band_thr64 = x->st.band * x->st.band;
+    launch_nn(d, a, NN_BAND, tile_cap(x), tmp, s);
+    launch_trim_compact(d, r, x->cap_dot, tmp, s);
+    launch_tasks(d, r, 2, task + 4 * x->B, s);
+    k_fill_d<<<grid1(x->cap_dot), 256, 0, s>>>(r.nn_d2, x->cap_dot, INFINITY);
+    k_fill_i<<<grid1(x->cap_dot), 256, 0, s>>>(r.nn_idx, x->cap_dot, -1);
+    NNArgs b = nn_args(x, 2);
+    b.q_f4 = r.trim_f4; b.q_idx = r.trim_idx; b.r_f4 = r.trim_f4; b.r_idx = r.trim_idx;
+    b.out_d2 = r.nn_d2; b.out_idx = r.nn_idx;
+    launch_nn(d, b, NN_ARGMIN, tile_cap(x), tmp, s);
+    launch_sc_stats(d, r, task + 4 * x->B, x->get<double>(cms_ctx::S_SC_SIDE), x->get<double>(cms_ctx::S_SC_OUT), s);
+}
+
+void enqueue_max(cms_ctx* x)
+{
+    Dev& d = x->d;
+    Rd& r = x->r;
+    cudaStream_t s = x->stream;
+    launch_area_values(d, r, x->cap_dot, s);
+    launch_per_atom_sum(d, r, x->cap_dot, x->get<double>(cms_ctx::S_PER_ATOM_MAX), scan_tmp(x), s);
+    launch_atom_totals(d, x->get<double>(cms_ctx::S_PER_ATOM_MAX), x->get<double>(cms_ctx::S_TOT_MAX), s);
+}
+
+void enqueue_summary(cms_ctx* x)
+{
+    k_summary<<<1, 32, 0, x->stream>>>(x->d, x->r, x->get<long long>(cms_ctx::S_SUMMARY));
+}
+
+// host mirrors of per-complex offsets, status and coincident pairs
+void pull_host_state(cms_ctx* x)
+{
+    const int B = x->B;
+    const long long N = x->N;
+    cudaStream_t s = x->stream;
+    ck(cudaMemcpyAsync(x->pinned, x->get<long long>(cms_ctx::S_SUMMARY), 8 * sizeof(long long),
+                       cudaMemcpyDeviceToHost, s), "summary");
+    x->h_status.resize(B);
+    x->h_coin.resize(B);
+    x->h_dot_off.resize(2 * B + 1);
+    x->h_seg.resize(8 * B);
+    std::vector<Cplx> cx(B);
+    ck(cudaMemcpyAsync(x->h_status.data(), x->d.status, sizeof(int) * B, cudaMemcpyDeviceToHost, s), "status");
+    ck(cudaMemcpyAsync(x->h_coin.data(), x->d.coin, sizeof(unsigned long long) * B, cudaMemcpyDeviceToHost, s), "coin");
+    ck(cudaMemcpyAsync(x->h_dot_off.data(), x->d.dot_off, sizeof(long long) * (2 * B + 1), cudaMemcpyDeviceToHost, s), "dot_off");
+    ck(cudaMemcpyAsync(x->h_seg.data(), x->d.seg, sizeof(Seg) * 8 * B, cudaMemcpyDeviceToHost, s), "seg");
+    ck(cudaMemcpyAsync(cx.data(), x->d.cx, sizeof(Cplx) * B, cudaMemcpyDeviceToHost, s), "cx");
+    ck(cudaStreamSynchronize(s), "sync");
+    for (int k = 0; k < 6; ++k) x->tot[k] = x->pinned[k];
+    x->h_radmax.resize(B);
+    for (int c = 0; c < B; ++c) x->h_radmax[c] = cx[c].radmax;
+    (void)N;
+}
+
+bool over_capacity(cms_ctx* x)
+{
+    return x->tot[0] > x->cap_cells || x->tot[1] > x->cap_nb || x->tot[2] > x->cap_bu || x->tot[3] > x->cap_tor ||
+           x->tot[4] > x->cap_probe || x->tot[5] > x->cap_dot;
+}
+
+void run_sized_surface(cms_ctx* x, int all_atoms)
+{
+    x->d.all_atoms = all_atoms;
+    set_settings_dev(x);
+    bind_caps(x);
+    enqueue_surface(x, true);
+    launch_split_buried(x->d, x->r, x->cap_dot, scan_tmp(x), x->stream);
+    enqueue_summary(x);
+    pull_host_state(x);
+    x->surf_ok = true;
+    x->surf_all_atoms = all_atoms;
+    x->cms_ok = x->sc_ok = x->max_ok = false;
+}
+
+long long host_ll(cms_ctx* x, const long long* dev_ptr)
+{
+    long long v = 0;
+    ck(cudaMemcpy(&v, dev_ptr, sizeof(long long), cudaMemcpyDeviceToHost), "readback");
+    return v;
+}
+
+cms_status fail(cms_ctx* x, cms_status code, const std::string& m)
+{
+    if (x) x->err = m;
+    return code;
+}
+
+#define API_BEGIN try {
+#define API_END                                                    \
+    }                                                              \
+    catch (const Fail& f) { return fail(x, f.code, f.msg); }      \
+    catch (const std::string& m) { return fail(x, CMS_ERR_CUDA, m); } \
+    catch (...) { return fail(x, CMS_ERR_CUDA, "unknown error"); } \
+    return CMS_OK;
+
+void copy_out(cms_ctx* x, void* dst, const void* src, size_t bytes, int where)
+{
+    ck(cudaMemcpyAsync(dst, src, bytes, where == CMS_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                       x->stream), "copy out");
+    ck(cudaStreamSynchronize(x->stream), "sync");
+}
+
+void need_surface(cms_ctx* x)
+{
+    if (!x->have_batch) throw Fail{CMS_ERR_STATE, "no batch loaded"};
+    if (!x->surf_ok) throw Fail{CMS_ERR_STATE, "surfaces not generated"};
+}
+
+void check_complex(cms_ctx* x, int c)
+{
+    need_surface(x);
+    if (c < 0 || c >= x->B) throw Fail{CMS_ERR_ARG, "complex index out of range"};
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cms_version(void) { return "cms_b200 0.1.0 (sm_100a)"; }
+
+int32_t cms_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+const char* cms_last_error(cms_ctx* x) { return x ? x->err.c_str() : "null context"; }
+
+cms_status cms_ctx_create(cms_ctx** out, int device, void* stream)
+{
+    cms_ctx* x = nullptr;
+    if (!out) return CMS_ERR_ARG;
+    try {
+        x = new cms_ctx();
+        x->device = device;
+        ck(cudaSetDevice(device), "cudaSetDevice");
+        if (stream) {
+            x->stream = (cudaStream_t)stream;
+        } else {
+            ck(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking), "stream");
+            x->own_stream = true;
+        }
+        ck(cudaMallocHost(&x->pinned, 64 * sizeof(long long)), "pinned");
+    } catch (const Fail& f) {
+        *out = x;
+        return fail(x, f.code, f.msg);
+    }
+    *out = x;
+    return CMS_OK;
+}
+
+cms_status cms_ctx_destroy(cms_ctx* x)
+{
+    if (!x) return CMS_OK;
+    cudaSetDevice(x->device);
+    if (x->stream) cudaStreamSynchronize(x->stream);
+    if (x->gexec) cudaGraphExecDestroy(x->gexec);
+    if (x->graph) cudaGraphDestroy(x->graph);
+    for (auto& b : x->bufs) if (b.p) cudaFree(b.p);
+    if (x->pinned) cudaFreeHost(x->pinned);
+    if (x->own_stream && x->stream) cudaStreamDestroy(x->stream);
+    delete x;
+    return CMS_OK;
+}
+
+cms_status cms_set_settings(cms_ctx* x, const cms_settings* s)
+{
+    if (!x || !s) return fail(x, CMS_ERR_ARG, "null argument");
+    x->st = *s;
+    x->surf_ok = false;
+    return CMS_OK;
+}
+
+cms_status cms_get_settings(cms_ctx* x, cms_settings* s)
+{
+    if (!x || !s) return fail(x, CMS_ERR_ARG, "null argument");
+    *s = x->st;
+    return CMS_OK;
+}
+
+cms_status cms_load_batch(cms_ctx* x, int32_t B, const int64_t* atom_off, const int64_t* n_binder, const double* xyz,
+                          const double* radius, const double* density, int32_t where)
+{
+    if (!x) return CMS_ERR_ARG;
+    if (B <= 0 || !atom_off || !n_binder || !xyz || !radius) return fail(x, CMS_ERR_ARG, "invalid batch arguments");
+    API_BEGIN
+    ck(cudaSetDevice(x->device), "cudaSetDevice");
+    x->h_off.assign(atom_off, atom_off + B + 1);
+    x->h_n0.assign(n_binder, n_binder + B);
+    if (x->h_off[0] != 0) throw Fail{CMS_ERR_ARG, "atom_off[0] must be 0"};
+    for (int c = 0; c < B; ++c) {
+        long long n = x->h_off[c + 1] - x->h_off[c];
+        if (n < 0) throw Fail{CMS_ERR_ARG, "atom_off must be non-decreasing"};
+        if (n == 0) throw Fail{CMS_ERR_EMPTY, "complex without atoms"};
+        if (x->h_n0[c] < 0 || x->h_n0[c] > n) throw Fail{CMS_ERR_ARG, "n_binder out of range"};
+    }
+    const long long N = x->h_off[B];
+    if (N >= (1LL << 31)) throw Fail{CMS_ERR_ARG, "too many atoms in one batch"};
+    const bool same_shape = x->have_batch && x->B == B && x->N == N;
+    x->B = B;
+    x->N = N;
+    bind_batch(x);
+    cudaStream_t s = x->stream;
+    std::vector<int> off32(B + 1), n032(B);
+    for (int c = 0; c <= B; ++c) off32[c] = (int)x->h_off[c];
+    for (int c = 0; c < B; ++c) n032[c] = (int)x->h_n0[c];
+    ck(cudaMemcpyAsync((void*)x->d.atom_off, off32.data(), sizeof(int) * (B + 1), cudaMemcpyHostToDevice, s), "upload");
+    ck(cudaMemcpyAsync((void*)x->d.n0, n032.data(), sizeof(int) * B, cudaMemcpyHostToDevice, s), "upload");
+    const double* dxyz = xyz;
+    const double* drad = radius;
+    const double* ddens = density;
+    if (where == CMS_HOST) {
+        double* bx = x->ensure<double>(cms_ctx::S_IN_XYZ, 3 * N);
+        double* br = x->ensure<double>(cms_ctx::S_IN_RAD, N);
+        ck(cudaMemcpyAsync(bx, xyz, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, s), "upload xyz");
+        ck(cudaMemcpyAsync(br, radius, sizeof(double) * N, cudaMemcpyHostToDevice, s), "upload radius");
+        dxyz = bx;
+        drad = br;
+        if (density) {
+            double* bd = x->ensure<double>(cms_ctx::S_IN_DENS, N);
+            ck(cudaMemcpyAsync(bd, density, sizeof(double) * N, cudaMemcpyHostToDevice, s), "upload density");
+            ddens = bd;
+        }
+    }
+    k_pack_atoms<<<grid1(N), 256, 0, s>>>(N, dxyz, drad, ddens, x->st.density, x->d.xyzr, x->d.dens);
+    ck(cudaGetLastError(), "pack");
+    if (where == CMS_HOST) ck(cudaStreamSynchronize(s), "sync");   // host buffers may be released after return
+    x->have_batch = true;
+    x->surf_ok = x->cms_ok = x->sc_ok = x->max_ok = false;
+    if (!same_shape) x->graph_key[0] = -1;
+    API_END
+}
+
+cms_status cms_generate_surfaces(cms_ctx* x, int32_t all_atoms)
+{
+    if (!x) return CMS_ERR_ARG;
+    API_BEGIN
+    if (!x->have_batch) throw Fail{CMS_ERR_STATE, "no batch loaded"};
+    ck(cudaSetDevice(x->device), "cudaSetDevice");
+    run_sized_surface(x, all_atoms ? 1 : 0);
+    ck(cudaGetLastError(), "surface kernels");
+    API_END
+}
+
+cms_status cms_contact_ms(cms_ctx* x, double* per_atom, double* totals, int32_t where)
+{
+    if (!x) return CMS_ERR_ARG;
+    API_BEGIN
+    need_surface(x);
+    if (!x->cms_ok) {
+        enqueue_cms(x);
+        ck(cudaGetLastError(), "cms kernels");
+        x->cms_ok = true;
+    }
+    if (per_atom) copy_out(x, per_atom, x->get<double>(cms_ctx::S_PER_ATOM_CMS), sizeof(double) * x->N, where);
+    if (totals) copy_out(x, totals, x->get<double>(cms_ctx::S_TOT_CMS), sizeof(double) * 2 * x->B, where);
+    API_END
+}
+
+cms_status cms_max_contact_ms(cms_ctx* x, double* per_atom, double* totals, int32_t where)
+{
+    if (!x) return CMS_ERR_ARG;
+    API_BEGIN
+    need_surface(x);
+    if (!x->max_ok) {
+        enqueue_max(x);
+        ck(cudaGetLastError(), "max cms kernels");
+        x->max_ok = true;
+    }
+    if (per_atom) copy_out(x, per_atom, x->get<double>(cms_ctx::S_PER_ATOM_MAX), sizeof(double) * x->N, where);
+    if (totals) {
+        std::vector<double> t(2 * x->B), o(x->B);
+        copy_out(x, t.data(), x->get<double>(cms_ctx::S_TOT_MAX), sizeof(double) * 2 * x->B, CMS_HOST);
+        for (int c = 0; c < x->B; ++c) o[c] = t[2 * c];
+        if (where == CMS_HOST) std::memcpy(totals, o.data(), sizeof(double) * x->B);
+        else ck(cudaMemcpy(totals, o.data(), sizeof(double) * x->B, cudaMemcpyHostToDevice), "copy");
+    }
+    API_END
+}
+
+cms_status cms_shape_complementarity(cms_ctx* x, double* sc, double* sides, int32_t where)
+{
+    if (!x) return CMS_ERR_ARG;
+    API_BEGIN
+    need_surface(x);
+    if (!x->sc_ok) {
+        enqueue_sc(x);
+        ck(cudaGetLastError(), "sc kernels");
+        x->sc_ok = true;
+    }
+    if (sc) copy_out(x, sc, x->get<double>(cms_ctx::S_SC_OUT), sizeof(double) * SC_FIELDS * x->B, where);
+    if (sides) copy_out(x, sides, x->get<double>(cms_ctx::S_SC_SIDE), sizeof(double) * SC_SIDE_FIELDS * 2 * x->B, where);
+    API_END
+}
+
+cms_status cms_complex_info_get(cms_ctx* x, int32_t c, cms_complex_info* info)
+{
+    if (!x || !info) return fail(x, CMS_ERR_ARG, "null argument");
+    API_BEGIN
+    check_complex(x, c);
+    cms_complex_info I;
+    std::memset(&I, 0, sizeof(I));
+    const long long a0 = x->h_off[c], a1 = x->h_off[c + 1], s1 = a0 + x->h_n0[c];
+    I.n_atoms = a1 - a0;
+    I.n_binder = x->h_n0[c];
+    I.nb_entries = host_ll(x, x->d.nb_off + a1) - host_ll(x, x->d.nb_off + a0);
+    I.bu_entries = host_ll(x, x->d.bu_off + a1) - host_ll(x, x->d.bu_off + a0);
+    std::vector<int> nn(I.n_atoms), nb(I.n_atoms);
+    ck(cudaMemcpy(nn.data(), x->d.nnb + a0, sizeof(int) * I.n_atoms, cudaMemcpyDeviceToHost), "copy");
+    ck(cudaMemcpy(nb.data(), x->d.nbur + a0, sizeof(int) * I.n_atoms, cudaMemcpyDeviceToHost), "copy");
+    I.max_nb = 1; I.max_bu = 1;
+    for (long long i = 0; i < I.n_atoms; ++i) { I.max_nb = std::max<int64_t>(I.max_nb, nn[i]); I.max_bu = std::max<int64_t>(I.max_bu, nb[i]); }
+    I.n_toroid = host_ll(x, x->d.tor_off + a1) - host_ll(x, x->d.tor_off + a0);
+    const long long p0 = host_ll(x, x->d.plus_off + a0), p1 = host_ll(x, x->d.plus_off + s1), p2 = host_ll(x, x->d.plus_off + a1);
+    const long long m0 = host_ll(x, x->d.minus_off + a0), m1 = host_ll(x, x->d.minus_off + s1), m2 = host_ll(x, x->d.minus_off + a1);
+    I.n_probes_plus[0] = p1 - p0; I.n_probes_plus[1] = p2 - p1;
+    I.n_probes_minus[0] = m1 - m0; I.n_probes_minus[1] = m2 - m1;
+    I.n_probes = (p2 - p0) + (m2 - m0);
+    for (int m = 0; m < 2; ++m) I.n_dots[m] = x->h_dot_off[2 * c + m + 1] - x->h_dot_off[2 * c + m];
+    long long cnt[4] = {0, 0, 0, 0};
+    for (int m = 0; m < 2; ++m)
+        for (int t = 0; t < 4; ++t) {
+            long long e = t < 3 ? x->h_seg[(c * 2 + m) * 4 + t + 1].dot0 : x->h_dot_off[2 * c + m + 1];
+            cnt[t] += e - x->h_seg[(c * 2 + m) * 4 + t].dot0;
+        }
+    I.convex = cnt[0]; I.toroidal = cnt[1] + cnt[2]; I.concave = cnt[3];
+    if (x->sc_ok) {
+        for (int m = 0; m < 2; ++m) {
+            long long ds = x->h_dot_off[2 * c + m], de = x->h_dot_off[2 * c + m + 1];
+            long long bs = host_ll(x, x->r.bur_scan + ds), be = host_ll(x, x->r.bur_scan + de);
+            I.n_trimmed[m] = host_ll(x, x->r.trim_scan + be) - host_ll(x, x->r.trim_scan + bs);
+        }
+    }
+    I.status = x->h_status[c];
+    unsigned long long k = x->h_coin[c];
+    if (k != ~0ull) {
+        I.status |= ST_COINCIDENT;
+        I.coincident_i = (int32_t)(k >> 32);
+        I.coincident_j = (int32_t)(k & 0xffffffffu);
+    } else {
+        I.coincident_i = I.coincident_j = -1;
+    }
+    I.radmax = x->h_radmax[c];
+    *info = I;
+    API_END
+}
+
+cms_status cms_export_atoms(cms_ctx* x, int32_t c, int8_t* atten, int8_t* access, int32_t* n_neighbors, int32_t* n_buried)
+{
+    if (!x) return CMS_ERR_ARG;
+    API_BEGIN
+    check_complex(x, c);
+    const long long a0 = x->h_off[c], n = x->h_off[c + 1] - a0;
+    if (atten) ck(cudaMemcpy(atten, x->d.atten + a0, n, cudaMemcpyDeviceToHost), "copy");
+    if (access) ck(cudaMemcpy(access, x->d.access + a0, n, cudaMemcpyDeviceToHost), "copy");
+    if (n_neighbors) ck(cudaMemcpy(n_neighbors, x->d.nnb + a0, 4 * n, cudaMemcpyDeviceToHost), "copy");
+    if (n_buried) ck(cudaMemcpy(n_buried, x->d.nbur + a0, 4 * n, cudaMemcpyDeviceToHost), "copy");
+    API_END
+}
+
+cms_status cms_export_neighbors(cms_ctx* x, int32_t c, int64_t* nb_off, int32_t* nb_id, int64_t* bu_off, int32_t* bu_id)
+{
+    if (!x) return CMS_ERR_ARG;
+    API_BEGIN
+    check_complex(x, c);
+    const long long a0 = x->h_off[c], n = x->h_off[c + 1] - a0;
+    std::vector<long long> off(n + 1);
+    for (int pass = 0; pass < 2; ++pass) {
+        const long long* doff = pass == 0 ? x->d.nb_off : x->d.bu_off;
+        const int* did = pass == 0 ? x->d.nb_id : x->d.bu_id;
+        int64_t* ooff = pass == 0 ? nb_off : bu_off;
+        int32_t* oid = pass == 0 ? nb_id : bu_id;
+        ck(cudaMemcpy(off.data(), doff + a0, sizeof(long long) * (n + 1), cudaMemcpyDeviceToHost), "copy");
+        const long long base = off[0], cnt = off[n] - off[0];
+        if (ooff) for (long long i = 0; i <= n; ++i) ooff[i] = off[i] - base;
+        if (oid && cnt > 0) {
+            ck(cudaMemcpy(oid, did + base, sizeof(int) * cnt, cudaMemcpyDeviceToHost), "copy");
+            for (long long i = 0; i < cnt; ++i) oid[i] -= (int32_t)a0;
+        }
+    }
+    API_END
+}
+
+cms_status cms_export_toroid(cms_ctx* x, int32_t c, int32_t* atom1, int32_t* atom2, double* uij, double* tij, double* rij,
+                             int8_t* between)
+{
+    if (!x) return CMS_ERR_ARG;
+    API_BEGIN
+    check_complex(x, c);
+    const long long a0 = x->h_off[c], a1 = x->h_off[c + 1];
+    const long long q0 = host_ll(x, x->d.tor_off + a0), n = host_ll(x, x->d.tor_off + a1) - q0;
+    if (n > 0) {
+        std::vector<int> ti(n), tj(n);
+        ck(cudaMemcpy(ti.data(), x->d.tor_i + q0, sizeof(int) * n, cudaMemcpyDeviceToHost), "copy");
+        ck(cudaMemcpy(tj.data(), x->d.tor_j + q0, sizeof(int) * n, cudaMemcpyDeviceToHost), "copy");
+        for (long long k = 0; k < n; ++k) {
+            if (atom1) atom1[k] = ti[k] - (int)a0;
+            if (atom2) atom2[k] = tj[k] - (int)a0;
+        }
+        double* buf = x->ensure<double>(cms_ctx::S_EXPORT, 8 * n);
+        k_export_toroid<<<grid1(n), 256, 0, x->stream>>>(x->d, q0, n, buf);
+        std::vector<double> h(8 * n);
+        ck(cudaMemcpyAsync(h.data(), buf, sizeof(double) * 8 * n, cudaMemcpyDeviceToHost, x->stream), "copy");
+        ck(cudaStreamSynchronize(x->stream), "sync");
+        for (long long k = 0; k < n; ++k) {
+            const double* o = &h[8 * k];
+            if (uij) { uij[3 * k] = o[0]; uij[3 * k + 1] = o[1]; uij[3 * k + 2] = o[2]; }
+            if (tij) { tij[3 * k] = o[3]; tij[3 * k + 1] = o[4]; tij[3 * k + 2] = o[5]; }
+            if (rij) rij[k] = o[6];
+            if (between) between[k] = o[7] != 0.0;
+        }
+    }
+    API_END
+}
+
+cms_status cms_export_probes(cms_ctx* x, int32_t c, int32_t* a0, int32_t* a1, int32_t* a2, double* height, double* point,
+                             double* alt)
+{
+    if (!x) return CMS_ERR_ARG;
+    API_BEGIN
+    check_complex(x, c);
+    cms_complex_info I;
+    cms_status st = cms_complex_info_get(x, c, &I);
+    if (st != CMS_OK) return st;
+    const long long at0 = x->h_off[c];
+    const long long base = host_ll(x, x->d.plus_off + at0) + host_ll(x, x->d.minus_off + at0);
+    // device layout [+mol0 | -mol0 | +mol1 | -mol1]; reference order [+mol0 | +mol1 | -mol0 | -mol1]
+    const long long pp0 = I.n_probes_plus[0], pm0 = I.n_probes_minus[0], pp1 = I.n_probes_plus[1], pm1 = I.n_probes_minus[1];
+    const long long src[4] = {0, pp0 + pm0, pp0, pp0 + pm0 + pp1};
+    const long long len[4] = {pp0, pp1, pm0, pm1};
+    long long dst = 0;
+    for (int b = 0; b < 4; ++b) {
+        const long long n = len[b], q = base + src[b];
+        if (n > 0) {
+            std::vector<int> t(n);
+            int32_t* outs[3] = {a0, a1, a2};
+            const int* ins[3] = {x->d.pa0, x->d.pa1, x->d.pa2};
+            for (int k = 0; k < 3; ++k) {
+                if (!outs[k]) continue;
+                ck(cudaMemcpy(t.data(), ins[k] + q, sizeof(int) * n, cudaMemcpyDeviceToHost), "copy");
+                for (long long i = 0; i < n; ++i) outs[k][dst + i] = t[i] - (int)at0;
+            }
+            if (height) ck(cudaMemcpy(height + dst, x->d.ph + q, sizeof(double) * n, cudaMemcpyDeviceToHost), "copy");
+            if (point) ck(cudaMemcpy(point + 3 * dst, x->d.pxyz + 3 * q, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost), "copy");
+            if (alt) ck(cudaMemcpy(alt + 3 * dst, x->d.palt + 3 * q, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost), "copy");
+        }
+        dst += n;
+    }
+    API_END
+}
+
+cms_status cms_export_dots(cms_ctx* x, int32_t c, int32_t molecule, double* coor, double* outnml, double* area,
+                           int8_t* buried, int8_t* type, int32_t* atom_idx)
+{
+    if (!x) return CMS_ERR_ARG;
+    API_BEGIN
+    check_complex(x, c);
+    if (molecule != 0 && molecule != 1) throw Fail{CMS_ERR_ARG, "molecule must be 0 or 1"};
+    const long long ds = x->h_dot_off[2 * c + molecule], n = x->h_dot_off[2 * c + molecule + 1] - ds;
+    if (n > 0) {
+        if (coor) ck(cudaMemcpy(coor, x->d.dxyz + 3 * ds, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost), "copy");
+        if (outnml) ck(cudaMemcpy(outnml, x->d.dnml + 3 * ds, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost), "copy");
+        if (area) ck(cudaMemcpy(area, x->d.darea + ds, sizeof(double) * n, cudaMemcpyDeviceToHost), "copy");
+        if (buried) ck(cudaMemcpy(buried, x->d.dbur + ds, n, cudaMemcpyDeviceToHost), "copy");
+        if (type) ck(cudaMemcpy(type, x->d.dtype + ds, n, cudaMemcpyDeviceToHost), "copy");
+        if (atom_idx) {
+            ck(cudaMemcpy(atom_idx, x->d.datom + ds, sizeof(int) * n, cudaMemcpyDeviceToHost), "copy");
+            const int a0 = (int)x->h_off[c];
+            for (long long i = 0; i < n; ++i) atom_idx[i] -= a0;
+        }
+    }
+    API_END
+}
+
+cms_status cms_export_trimmed(cms_ctx* x, int32_t c, int32_t molecule, int32_t* dot_index)
+{
+    if (!x) return CMS_ERR_ARG;
+    API_BEGIN
+    check_complex(x, c);
+    if (!x->sc_ok) throw Fail{CMS_ERR_STATE, "shape complementarity not computed"};
+    const long long ds = x->h_dot_off[2 * c + molecule], de = x->h_dot_off[2 * c + molecule + 1];
+    const long long bs = host_ll(x, x->r.bur_scan + ds), be = host_ll(x, x->r.bur_scan + de);
+    const long long ts = host_ll(x, x->r.trim_scan + bs), te = host_ll(x, x->r.trim_scan + be);
+    if (te > ts && dot_index) {
+        ck(cudaMemcpy(dot_index, x->r.trim_idx + ts, sizeof(int) * (te - ts), cudaMemcpyDeviceToHost), "copy");
+        for (long long i = 0; i < te - ts; ++i) dot_index[i] -= (int32_t)ds;
+    }
+    API_END
+}
+
+cms_status cms_run_graph(cms_ctx* x)
+{
+    if (!x) return CMS_ERR_ARG;
+    API_BEGIN
+    if (!x->have_batch) throw Fail{CMS_ERR_STATE, "no batch loaded"};
+    ck(cudaSetDevice(x->device), "cudaSetDevice");
+    if (x->cap_dot == 0) {
+        // size every buffer once with the stage-synchronised path
+        run_sized_surface(x, 0);
+    }
+    const long long key[3] = {x->B, x->N, x->cap_dot};
+    if (!x->gexec || std::memcmp(key, x->graph_key, sizeof(key)) != 0) {
+        if (x->gexec) { cudaGraphExecDestroy(x->gexec); x->gexec = nullptr; }
+        if (x->graph) { cudaGraphDestroy(x->graph); x->graph = nullptr; }
+        x->d.all_atoms = 0;
+        set_settings_dev(x);
+        bind_caps(x);
+        ck(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        try {
+            enqueue_surface(x, false);
+            launch_split_buried(x->d, x->r, x->cap_dot, scan_tmp(x), x->stream);
+            enqueue_cms(x);
+            enqueue_sc(x);
+            enqueue_summary(x);
+        } catch (...) {
+            cudaGraph_t g;
+            cudaStreamEndCapture(x->stream, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        ck(cudaStreamEndCapture(x->stream, &x->graph), "end capture");
+        ck(cudaGraphInstantiate(&x->gexec, x->graph, 0), "instantiate");
+        size_t nn = 0;
+        ck(cudaGraphGetNodes(x->graph, nullptr, &nn), "nodes");
+        std::vector<cudaGraphNode_t> nodes(nn);
+        ck(cudaGraphGetNodes(x->graph, nodes.data(), &nn), "nodes");
+        long long kernels = 0;
+        for (auto& n : nodes) {
+            cudaGraphNodeType t;
+            cudaGraphNodeGetType(n, &t);
+            if (t == cudaGraphNodeTypeKernel) ++kernels;
+        }
+        x->launches = kernels;
+        std::memcpy(x->graph_key, key, sizeof(key));
+    }
+    ck(cudaGraphLaunch(x->gexec, x->stream), "graph launch");
+    pull_host_state(x);
+    if (over_capacity(x)) {
+        // a capacity was exceeded: size again and rerun without the graph
+        run_sized_surface(x, 0);
+        enqueue_cms(x);
+        enqueue_sc(x);
+        enqueue_summary(x);
+        pull_host_state(x);
+        x->graph_key[0] = -1;
+    }
+    x->surf_ok = true;
+    x->surf_all_atoms = 0;
+    x->cms_ok = x->sc_ok = true;
+    x->max_ok = false;
+    API_END
+}
+
+int64_t cms_kernel_launches(cms_ctx* x) { return x ? x->launches : -1; }
+
+}  // extern "C"

@@ -1,0 +1,28 @@
+// Host-side launchers of every kernel of the surface pipeline and the readouts.
+#pragma once
+#include "cms_internal.cuh"
+
+namespace cms {
+
+// scans (k_scan.cu)
+long long scan_tmp_elems(long long n);
+void scan_counts(const int* in, long long* out, long long n, long long* tmp, cudaStream_t s);
+
+// surface front half (k_surface.cu)
+void launch_setup(const Dev& d, cudaStream_t s);
+void launch_cells(const Dev& d, long long n_cells, long long* scan_tmp, cudaStream_t s);
+void launch_attention(const Dev& d, cudaStream_t s);
+void launch_neighbor_count(const Dev& d, cudaStream_t s);
+void launch_neighbor_emit(const Dev& d, cudaStream_t s);
+void launch_pairs(const Dev& d, bool emit, cudaStream_t s);
+void launch_triples(const Dev& d, bool emit, cudaStream_t s);
+void launch_low_probes(const Dev& d, long long probe_cap, long long* scan_tmp, cudaStream_t s);
+
+// dots (k_dots.cu)
+void launch_convex(const Dev& d, bool emit, cudaStream_t s);
+void launch_toroidal(const Dev& d, long long tor_grid, bool emit, cudaStream_t s);
+void launch_concave(const Dev& d, long long probe_grid, bool emit, cudaStream_t s);
+void launch_layout(const Dev& d, long long* cm_count_tmp, long long* scan_tmp, cudaStream_t s);
+void launch_tor_access(const Dev& d, long long tor_grid, cudaStream_t s);
+
+}  // namespace cms

@@ -1,0 +1,54 @@
+// Readout workspace and launchers (k_readout.cu).
+#pragma once
+#include "cms_kernels.cuh"
+
+namespace cms {
+
+enum { NN_MIN = 0, NN_ARGMIN = 1, NN_BAND = 2 };
+
+#define SC_SIDE_FIELDS 7   // d_mean, d_median, s_mean, s_median, trimmedArea, nTrimmedDots, nAllDots
+#define SC_FIELDS 5        // sc, area, distance, d_mean (surface 2), s_mean (surface 2)
+
+// one nearest-dot task: queries [q0, q0+qn) against references [r0, r0+rn)
+// of the same complex, both as positions in packed lists
+struct NNTask {
+    long long q0, qn, r0, rn;
+    int c;
+};
+
+struct NNArgs {
+    const NNTask* task;
+    int ntask;
+    int* tile_cnt;          // ntask
+    long long* tile_off;    // ntask + 1
+    const float4* q_f4; const int* q_idx;
+    const float4* r_f4; const int* r_idx;
+    double* out_d2; int* out_idx; int* out_flag;
+    double band_thr64;      // band^2 (BAND mode)
+    int band_mode;
+};
+
+// readout workspace, capacity = dot capacity unless noted
+struct Rd {
+    int* flag; long long* bur_scan;             // D, D+1
+    int* bur_idx; float4* bur_f4; int* bur_cm;  // buried dots, in dot order
+    int* acc_idx; float4* acc_f4;               // accessible dots, in dot order
+    int* keep; long long* trim_scan;            // per buried entry, +1
+    int* trim_idx; float4* trim_f4;             // trimmed dots
+    double* nn_d2; int* nn_idx;                 // per query entry
+    double* val; int* own;                      // per entry value / owner atom (-1: none)
+    int* acnt; int* afill; long long* aoff;     // N, N, N+1
+    int* aslot;                                 // D
+};
+
+void launch_split_buried(const Dev& d, const Rd& r, long long dot_cap, long long* scan_tmp, cudaStream_t s);
+void launch_tasks(const Dev& d, const Rd& r, int kind, NNTask* task, cudaStream_t s);
+void launch_nn(const Dev& d, NNArgs a, int mode, long long tile_cap, long long* scan_tmp, cudaStream_t s);
+void launch_cms_weights(const Dev& d, const Rd& r, long long cap, cudaStream_t s);
+void launch_area_values(const Dev& d, const Rd& r, long long cap, cudaStream_t s);
+void launch_per_atom_sum(const Dev& d, const Rd& r, long long cap, double* out, long long* scan_tmp, cudaStream_t s);
+void launch_atom_totals(const Dev& d, const double* per_atom, double* tot, cudaStream_t s);
+void launch_trim_compact(const Dev& d, const Rd& r, long long cap, long long* scan_tmp, cudaStream_t s);
+void launch_sc_stats(const Dev& d, const Rd& r, const NNTask* task, double* side, double* out, cudaStream_t s);
+
+}  // namespace cms

@@ -1,0 +1,663 @@
+// Surface pipeline, back half: convex, toroidal and concave dot generation
+// with the burial test, in two passes (count, then emit) that share one code
+// path so the two passes agree by construction.
+//
+// Reference behaviour (cms-cuda/_core.py):
+//   generate_convex_surface        _core.py:1646-1840
+//   generate_toroidal_surface(s)   _core.py:1234-1248, 1847-2067
+//   generate_concave_surface       _core.py:2069-2333
+//   add_dots                       _core.py:2337-2377
+//   vec_sub_arc / vec_sub_div / vec_sub_cir / vec_distance_point_to_line
+//                                  _core.py:2380-2527
+//
+// Dot order per complex and molecule is the reference's: all convex dots
+// (atom, latitude, point), then all arc-1 toroidal dots (toroid pair, torus
+// point, arc point), then all arc-2 toroidal dots, then all concave dots
+// (probe, latitude, point).  Each unit's dots start at
+// seg.dot0 + (unit scan - seg.scan0); inside a unit a warp orders its dots
+// with ballots.
+#include "cms_kernels.cuh"
+
+namespace cms {
+
+static constexpr int SM_COUNT = 148;
+
+static inline unsigned grid_for(long long items, int per_block, int max_blocks_per_sm = 16)
+{
+    long long b = (items + per_block - 1) / per_block;
+    long long cap = (long long)SM_COUNT * max_blocks_per_sm;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (unsigned)b;
+}
+
+// buried = any buried partner b of the owner with |pcen - x_b|^2 <= (r_b + rp)^2 (seq order)
+__device__ __forceinline__ int8_t buried_test(const Dev& d, int owner, V3 pcen)
+{
+    const long long s = d.bu_off[owner], e = d.bu_off[owner + 1];
+    const double rp = d.st.rp;
+    for (long long p = s; p < e; ++p) {
+        double4 b = d.xyzr[d.bu_id[p]];
+        double t = b.w + rp;
+        if (sq_seq(v3(b.x, b.y, b.z) - pcen) <= t * t) return 1;
+    }
+    return 0;
+}
+
+__device__ __forceinline__ void write_dot(const Dev& d, long long q, V3 pt, V3 pcen, double area, int owner,
+                                          int type, int unit, int sub)
+{
+    if (q >= d.dot_cap) return;
+    const double rp = d.st.rp;
+    V3 nml = rp <= 0.0 ? pt - atom_xyz(d, owner) : (pcen - pt) / rp;
+    st3(d.dxyz + 3 * q, pt);
+    st3(d.dnml + 3 * q, nml);
+    d.darea[q] = area;
+    d.dbur[q] = buried_test(d, owner, pcen);
+    d.dtype[q] = (int8_t)type;
+    d.datom[q] = owner;
+    d.dunit[q] = unit;
+    d.dsub[q] = sub;
+}
+
+__device__ __forceinline__ long long unit_base(const Dev& d, int c, int m, int t, long long unit_scan)
+{
+    const Seg s = d.seg[(c * 2 + m) * 4 + t];
+    return s.dot0 + (unit_scan - s.scan0);
+}
+
+// ---------------------------------------------------------------------------
+// convex dots: one warp per atom of the convex queue
+// ---------------------------------------------------------------------------
+static constexpr int CV_WARPS = 4;
+
+struct LatTable {
+    double cx[CMS_MAX_SUBDIV], cy[CMS_MAX_SUBDIV], cz[CMS_MAX_SUBDIV];
+    double rad[CMS_MAX_SUBDIV], delta[CMS_MAX_SUBDIV], area[CMS_MAX_SUBDIV];
+    int start[CMS_MAX_SUBDIV + 1];
+};
+
+__device__ __forceinline__ int find_lat(const LatTable& L, int nl, int t)
+{
+    // largest l with start[l] <= t
+    int lo = 0, hi = nl - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (L.start[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void lat_prefix(LatTable& L, const int* nc, int nl)
+{
+    if ((threadIdx.x & 31) == 0) {
+        int s = 0;
+        for (int l = 0; l < nl; ++l) { L.start[l] = s; s += nc[l]; }
+        L.start[nl] = s;
+    }
+    __syncwarp();
+}
+
+template <bool EMIT>
+__global__ void __launch_bounds__(CV_WARPS * 32) k_convex(Dev d)
+{
+    __shared__ LatTable tab[CV_WARPS];
+    __shared__ int ncs[CV_WARPS][CMS_MAX_SUBDIV];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    LatTable& L = tab[w];
+    const double rp = d.st.rp;
+    const long long wid = blockIdx.x * (long long)CV_WARPS + w;
+    const long long nw = (long long)gridDim.x * CV_WARPS;
+    for (long long gg = wid; gg < d.N; gg += nw) {
+        const int g = (int)gg;
+        const int K = d.nnb[g];
+        if (!(K > 0 && d.access[g] != 0 && d.atten[g] > 1)) {
+            if (!EMIT && lane == 0) d.conv_cnt[g] = 0;
+            continue;
+        }
+        const double4 ai = d.xyzr[g];
+        const V3 xi = v3(ai.x, ai.y, ai.z);
+        const double ri = ai.w, eri = ri + rp, dens = d.dens[g];
+        const long long off = d.nb_off[g];
+        // frame from the nearest neighbour (_core.py:1665-1726)
+        const int n0 = d.nb_id[off];
+        const double4 an = d.xyzr[n0];
+        const V3 xn = v3(an.x, an.y, an.z);
+        const V3 north = normalize3(xi - xn);
+        V3 vt = v3(north.y * north.y + north.z * north.z, north.x * north.x + north.z * north.z,
+                   north.x * north.x + north.y * north.y);
+        vt = normalize3(vt);
+        if (fabs(dot_seq(vt, north)) > 0.99) vt = v3(1.0, 0.0, 0.0);
+        const V3 eq = normalize3(cross3(north, vt));
+        const V3 vql = cross3(eq, north);
+        V3 south = v3(0.0, 0.0, -1.0);
+        {
+            const double rj = an.w, erj = rj + rp;
+            const double dij = norm3(xn - xi);
+            const V3 uij = (xn - xi) / dij;
+            const double asymm = (eri * eri - erj * erj) / dij;
+            const V3 tij = ((xi + xn) * 0.5) + uij * (asymm * 0.5);
+            const double far_sq = (eri + erj) * (eri + erj) - dij * dij;
+            const double rd = ri - rj;
+            const double contain_sq = dij * dij - rd * rd;
+            if (far_sq > 0.0 && contain_sq > 0.0) {
+                const double rij = ((0.5 * sqrt(far_sq)) * sqrt(contain_sq)) / dij;
+                const V3 pij = tij + vql * rij;
+                south = (pij - xi) / eri;
+            }
+        }
+        // latitude arc from north to south in the (north, eq x north) plane
+        V3 ylat;
+        const double ang = arc_angle(eq, north, south, ylat);
+        const double dl = subdiv_delta(dens, ri);
+        const int nl = subdiv_count(dl, ang);
+        const double cs = subdiv_ps(ri, ang, nl);
+        V3 fx, fy;
+        circle_frame(north, fx, fy);
+        for (int l = lane; l < nl; l += 32) {
+            V3 lat = subdiv_point(v3(0.0, 0.0, 0.0), ri, north, ylat, dl, l);
+            double dt = dot_seq(lat, north);
+            V3 cen = xi + north * dt;
+            double rsq = ri * ri - dt * dt;
+            double rad = rsq > 0.0 ? sqrt(rsq) : 0.0;
+            int nc = 0;
+            double delta = 0.0, ps = 0.0;
+            if (rad > 0.0) {
+                delta = subdiv_delta(dens, rad);
+                nc = subdiv_count(delta, CMS_TWO_PI);
+                ps = subdiv_ps(rad, CMS_TWO_PI, nc);
+            }
+            L.cx[l] = cen.x; L.cy[l] = cen.y; L.cz[l] = cen.z;
+            L.rad[l] = rad; L.delta[l] = delta; L.area[l] = ps * cs;
+            ncs[w][l] = nc;
+        }
+        __syncwarp();
+        lat_prefix(L, ncs[w], nl);
+        const int total = nl > 0 ? L.start[nl] : 0;
+        long long base = 0;
+        if (EMIT) base = unit_base(d, d.cplx[g], d.mol[g], 0, d.conv_off[g]);
+        int kept = 0;
+        const double scale = eri / ri;
+        for (int t0 = 0; t0 < total; t0 += 32) {
+            const int t = t0 + lane;
+            bool keep = false;
+            V3 pt, pcen;
+            int l = 0, i = 0;
+            if (t < total) {
+                l = find_lat(L, nl, t);
+                i = t - L.start[l];
+                pt = subdiv_point(v3(L.cx[l], L.cy[l], L.cz[l]), L.rad[l], fx, fy, L.delta[l], i);
+                pcen = xi + (pt - xi) * scale;
+                keep = true;
+                for (int s = 1; s < K; ++s) {        // slot 0 (the frame atom) is skipped
+                    double4 b = d.xyzr[d.nb_id[off + s]];
+                    double tt = b.w + rp;
+                    if (sq_seq(v3(b.x, b.y, b.z) - pcen) <= tt * tt) { keep = false; break; }
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
+            if (EMIT && keep) write_dot(d, base + kept + __popc(m & lt), pt, pcen, L.area[l], g, 1, g, (l << 16) | i);
+            kept += __popc(m);
+        }
+        if (!EMIT && lane == 0) d.conv_cnt[g] = kept;
+        __syncwarp();
+    }
+}
+
+void launch_convex(const Dev& d, bool emit, cudaStream_t s)
+{
+    if (emit) k_convex<true><<<grid_for(d.N, CV_WARPS), CV_WARPS * 32, 0, s>>>(d);
+    else k_convex<false><<<grid_for(d.N, CV_WARPS), CV_WARPS * 32, 0, s>>>(d);
+}
+
+// ---------------------------------------------------------------------------
+// toroidal dots: one warp per toroid pair, lanes over torus points
+// ---------------------------------------------------------------------------
+struct TorPair {
+    int i, j;
+    V3 xi, xj, uij, tij;
+    double ri, rj, eri, erj, rij, density, ts, dtor, darc;
+    bool between;
+    int ns;
+    V3 fx, fy;
+};
+
+__device__ __forceinline__ TorPair tor_pair(const Dev& d, long long q)
+{
+    TorPair T;
+    const double rp = d.st.rp;
+    T.i = d.tor_i[q]; T.j = d.tor_j[q];
+    double4 a = d.xyzr[T.i], b = d.xyzr[T.j];
+    T.xi = v3(a.x, a.y, a.z); T.xj = v3(b.x, b.y, b.z);
+    T.ri = a.w; T.rj = b.w;
+    // pair geometry, as second_loop computes it (_core.py:1372-1416)
+    V3 diff = T.xj - T.xi;
+    double dij_sq = sq_alt(diff);
+    double dij = sqrt(dij_sq);
+    T.eri = T.ri + rp; T.erj = T.rj + rp;
+    double asymm = (T.eri * T.eri - T.erj * T.erj) / dij;
+    T.between = fabs(asymm) < dij;
+    T.uij = diff / dij;
+    T.tij = ((T.xi + T.xj) * 0.5) + T.uij * (asymm * 0.5);
+    double far_sq = (T.eri + T.erj) * (T.eri + T.erj) - dij_sq;
+    double rd = T.ri - T.rj;
+    double cont_sq = dij_sq - rd * rd;
+    T.rij = ((0.5 * sqrt(far_sq)) * sqrt(cont_sq)) / dij;
+    // torus circle subdivision (_core.py:1863-1885)
+    T.density = (d.dens[T.i] + d.dens[T.j]) * 0.5;
+    double rci = (T.rij * T.ri) / T.eri;
+    double rcj = (T.rij * T.rj) / T.erj;
+    double rbt = T.rij - rp;
+    double rb = rbt < 0.0 ? 0.0 : rbt;                 // np.maximum keeps NaN
+    double rs = ((rci + 2.0 * rb) + rcj) * 0.25;
+    double e = rs / T.rij;
+    double edens = (e * e) * T.density;
+    circle_frame(T.uij, T.fx, T.fy);
+    T.dtor = subdiv_delta(edens, T.rij);
+    T.ns = subdiv_count(T.dtor, CMS_TWO_PI);
+    T.ts = subdiv_ps(T.rij, CMS_TWO_PI, T.ns);
+    T.darc = subdiv_delta(T.density, rp);
+    return T;
+}
+
+struct TorPoint {
+    V3 pij, pi, pj, axis, pqi, pqj;
+    bool valid;    // survives the neighbour collision test (gives access)
+    bool arcs;     // also passes the angle test (generates dots)
+};
+
+__device__ __forceinline__ TorPoint tor_point(const Dev& d, const TorPair& T, int s)
+{
+    TorPoint P;
+    const double rp = d.st.rp;
+    P.pij = subdiv_point(T.tij, T.rij, T.fx, T.fy, T.dtor, s);
+    P.valid = true;
+    P.arcs = false;
+    const long long off = d.nb_off[T.i];
+    const int K = d.nnb[T.i];
+    for (int k = 0; k < K; ++k) {                         // atom1's neighbours except atom2, strict <
+        int n = d.nb_id[off + k];
+        if (n == T.j) continue;
+        double4 b = d.xyzr[n];
+        double t = b.w + rp;
+        if (sq_alt(P.pij - v3(b.x, b.y, b.z)) < t * t) { P.valid = false; break; }
+    }
+    if (!P.valid) return P;
+    P.pi = (T.xi - P.pij) / T.eri;
+    P.pj = (T.xj - P.pij) / T.erj;
+    P.axis = normalize3(cross3(P.pi, P.pj));
+    const double dtq = rp * rp - T.rij * T.rij;
+    if (dtq > 0.0 && T.between) {
+        double dtq_s = sqrt(dtq);
+        V3 qij = T.tij - T.uij * dtq_s;
+        P.pqi = (qij - P.pij) / rp;
+        P.pqj = v3(0.0, 0.0, 0.0);
+    } else {
+        V3 mid = normalize3(P.pi + P.pj);
+        P.pqi = mid;
+        P.pqj = mid;
+    }
+    double dt1 = dot_seq(P.pqi, P.pi);
+    double dt2 = dot_seq(P.pqj, P.pj);
+    P.arcs = fabs(dt1) < 1.0 && fabs(dt2) < 1.0;
+    return P;
+}
+
+// area of a toroidal dot: ps * ts * (distance of the point from the torus axis) / rij
+__device__ __forceinline__ double tor_area(const TorPair& T, double ps, V3 pt)
+{
+    V3 vec = pt - T.tij;
+    double dt = dot_seq(vec, T.uij);
+    double d2 = sq_seq(vec) - dt * dt;
+    double dist = d2 < 0.0 ? 0.0 : sqrt(d2);
+    return ((ps * T.ts) * dist) / T.rij;
+}
+
+// one arc of a torus point: x -> v around `axis` on the probe sphere at pij
+struct Arc { V3 x, y; double angle, ps; int n; };
+
+__device__ __forceinline__ Arc tor_arc(const TorPair& T, const TorPoint& P, V3 x, V3 v, double rp)
+{
+    Arc A;
+    A.x = x;
+    A.angle = arc_angle(P.axis, x, v, A.y);
+    A.n = subdiv_count(T.darc, A.angle);
+    A.ps = subdiv_ps(rp, A.angle, A.n);
+    return A;
+}
+
+__device__ __forceinline__ int arc_count(const TorPair& T, const TorPoint& P, const Arc& A, double rp)
+{
+    int c = 0;
+    for (int t = 0; t < A.n; ++t) {
+        V3 pt = subdiv_point(P.pij, rp, A.x, A.y, T.darc, t);
+        if (!isnan(tor_area(T, A.ps, pt))) ++c;
+    }
+    return c;
+}
+
+__device__ __forceinline__ void arc_emit(const Dev& d, const TorPair& T, const TorPoint& P, const Arc& A, double rp,
+                                         long long q0, int owner, long long unit, int s, int arcbit)
+{
+    int c = 0;
+    for (int t = 0; t < A.n; ++t) {
+        V3 pt = subdiv_point(P.pij, rp, A.x, A.y, T.darc, t);
+        double area = tor_area(T, A.ps, pt);
+        if (isnan(area)) continue;
+        write_dot(d, q0 + c, pt, P.pij, area, owner, 2, (int)unit, (s << 16) | arcbit | t);
+        ++c;
+    }
+}
+
+__device__ __forceinline__ int warp_excl_scan(int v, int& total)
+{
+    const int lane = threadIdx.x & 31;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    total = __shfl_sync(0xffffffffu, x, 31);
+    return x - v;
+}
+
+static constexpr int TO_WARPS = 4;
+
+template <bool EMIT>
+__global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
+{
+    const int lane = threadIdx.x & 31;
+    const double rp = d.st.rp;
+    const long long NT = min(d.tor_off[d.N], d.tor_cap);
+    const long long wid = blockIdx.x * (long long)TO_WARPS + (threadIdx.x >> 5);
+    const long long nw = (long long)gridDim.x * TO_WARPS;
+    for (long long q = wid; q < NT; q += nw) {
+        const TorPair T = tor_pair(d, q);
+        const bool arc1 = d.atten[T.i] >= 2, arc2 = d.atten[T.j] >= 2;
+        long long b1 = 0, b2 = 0;
+        if (EMIT) {
+            const int c = d.cplx[T.i], m = d.mol[T.i];
+            b1 = unit_base(d, c, m, 1, d.tor1_off[q]);
+            b2 = unit_base(d, c, m, 2, d.tor2_off[q]);
+        }
+        int n1 = 0, n2 = 0;
+        bool has = false;
+        for (int s0 = 0; s0 < T.ns; s0 += 32) {
+            const int s = s0 + lane;
+            int c1 = 0, c2 = 0;
+            bool valid = false;
+            TorPoint P;
+            Arc A1, A2;
+            if (s < T.ns) {
+                P = tor_point(d, T, s);
+                valid = P.valid;
+                if (P.arcs) {
+                    if (arc1) { A1 = tor_arc(T, P, P.pi, P.pqi, rp); c1 = arc_count(T, P, A1, rp); }
+                    if (arc2) { A2 = tor_arc(T, P, P.pqj, P.pj, rp); c2 = arc_count(T, P, A2, rp); }
+                }
+            }
+            has |= __any_sync(0xffffffffu, valid);
+            int t1, t2;
+            int e1 = warp_excl_scan(c1, t1);
+            int e2 = warp_excl_scan(c2, t2);
+            if (EMIT) {
+                if (c1) arc_emit(d, T, P, A1, rp, b1 + n1 + e1, T.i, q, s, 0);
+                if (c2) arc_emit(d, T, P, A2, rp, b2 + n2 + e2, T.j, q, s, 1 << 15);
+            }
+            n1 += t1;
+            n2 += t2;
+        }
+        if (!EMIT && lane == 0) { d.tor1_cnt[q] = n1; d.tor2_cnt[q] = n2; d.tor_has[q] = has ? 1 : 0; }
+    }
+}
+
+void launch_toroidal(const Dev& d, long long tor_grid, bool emit, cudaStream_t s)
+{
+    if (emit) k_toroidal<true><<<grid_for(tor_grid, TO_WARPS), TO_WARPS * 32, 0, s>>>(d);
+    else k_toroidal<false><<<grid_for(tor_grid, TO_WARPS), TO_WARPS * 32, 0, s>>>(d);
+}
+
+// ---------------------------------------------------------------------------
+// concave dots: one warp per probe
+// ---------------------------------------------------------------------------
+static constexpr int CC_WARPS = 4;
+
+template <bool EMIT>
+__global__ void __launch_bounds__(CC_WARPS * 32) k_concave(Dev d)
+{
+    __shared__ LatTable tab[CC_WARPS];
+    __shared__ int ncs[CC_WARPS][CMS_MAX_SUBDIV];
+    __shared__ int nears[CC_WARPS][CMS_NEAR_CAP];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    LatTable& L = tab[w];
+    const double rp = d.st.rp, rp2 = rp * rp;
+    const long long NP = min(d.plus_off[d.N] + d.minus_off[d.N], d.probe_cap);
+    const long long wid = blockIdx.x * (long long)CC_WARPS + w;
+    const long long nw = (long long)gridDim.x * CC_WARPS;
+    for (long long p = wid; p < NP; p += nw) {
+        const int ia[3] = {d.pa0[p], d.pa1[p], d.pa2[p]};
+        V3 xa[3];
+        double ra[3];
+        for (int k = 0; k < 3; ++k) { double4 a = d.xyzr[ia[k]]; xa[k] = v3(a.x, a.y, a.z); ra[k] = a.w; }
+        const double density = ((d.dens[ia[0]] + d.dens[ia[1]]) + d.dens[ia[2]]) / 3.0;
+        const V3 pijk = ld3(d.pxyz + 3 * p);
+        const V3 uijk = ld3(d.palt + 3 * p);
+        const bool low = d.ph[p] < rp;
+        const int c = d.cplx[ia[0]];
+        // nearby low probes of the same complex (d2 <= 4 rp^2), self excluded
+        int nnear = 0;
+        if (low) {
+            const Cplx C = d.cx[c];
+            const int s0 = C.a0, e1 = C.a0 + C.n;
+            const long long pb = min(d.plus_off[s0] + d.minus_off[s0], d.probe_cap);
+            const long long pe = min(d.plus_off[e1] + d.minus_off[e1], d.probe_cap);
+            const long long ls = d.plow_off[pb], le = d.plow_off[pe];
+            for (long long b = ls; b < le; b += 32) {
+                long long li = b + lane;
+                bool near = false;
+                int qi = -1;
+                if (li < le) {
+                    qi = d.plow_list[li];
+                    if (qi != p) near = sq_seq(pijk - ld3(d.pxyz + 3 * (long long)qi)) <= 4 * rp2;
+                }
+                unsigned m = __ballot_sync(0xffffffffu, near);
+                int pos = nnear + __popc(m & lt);
+                if (near && pos < CMS_NEAR_CAP) nears[w][pos] = qi;
+                nnear += __popc(m);
+            }
+            if (nnear > CMS_NEAR_CAP) {
+                if (lane == 0) atomicOr(&d.status[c], ST_NEAR_OVERFLOW);
+                nnear = CMS_NEAR_CAP;
+            }
+            __syncwarp();
+        }
+        // spherical-triangle frame (_core.py:2140-2164)
+        V3 vp[3];
+        for (int k = 0; k < 3; ++k) vp[k] = normalize3(xa[k] - pijk);
+        const V3 vec0 = normalize3(cross3(vp[0], vp[1]));
+        const V3 vec1 = normalize3(cross3(vp[1], vp[2]));
+        const V3 vec2 = normalize3(cross3(vp[2], vp[0]));
+        double dts[3];
+        for (int k = 0; k < 3; ++k) dts[k] = dot_seq(uijk, vp[k]);
+        int mm = 0;                                   // np.argmax: first maximum, NaN wins
+        if (!isnan(dts[0])) {
+            for (int k = 1; k < 3; ++k) {
+                if (isnan(dts[k])) { mm = k; break; }
+                if (dts[k] > dts[mm]) mm = k;
+            }
+        }
+        const V3 south = -uijk;
+        const V3 vtop = vp[mm];
+        const V3 axis = normalize3(cross3(vtop, south));
+        V3 ylat;
+        const double ang = arc_angle(axis, vtop, south, ylat);
+        const double dl = subdiv_delta(density, rp);
+        const int nl = subdiv_count(dl, ang);
+        const double cs = subdiv_ps(rp, ang, nl);
+        V3 fx, fy;
+        circle_frame(south, fx, fy);
+        for (int l = lane; l < nl; l += 32) {
+            V3 lat = subdiv_point(v3(0.0, 0.0, 0.0), rp, vtop, ylat, dl, l);
+            double dt = dot_seq(lat, south);
+            V3 cen = south * dt;
+            double rsq = rp2 - dt * dt;
+            double rad = sqrt(rsq < 0.0 ? 0.0 : rsq);
+            int nc = 0;
+            double delta = 0.0, ps = 0.0;
+            if (rad > 0.0) {
+                delta = subdiv_delta(density, rad);
+                nc = subdiv_count(delta, CMS_TWO_PI);
+                ps = subdiv_ps(rad, CMS_TWO_PI, nc);
+            }
+            L.cx[l] = cen.x; L.cy[l] = cen.y; L.cz[l] = cen.z;
+            L.rad[l] = rad; L.delta[l] = delta; L.area[l] = ps * cs;
+            ncs[w][l] = nc;
+        }
+        __syncwarp();
+        lat_prefix(L, ncs[w], nl);
+        const int total = nl > 0 ? L.start[nl] : 0;
+        long long base = 0;
+        if (EMIT) base = unit_base(d, c, d.mol[ia[0]], 3, d.conc_off[p]);
+        int kept = 0;
+        for (int t0 = 0; t0 < total; t0 += 32) {
+            const int t = t0 + lane;
+            bool keep = false;
+            V3 pts;
+            int l = 0, i = 0, mc = 0;
+            if (t < total) {
+                l = find_lat(L, nl, t);
+                i = t - L.start[l];
+                V3 pt = subdiv_point(v3(L.cx[l], L.cy[l], L.cz[l]), L.rad[l], fx, fy, L.delta[l], i);
+                keep = !(dot_seq(pt, vec0) >= 0 || dot_seq(pt, vec1) >= 0 || dot_seq(pt, vec2) >= 0);
+                if (keep) {
+                    pts = pt + pijk;
+                    if (low) {
+                        for (int k = 0; k < nnear; ++k) {
+                            if (sq_alt(pts - ld3(d.pxyz + 3 * (long long)nears[w][k])) < rp2) { keep = false; break; }
+                        }
+                    }
+                }
+                if (keep) {
+                    double dd[3];
+                    for (int k = 0; k < 3; ++k) dd[k] = norm3(pts - xa[k]) - ra[k];
+                    mc = 0;                            // np.argmin: first minimum, NaN wins
+                    if (!isnan(dd[0])) {
+                        for (int k = 1; k < 3; ++k) {
+                            if (isnan(dd[k])) { mc = k; break; }
+                            if (dd[k] < dd[mc]) mc = k;
+                        }
+                    }
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
+            if (EMIT && keep) write_dot(d, base + kept + __popc(m & lt), pts, pijk, L.area[l], ia[mc], 3, (int)p, (l << 16) | i);
+            kept += __popc(m);
+        }
+        if (!EMIT && lane == 0) d.conc_cnt[p] = kept;
+        __syncwarp();
+    }
+}
+
+void launch_concave(const Dev& d, long long probe_grid, bool emit, cudaStream_t s)
+{
+    if (emit) k_concave<true><<<grid_for(probe_grid, CC_WARPS), CC_WARPS * 32, 0, s>>>(d);
+    else k_concave<false><<<grid_for(probe_grid, CC_WARPS), CC_WARPS * 32, 0, s>>>(d);
+}
+
+// ---------------------------------------------------------------------------
+// layout: dot segment offsets per complex, molecule and type
+// ---------------------------------------------------------------------------
+struct SegCounts { long long cnt[2][4], scan0[2][4]; };
+
+__device__ __forceinline__ SegCounts seg_counts(const Dev& d, int c)
+{
+    SegCounts S;
+    const Cplx C = d.cx[c];
+    const int s0 = C.a0, s1 = C.a0 + C.n0, e1 = C.a0 + C.n;
+    const int as[2] = {s0, s1}, ae[2] = {s1, e1};
+    const long long pb = d.plus_off[s0] + d.minus_off[s0];
+    const long long P0 = (d.plus_off[s1] - d.plus_off[s0]) + (d.minus_off[s1] - d.minus_off[s0]);
+    const long long P1 = (d.plus_off[e1] - d.plus_off[s1]) + (d.minus_off[e1] - d.minus_off[s1]);
+    const long long ps[2] = {pb, pb + P0}, pe[2] = {pb + P0, pb + P0 + P1};
+    for (int m = 0; m < 2; ++m) {
+        S.scan0[m][0] = d.conv_off[as[m]];
+        S.cnt[m][0] = d.conv_off[ae[m]] - S.scan0[m][0];
+        // clamped to the capacities: past them the run is flagged and redone
+        const long long ts = min(d.tor_off[as[m]], d.tor_cap), te = min(d.tor_off[ae[m]], d.tor_cap);
+        S.scan0[m][1] = d.tor1_off[ts];
+        S.cnt[m][1] = d.tor1_off[te] - S.scan0[m][1];
+        S.scan0[m][2] = d.tor2_off[ts];
+        S.cnt[m][2] = d.tor2_off[te] - S.scan0[m][2];
+        S.scan0[m][3] = d.conc_off[min(ps[m], d.probe_cap)];
+        S.cnt[m][3] = d.conc_off[min(pe[m], d.probe_cap)] - S.scan0[m][3];
+    }
+    return S;
+}
+
+__global__ void k_layout_counts(Dev d, int* cm_count)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.B; c += gridDim.x * blockDim.x) {
+        SegCounts S = seg_counts(d, c);
+        for (int m = 0; m < 2; ++m)
+            cm_count[c * 2 + m] = (int)(S.cnt[m][0] + S.cnt[m][1] + S.cnt[m][2] + S.cnt[m][3]);
+    }
+}
+
+__global__ void k_layout_seg(Dev d)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.B; c += gridDim.x * blockDim.x) {
+        SegCounts S = seg_counts(d, c);
+        for (int m = 0; m < 2; ++m) {
+            long long pos = d.dot_off[c * 2 + m];
+            for (int t = 0; t < 4; ++t) {
+                Seg g;
+                g.dot0 = pos;
+                g.scan0 = S.scan0[m][t];
+                d.seg[(c * 2 + m) * 4 + t] = g;
+                pos += S.cnt[m][t];
+            }
+        }
+    }
+}
+
+void launch_layout(const Dev& d, long long* cm_count_tmp, long long* scan_tmp, cudaStream_t s)
+{
+    int* cm = reinterpret_cast<int*>(cm_count_tmp);
+    k_layout_counts<<<grid_for(d.B, 128), 128, 0, s>>>(d, cm);
+    scan_counts(cm, d.dot_off, 2LL * d.B, scan_tmp, s);
+    k_layout_seg<<<grid_for(d.B, 128), 128, 0, s>>>(d);
+}
+
+// ---------------------------------------------------------------------------
+// toroidal access flags: access[natoms1] |= has, then access[natoms2] |= has,
+// where NumPy's fancy-index read-modify-write keeps, for a repeated atom, the
+// value computed for its last occurrence (_core.py:1247-1248)
+// ---------------------------------------------------------------------------
+__global__ void k_tor_last(Dev d)
+{
+    const long long NT = min(d.tor_off[d.N], d.tor_cap);
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < NT; q += (long long)gridDim.x * blockDim.x)
+        atomicMax(&d.tor_last2[d.tor_j[q]], (unsigned long long)(q + 1));
+}
+
+__global__ void k_tor_access_apply(Dev d)
+{
+    for (long long a = blockIdx.x * (long long)blockDim.x + threadIdx.x; a < d.N; a += (long long)gridDim.x * blockDim.x) {
+        int8_t v = d.access[a];
+        if (d.tor_off[a + 1] > d.tor_off[a]) v |= d.tor_has[d.tor_off[a + 1] - 1];   // rows are grouped by atom1
+        unsigned long long l2 = d.tor_last2[a];
+        if (l2 > 0) v |= d.tor_has[l2 - 1];
+        d.access[a] = v;
+    }
+}
+
+void launch_tor_access(const Dev& d, long long tor_grid, cudaStream_t s)
+{
+    cudaMemsetAsync(d.tor_last2, 0, sizeof(unsigned long long) * d.N, s);
+    k_tor_last<<<grid_for(tor_grid, 256), 256, 0, s>>>(d);
+    k_tor_access_apply<<<grid_for(d.N, 256), 256, 0, s>>>(d);
+}
+
+}  // namespace cms

@@ -1,0 +1,529 @@
+// Readouts of a generated surface: CMS (both sides), maximum possible CMS and
+// Lawrence & Colman shape complementarity.
+//
+// Reference behaviour (cms-cuda/_core.py):
+//   calc_contact_molecular_surface                 _core.py:946-1004
+//   calc_max_possible_contact_molecular_surface    _core.py:1007-1034
+//   trim_peripheral_band_vectorized                _core.py:1037-1077
+//   _binned_median                                 _core.py:1080-1104
+//   calc_neighbor_distance_vectorized              _core.py:1107-1147
+//   CalcLoadedSC                                   _core.py:807-863
+//
+// The nearest-dot search is brute force over every (query, reference) pair.
+// Coordinates relative to the complex centre are staged in FP32; the FP32
+// squared distance filters candidates and every reference whose FP32 value is
+// within a proven error bound of the running FP32 minimum is re-evaluated in
+// FP64 in the reference's (cdist) order, so the minimum and the first index
+// attaining it are exactly those of the FP64 search.
+#include "cms_readout.cuh"
+
+namespace cms {
+
+static constexpr int SM_COUNT = 148;
+
+static inline unsigned grid_for(long long items, int per_block, int max_blocks_per_sm = 16)
+{
+    long long b = (items + per_block - 1) / per_block;
+    long long cap = (long long)SM_COUNT * max_blocks_per_sm;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (unsigned)b;
+}
+
+// dot offset per complex & molecule, clamped to the dot capacity (a run past
+// the capacity is flagged and redone, but must not read out of bounds)
+__device__ __forceinline__ long long doff(const Dev& d, long long i) { return min(d.dot_off[i], d.dot_cap); }
+
+// ---------------------------------------------------------------------------
+// compaction of buried / accessible dots, FP32 packing
+// ---------------------------------------------------------------------------
+__global__ void k_flag_buried(Dev d, Rd r, long long cap)
+{
+    const long long D = doff(d, 2LL * d.B);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cap; i += (long long)gridDim.x * blockDim.x)
+        r.flag[i] = (i < D && d.dbur[i]) ? 1 : 0;
+}
+
+__device__ __forceinline__ float4 pack_f4(const Dev& d, long long dot, int c)
+{
+    const Cplx& C = d.cx[c];
+    const double* p = d.dxyz + 3 * dot;
+    return make_float4((float)(p[0] - C.ctr[0]), (float)(p[1] - C.ctr[1]), (float)(p[2] - C.ctr[2]), 0.f);
+}
+
+// dot -> complex via binary search of dot_off (per complex & molecule)
+__device__ __forceinline__ int dot_cm(const Dev& d, long long dot)
+{
+    int lo = 0, hi = 2 * d.B - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (doff(d, mid) <= dot) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void k_split_buried(Dev d, Rd r, long long cap)
+{
+    const long long D = doff(d, 2LL * d.B);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cap && i < D; i += (long long)gridDim.x * blockDim.x) {
+        const int cm = dot_cm(d, i);
+        const float4 f = pack_f4(d, i, cm >> 1);
+        if (r.flag[i]) {
+            long long k = r.bur_scan[i];
+            r.bur_idx[k] = (int)i;
+            r.bur_f4[k] = f;
+            r.bur_cm[k] = cm;
+        } else {
+            long long k = i - r.bur_scan[i];
+            r.acc_idx[k] = (int)i;
+            r.acc_f4[k] = f;
+        }
+    }
+}
+
+void launch_split_buried(const Dev& d, const Rd& r, long long dot_cap, long long* scan_tmp, cudaStream_t s)
+{
+    k_flag_buried<<<grid_for(dot_cap, 256), 256, 0, s>>>(d, r, dot_cap);
+    scan_counts(r.flag, r.bur_scan, dot_cap, scan_tmp, s);
+    k_split_buried<<<grid_for(dot_cap, 256), 256, 0, s>>>(d, r, dot_cap);
+}
+
+// ---------------------------------------------------------------------------
+// brute-force nearest-dot search, FP32 filter + FP64 recheck
+// ---------------------------------------------------------------------------
+// Error model (u = 2^-24): coordinates relative to the centre are within R of
+// it per axis.  For any pair, |sqrt(D32) - sqrt(D)| <= E + rho*sqrt(D) with
+// E = 3.53 u R and rho = 2.7 u (input rounding of both points, the rounded
+// difference and the three-term FP32 sum).  A reference that attains the
+// FP64 minimum therefore has sqrt(D32) <= (sqrt(m) + E)(1 + 3 rho) + E,
+// m = smallest D32 seen; the kernel rechecks everything under that bound.
+__device__ __forceinline__ float nn_threshold(float m, double E)
+{
+    if (!(m < INFINITY)) return INFINITY;
+    double t = (sqrt((double)m) + E) * (1.0 + 1e-6) + E;
+    return __double2float_ru(t * t * (1.0 + 1e-6));
+}
+
+__device__ __forceinline__ double exact_d2(const double* a, const double* b)
+{
+    // cdist(ref, query, 'sqeuclidean') order: (d0*d0 + d1*d1) + d2*d2
+    double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+    return (dx * dx + dy * dy) + dz * dz;
+}
+
+static constexpr int NN_T = 256;     // queries per tile (one per thread)
+static constexpr int NN_R = 1024;    // references staged per round
+
+template <int MODE>
+__global__ void __launch_bounds__(NN_T) k_nn(Dev d, NNArgs a)
+{
+    __shared__ float4 sref[NN_R];
+    const long long ntiles = a.tile_off[a.ntask];
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        // task of this tile
+        int lo = 0, hi = a.ntask - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (a.tile_off[mid] <= tile) lo = mid; else hi = mid - 1;
+        }
+        const NNTask T = a.task[lo];
+        const long long qi = (tile - a.tile_off[lo]) * NN_T + threadIdx.x;
+        const bool live = qi < T.qn;
+        const Cplx& C = d.cx[T.c];
+        const double E = 2.5e-7 * C.R;
+        float qx = 0, qy = 0, qz = 0;
+        double q64[3] = {0, 0, 0};
+        if (live) {
+            float4 f = a.q_f4[T.q0 + qi];
+            qx = f.x; qy = f.y; qz = f.z;
+            const double* p = d.dxyz + 3LL * a.q_idx[T.q0 + qi];
+            q64[0] = p[0]; q64[1] = p[1]; q64[2] = p[2];
+        }
+        float mf = INFINITY;
+        float thr = INFINITY;
+        if (MODE == NN_BAND) {
+            double t = (sqrt(a.band_thr64) * (1.0 + 1e-6)) + E;
+            thr = __double2float_ru(t * t * (1.0 + 1e-6));
+        }
+        double best = INFINITY;
+        int bidx = -1;
+        bool done = !live;
+        for (long long rb = 0; rb < T.rn; rb += NN_R) {
+            const int nr = (int)min((long long)NN_R, T.rn - rb);
+            __syncthreads();
+            for (int k = threadIdx.x; k < nr; k += NN_T) sref[k] = a.r_f4[T.r0 + rb + k];
+            __syncthreads();
+            if (!done) {
+                for (int k = 0; k < nr; ++k) {
+                    const float4 r4 = sref[k];
+                    const float dx = r4.x - qx, dy = r4.y - qy, dz = r4.z - qz;
+                    const float d2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, dx * dx));
+                    if (d2 <= thr) {
+                        const double* rp = d.dxyz + 3LL * a.r_idx[T.r0 + rb + k];
+                        const double e = exact_d2(rp, q64);
+                        if (MODE == NN_BAND) {
+                            if (e <= a.band_thr64) { done = true; best = e; break; }
+                        } else {
+                            if (e < best) { best = e; bidx = (int)(rb + k); }
+                            if (d2 < mf) { mf = d2; thr = nn_threshold(mf, E); }
+                        }
+                    }
+                }
+            }
+            if (MODE == NN_BAND) {
+                if (__syncthreads_and(done)) break;
+            }
+        }
+        if (live) {
+            const long long o = T.q0 + qi;
+            if (MODE == NN_BAND) a.out_flag[o] = done ? 0 : 1;      // keep iff no reference within the band
+            else {
+                a.out_d2[o] = best;
+                if (MODE == NN_ARGMIN) a.out_idx[o] = bidx;
+            }
+        }
+    }
+}
+
+__global__ void k_nn_tiles(NNArgs a)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < a.ntask; t += gridDim.x * blockDim.x) {
+        const NNTask T = a.task[t];
+        a.tile_cnt[t] = (T.qn > 0 && (T.rn > 0 || a.band_mode)) ? (int)((T.qn + NN_T - 1) / NN_T) : 0;
+    }
+}
+
+void launch_nn(const Dev& d, NNArgs a, int mode, long long tile_cap, long long* scan_tmp, cudaStream_t s)
+{
+    a.band_mode = mode == NN_BAND;
+    k_nn_tiles<<<grid_for(a.ntask, 128), 128, 0, s>>>(a);
+    scan_counts(a.tile_cnt, a.tile_off, a.ntask, scan_tmp, s);
+    const unsigned grid = grid_for(tile_cap, 1, 8);
+    if (mode == NN_MIN) k_nn<NN_MIN><<<grid, NN_T, 0, s>>>(d, a);
+    else if (mode == NN_ARGMIN) k_nn<NN_ARGMIN><<<grid, NN_T, 0, s>>>(d, a);
+    else k_nn<NN_BAND><<<grid, NN_T, 0, s>>>(d, a);
+}
+
+// ---------------------------------------------------------------------------
+// task tables
+// ---------------------------------------------------------------------------
+// CMS: queries = buried dots of molecule m, references = buried dots of 1-m
+__global__ void k_tasks_cms(Dev d, Rd r, NNTask* task)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 2 * d.B; t += gridDim.x * blockDim.x) {
+        const int c = t >> 1, m = t & 1, o = (c * 2) + (1 - m);
+        NNTask T;
+        T.c = c;
+        T.q0 = r.bur_scan[doff(d, t)];
+        T.qn = r.bur_scan[doff(d, t + 1)] - T.q0;
+        T.r0 = r.bur_scan[doff(d, o)];
+        T.rn = r.bur_scan[doff(d, o + 1)] - T.r0;
+        task[t] = T;
+    }
+}
+
+// SC trim: queries = buried dots of molecule m, references = accessible dots of m
+__global__ void k_tasks_trim(Dev d, Rd r, NNTask* task)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 2 * d.B; t += gridDim.x * blockDim.x) {
+        const long long ds = doff(d, t), de = doff(d, t + 1);
+        NNTask T;
+        T.c = t >> 1;
+        T.q0 = r.bur_scan[ds];
+        T.qn = r.bur_scan[de] - T.q0;
+        T.r0 = ds - r.bur_scan[ds];
+        T.rn = (de - r.bur_scan[de]) - T.r0;
+        task[t] = T;
+    }
+}
+
+// SC neighbour distance: queries = trimmed dots of m, references = trimmed dots of 1-m
+__global__ void k_tasks_sc(Dev d, Rd r, NNTask* task)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 2 * d.B; t += gridDim.x * blockDim.x) {
+        const int c = t >> 1, m = t & 1, o = (c * 2) + (1 - m);
+        NNTask T;
+        T.c = c;
+        T.q0 = r.trim_scan[r.bur_scan[doff(d, t)]];
+        T.qn = r.trim_scan[r.bur_scan[doff(d, t + 1)]] - T.q0;
+        T.r0 = r.trim_scan[r.bur_scan[doff(d, o)]];
+        T.rn = r.trim_scan[r.bur_scan[doff(d, o + 1)]] - T.r0;
+        if (T.rn == 0) T.qn = 0;
+        task[t] = T;
+    }
+}
+
+void launch_tasks(const Dev& d, const Rd& r, int kind, NNTask* task, cudaStream_t s)
+{
+    const unsigned g = grid_for(2LL * d.B, 128);
+    if (kind == 0) k_tasks_cms<<<g, 128, 0, s>>>(d, r, task);
+    else if (kind == 1) k_tasks_trim<<<g, 128, 0, s>>>(d, r, task);
+    else k_tasks_sc<<<g, 128, 0, s>>>(d, r, task);
+}
+
+// ---------------------------------------------------------------------------
+// per-dot CMS weights and deterministic per-atom sums (np.bincount order)
+// ---------------------------------------------------------------------------
+// per buried dot: area * exp(-d2 * weight) against the other molecule's buried dots
+__global__ void k_cms_weights(Dev d, Rd r, long long cap)
+{
+    const long long NB = r.bur_scan[doff(d, 2LL * d.B)];
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cap; k += (long long)gridDim.x * blockDim.x) {
+        if (k < NB) {
+            const int dot = r.bur_idx[k];
+            r.val[k] = d.darea[dot] * exp((-r.nn_d2[k]) * d.st.weight);
+            r.own[k] = d.datom[dot];
+        } else {
+            r.own[k] = -1;
+        }
+    }
+}
+
+// values of every dot of molecule 0 (maximum possible CMS): own = owner or -1
+__global__ void k_area_values(Dev d, Rd r, long long cap)
+{
+    const long long D = doff(d, 2LL * d.B);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cap; i += (long long)gridDim.x * blockDim.x) {
+        if (i < D) {
+            const int cm = dot_cm(d, i);
+            r.val[i] = d.darea[i];
+            r.own[i] = (cm & 1) == 0 ? d.datom[i] : -1;
+        } else {
+            r.own[i] = -1;
+        }
+    }
+}
+
+__global__ void k_own_count(Rd r, long long cap, int* cnt)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cap; k += (long long)gridDim.x * blockDim.x) {
+        int a = r.own[k];
+        if (a >= 0) atomicAdd(&cnt[a], 1);
+    }
+}
+
+__global__ void k_own_scatter(Rd r, long long cap, const long long* off, int* fill, int* slot)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cap; k += (long long)gridDim.x * blockDim.x) {
+        int a = r.own[k];
+        if (a >= 0) slot[off[a] + atomicAdd(&fill[a], 1)] = (int)k;
+    }
+}
+
+__global__ void k_own_sum(long long N, const long long* off, int* slot, const double* val, double* out)
+{
+    for (long long a = blockIdx.x * (long long)blockDim.x + threadIdx.x; a < N; a += (long long)gridDim.x * blockDim.x) {
+        const long long s = off[a], e = off[a + 1];
+        for (long long i = s + 1; i < e; ++i) {           // entries in increasing dot order
+            int v = slot[i];
+            long long k = i - 1;
+            while (k >= s && slot[k] > v) { slot[k + 1] = slot[k]; --k; }
+            slot[k + 1] = v;
+        }
+        double acc = 0.0;
+        for (long long i = s; i < e; ++i) acc += val[slot[i]];
+        out[a] = acc;
+    }
+}
+
+void launch_per_atom_sum(const Dev& d, const Rd& r, long long cap, double* out, long long* scan_tmp, cudaStream_t s)
+{
+    cudaMemsetAsync(r.acnt, 0, sizeof(int) * d.N, s);
+    cudaMemsetAsync(r.afill, 0, sizeof(int) * d.N, s);
+    k_own_count<<<grid_for(cap, 256), 256, 0, s>>>(r, cap, r.acnt);
+    scan_counts(r.acnt, r.aoff, d.N, scan_tmp, s);
+    k_own_scatter<<<grid_for(cap, 256), 256, 0, s>>>(r, cap, r.aoff, r.afill, r.aslot);
+    k_own_sum<<<grid_for(d.N, 128), 128, 0, s>>>(d.N, r.aoff, r.aslot, r.val, out);
+}
+
+void launch_cms_weights(const Dev& d, const Rd& r, long long cap, cudaStream_t s)
+{
+    k_cms_weights<<<grid_for(cap, 256), 256, 0, s>>>(d, r, cap);
+}
+
+void launch_area_values(const Dev& d, const Rd& r, long long cap, cudaStream_t s)
+{
+    k_area_values<<<grid_for(cap, 256), 256, 0, s>>>(d, r, cap);
+}
+
+// per complex & molecule: total of per-atom values (deterministic block tree)
+__device__ __forceinline__ double block_sum(double v, double* sh)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0) for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += sh[i];
+    __syncthreads();
+    return t;
+}
+
+__global__ void k_atom_totals(Dev d, const double* per_atom, double* tot)
+{
+    __shared__ double sh[32];
+    const int t = blockIdx.x;                      // complex * 2 + molecule
+    const int c = t >> 1, m = t & 1;
+    const Cplx C = d.cx[c];
+    const int s = C.a0 + (m ? C.n0 : 0), e = m ? C.a0 + C.n : C.a0 + C.n0;
+    double v = 0.0;
+    for (int a = s + threadIdx.x; a < e; a += blockDim.x) v += per_atom[a];
+    double total = block_sum(v, sh);
+    if (threadIdx.x == 0) tot[t] = total;
+}
+
+void launch_atom_totals(const Dev& d, const double* per_atom, double* tot, cudaStream_t s)
+{
+    k_atom_totals<<<2 * d.B, 256, 0, s>>>(d, per_atom, tot);
+}
+
+// ---------------------------------------------------------------------------
+// shape complementarity
+// ---------------------------------------------------------------------------
+__global__ void k_trim_compact_flags(Dev d, Rd r, long long cap)
+{
+    const long long NB = r.bur_scan[doff(d, 2LL * d.B)];
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cap; k += (long long)gridDim.x * blockDim.x)
+        if (k >= NB) r.keep[k] = 0;
+}
+
+__global__ void k_trim_fill(Dev d, Rd r, long long cap)
+{
+    const long long NB = r.bur_scan[doff(d, 2LL * d.B)];
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cap && k < NB; k += (long long)gridDim.x * blockDim.x) {
+        if (r.keep[k]) {
+            long long t = r.trim_scan[k];
+            r.trim_idx[t] = r.bur_idx[k];
+            r.trim_f4[t] = r.bur_f4[k];
+        }
+    }
+}
+
+void launch_trim_compact(const Dev& d, const Rd& r, long long cap, long long* scan_tmp, cudaStream_t s)
+{
+    k_trim_compact_flags<<<grid_for(cap, 256), 256, 0, s>>>(d, r, cap);
+    scan_counts(r.keep, r.trim_scan, cap, scan_tmp, s);
+    k_trim_fill<<<grid_for(cap, 256), 256, 0, s>>>(d, r, cap);
+}
+
+// grouped-data median (_core.py:1080-1104) of n values produced by `get`
+template <class G>
+__device__ double binned_median(long long n, double w, G&& get, long long* shl)
+{
+    if (n == 0) return 0.0;
+    long long lo = LLONG_MAX, hi = LLONG_MIN;
+    for (long long k = threadIdx.x; k < n; k += blockDim.x) {
+        long long b = (long long)floor(get(k) / w);
+        lo = min(lo, b); hi = max(hi, b);
+    }
+    // block min / max
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (lane == 0) { shl[wp] = lo; shl[32 + wp] = hi; }
+    __syncthreads();
+    lo = shl[0]; hi = shl[32];
+    for (int i = 1; i < nw; ++i) { lo = min(lo, shl[i]); hi = max(hi, shl[32 + i]); }
+    __syncthreads();
+    const double pct = 100.0 / (double)n;
+    // count of values with bin <= t
+    auto count_le = [&](long long t) -> long long {
+        long long c = 0;
+        for (long long k = threadIdx.x; k < n; k += blockDim.x)
+            c += ((long long)floor(get(k) / w) <= t) ? 1 : 0;
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        __syncthreads();
+        if (lane == 0) shl[wp] = c;
+        __syncthreads();
+        long long s = 0;
+        for (int i = 0; i < nw; ++i) s += shl[i];
+        __syncthreads();
+        return s;
+    };
+    // smallest bin t with cumulative percentage >= 50 (np.searchsorted 'left')
+    long long a = lo, b = hi;
+    while (a < b) {
+        long long mid = a + ((b - a) >> 1);
+        if ((double)count_le(mid) * pct >= 50.0) b = mid; else a = mid + 1;
+    }
+    const long long cum = count_le(a);
+    const long long cnt = cum - count_le(a - 1);
+    const double cumperc = (double)cum * pct;
+    const double before = cumperc - (double)cnt * pct;
+    const double bin_perc = (double)cnt * pct;
+    return (double)a * w + (50.0 - before) * w / bin_perc;
+}
+
+// one block per (complex, molecule): trimmed area, neighbour statistics
+__global__ void k_sc_stats(Dev d, Rd r, const NNTask* task, double* out)
+{
+    __shared__ double sh[32];
+    __shared__ long long shl[64];
+    const int t = blockIdx.x;
+    const int c = t >> 1, m = t & 1;
+    const long long ds = doff(d, t), de = doff(d, t + 1);
+    const long long bs = r.bur_scan[ds], be = r.bur_scan[de];
+    // trimmed area: sum of areas of kept buried dots
+    double v = 0.0;
+    for (long long k = bs + threadIdx.x; k < be; k += blockDim.x)
+        if (r.keep[k]) v += d.darea[r.bur_idx[k]];
+    const double area = block_sum(v, sh);
+    const long long ntrim = r.trim_scan[be] - r.trim_scan[bs];
+    const NNTask T = task[t];
+    double dmean = 0.0, dmed = 0.0, smean = 0.0, smed = 0.0;
+    if (T.qn > 0 && T.rn > 0) {
+        const long long q0 = T.q0, n = T.qn;
+        const double weight = d.st.weight;
+        auto distk = [&](long long k) -> double { return sqrt(r.nn_d2[q0 + k]); };
+        auto rk = [&](long long k) -> double {
+            const long long o = q0 + k;
+            const V3 nm = ld3(d.dnml + 3LL * r.trim_idx[o]);
+            const V3 nt = ld3(d.dnml + 3LL * r.trim_idx[T.r0 + r.nn_idx[o]]);
+            const double dist = sqrt(r.nn_d2[o]);
+            double rv = dot_alt(nm, nt);
+            rv = rv * exp((-(dist * dist)) * weight);
+            return rv < -0.999 ? -0.999 : (rv > 0.999 ? 0.999 : rv);
+        };
+        double sd = 0.0, sr = 0.0;
+        for (long long k = threadIdx.x; k < n; k += blockDim.x) { sd += distk(k); sr += rk(k); }
+        const double tot_d = block_sum(sd, sh);
+        const double tot_r = block_sum(sr, sh);
+        dmed = binned_median(n, d.st.bw_dist, distk, shl);
+        const double rmed = binned_median(n, d.st.bw_norm, rk, shl);
+        dmean = tot_d / (double)n;
+        smean = -(tot_r / (double)n);
+        smed = -rmed;
+    }
+    if (threadIdx.x == 0) {
+        double* o = out + (long long)t * SC_SIDE_FIELDS;
+        o[0] = dmean; o[1] = dmed; o[2] = smean; o[3] = smed; o[4] = area;
+        o[5] = (double)ntrim; o[6] = (double)(de - ds);
+    }
+}
+
+__global__ void k_sc_final(Dev d, const double* side, double* out)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.B; c += gridDim.x * blockDim.x) {
+        const double* s0 = side + (long long)(2 * c) * SC_SIDE_FIELDS;
+        const double* s1 = side + (long long)(2 * c + 1) * SC_SIDE_FIELDS;
+        double* o = out + (long long)c * SC_FIELDS;
+        const double dmean = (s0[0] + s1[0]) / 2, dmed = (s0[1] + s1[1]) / 2;
+        const double smean = (s0[2] + s1[2]) / 2, smed = (s0[3] + s1[3]) / 2;
+        o[0] = smed;                 // sc
+        o[1] = s0[4] + s1[4];        // trimmed interface area
+        o[2] = dmed;                 // median distance
+        o[3] = dmean; o[4] = smean;
+    }
+}
+
+void launch_sc_stats(const Dev& d, const Rd& r, const NNTask* task, double* side, double* out, cudaStream_t s)
+{
+    k_sc_stats<<<2 * d.B, 256, 0, s>>>(d, r, task, side);
+    k_sc_final<<<grid_for(d.B, 128), 128, 0, s>>>(d, side, out);
+}
+
+}  // namespace cms

@@ -1,0 +1,660 @@
+// Surface pipeline, front half: per-complex setup, cell lists, attention
+// numbers, neighbour / buried-partner lists, the pair loop and the triple
+// (probe placement) loop.
+//
+// Reference behaviour (cms-cuda/_core.py):
+//   assign_attention_numbers   _core.py:1150-1195
+//   build_neighbor_arrays      _core.py:1251-1349
+//   second_loop                _core.py:1351-1442
+//   vec_third_loop             _core.py:1445-1643
+// Every distance test keeps the reference's summation order (dot_seq for
+// cdist / np.sum / norm, dot_alt for einsum) and strictness.
+#include "cms_kernels.cuh"
+
+namespace cms {
+
+static constexpr int SM_COUNT = 148;
+
+static inline unsigned grid_for(long long items, int per_block, int max_blocks_per_sm = 16)
+{
+    long long b = (items + per_block - 1) / per_block;
+    long long cap = (long long)SM_COUNT * max_blocks_per_sm;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (unsigned)b;
+}
+
+// ---------------------------------------------------------------------------
+// per-complex setup: bounding box, radmax, cell grid
+// ---------------------------------------------------------------------------
+static constexpr long long MAX_CELLS_PER_COMPLEX = 1ll << 21;
+
+__global__ void k_setup(Dev d, int* ncell)
+{
+    const int c = blockIdx.x;
+    const int a0 = d.atom_off[c], a1 = d.atom_off[c + 1];
+    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    double rmax = -INFINITY;
+    for (int g = a0 + threadIdx.x; g < a1; g += blockDim.x) {
+        double4 a = d.xyzr[g];
+        mn[0] = fmin(mn[0], a.x); mn[1] = fmin(mn[1], a.y); mn[2] = fmin(mn[2], a.z);
+        mx[0] = fmax(mx[0], a.x); mx[1] = fmax(mx[1], a.y); mx[2] = fmax(mx[2], a.z);
+        rmax = fmax(rmax, a.w);
+        d.cplx[g] = c;
+        d.mol[g] = (g - a0) < d.n0[c] ? 0 : 1;
+    }
+    __shared__ double sh[7][32];
+    double v[7] = {mn[0], mn[1], mn[2], -mx[0], -mx[1], -mx[2], -rmax};
+    for (int k = 0; k < 7; ++k)
+        for (int o = 16; o > 0; o >>= 1) v[k] = fmin(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0) for (int k = 0; k < 7; ++k) sh[k][w] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 7; ++k) { double m = sh[k][0]; for (int i = 1; i < nw; ++i) m = fmin(m, sh[k][i]); v[k] = m; }
+        Cplx C;
+        C.a0 = a0; C.n = a1 - a0; C.n0 = d.n0[c];
+        const double rp = d.st.rp;
+        if (C.n <= 0) {
+            C.radmax = 0; C.h = 1; C.R = 1;
+            for (int k = 0; k < 3; ++k) { C.dims[k] = 1; C.org[k] = 0; C.ctr[k] = 0; }
+            d.status[c] |= ST_EMPTY;
+            ncell[c] = 0;
+        } else {
+            double lo[3] = {v[0], v[1], v[2]}, hi[3] = {-v[3], -v[4], -v[5]};
+            C.radmax = -v[6];
+            double cut = 2.0 * fmax(C.radmax, 0.0) + 2.0 * fmax(rp, 0.0);
+            if (!d.all_atoms && d.st.sep > cut) cut = d.st.sep;
+            double h = fmax(cut, 1e-3) * (1.0 + 1e-6) + 1e-6;
+            long long nc;
+            for (;;) {
+                nc = 1;
+                for (int k = 0; k < 3; ++k) {
+                    C.dims[k] = (int)floor((hi[k] - lo[k]) / h) + 1;
+                    nc *= C.dims[k];
+                }
+                if (nc <= MAX_CELLS_PER_COMPLEX) break;
+                h *= 1.25;
+            }
+            C.h = h;
+            double half = 0.0;
+            for (int k = 0; k < 3; ++k) {
+                C.org[k] = lo[k];
+                C.ctr[k] = 0.5 * (lo[k] + hi[k]);
+                half = fmax(half, 0.5 * (hi[k] - lo[k]));
+            }
+            C.R = half + fmax(C.radmax, 0.0) + 2.0 * fmax(rp, 0.0) + 1.0;
+            ncell[c] = (int)nc;
+        }
+        C.cell0 = 0;
+        d.cx[c] = C;
+        d.coin[c] = ~0ull;
+    }
+}
+
+void launch_setup(const Dev& d, cudaStream_t s)
+{
+    k_setup<<<d.B, 256, 0, s>>>(d, d.ncell);
+}
+
+// ---------------------------------------------------------------------------
+// cell lists (counting sort of atoms by cell, then each cell sorted by atom id)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void atom_cell(const Dev& d, int g, int c, int& cx, int& cy, int& cz)
+{
+    const Cplx& C = d.cx[c];
+    double4 a = d.xyzr[g];
+    cx = cell_coord(a.x, C.org[0], C.h, C.dims[0]);
+    cy = cell_coord(a.y, C.org[1], C.h, C.dims[1]);
+    cz = cell_coord(a.z, C.org[2], C.h, C.dims[2]);
+}
+
+__global__ void k_cell_count(Dev d)
+{
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < d.N; g += (long long)gridDim.x * blockDim.x) {
+        int c = d.cplx[g];
+        int x, y, z;
+        atom_cell(d, (int)g, c, x, y, z);
+        const Cplx& C = d.cx[c];
+        long long cell = d.ncell_scan[c] + ((long long)x * C.dims[1] + y) * C.dims[2] + z;
+        if (cell >= d.cells_cap) { atomicOr(&d.status[c], ST_OVERFLOW); cell = -1; }
+        d.cell_of[g] = (int)cell;
+        if (cell >= 0) atomicAdd(&d.cell_cnt[cell], 1);
+    }
+}
+
+__global__ void k_cell_fill(Dev d)
+{
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < d.N; g += (long long)gridDim.x * blockDim.x) {
+        int cell = d.cell_of[g];
+        if (cell < 0) continue;
+        int pos = atomicAdd(&d.cell_fill[cell], 1);
+        d.cell_atom[d.cell_start[cell] + pos] = (int)g;
+    }
+}
+
+__global__ void k_cell_sort(Dev d, long long ncells_cap)
+{
+    const long long ncells = d.ncell_scan[d.B];
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncells && c < ncells_cap;
+         c += (long long)gridDim.x * blockDim.x) {
+        long long s = d.cell_start[c], e = d.cell_start[c + 1];
+        for (long long i = s + 1; i < e; ++i) {
+            int v = d.cell_atom[i];
+            long long k = i - 1;
+            while (k >= s && d.cell_atom[k] > v) { d.cell_atom[k + 1] = d.cell_atom[k]; --k; }
+            d.cell_atom[k + 1] = v;
+        }
+    }
+}
+
+__global__ void k_zero_int(int* p, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = 0;
+}
+
+void launch_cells(const Dev& d, long long n_cells, long long* scan_tmp, cudaStream_t s)
+{
+    scan_counts(d.ncell, d.ncell_scan, d.B, scan_tmp, s);
+    k_zero_int<<<grid_for(n_cells, 256), 256, 0, s>>>(d.cell_cnt, n_cells);
+    k_zero_int<<<grid_for(n_cells, 256), 256, 0, s>>>(d.cell_fill, n_cells);
+    k_cell_count<<<grid_for(d.N, 256), 256, 0, s>>>(d);
+    scan_counts(d.cell_cnt, d.cell_start, n_cells, scan_tmp, s);
+    k_cell_fill<<<grid_for(d.N, 256), 256, 0, s>>>(d);
+    k_cell_sort<<<grid_for(n_cells, 128), 128, 0, s>>>(d, n_cells);
+}
+
+// visit every atom in the 27 cells around atom g's cell
+template <class F>
+__device__ __forceinline__ void for_near_atoms(const Dev& d, int g, int c, F&& f)
+{
+    const Cplx& C = d.cx[c];
+    int x, y, z;
+    atom_cell(d, g, c, x, y, z);
+    const long long c0 = d.ncell_scan[c];
+    for (int ix = max(x - 1, 0); ix <= min(x + 1, C.dims[0] - 1); ++ix)
+        for (int iy = max(y - 1, 0); iy <= min(y + 1, C.dims[1] - 1); ++iy)
+            for (int iz = max(z - 1, 0); iz <= min(z + 1, C.dims[2] - 1); ++iz) {
+                long long cell = c0 + ((long long)ix * C.dims[1] + iy) * C.dims[2] + iz;
+                long long s = d.cell_start[cell], e = d.cell_start[cell + 1];
+                for (long long p = s; p < e; ++p) f(d.cell_atom[p]);
+            }
+}
+
+// ---------------------------------------------------------------------------
+// attention numbers: blocker (1) when the closest atom of the other molecule
+// is at least `sep` away, else 5; every atom gets 5 in all-atoms mode
+// ---------------------------------------------------------------------------
+__global__ void k_attention(Dev d)
+{
+    for (long long gg = blockIdx.x * (long long)blockDim.x + threadIdx.x; gg < d.N; gg += (long long)gridDim.x * blockDim.x) {
+        const int g = (int)gg;
+        if (d.all_atoms) { d.atten[g] = 5; continue; }
+        const int c = d.cplx[g];
+        const V3 xi = atom_xyz(d, g);
+        const int8_t mi = d.mol[g];
+        double best = INFINITY;
+        for_near_atoms(d, g, c, [&](int j) {
+            if (d.mol[j] != mi) {
+                double d2 = sq_seq(xi - atom_xyz(d, j));
+                best = fmin(best, d2);
+            }
+        });
+        d.atten[g] = (sqrt(best) >= d.st.sep) ? 1 : 5;
+    }
+}
+
+void launch_attention(const Dev& d, cudaStream_t s)
+{
+    k_attention<<<grid_for(d.N, 128), 128, 0, s>>>(d);
+}
+
+// ---------------------------------------------------------------------------
+// neighbour / buried-partner lists
+//   neighbour:  same molecule, j != i, d2 < ((ri + rj) + 2 rp)^2
+//   buried:     other molecule, atten_j >= 5, same bridge test
+//   coincident: same molecule, j != i, d2 <= 1e-4 (first pair reported)
+// rows sorted by (d2, j) (neighbours) and by j (buried partners)
+// ---------------------------------------------------------------------------
+static constexpr int NB_WARPS = 4;
+static constexpr int NB_CAP = 256;
+
+struct NearScan {
+    // warp-cooperative walk over the 27 cells; calls f(j, valid) with all 32 lanes
+    template <class F>
+    __device__ __forceinline__ static void run(const Dev& d, int g, int c, F&& f)
+    {
+        const Cplx& C = d.cx[c];
+        int x, y, z;
+        atom_cell(d, g, c, x, y, z);
+        const long long c0 = d.ncell_scan[c];
+        const int lane = threadIdx.x & 31;
+        for (int ix = max(x - 1, 0); ix <= min(x + 1, C.dims[0] - 1); ++ix)
+            for (int iy = max(y - 1, 0); iy <= min(y + 1, C.dims[1] - 1); ++iy)
+                for (int iz = max(z - 1, 0); iz <= min(z + 1, C.dims[2] - 1); ++iz) {
+                    long long cell = c0 + ((long long)ix * C.dims[1] + iy) * C.dims[2] + iz;
+                    long long s = d.cell_start[cell], e = d.cell_start[cell + 1];
+                    for (long long b = s; b < e; b += 32) {
+                        long long p = b + lane;
+                        int j = p < e ? d.cell_atom[p] : -1;
+                        f(j);
+                    }
+                }
+    }
+};
+
+__device__ __forceinline__ void classify(const Dev& d, int g, V3 xi, double ri, int8_t mi, int j,
+                                         bool& is_nb, bool& is_bur, bool& coin, double& d2)
+{
+    is_nb = is_bur = coin = false;
+    d2 = 0;
+    if (j < 0 || j == g) return;
+    double4 aj = d.xyzr[j];
+    d2 = sq_seq(xi - v3(aj.x, aj.y, aj.z));
+    double rs = ri + aj.w;
+    double t = rs + 2.0 * d.st.rp;
+    double b2 = t * t;
+    if (d.mol[j] == mi) {
+        coin = d2 <= 0.0001;
+        is_nb = d2 < b2;
+    } else {
+        is_bur = d.atten[j] >= 5 && d2 < b2;
+    }
+}
+
+__global__ void __launch_bounds__(NB_WARPS * 32) k_nb_count(Dev d)
+{
+    const int lane = threadIdx.x & 31;
+    const long long wid = blockIdx.x * (long long)NB_WARPS + (threadIdx.x >> 5);
+    const long long nw = (long long)gridDim.x * NB_WARPS;
+    for (long long gg = wid; gg < d.N; gg += nw) {
+        const int g = (int)gg;
+        const int c = d.cplx[g];
+        double4 ai = d.xyzr[g];
+        const V3 xi = v3(ai.x, ai.y, ai.z);
+        const int8_t mi = d.mol[g];
+        int nn = 0, nb = 0;
+        NearScan::run(d, g, c, [&](int j) {
+            bool is_nb, is_bur, coin; double d2;
+            classify(d, g, xi, ai.w, mi, j, is_nb, is_bur, coin, d2);
+            nn += __popc(__ballot_sync(0xffffffffu, is_nb));
+            nb += __popc(__ballot_sync(0xffffffffu, is_bur));
+            if (coin) {
+                const int a0 = d.cx[c].a0;
+                unsigned long long key = ((unsigned long long)(g - a0) << 32) | (unsigned)(j - a0);
+                atomicMin(&d.coin[c], key);
+            }
+        });
+        if (lane == 0) {
+            d.nnb[g] = nn;
+            d.nbur[g] = nb;
+            d.access[g] = nn == 0 ? 1 : 0;
+        }
+    }
+}
+
+void launch_neighbor_count(const Dev& d, cudaStream_t s)
+{
+    k_nb_count<<<grid_for(d.N, NB_WARPS), NB_WARPS * 32, 0, s>>>(d);
+}
+
+__global__ void __launch_bounds__(NB_WARPS * 32) k_nb_emit(Dev d, int* __restrict__ tmp_id)
+{
+    __shared__ double sd2[NB_WARPS][NB_CAP];
+    __shared__ int sid[NB_WARPS][NB_CAP];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const long long wid = blockIdx.x * (long long)NB_WARPS + w;
+    const long long nw = (long long)gridDim.x * NB_WARPS;
+    for (long long gg = wid; gg < d.N; gg += nw) {
+        const int g = (int)gg;
+        const int c = d.cplx[g];
+        double4 ai = d.xyzr[g];
+        const V3 xi = v3(ai.x, ai.y, ai.z);
+        const int8_t mi = d.mol[g];
+        const int K = d.nnb[g];
+        const long long off = d.nb_off[g];
+        if (off + K > d.nb_cap || d.bu_off[g] + d.nbur[g] > d.bu_cap) {
+            if (lane == 0) atomicOr(&d.status[c], ST_OVERFLOW);
+            continue;
+        }
+        const bool in_sh = K <= NB_CAP;
+        // ---- neighbours: gather unsorted, then place each by its rank ----
+        int cnt = 0;
+        NearScan::run(d, g, c, [&](int j) {
+            bool is_nb, is_bur, coin; double d2;
+            classify(d, g, xi, ai.w, mi, j, is_nb, is_bur, coin, d2);
+            unsigned m = __ballot_sync(0xffffffffu, is_nb);
+            if (is_nb) {
+                int pos = cnt + __popc(m & lt);
+                if (pos < K) {
+                    if (in_sh) { sd2[w][pos] = d2; sid[w][pos] = j; }
+                    else { d.nb_d2[off + pos] = d2; tmp_id[off + pos] = j; }
+                }
+            }
+            cnt += __popc(m);
+        });
+        __syncwarp();
+        for (int e = lane; e < K; e += 32) {
+            double ke = in_sh ? sd2[w][e] : d.nb_d2[off + e];
+            int je = in_sh ? sid[w][e] : tmp_id[off + e];
+            int rank = 0;
+            for (int f = 0; f < K; ++f) {
+                double kf = in_sh ? sd2[w][f] : d.nb_d2[off + f];
+                int jf = in_sh ? sid[w][f] : tmp_id[off + f];
+                rank += (kf < ke || (kf == ke && jf < je)) ? 1 : 0;
+            }
+            d.nb_id[off + rank] = je;
+        }
+        __syncwarp();
+        // ---- buried partners: ascending atom index ----
+        const int KB = d.nbur[g];
+        const long long boff = d.bu_off[g];
+        const bool b_sh = KB <= NB_CAP;
+        cnt = 0;
+        NearScan::run(d, g, c, [&](int j) {
+            bool is_nb, is_bur, coin; double d2;
+            classify(d, g, xi, ai.w, mi, j, is_nb, is_bur, coin, d2);
+            unsigned m = __ballot_sync(0xffffffffu, is_bur);
+            if (is_bur) {
+                int pos = cnt + __popc(m & lt);
+                if (pos < KB) {
+                    if (b_sh) sid[w][pos] = j;
+                    else d.bu_id[boff + pos] = j;
+                }
+            }
+            cnt += __popc(m);
+        });
+        __syncwarp();
+        if (b_sh) {
+            for (int e = lane; e < KB; e += 32) {
+                int je = sid[w][e];
+                int rank = 0;
+                for (int f = 0; f < KB; ++f) rank += sid[w][f] < je ? 1 : 0;
+                d.bu_id[boff + rank] = je;
+            }
+        } else if (lane == 0) {
+            for (long long i = boff + 1; i < boff + KB; ++i) {
+                int v = d.bu_id[i];
+                long long k = i - 1;
+                while (k >= boff && d.bu_id[k] > v) { d.bu_id[k + 1] = d.bu_id[k]; --k; }
+                d.bu_id[k + 1] = v;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+void launch_neighbor_emit(const Dev& d, cudaStream_t s)
+{
+    k_nb_emit<<<grid_for(d.N, NB_WARPS), NB_WARPS * 32, 0, s>>>(d, d.nb_tmp);
+}
+
+// ---------------------------------------------------------------------------
+// pair geometry (second_loop, _core.py:1372-1416)
+// ---------------------------------------------------------------------------
+struct PairGeo {
+    V3 uij, tij;
+    double dij, rij;
+    bool between, ok;
+};
+
+__device__ __forceinline__ PairGeo pair_geo(V3 xi, double ri, V3 xj, double rj, double rp)
+{
+    PairGeo p;
+    V3 diff = xj - xi;
+    double dij_sq = sq_alt(diff);
+    p.dij = sqrt(dij_sq);
+    double eri = ri + rp, erj = rj + rp;
+    double asymm = (eri * eri - erj * erj) / p.dij;
+    p.between = fabs(asymm) < p.dij;
+    p.uij = diff / p.dij;
+    p.tij = ((xi + xj) * 0.5) + p.uij * (asymm * 0.5);
+    double far_sq = (eri + erj) * (eri + erj) - dij_sq;
+    double rd = ri - rj;
+    double cont_sq = dij_sq - rd * rd;
+    p.ok = far_sq > 0.0 && cont_sq > 0.0;
+    p.rij = ((0.5 * sqrt(far_sq)) * sqrt(cont_sq)) / p.dij;
+    return p;
+}
+
+// ---------------------------------------------------------------------------
+// pair loop: single-neighbour shortcut, toroid queue
+// ---------------------------------------------------------------------------
+template <bool EMIT>
+__global__ void k_pairs(Dev d)
+{
+    const double rp = d.st.rp;
+    for (long long gg = blockIdx.x * (long long)blockDim.x + threadIdx.x; gg < d.N; gg += (long long)gridDim.x * blockDim.x) {
+        const int g = (int)gg;
+        const int K = d.nnb[g];
+        int ntor = 0;
+        if (K > 0) {
+            double4 ai = d.xyzr[g];
+            const V3 xi = v3(ai.x, ai.y, ai.z);
+            const long long off = d.nb_off[g];
+            const int8_t ati = d.atten[g];
+            if (K <= 1) {
+                // shortcut: a single forward, well-formed neighbour marks both atoms
+                // accessible and the atom contributes no pairs (_core.py:1393-1400)
+                int j = d.nb_id[off];
+                if (!EMIT && j > g) {
+                    double4 aj = d.xyzr[j];
+                    PairGeo p = pair_geo(xi, ai.w, v3(aj.x, aj.y, aj.z), aj.w, rp);
+                    if (p.ok) { d.access[g] = 1; d.access[j] = 1; }
+                }
+            } else {
+                const long long base = EMIT ? d.tor_off[g] : 0;
+                for (int k = 0; k < K; ++k) {
+                    int j = d.nb_id[off + k];
+                    if (j <= g) continue;
+                    double4 aj = d.xyzr[j];
+                    PairGeo p = pair_geo(xi, ai.w, v3(aj.x, aj.y, aj.z), aj.w, rp);
+                    if (!p.ok) continue;
+                    bool need = ati > 1 || (d.atten[j] > 1 && rp > 0.0);
+                    if (need) {
+                        if (EMIT && base + ntor < d.tor_cap) { d.tor_i[base + ntor] = g; d.tor_j[base + ntor] = j; }
+                        ++ntor;
+                    }
+                }
+            }
+        }
+        if (!EMIT) d.ntor[g] = ntor;
+    }
+}
+
+void launch_pairs(const Dev& d, bool emit, cudaStream_t s)
+{
+    if (emit) k_pairs<true><<<grid_for(d.N, 128), 128, 0, s>>>(d);
+    else k_pairs<false><<<grid_for(d.N, 128), 128, 0, s>>>(d);
+}
+
+// ---------------------------------------------------------------------------
+// triple loop: probe placement over (i, j, k) with j, k neighbours of i,
+// natom_k > natom_j; probes ordered as all "+" then all "-" per complex
+// ---------------------------------------------------------------------------
+struct Triple {
+    bool valid, degenerate, kills;
+    V3 xk; double rk; int k;
+    V3 uik; double dik, swijk;
+};
+
+__device__ __forceinline__ Triple triple_test(const Dev& d, int g, V3 xi, double eri, int j, V3 xj, double erj,
+                                              const PairGeo& p, int8_t ati, int8_t atj, int kslot, long long off,
+                                              int K)
+{
+    Triple t;
+    t.valid = false; t.degenerate = false; t.kills = false;
+    if (kslot >= K) return t;
+    const double rp = d.st.rp;
+    int k = d.nb_id[off + kslot];
+    t.k = k;
+    if (k <= j) return t;
+    double4 ak = d.xyzr[k];
+    t.xk = v3(ak.x, ak.y, ak.z);
+    t.rk = ak.w;
+    double erk = ak.w + rp;
+    double djk = norm3(t.xk - xj);
+    if (!(djk < erj + erk)) return t;
+    t.dik = norm3(t.xk - xi);
+    if (!(t.dik < eri + erk)) return t;
+    if (ati <= 1 && atj <= 1 && d.atten[k] <= 1) return t;
+    t.valid = true;
+    t.uik = (t.xk - xi) / t.dik;
+    double dt = dot_alt(p.uij, t.uik);
+    double wijk = acos(dt < -1.0 ? -1.0 : (dt > 1.0 ? 1.0 : dt));   // np.clip keeps NaN
+    t.swijk = sin(wijk);
+    t.degenerate = (dt >= 1.0) || (dt <= -1.0) || (wijk <= 0.0) || (t.swijk <= 0.0);
+    if (t.degenerate) {
+        double dtijk2 = sq_seq(p.tij - t.xk);
+        double rkp2 = erk * erk - p.rij * p.rij;
+        t.kills = dtijk2 < rkp2;
+    }
+    return t;
+}
+
+// probe collision against atom1's neighbours except atom2 and atom3 (alt, <=)
+__device__ __forceinline__ bool probe_collides(const Dev& d, V3 pt, long long off, int K, int j, int k, double rp)
+{
+    for (int s = 0; s < K; ++s) {
+        int n = d.nb_id[off + s];
+        if (n == j || n == k) continue;
+        double4 an = d.xyzr[n];
+        double t = an.w + rp;
+        if (sq_alt(pt - v3(an.x, an.y, an.z)) <= t * t) return true;
+    }
+    return false;
+}
+
+static constexpr int TR_WARPS = 4;
+
+template <bool EMIT>
+__global__ void __launch_bounds__(TR_WARPS * 32) k_triples(Dev d)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const long long wid = blockIdx.x * (long long)TR_WARPS + (threadIdx.x >> 5);
+    const long long nw = (long long)gridDim.x * TR_WARPS;
+    const double rp = d.st.rp;
+    for (long long gg = wid; gg < d.N; gg += nw) {
+        const int g = (int)gg;
+        const int K = d.nnb[g];
+        int nplus = 0, nminus = 0;
+        if (K > 1) {
+            double4 ai = d.xyzr[g];
+            const V3 xi = v3(ai.x, ai.y, ai.z);
+            const double eri = ai.w + rp;
+            const long long off = d.nb_off[g];
+            const int8_t ati = d.atten[g];
+            long long pbase = 0, mbase = 0;
+            if (EMIT) {
+                // probe layout per complex: [+mol0 | -mol0 | +mol1 | -mol1]
+                const int c = d.cplx[g];
+                const Cplx C = d.cx[c];
+                const int s0 = C.a0, s1 = C.a0 + C.n0, e1 = C.a0 + C.n;
+                const int ms = d.mol[g] == 0 ? s0 : s1, me = d.mol[g] == 0 ? s1 : e1;
+                long long cbase = d.plus_off[s0] + d.minus_off[s0];
+                long long m0 = (d.plus_off[s1] - d.plus_off[s0]) + (d.minus_off[s1] - d.minus_off[s0]);
+                long long mb = cbase + (d.mol[g] == 0 ? 0 : m0);
+                pbase = mb + (d.plus_off[g] - d.plus_off[ms]);
+                mbase = mb + (d.plus_off[me] - d.plus_off[ms]) + (d.minus_off[g] - d.minus_off[ms]);
+            }
+            for (int ps = 0; ps < K; ++ps) {
+                const int j = d.nb_id[off + ps];
+                if (j <= g) continue;
+                double4 aj = d.xyzr[j];
+                const V3 xj = v3(aj.x, aj.y, aj.z);
+                const PairGeo p = pair_geo(xi, ai.w, xj, aj.w, rp);
+                if (!p.ok) continue;
+                const double erj = aj.w + rp;
+                const int8_t atj = d.atten[j];
+                // pass 1: does a degenerate triple kill the whole pair?
+                bool kill = false;
+                for (int kb = 0; kb < K; kb += 32) {
+                    Triple t = triple_test(d, g, xi, eri, j, xj, erj, p, ati, atj, kb + lane, off, K);
+                    kill |= __any_sync(0xffffffffu, t.valid && t.kills);
+                }
+                if (kill) continue;
+                // pass 2: probes
+                for (int kb = 0; kb < K; kb += 32) {
+                    Triple t = triple_test(d, g, xi, eri, j, xj, erj, p, ati, atj, kb + lane, off, K);
+                    bool okp = false, okm = false;
+                    V3 pp, pm, up; double h = 0;
+                    if (t.valid && !t.degenerate) {
+                        const double erk = t.rk + rp;
+                        V3 uijk = cross3(p.uij, t.uik) / t.swijk;
+                        V3 utb = cross3(uijk, p.uij);
+                        double asymm = (eri * eri - erk * erk) / t.dik;
+                        V3 tik = (xi + t.xk) * 0.5 + t.uik * (asymm * 0.5);
+                        double dtb = dot_alt(t.uik, tik - p.tij);
+                        V3 bijk = p.tij + utb * (dtb / t.swijk);
+                        V3 bma = bijk - xi;
+                        double h2 = eri * eri - dot_alt(bma, bma);
+                        if (h2 > 0.0) {
+                            h = sqrt(h2);
+                            up = uijk;
+                            pp = bijk + uijk * (h * 1.0);
+                            pm = bijk + uijk * (h * -1.0);
+                            okp = !probe_collides(d, pp, off, K, j, t.k, rp);
+                            okm = !probe_collides(d, pm, off, K, j, t.k, rp);
+                        }
+                    }
+                    unsigned bp = __ballot_sync(0xffffffffu, okp);
+                    unsigned bm = __ballot_sync(0xffffffffu, okm);
+                    if (EMIT) {
+                        if (okp) {
+                            long long q = pbase + nplus + __popc(bp & lt);
+                            if (q < d.probe_cap) {
+                                d.pa0[q] = g; d.pa1[q] = j; d.pa2[q] = t.k;
+                                d.ph[q] = h; st3(d.pxyz + 3 * q, pp); st3(d.palt + 3 * q, up * 1.0);
+                            }
+                        }
+                        if (okm) {
+                            long long q = mbase + nminus + __popc(bm & lt);
+                            if (q < d.probe_cap) {
+                                d.pa0[q] = j; d.pa1[q] = g; d.pa2[q] = t.k;
+                                d.ph[q] = h; st3(d.pxyz + 3 * q, pm); st3(d.palt + 3 * q, up * -1.0);
+                            }
+                        }
+                        if (okp || okm) { d.access[g] = 1; d.access[j] = 1; d.access[t.k] = 1; }
+                    }
+                    nplus += __popc(bp);
+                    nminus += __popc(bm);
+                }
+            }
+        }
+        if (!EMIT && lane == 0) { d.nplus[g] = nplus; d.nminus[g] = nminus; }
+    }
+}
+
+void launch_triples(const Dev& d, bool emit, cudaStream_t s)
+{
+    if (emit) k_triples<true><<<grid_for(d.N, TR_WARPS), TR_WARPS * 32, 0, s>>>(d);
+    else k_triples<false><<<grid_for(d.N, TR_WARPS), TR_WARPS * 32, 0, s>>>(d);
+}
+
+// ---------------------------------------------------------------------------
+// low probes (height < rp): flag, scan, compact -- per complex contiguous
+// ---------------------------------------------------------------------------
+__global__ void k_low_flag(Dev d, long long cap)
+{
+    const long long P = d.plus_off[d.N] + d.minus_off[d.N];
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < cap; p += (long long)gridDim.x * blockDim.x)
+        d.plow_flag[p] = (p < P && d.ph[p] < d.st.rp) ? 1 : 0;
+}
+
+__global__ void k_low_fill(Dev d, long long cap)
+{
+    const long long P = d.plus_off[d.N] + d.minus_off[d.N];
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < cap && p < P; p += (long long)gridDim.x * blockDim.x)
+        if (d.plow_flag[p]) d.plow_list[d.plow_off[p]] = (int)p;
+}
+
+void launch_low_probes(const Dev& d, long long probe_cap, long long* scan_tmp, cudaStream_t s)
+{
+    k_low_flag<<<grid_for(probe_cap, 256), 256, 0, s>>>(d, probe_cap);
+    scan_counts(d.plow_flag, d.plow_off, probe_cap, scan_tmp, s);
+    k_low_fill<<<grid_for(probe_cap, 256), 256, 0, s>>>(d, probe_cap);
+}
+
+}  // namespace cms

@@ -1,0 +1,157 @@
+/*
+ * cms_b200.h -- C ABI of the B200 contact-molecular-surface library
+ * (libcms_b200.so).
+ *
+ * The reference package (ullahsamee/cms-cuda) has no native interface: its
+ * hot path is the Python class MolecularSurfaceCalculator
+ * (cms-cuda/_core.py:762-1147, GPU twin cms-cuda/_gpu.py:310-686).  Each entry
+ * point below replaces one method or step of that class; the citation in its
+ * comment names it.  A Python binding (ctypes) of exactly these symbols is the
+ * package `cms_cuda` next to the CUDA sources.
+ *
+ * Conventions
+ *  - Every function returns cms_status (0 = success).  On failure
+ *    cms_last_error() returns a message; no C++ exception crosses the ABI.
+ *  - A batch holds B independent complexes.  Complex c owns atoms
+ *    [atom_off[c], atom_off[c+1]) of the concatenated arrays, binder
+ *    (molecule 0) first: n_binder[c] atoms, then the target (molecule 1).
+ *    This is the reference's natom numbering (_core.py:918-943) per complex.
+ *  - `where` arguments say whether pointers are host (CMS_HOST) or device
+ *    (CMS_DEVICE) memory; host buffers are copied on the context's stream.
+ *  - A context is bound to one device and one CUDA stream and is not
+ *    thread-safe (one context per host thread, as the reference keeps one
+ *    stream per thread, _gpu.py:70-83).
+ */
+#ifndef CMS_B200_H
+#define CMS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cms_ctx cms_ctx;
+typedef int32_t cms_status;
+
+enum {
+    CMS_OK = 0,
+    CMS_ERR_ARG = -1,          /* invalid argument (ValueError in Python) */
+    CMS_ERR_CUDA = -2,         /* CUDA runtime error */
+    CMS_ERR_STATE = -3,        /* call order (RuntimeError: cache / mode mismatch) */
+    CMS_ERR_COINCIDENT = -4,   /* coincident atoms (RuntimeError, _core.py:1286-1293) */
+    CMS_ERR_EMPTY = -5,        /* complex without atoms (AssertionError, _core.py:895) */
+    CMS_ERR_CAPACITY = -6      /* a fixed capacity was exceeded in graph mode */
+};
+
+enum { CMS_HOST = 0, CMS_DEVICE = 1 };
+
+/* Settings of the calculator; defaults of _core.py:766-773. */
+typedef struct {
+    double rp;             /* probe radius, 1.7 */
+    double density;        /* dots per A^2, 15.0 */
+    double band;           /* SC peripheral band, 1.5 */
+    double sep;            /* attention separation, 8.0 */
+    double weight;         /* CMS distance weight, 0.5 */
+    double binwidth_dist;  /* SC distance median bin, 0.02 */
+    double binwidth_norm;  /* SC normal median bin, 0.02 */
+} cms_settings;
+
+/* Per-complex sizes after surface generation (for export buffers). */
+typedef struct {
+    int64_t n_atoms, n_binder;
+    int64_t nb_entries, bu_entries;       /* neighbour / buried-partner list entries */
+    int64_t max_nb, max_bu;               /* longest row (>= 1), padded width of the reference */
+    int64_t n_toroid;                     /* toroid queue length */
+    int64_t n_probes;
+    int64_t n_probes_plus[2], n_probes_minus[2];
+    int64_t n_dots[2];                    /* dots per molecule */
+    int64_t n_trimmed[2];                 /* SC trimmed dots per molecule (after cms_shape_complementarity) */
+    int64_t convex, toroidal, concave;    /* results.dots counters */
+    int32_t status;                       /* per-complex status bits */
+    int32_t coincident_i, coincident_j;   /* first coincident pair (local indices) or -1 */
+    double radmax;
+} cms_complex_info;
+
+/* Create a context on `device` using CUDA stream `stream` (NULL: a new
+ * non-blocking stream owned by the context).  Replaces the calculator
+ * constructor (_core.py:762-775, _gpu.py:312-330). */
+cms_status cms_ctx_create(cms_ctx** out, int device, void* stream);
+cms_status cms_ctx_destroy(cms_ctx* ctx);
+
+/* Calculator settings (the `settings` object, _core.py:766-773). */
+cms_status cms_set_settings(cms_ctx* ctx, const cms_settings* s);
+cms_status cms_get_settings(cms_ctx* ctx, cms_settings* s);
+
+/* Load B complexes: atom_off[B+1], n_binder[B] (host int64 arrays), xyz
+ * (N x 3, row-major f64), radius (N f64) and optional per-atom density
+ * (NULL: settings.density).  Replaces reset + add_binder_and_target /
+ * AddMolecule (_core.py:918-943). */
+cms_status cms_load_batch(cms_ctx* ctx, int32_t B, const int64_t* atom_off, const int64_t* n_binder,
+                          const double* xyz, const double* radius, const double* density, int32_t where);
+
+/* Generate the molecular surfaces of every loaded complex: attention numbers,
+ * neighbour lists, pair/triple loops and convex, toroidal and concave dots.
+ * all_atoms = 1 is the single-molecule mode of maximum possible CMS.
+ * Replaces _ensure_surfaces_generated (_core.py:865-909). */
+cms_status cms_generate_surfaces(cms_ctx* ctx, int32_t all_atoms);
+
+/* Contact molecular surface of both sides of every complex.
+ * per_atom (N): for a target atom, its target-side CMS; for a binder atom,
+ * its binder-side CMS.  totals (2B): totals[2c+1] target side,
+ * totals[2c] binder side.  Replaces calc_contact_molecular_surface
+ * (_core.py:946-1004) for target_side True and False. */
+cms_status cms_contact_ms(cms_ctx* ctx, double* per_atom, double* totals, int32_t where);
+
+/* Maximum possible CMS (per-atom dot area of molecule 0, surface generated
+ * with all_atoms = 1).  per_atom (N; molecule-0 atoms), totals (B).
+ * Replaces calc_max_possible_contact_molecular_surface (_core.py:1007-1034). */
+cms_status cms_max_contact_ms(cms_ctx* ctx, double* per_atom, double* totals, int32_t where);
+
+/* Shape complementarity.  sc (B x 5): sc, interface area, median distance,
+ * mean distance, mean normal score (surface 2).  sides (B x 2 x 7):
+ * d_mean, d_median, s_mean, s_median, trimmedArea, nTrimmedDots, nAllDots of
+ * each molecule.  Replaces CalcLoadedSC (_core.py:807-863) with
+ * trim_peripheral_band_vectorized, calc_neighbor_distance_vectorized and
+ * _binned_median (_core.py:1037-1147). */
+cms_status cms_shape_complementarity(cms_ctx* ctx, double* sc, double* sides, int32_t where);
+
+/* Sizes and status of complex c (valid after cms_generate_surfaces). */
+cms_status cms_complex_info_get(cms_ctx* ctx, int32_t c, cms_complex_info* info);
+
+/* Host copies of complex c's state, the arrays the reference keeps in
+ * calc.run (_core.py:777-789); atom indices are local to the complex. */
+cms_status cms_export_atoms(cms_ctx* ctx, int32_t c, int8_t* atten, int8_t* access, int32_t* n_neighbors,
+                            int32_t* n_buried);
+cms_status cms_export_neighbors(cms_ctx* ctx, int32_t c, int64_t* nb_off, int32_t* nb_id, int64_t* bu_off,
+                                int32_t* bu_id);
+cms_status cms_export_toroid(cms_ctx* ctx, int32_t c, int32_t* atom1, int32_t* atom2, double* uij, double* tij,
+                             double* rij, int8_t* between);
+cms_status cms_export_probes(cms_ctx* ctx, int32_t c, int32_t* a0, int32_t* a1, int32_t* a2, double* height,
+                             double* point, double* alt);
+cms_status cms_export_dots(cms_ctx* ctx, int32_t c, int32_t molecule, double* coor, double* outnml, double* area,
+                           int8_t* buried, int8_t* type, int32_t* atom_idx);
+/* local dot indices (within the molecule's dot array) of the SC trimmed dots */
+cms_status cms_export_trimmed(cms_ctx* ctx, int32_t c, int32_t molecule, int32_t* dot_index);
+
+/* Capture the whole pipeline (surfaces + CMS + SC) of the loaded batch shape
+ * in a CUDA graph with the current capacities (run it once first), then
+ * replay it; later cms_load_batch calls with the same B, N and offsets reuse
+ * it.  Falls back to the stage-synchronised path on capacity overflow. */
+cms_status cms_run_graph(cms_ctx* ctx);
+
+/* Number of kernels the last pipeline run launched. */
+int64_t cms_kernel_launches(cms_ctx* ctx);
+
+const char* cms_last_error(cms_ctx* ctx);
+const char* cms_version(void);
+
+/* Number of visible CUDA devices (0 when none or no driver); replaces the
+ * reference's gpu_available() probe (cms-cuda/_api.py:15-22). */
+int32_t cms_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CMS_B200_H */
