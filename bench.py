@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""
+Benchmark: batched CMS + SC throughput (complexes/s) on B200.
+
+Workload: 4096 synthetic complexes of uneven size (target log-uniform
+600-4000 heavy atoms, binder log-uniform 80-1200, ~5 % ligand-like 20-60 atom
+binders), seeded; each step runs the whole pipeline on the whole batch --
+attention, neighbour lists, pairs/triples, convex/toroidal/concave dots with
+burial, CMS of both sides and shape complementarity -- as one replay of a
+captured CUDA graph.  Inputs (9 M atoms, ~290 MB of coordinates) are larger
+than L2, so no explicit flush is needed between steps.
+
+  value     device time of K graph replays with inputs resident (CUDA events on
+            the pipeline's stream), max over ranks, all ranks' complexes
+  e2e       the public batch API from pinned host buffers: upload, pipeline,
+            per-complex results back to the host, every step
+  plain_gpu one complex per call through the drop-in calculator (the reference's
+            usage pattern) on the same GPU, for the batched-vs-plain ratio
+  cpu_baseline  the CPU oracle (NumPy restatement of the reference) on a
+            bounded sample, one core
+  roofline  the dominant pipeline stage against its bound
+
+--impl reference times the reference's CPU algorithm (the oracle port: the
+reference itself is a Python package that cannot be installed on the GPU
+box) on all host cores, on bounded samples of the same workload.
+
+Multi-GPU (torchrun): weak scaling, each rank evaluates its own batch of
+independent complexes; the only collective is the max of the step time.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "cms-cuda_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np
+
+METRIC = "complexes/s CMS+SC(+grad), batched vs plain GPU path, dot counts bit-exact"
+UNIT = "complexes/s"
+WORKLOAD = ("batched 4096 complexes: target log-uniform 600-4000, binder log-uniform 80-1200 heavy atoms, "
+            "~5% ligand binders of 20-60 atoms; surfaces + CMS (both sides) + SC per complex")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--cpu-sample", type=int, default=2)
+    ap.add_argument("--plain-sample", type=int, default=32)
+    ap.add_argument("--no-extras", action="store_true", help="skip plain / CPU baselines (profiling runs)")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.file.read().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.file.name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (the oracle is the checker / baseline, never the product)
+# ---------------------------------------------------------------------------
+def _oracle_one(args):
+    bx, br, tx, tr = args
+    from oracle import cms_oracle
+    t = time.perf_counter()
+    out = cms_oracle.run_complex(bx, br, tx, tr, sc=True)
+    return time.perf_counter() - t, out["cms"]
+
+
+def sample_indices(batch, k, seed):
+    """k complexes spread over the batch's size distribution (deterministic)."""
+    sizes = np.diff(batch.atom_off)
+    order = np.argsort(sizes, kind="stable")
+    pos = np.linspace(0.2, 0.8, k) if k > 1 else np.array([0.5])
+    return [int(order[int(p * (len(order) - 1))]) for p in pos]
+
+
+def cpu_baseline_single(batch, k):
+    idx = sample_indices(batch, k, 0)
+    tot = 0.0
+    for c in idx:
+        dt, _ = _oracle_one(batch.complex(c))
+        tot += dt
+    atoms = int(np.mean([batch.atom_off[c + 1] - batch.atom_off[c] for c in idx]))
+    return {"value": len(idx) / tot, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{len(idx)} complexes of the batch (sizes at the 20-80th percentile, mean {atoms} atoms), "
+                      f"CMS both sides + SC, one process, {tot:.1f} s"}
+
+
+def run_reference(args):
+    """The reference's CPU algorithm on all host cores, bounded samples of the workload."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    from cms_cuda import synth
+    batch = synth.config_batched(args.batch, args.seed)
+    cores = os.cpu_count() or 1
+    # per step: one complex per core, rotating through a fixed sample of mid-sized complexes
+    pool_idx = sample_indices(batch, max(cores, 8), 0)
+    ctx = mp.get_context("spawn")
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    with ctx.Pool(cores) as pool:
+        def step(s):
+            sel = [pool_idx[(s * cores + i) % len(pool_idx)] for i in range(cores)]
+            t = time.perf_counter()
+            pool.map(_oracle_one, [batch.complex(c) for c in sel])
+            return len(sel), time.perf_counter() - t
+        for s in range(args.warmup):
+            step(s)
+        n, secs = 0, 0.0
+        for s in range(args.steps):
+            a, b = step(args.warmup + s)
+            n += a
+            secs += b
+    value = n / secs
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD, "sample_per_step": f"{cores} complexes, one per core"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{cores} mid-sized complexes of the batch per step, CMS both sides + SC"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------
+def stage_roofline(stages, work, peaks, fp32_peak):
+    """Roofline of the most expensive stage: FP32 nearest-dot search (8 FLOP per pair) or HBM bytes."""
+    nn = {"cms_nn": work["cms_pairs"], "sc_band_nn": work["band_pairs"], "sc_argmin_nn": work["sc_pairs"]}
+    name = max(stages, key=lambda k: stages[k])
+    ms = stages[name]
+    if name in nn:
+        achieved = 8.0 * nn[name] / (ms * 1e-3) / 1e12
+        return {"bound": "fp32", "kernel": f"k_nn ({name})", "achieved": achieved, "peak": fp32_peak,
+                "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                "traffic": None, "ms": ms,
+                "peak_source": "measured FP32 FMA throughput of this GPU (cms_fp32_peak, in this run)"}
+    return {"bound": "hbm", "kernel": name, "achieved": None, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+            "frac": None, "traffic": None, "ms": ms}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from cms_cuda import _lib, synth, MolecularSurfaceCalculator
+
+    batch = synth.config_batched(args.batch, args.seed + 1000 * rank)
+    B, N = batch.B, batch.N
+    # pinned host inputs for the end-to-end path
+    xyz_h = torch.from_numpy(batch.xyz).pin_memory()
+    rad_h = torch.from_numpy(batch.radius).pin_memory()
+    xyz_np, rad_np = xyz_h.numpy(), rad_h.numpy()
+
+    stream = torch.cuda.Stream(device=dev)
+    ctx = _lib.Context(local, stream=stream.cuda_stream)
+    ctx.load_batch(batch.atom_off, batch.n_binder, xyz_np, rad_np)
+    ctx.run_graph()                                  # sizes the workspace, captures, replays once
+    statuses = [ctx.info(c).status for c in range(B)]
+    work = ctx.nn_work()
+    launches = ctx.kernel_launches()
+
+    # ---- device throughput: graph replays with inputs resident -------------
+    for _ in range(args.warmup):
+        ctx.graph_launch()
+    stream.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clk = ClockSampler(local)
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx.graph_launch()
+    e1.record(stream)
+    e1.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    ctx.graph_check()
+    torch.cuda.synchronize(dev)
+    t = torch.tensor([ms], device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    ms_max = float(t.item())
+    value = world * B / (ms_max * 1e-3)
+    _, totals = ctx.contact_ms(per_atom=False)
+    sc, _ = ctx.shape_complementarity()
+
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        stages = ctx.profile_stages()
+        fp32 = ctx.fp32_peak()
+        peaks = {}
+        pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        if os.path.exists(pk):
+            peaks = json.load(open(pk))
+        extras["roofline"] = stage_roofline(stages, work, peaks, fp32)
+        extras["stages_ms"] = {k: round(v, 3) for k, v in stages.items()}
+        extras["nn_work"] = work
+    del ctx
+    torch.cuda.synchronize(dev)
+
+    # ---- end to end through the public batch API ---------------------------
+    from cms_cuda.batch import BatchCalculator
+    bc = BatchCalculator(local)
+    bc.load(batch.atom_off, batch.n_binder, xyz_np, rad_np)
+    r = bc.run(graph=True)
+    for _ in range(args.warmup):
+        bc.load(batch.atom_off, batch.n_binder, xyz_np, rad_np)
+        r = bc.run(graph=True)
+    h0, d0 = bc.ctx.transfer_bytes()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        bc.load(batch.atom_off, batch.n_binder, xyz_np, rad_np)
+        r = bc.run(graph=True)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    h1, d1 = bc.ctx.transfer_bytes()
+    same = bool(np.array_equal(r.cms, totals[:, 1]) and np.array_equal(r.sc, sc[:, 0]))
+    del bc
+    e2e_t = torch.tensor([e2e_s], device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e = {"value": world * B / float(e2e_t.item()), "unit": UNIT,
+           "h2d_bytes_per_step": (h1 - h0) // args.steps, "d2h_bytes_per_step": (d1 - d0) // args.steps,
+           "results_match_device_run": same}
+
+    if rank == 0 and world == 1 and not args.no_extras:
+        # plain GPU path: one complex per call through the drop-in calculator
+        idx = list(range(min(args.plain_sample, B)))
+        for c in idx[:2]:
+            m = MolecularSurfaceCalculator(local)
+            m.add_binder_and_target(*batch.complex(c))
+            m.CalcLoaded(); m.CalcLoadedSC()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        plain_match = True
+        for c in idx:
+            m = MolecularSurfaceCalculator(local)
+            m.add_binder_and_target(*batch.complex(c))
+            cms, _ = m.CalcLoaded()
+            s = m.CalcLoadedSC()
+            plain_match &= (cms == totals[c, 1]) and (s[0] == sc[c, 0])
+        plain = len(idx) / (time.perf_counter() - t0)
+        extras["plain_gpu"] = {"value": plain, "unit": UNIT, "sample": f"first {len(idx)} complexes, one per call",
+                               "results_match_batched": bool(plain_match)}
+        extras["batched_vs_plain"] = value / plain
+        extras["cpu_baseline"] = cpu_baseline_single(batch, args.cpu_sample)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, complexes of random residues)",
+                "config": {"workload": WORKLOAD, "complexes_per_gpu": B, "atoms_per_gpu": N,
+                           "parallelism": f"replicas x{world} (independent complexes per GPU)",
+                           "l2": "inputs larger than L2 (9M atoms), no flush",
+                           "nn_search": "FP32 filter + FP64 recheck, brute force",
+                           "grad": "not included"},
+                "e2e": e2e, "gpu_launches": launches * args.steps, "clocks": clocks,
+                "complex_status_nonzero": int(sum(1 for s in statuses if s))}
+        line.update(extras)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

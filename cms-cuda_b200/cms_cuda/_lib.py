@@ -26,7 +26,8 @@ EXPORTED = (
     "cms_generate_surfaces", "cms_contact_ms", "cms_max_contact_ms", "cms_shape_complementarity",
     "cms_complex_info_get", "cms_export_atoms", "cms_export_neighbors", "cms_export_toroid",
     "cms_export_probes", "cms_export_dots", "cms_export_trimmed", "cms_run_graph", "cms_kernel_launches",
-    "cms_last_error", "cms_version", "cms_device_count",
+    "cms_last_error", "cms_version", "cms_device_count", "cms_profile_stages", "cms_stage_name",
+    "cms_graph_launch", "cms_graph_check", "cms_nn_work", "cms_transfer_bytes", "cms_fp32_peak",
 )
 
 
@@ -94,6 +95,11 @@ def load():
             "cms_export_dots": [_VP, _I32, _I32, _VP, _VP, _VP, _VP, _VP, _VP],
             "cms_export_trimmed": [_VP, _I32, _I32, _VP],
             "cms_run_graph": [_VP],
+            "cms_graph_launch": [_VP],
+            "cms_graph_check": [_VP],
+            "cms_nn_work": [_VP, _PI64],
+            "cms_transfer_bytes": [_VP, _PI64, _PI64],
+            "cms_fp32_peak": [_VP, ctypes.POINTER(ctypes.c_double)],
         }
         for name, args in sig.items():
             f = getattr(lib, name)
@@ -107,6 +113,10 @@ def load():
         lib.cms_version.restype = ctypes.c_char_p
         lib.cms_device_count.argtypes = []
         lib.cms_device_count.restype = ctypes.c_int32
+        lib.cms_profile_stages.argtypes = [_VP, _VP, _I32, ctypes.POINTER(_I32)]
+        lib.cms_profile_stages.restype = ctypes.c_int32
+        lib.cms_stage_name.argtypes = [_I32]
+        lib.cms_stage_name.restype = ctypes.c_char_p
         _lib = lib
         return lib
 
@@ -181,11 +191,41 @@ class Context:
     def run_graph(self):
         self._check(self.lib.cms_run_graph(self.h))
 
+    def graph_launch(self):
+        """Replay the captured pipeline asynchronously on the context's stream."""
+        self._check(self.lib.cms_graph_launch(self.h))
+
+    def graph_check(self):
+        self._check(self.lib.cms_graph_check(self.h))
+
+    def nn_work(self):
+        w = np.zeros(6, dtype=np.int64)
+        self._check(self.lib.cms_nn_work(self.h, w.ctypes.data_as(_PI64)))
+        return dict(cms_pairs=int(w[0]), cms_queries=int(w[1]), band_pairs=int(w[2]), band_queries=int(w[3]),
+                    sc_pairs=int(w[4]), sc_queries=int(w[5]))
+
     def kernel_launches(self):
         return int(self.lib.cms_kernel_launches(self.h))
 
-    def contact_ms(self):
-        per_atom = np.empty(self.N, dtype=np.float64)
+    def profile_stages(self):
+        """{stage name: milliseconds} of one pipeline run with an event after every stage."""
+        ms = np.zeros(64)
+        n = ctypes.c_int32(0)
+        self._check(self.lib.cms_profile_stages(self.h, _ptr(ms), 64, ctypes.byref(n)))
+        return {self.lib.cms_stage_name(i).decode(): float(ms[i]) for i in range(n.value)}
+
+    def fp32_peak(self):
+        v = ctypes.c_double(0)
+        self._check(self.lib.cms_fp32_peak(self.h, ctypes.byref(v)))
+        return v.value
+
+    def transfer_bytes(self):
+        a, b = ctypes.c_int64(0), ctypes.c_int64(0)
+        self._check(self.lib.cms_transfer_bytes(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def contact_ms(self, per_atom=True):
+        per_atom = np.empty(self.N, dtype=np.float64) if per_atom else None
         totals = np.empty(2 * self.B, dtype=np.float64)
         self._check(self.lib.cms_contact_ms(self.h, _ptr(per_atom), _ptr(totals), CMS_HOST))
         return per_atom, totals.reshape(self.B, 2)

@@ -1,0 +1,87 @@
+"""
+Batched evaluation of many independent complexes in one pass of the CUDA
+pipeline (one set of launches for the whole batch, captured once in a CUDA
+graph and replayed).
+
+The reference evaluates one complex per calculator (cms-cuda/_api.py:41-133,
+and the CLI's serial loop examples/calculate_cms_sc.py:130-212); this module
+is the batched form of the same readouts: per complex the target- and
+binder-side CMS (with per-atom arrays) and the SC triple.
+"""
+
+import numpy as np
+
+from . import _lib
+
+
+class BatchResult:
+    """Per-complex outputs of one batched run."""
+
+    def __init__(self, totals, sc, sides, per_atom=None):
+        self.cms = totals[:, 1].copy()              # target side (calculate_contact_ms)
+        self.cms_binder = totals[:, 0].copy()
+        self.sc = sc[:, 0].copy()
+        self.sc_area = sc[:, 1].copy()
+        self.sc_distance = sc[:, 2].copy()
+        self.sides = sides
+        self.per_atom = per_atom
+
+
+class BatchCalculator:
+    """
+    Holds one device context and the workspace of a batch shape.  load() the
+    concatenated batch (binder atoms then target atoms per complex), then
+    run().  Re-loading a batch of the same shape replays the captured graph.
+    """
+
+    def __init__(self, device=0, settings=None):
+        self.ctx = _lib.Context(device)
+        if settings is not None:
+            self.ctx.set_settings(settings)
+        self._settings = settings
+
+    def set_settings(self, settings):
+        self.ctx.set_settings(settings)
+        self._settings = settings
+
+    def load(self, atom_off, n_binder, xyz, radius, density=None):
+        self.ctx.load_batch(atom_off, n_binder, xyz, radius, density)
+
+    def run(self, graph=True, per_atom=False):
+        """Surfaces + CMS (both sides) + SC of every loaded complex."""
+        if graph:
+            self.ctx.run_graph()
+        else:
+            self.ctx.generate(all_atoms=False)
+        pa, totals = self.ctx.contact_ms(per_atom=per_atom)
+        sc, sides = self.ctx.shape_complementarity()
+        return BatchResult(totals, sc, sides, pa if per_atom else None)
+
+    def statuses(self):
+        return np.array([self.ctx.info(c).status for c in range(self.ctx.B)], dtype=np.int32)
+
+    def kernel_launches(self):
+        return self.ctx.kernel_launches()
+
+    def profile_stages(self):
+        return self.ctx.profile_stages()
+
+
+def pack(complexes):
+    """Concatenate [(binder_xyz, binder_radii, target_xyz, target_radii), ...] into batch arrays."""
+    xyz, rad, off, nb = [], [], [0], []
+    for bx, br, tx, tr in complexes:
+        bx = np.asarray(bx, np.float64).reshape(-1, 3)
+        tx = np.asarray(tx, np.float64).reshape(-1, 3)
+        xyz += [bx, tx]
+        rad += [np.asarray(br, np.float64), np.asarray(tr, np.float64)]
+        nb.append(len(bx))
+        off.append(off[-1] + len(bx) + len(tx))
+    return (np.array(off, np.int64), np.array(nb, np.int64), np.concatenate(xyz), np.concatenate(rad))
+
+
+def calculate_batch(complexes, device=0, graph=False, per_atom=False):
+    """CMS (target and binder side) and SC of every complex in one batched GPU pass."""
+    calc = BatchCalculator(device)
+    calc.load(*pack(complexes))
+    return calc.run(graph=graph, per_atom=per_atom)

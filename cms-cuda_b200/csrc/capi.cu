@@ -81,6 +81,21 @@ __global__ void k_export_toroid(Dev d, long long q0, long long n, double* out)
     }
 }
 
+// FP32 FMA throughput probe: 8 independent FMA chains per thread, the result
+// folded into one store so nothing is optimised away
+__global__ void __launch_bounds__(256) k_fp32_peak(float* out, int iters, float a, float b)
+{
+    float x[8];
+    for (int k = 0; k < 8; ++k) x[k] = (float)(threadIdx.x + k) * 1e-3f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) x[k] = __fmaf_rn(x[k], a, b);
+    }
+    float s = 0.f;
+    for (int k = 0; k < 8; ++k) s += x[k];
+    if (s == 12345.678f) out[blockIdx.x] = s;
+}
+
 }  // namespace
 
 struct cms_ctx {
@@ -111,6 +126,11 @@ struct cms_ctx {
     long long graph_key[3] = {-1, -1, -1};
     long long launches = -1;
     std::string err;
+    // stage timing: an event after each pipeline stage when profiling
+    bool profiling = false;
+    long long h2d_bytes = 0, d2h_bytes = 0;   // host<->device bytes moved by the hot path
+    std::vector<cudaEvent_t> marks;
+    std::vector<int> mark_ids;
 
     // named buffer slots
     enum Slot {
@@ -166,6 +186,7 @@ void ck(cudaError_t e, const char* what)
 
 long long read_ll(cms_ctx* x, const long long* dev)
 {
+    x->d2h_bytes += sizeof(long long);
     ck(cudaMemcpyAsync(x->pinned, dev, sizeof(long long), cudaMemcpyDeviceToHost, x->stream), "readback");
     ck(cudaStreamSynchronize(x->stream), "sync");
     return x->pinned[0];
@@ -300,6 +321,23 @@ void set_settings_dev(cms_ctx* x)
 
 long long* scan_tmp(cms_ctx* x) { return x->get<long long>(cms_ctx::S_SCAN_TMP); }
 
+// pipeline stages, in enqueue order (cms_profile_stages reports one time each)
+enum Stage {
+    P_CELLS, P_ATTENTION, P_NB_COUNT, P_NB_EMIT, P_PAIRS, P_TRIPLES_COUNT, P_TRIPLES_EMIT, P_CONVEX_COUNT,
+    P_TOROIDAL_COUNT, P_CONCAVE_COUNT, P_LAYOUT, P_CONVEX_EMIT, P_TOROIDAL_EMIT, P_CONCAVE_EMIT, P_SPLIT,
+    P_CMS_NN, P_CMS_SUM, P_SC_BAND_NN, P_SC_ARGMIN_NN, P_SC_STATS, P_MAX_SUM, P_NSTAGES
+};
+
+void mark(cms_ctx* x, int stage)
+{
+    if (!x->profiling) return;
+    cudaEvent_t e;
+    ck(cudaEventCreate(&e), "event");
+    ck(cudaEventRecord(e, x->stream), "event record");
+    x->marks.push_back(e);
+    x->mark_ids.push_back(stage);
+}
+
 // ---------------------------------------------------------------------------
 // the pipeline.  sized = true: read each stage's total back and grow the
 // buffers to fit (host syncs between stages); sized = false: enqueue every
@@ -315,6 +353,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
     Dev& d = x->d;
     cudaStream_t s = x->stream;
     long long* tmp = scan_tmp(x);
+    mark(x, -1);
     ck(cudaMemsetAsync(d.status, 0, sizeof(int) * x->B, s), "memset");
     launch_setup(d, s);
     scan_counts(d.ncell, d.ncell_scan, d.B, tmp, s);
@@ -325,10 +364,13 @@ void enqueue_surface(cms_ctx* x, bool sized)
         tmp = scan_tmp(x);
     }
     launch_cells(d, x->cap_cells, tmp, s);
+    mark(x, P_CELLS);
     launch_attention(d, s);
+    mark(x, P_ATTENTION);
     launch_neighbor_count(d, s);
     scan_counts(d.nnb, d.nb_off, d.N, tmp, s);
     scan_counts(d.nbur, d.bu_off, d.N, tmp, s);
+    mark(x, P_NB_COUNT);
     if (sized) {
         grow(x->cap_nb, read_ll(x, d.nb_off + d.N));
         grow(x->cap_bu, read_ll(x, d.bu_off + d.N));
@@ -336,6 +378,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
         tmp = scan_tmp(x);
     }
     launch_neighbor_emit(d, s);
+    mark(x, P_NB_EMIT);
     launch_pairs(d, false, s);
     scan_counts(d.ntor, d.tor_off, d.N, tmp, s);
     if (sized) {
@@ -344,9 +387,11 @@ void enqueue_surface(cms_ctx* x, bool sized)
         tmp = scan_tmp(x);
     }
     launch_pairs(d, true, s);
+    mark(x, P_PAIRS);
     launch_triples(d, false, s);
     scan_counts(d.nplus, d.plus_off, d.N, tmp, s);
     scan_counts(d.nminus, d.minus_off, d.N, tmp, s);
+    mark(x, P_TRIPLES_COUNT);
     if (sized) {
         grow(x->cap_probe, read_ll(x, d.plus_off + d.N) + read_ll(x, d.minus_off + d.N));
         bind_caps(x);
@@ -354,26 +399,40 @@ void enqueue_surface(cms_ctx* x, bool sized)
     }
     launch_triples(d, true, s);
     launch_low_probes(d, x->cap_probe, tmp, s);
+    mark(x, P_TRIPLES_EMIT);
     ck(cudaMemsetAsync(d.tor1_cnt, 0, sizeof(int) * x->cap_tor, s), "memset");
     ck(cudaMemsetAsync(d.tor2_cnt, 0, sizeof(int) * x->cap_tor, s), "memset");
     ck(cudaMemsetAsync(d.conc_cnt, 0, sizeof(int) * x->cap_probe, s), "memset");
     launch_convex(d, false, s);
+    mark(x, P_CONVEX_COUNT);
     launch_toroidal(d, x->cap_tor, false, s);
+    mark(x, P_TOROIDAL_COUNT);
     launch_concave(d, x->cap_probe, false, s);
+    mark(x, P_CONCAVE_COUNT);
     scan_counts(d.conv_cnt, d.conv_off, d.N, tmp, s);
     scan_counts(d.tor1_cnt, d.tor1_off, x->cap_tor, tmp, s);
     scan_counts(d.tor2_cnt, d.tor2_off, x->cap_tor, tmp, s);
     scan_counts(d.conc_cnt, d.conc_off, x->cap_probe, tmp, s);
     launch_layout(d, (long long*)x->get<int>(cms_ctx::S_CM_TMP), tmp, s);
+    mark(x, P_LAYOUT);
     if (sized) {
         grow(x->cap_dot, read_ll(x, d.dot_off + 2LL * d.B));
         bind_caps(x);
         tmp = scan_tmp(x);
     }
     launch_convex(d, true, s);
+    mark(x, P_CONVEX_EMIT);
     launch_toroidal(d, x->cap_tor, true, s);
+    mark(x, P_TOROIDAL_EMIT);
     launch_concave(d, x->cap_probe, true, s);
+    mark(x, P_CONCAVE_EMIT);
     launch_tor_access(d, x->cap_tor, s);
+}
+
+void enqueue_split(cms_ctx* x)
+{
+    launch_split_buried(x->d, x->r, x->cap_dot, scan_tmp(x), x->stream);
+    mark(x, P_SPLIT);
 }
 
 NNArgs nn_args(cms_ctx* x, int kind)
@@ -401,9 +460,11 @@ void enqueue_cms(cms_ctx* x)
     a.q_f4 = r.bur_f4; a.q_idx = r.bur_idx; a.r_f4 = r.bur_f4; a.r_idx = r.bur_idx;
     a.out_d2 = r.nn_d2;
     launch_nn(d, a, NN_MIN, tile_cap(x), tmp, s);
+    mark(x, P_CMS_NN);
     launch_cms_weights(d, r, x->cap_dot, s);
     launch_per_atom_sum(d, r, x->cap_dot, x->get<double>(cms_ctx::S_PER_ATOM_CMS), tmp, s);
     launch_atom_totals(d, x->get<double>(cms_ctx::S_PER_ATOM_CMS), x->get<double>(cms_ctx::S_TOT_CMS), s);
+    mark(x, P_CMS_SUM);
 }
 
 void enqueue_sc(cms_ctx* x)
@@ -419,6 +480,7 @@ void enqueue_sc(cms_ctx* x)
     a.out_flag = r.keep;
     a.band_thr64 = x->st.band * x->st.band;
     launch_nn(d, a, NN_BAND, tile_cap(x), tmp, s);
+    mark(x, P_SC_BAND_NN);
     launch_trim_compact(d, r, x->cap_dot, tmp, s);
     launch_tasks(d, r, 2, task + 4 * x->B, s);
     k_fill_d<<<grid1(x->cap_dot), 256, 0, s>>>(r.nn_d2, x->cap_dot, INFINITY);
@@ -427,7 +489,9 @@ void enqueue_sc(cms_ctx* x)
     b.q_f4 = r.trim_f4; b.q_idx = r.trim_idx; b.r_f4 = r.trim_f4; b.r_idx = r.trim_idx;
     b.out_d2 = r.nn_d2; b.out_idx = r.nn_idx;
     launch_nn(d, b, NN_ARGMIN, tile_cap(x), tmp, s);
+    mark(x, P_SC_ARGMIN_NN);
     launch_sc_stats(d, r, task + 4 * x->B, x->get<double>(cms_ctx::S_SC_SIDE), x->get<double>(cms_ctx::S_SC_OUT), s);
+    mark(x, P_SC_STATS);
 }
 
 void enqueue_max(cms_ctx* x)
@@ -464,6 +528,8 @@ void pull_host_state(cms_ctx* x)
     ck(cudaMemcpyAsync(x->h_seg.data(), x->d.seg, sizeof(Seg) * 8 * B, cudaMemcpyDeviceToHost, s), "seg");
     ck(cudaMemcpyAsync(cx.data(), x->d.cx, sizeof(Cplx) * B, cudaMemcpyDeviceToHost, s), "cx");
     ck(cudaStreamSynchronize(s), "sync");
+    x->d2h_bytes += 8 * (long long)sizeof(long long) + (long long)B * (sizeof(int) + sizeof(unsigned long long) +
+                    8 * sizeof(Seg) + sizeof(Cplx)) + (2LL * B + 1) * (long long)sizeof(long long);
     for (int k = 0; k < 6; ++k) x->tot[k] = x->pinned[k];
     x->h_radmax.resize(B);
     for (int c = 0; c < B; ++c) x->h_radmax[c] = cx[c].radmax;
@@ -482,7 +548,7 @@ void run_sized_surface(cms_ctx* x, int all_atoms)
     set_settings_dev(x);
     bind_caps(x);
     enqueue_surface(x, true);
-    launch_split_buried(x->d, x->r, x->cap_dot, scan_tmp(x), x->stream);
+    enqueue_split(x);
     enqueue_summary(x);
     pull_host_state(x);
     x->surf_ok = true;
@@ -513,6 +579,7 @@ cms_status fail(cms_ctx* x, cms_status code, const std::string& m)
 
 void copy_out(cms_ctx* x, void* dst, const void* src, size_t bytes, int where)
 {
+    if (where == CMS_HOST) x->d2h_bytes += (long long)bytes;
     ck(cudaMemcpyAsync(dst, src, bytes, where == CMS_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
                        x->stream), "copy out");
     ck(cudaStreamSynchronize(x->stream), "sync");
@@ -628,6 +695,7 @@ cms_status cms_load_batch(cms_ctx* x, int32_t B, const int64_t* atom_off, const 
     for (int c = 0; c < B; ++c) n032[c] = (int)x->h_n0[c];
     ck(cudaMemcpyAsync((void*)x->d.atom_off, off32.data(), sizeof(int) * (B + 1), cudaMemcpyHostToDevice, s), "upload");
     ck(cudaMemcpyAsync((void*)x->d.n0, n032.data(), sizeof(int) * B, cudaMemcpyHostToDevice, s), "upload");
+    x->h2d_bytes += (long long)sizeof(int) * (2LL * B + 1);
     const double* dxyz = xyz;
     const double* drad = radius;
     const double* ddens = density;
@@ -638,10 +706,12 @@ cms_status cms_load_batch(cms_ctx* x, int32_t B, const int64_t* atom_off, const 
         ck(cudaMemcpyAsync(br, radius, sizeof(double) * N, cudaMemcpyHostToDevice, s), "upload radius");
         dxyz = bx;
         drad = br;
+        x->h2d_bytes += (long long)sizeof(double) * 4 * N;
         if (density) {
             double* bd = x->ensure<double>(cms_ctx::S_IN_DENS, N);
             ck(cudaMemcpyAsync(bd, density, sizeof(double) * N, cudaMemcpyHostToDevice, s), "upload density");
             ddens = bd;
+            x->h2d_bytes += (long long)sizeof(double) * N;
         }
     }
     k_pack_atoms<<<grid1(N), 256, 0, s>>>(N, dxyz, drad, ddens, x->st.density, x->d.xyzr, x->d.dens);
@@ -910,51 +980,69 @@ cms_status cms_export_trimmed(cms_ctx* x, int32_t c, int32_t molecule, int32_t* 
     API_END
 }
 
+}  // extern "C"
+
+namespace {
+
+// capture the whole batched pipeline into a CUDA graph for the current shape
+void capture_graph(cms_ctx* x)
+{
+    if (x->cap_dot == 0) run_sized_surface(x, 0);       // size every buffer once
+    const long long key[3] = {x->B, x->N, x->cap_dot};
+    if (x->gexec && std::memcmp(key, x->graph_key, sizeof(key)) == 0) return;
+    if (x->gexec) { cudaGraphExecDestroy(x->gexec); x->gexec = nullptr; }
+    if (x->graph) { cudaGraphDestroy(x->graph); x->graph = nullptr; }
+    x->d.all_atoms = 0;
+    set_settings_dev(x);
+    bind_caps(x);
+    ck(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+        enqueue_surface(x, false);
+        enqueue_split(x);
+        enqueue_cms(x);
+        enqueue_sc(x);
+        enqueue_summary(x);
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(x->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    ck(cudaStreamEndCapture(x->stream, &x->graph), "end capture");
+    ck(cudaGraphInstantiate(&x->gexec, x->graph, 0), "instantiate");
+    size_t nn = 0;
+    ck(cudaGraphGetNodes(x->graph, nullptr, &nn), "nodes");
+    std::vector<cudaGraphNode_t> nodes(nn);
+    ck(cudaGraphGetNodes(x->graph, nodes.data(), &nn), "nodes");
+    long long kernels = 0;
+    for (auto& n : nodes) {
+        cudaGraphNodeType t;
+        cudaGraphNodeGetType(n, &t);
+        if (t == cudaGraphNodeTypeKernel) ++kernels;
+    }
+    x->launches = kernels;
+    std::memcpy(x->graph_key, key, sizeof(key));
+}
+
+void mark_graph_results(cms_ctx* x)
+{
+    x->surf_ok = true;
+    x->surf_all_atoms = 0;
+    x->cms_ok = x->sc_ok = true;
+    x->max_ok = false;
+}
+
+}  // namespace
+
+extern "C" {
+
 cms_status cms_run_graph(cms_ctx* x)
 {
     if (!x) return CMS_ERR_ARG;
     API_BEGIN
     if (!x->have_batch) throw Fail{CMS_ERR_STATE, "no batch loaded"};
     ck(cudaSetDevice(x->device), "cudaSetDevice");
-    if (x->cap_dot == 0) {
-        // size every buffer once with the stage-synchronised path
-        run_sized_surface(x, 0);
-    }
-    const long long key[3] = {x->B, x->N, x->cap_dot};
-    if (!x->gexec || std::memcmp(key, x->graph_key, sizeof(key)) != 0) {
-        if (x->gexec) { cudaGraphExecDestroy(x->gexec); x->gexec = nullptr; }
-        if (x->graph) { cudaGraphDestroy(x->graph); x->graph = nullptr; }
-        x->d.all_atoms = 0;
-        set_settings_dev(x);
-        bind_caps(x);
-        ck(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-        try {
-            enqueue_surface(x, false);
-            launch_split_buried(x->d, x->r, x->cap_dot, scan_tmp(x), x->stream);
-            enqueue_cms(x);
-            enqueue_sc(x);
-            enqueue_summary(x);
-        } catch (...) {
-            cudaGraph_t g;
-            cudaStreamEndCapture(x->stream, &g);
-            if (g) cudaGraphDestroy(g);
-            throw;
-        }
-        ck(cudaStreamEndCapture(x->stream, &x->graph), "end capture");
-        ck(cudaGraphInstantiate(&x->gexec, x->graph, 0), "instantiate");
-        size_t nn = 0;
-        ck(cudaGraphGetNodes(x->graph, nullptr, &nn), "nodes");
-        std::vector<cudaGraphNode_t> nodes(nn);
-        ck(cudaGraphGetNodes(x->graph, nodes.data(), &nn), "nodes");
-        long long kernels = 0;
-        for (auto& n : nodes) {
-            cudaGraphNodeType t;
-            cudaGraphNodeGetType(n, &t);
-            if (t == cudaGraphNodeTypeKernel) ++kernels;
-        }
-        x->launches = kernels;
-        std::memcpy(x->graph_key, key, sizeof(key));
-    }
+    capture_graph(x);
     ck(cudaGraphLaunch(x->gexec, x->stream), "graph launch");
     pull_host_state(x);
     if (over_capacity(x)) {
@@ -966,13 +1054,134 @@ cms_status cms_run_graph(cms_ctx* x)
         pull_host_state(x);
         x->graph_key[0] = -1;
     }
-    x->surf_ok = true;
-    x->surf_all_atoms = 0;
-    x->cms_ok = x->sc_ok = true;
-    x->max_ok = false;
+    mark_graph_results(x);
+    API_END
+}
+
+cms_status cms_graph_launch(cms_ctx* x)
+{
+    if (!x) return CMS_ERR_ARG;
+    API_BEGIN
+    if (!x->have_batch) throw Fail{CMS_ERR_STATE, "no batch loaded"};
+    capture_graph(x);
+    ck(cudaGraphLaunch(x->gexec, x->stream), "graph launch");
+    mark_graph_results(x);
+    API_END
+}
+
+cms_status cms_graph_check(cms_ctx* x)
+{
+    if (!x) return CMS_ERR_ARG;
+    API_BEGIN
+    pull_host_state(x);
+    if (over_capacity(x)) throw Fail{CMS_ERR_CAPACITY, "a workspace capacity was exceeded; rerun cms_run_graph"};
+    API_END
+}
+
+cms_status cms_nn_work(cms_ctx* x, int64_t* pairs)
+{
+    if (!x || !pairs) return fail(x, CMS_ERR_ARG, "null argument");
+    API_BEGIN
+    need_surface(x);
+    std::vector<NNTask> t(6 * (size_t)x->B);
+    ck(cudaMemcpy(t.data(), x->get<NNTask>(cms_ctx::S_TASKS), sizeof(NNTask) * t.size(), cudaMemcpyDeviceToHost), "copy");
+    for (int k = 0; k < 3; ++k) {
+        long long s = 0, q = 0;
+        for (int i = 0; i < 2 * x->B; ++i) {
+            const NNTask& T = t[(size_t)k * 2 * x->B + i];
+            s += T.qn * T.rn;
+            q += T.qn;
+        }
+        pairs[2 * k] = s;
+        pairs[2 * k + 1] = q;
+    }
     API_END
 }
 
 int64_t cms_kernel_launches(cms_ctx* x) { return x ? x->launches : -1; }
+
+cms_status cms_fp32_peak(cms_ctx* x, double* tflops)
+{
+    if (!x || !tflops) return fail(x, CMS_ERR_ARG, "null argument");
+    API_BEGIN
+    ck(cudaSetDevice(x->device), "cudaSetDevice");
+    int sms = 0;
+    ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, x->device), "attribute");
+    const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+    float* out = x->ensure<float>(cms_ctx::S_EXPORT, blocks);
+    cudaEvent_t e0, e1;
+    ck(cudaEventCreate(&e0), "event");
+    ck(cudaEventCreate(&e1), "event");
+    k_fp32_peak<<<blocks, threads, 0, x->stream>>>(out, 256, 0.999f, 1e-3f);     // warm-up
+    ck(cudaEventRecord(e0, x->stream), "event");
+    k_fp32_peak<<<blocks, threads, 0, x->stream>>>(out, iters, 0.999f, 1e-3f);
+    ck(cudaEventRecord(e1, x->stream), "event");
+    ck(cudaEventSynchronize(e1), "sync");
+    float ms = 0.f;
+    ck(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const double flops = 2.0 * 8.0 * iters * (double)threads * blocks;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    API_END
+}
+
+cms_status cms_transfer_bytes(cms_ctx* x, int64_t* h2d, int64_t* d2h)
+{
+    if (!x) return CMS_ERR_ARG;
+    if (h2d) *h2d = x->h2d_bytes;
+    if (d2h) *d2h = x->d2h_bytes;
+    return CMS_OK;
+}
+
+static const char* k_stage_names[P_NSTAGES] = {
+    "cells", "attention", "neighbor_count", "neighbor_emit", "pairs", "triples_count", "triples_emit",
+    "convex_count", "toroidal_count", "concave_count", "layout", "convex_emit", "toroidal_emit", "concave_emit",
+    "split_buried", "cms_nn", "cms_sum", "sc_band_nn", "sc_argmin_nn", "sc_stats", "max_sum"};
+
+const char* cms_stage_name(int32_t stage)
+{
+    return (stage >= 0 && stage < P_NSTAGES) ? k_stage_names[stage] : "";
+}
+
+cms_status cms_profile_stages(cms_ctx* x, double* ms, int32_t cap, int32_t* n_stages)
+{
+    if (!x || !ms) return fail(x, CMS_ERR_ARG, "null argument");
+    API_BEGIN
+    if (!x->have_batch) throw Fail{CMS_ERR_STATE, "no batch loaded"};
+    ck(cudaSetDevice(x->device), "cudaSetDevice");
+    if (x->cap_dot == 0) run_sized_surface(x, 0);
+    x->d.all_atoms = 0;
+    set_settings_dev(x);
+    bind_caps(x);
+    x->profiling = true;
+    try {
+        enqueue_surface(x, false);
+        enqueue_split(x);
+        enqueue_cms(x);
+        enqueue_sc(x);
+        enqueue_summary(x);
+    } catch (...) {
+        x->profiling = false;
+        throw;
+    }
+    x->profiling = false;
+    ck(cudaStreamSynchronize(x->stream), "sync");
+    for (int i = 0; i < cap; ++i) ms[i] = 0.0;
+    for (size_t k = 1; k < x->marks.size(); ++k) {
+        float t = 0.f;
+        ck(cudaEventElapsedTime(&t, x->marks[k - 1], x->marks[k]), "elapsed");
+        int id = x->mark_ids[k];
+        if (id >= 0 && id < cap) ms[id] += t;
+    }
+    for (auto e : x->marks) cudaEventDestroy(e);
+    x->marks.clear();
+    x->mark_ids.clear();
+    if (n_stages) *n_stages = P_NSTAGES;
+    pull_host_state(x);
+    x->surf_ok = x->cms_ok = x->sc_ok = true;
+    x->max_ok = false;
+    API_END
+}
 
 }  // extern "C"

@@ -140,8 +140,36 @@ cms_status cms_export_trimmed(cms_ctx* ctx, int32_t c, int32_t molecule, int32_t
  * it.  Falls back to the stage-synchronised path on capacity overflow. */
 cms_status cms_run_graph(cms_ctx* ctx);
 
-/* Number of kernels the last pipeline run launched. */
+/* Replay the captured pipeline graph on the context's stream without
+ * waiting (capturing it first if needed); results are read by the usual
+ * readout calls, which synchronise.  cms_graph_check waits and returns
+ * CMS_ERR_CAPACITY if the inputs outgrew the captured capacities (then call
+ * cms_run_graph, which re-sizes). */
+cms_status cms_graph_launch(cms_ctx* ctx);
+cms_status cms_graph_check(cms_ctx* ctx);
+
+/* Nearest-dot search work of the last run: pairs[0..5] = (query x reference
+ * pairs, queries) of the CMS search, the SC band (trim) search and the SC
+ * neighbour search -- the algorithmic work behind the FP32 roofline. */
+cms_status cms_nn_work(cms_ctx* ctx, int64_t* pairs);
+
+/* Measured FP32 FMA throughput of the context's device (TFLOP/s, FMA = 2
+ * FLOP): the denominator of the nearest-dot search's roofline. */
+cms_status cms_fp32_peak(cms_ctx* ctx, double* tflops);
+
+/* Cumulative host->device and device->host bytes moved by the context's
+ * loads, readouts and synchronising bookkeeping (exports excluded). */
+cms_status cms_transfer_bytes(cms_ctx* ctx, int64_t* h2d, int64_t* d2h);
+
+/* Number of kernel nodes in the captured pipeline graph (-1 before capture). */
 int64_t cms_kernel_launches(cms_ctx* ctx);
+
+/* Run the batched pipeline (surfaces, CMS, SC) once with the current
+ * capacities and a CUDA event after every stage; ms[s] receives stage s's
+ * milliseconds (s < cap), *n_stages the number of stages.  Diagnostic
+ * counterpart of the reference's per-stage NVTX ranges (_gpu.py:30). */
+cms_status cms_profile_stages(cms_ctx* ctx, double* ms, int32_t cap, int32_t* n_stages);
+const char* cms_stage_name(int32_t stage);
 
 const char* cms_last_error(cms_ctx* ctx);
 const char* cms_version(void);
