@@ -111,75 +111,146 @@ __device__ __forceinline__ double exact_d2(const double* a, const double* b)
     return (dx * dx + dy * dy) + dz * dz;
 }
 
-static constexpr int NN_T = 256;     // queries per tile (one per thread)
-static constexpr int NN_R = 1024;    // references staged per round
+// Packed FP32 pairs (Blackwell f32x2 arithmetic): one instruction does the
+// same IEEE round-to-nearest operation on two lanes, so the packed distances
+// equal the scalar ones bit for bit.
+typedef unsigned long long f2_t;
+__device__ __forceinline__ f2_t pk2(float a, float b) { f2_t r; asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b)); return r; }
+__device__ __forceinline__ void upk2(f2_t v, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
+__device__ __forceinline__ f2_t sub2(f2_t a, f2_t b) { f2_t r; asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b)); return r; }
+__device__ __forceinline__ f2_t mul2(f2_t a, f2_t b) { f2_t r; asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b)); return r; }
+__device__ __forceinline__ f2_t fma2(f2_t a, f2_t b, f2_t c) { f2_t r; asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c)); return r; }
+
+__device__ __forceinline__ float d2_f32(float rx, float ry, float rz, float qx, float qy, float qz)
+{
+    const float dx = rx - qx, dy = ry - qy, dz = rz - qz;
+    return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, dx * dx));
+}
+
+static constexpr int NN_T = 128;              // threads per tile
+static constexpr int NN_Q = 4;                // queries per thread (two packed pairs)
+static constexpr int NN_TILE = NN_T * NN_Q;   // queries per tile
+static constexpr int NN_R = 1024;             // references staged per round
+static constexpr int NN_SUB = 32;             // references per threshold check
+
+// one query's state
+struct NNQ {
+    float qx, qy, qz;
+    int dot;            // dot index of the query (its FP64 coordinates are read on recheck)
+    float mf, thr;
+    double best;
+    int bidx;
+    bool live, done;
+};
+
+// re-examine references [k0, k0+n) of the staged round for one query whose
+// block minimum fell under its threshold: FP32 filter, FP64 recheck in order
+template <int MODE>
+__device__ __forceinline__ void nn_rescan(const Dev& d, const NNArgs& a, const NNTask& T, NNQ& q,
+                                          const float4* sA, const float2* sB, int k0, int n, long long rb,
+                                          double E)
+{
+    for (int k = k0; k < k0 + n; ++k) {
+        const float d2 = d2_f32(sA[k].x, sA[k].z, sB[k].x, q.qx, q.qy, q.qz);
+        if (d2 <= q.thr) {
+            const double* rp = d.dxyz + 3LL * a.r_idx[T.r0 + rb + k];
+            const double e = exact_d2(rp, d.dxyz + 3LL * q.dot);
+            if (MODE == NN_BAND) {
+                if (e <= a.band_thr64) { q.done = true; q.best = e; return; }
+            } else {
+                if (e < q.best) { q.best = e; q.bidx = (int)(rb + k); }
+                if (d2 < q.mf) { q.mf = d2; q.thr = nn_threshold(q.mf, E); }
+            }
+        }
+    }
+}
 
 template <int MODE>
 __global__ void __launch_bounds__(NN_T) k_nn(Dev d, NNArgs a)
 {
-    __shared__ float4 sref[NN_R];
+    __shared__ float4 sA[NN_R];   // (x, x, y, y)
+    __shared__ float2 sB[NN_R];   // (z, z)
     const long long ntiles = a.tile_off[a.ntask];
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        // task of this tile
         int lo = 0, hi = a.ntask - 1;
         while (lo < hi) {
             int mid = (lo + hi + 1) >> 1;
             if (a.tile_off[mid] <= tile) lo = mid; else hi = mid - 1;
         }
         const NNTask T = a.task[lo];
-        const long long qi = (tile - a.tile_off[lo]) * NN_T + threadIdx.x;
-        const bool live = qi < T.qn;
-        const Cplx& C = d.cx[T.c];
-        const double E = 2.5e-7 * C.R;
-        float qx = 0, qy = 0, qz = 0;
-        double q64[3] = {0, 0, 0};
-        if (live) {
-            float4 f = a.q_f4[T.q0 + qi];
-            qx = f.x; qy = f.y; qz = f.z;
-            const double* p = d.dxyz + 3LL * a.q_idx[T.q0 + qi];
-            q64[0] = p[0]; q64[1] = p[1]; q64[2] = p[2];
-        }
-        float mf = INFINITY;
-        float thr = INFINITY;
+        const long long qb = (tile - a.tile_off[lo]) * NN_TILE + threadIdx.x;
+        const double E = 2.5e-7 * d.cx[T.c].R;
+        float band_thr = INFINITY;
         if (MODE == NN_BAND) {
             double t = (sqrt(a.band_thr64) * (1.0 + 1e-6)) + E;
-            thr = __double2float_ru(t * t * (1.0 + 1e-6));
+            band_thr = __double2float_ru(t * t * (1.0 + 1e-6));
         }
-        double best = INFINITY;
-        int bidx = -1;
-        bool done = !live;
+        NNQ q[NN_Q];
+#pragma unroll
+        for (int j = 0; j < NN_Q; ++j) {
+            const long long qi = qb + (long long)j * NN_T;
+            q[j].live = qi < T.qn;
+            q[j].qx = q[j].qy = q[j].qz = 0.f;
+            q[j].dot = 0;
+            if (q[j].live) {
+                const float4 f = a.q_f4[T.q0 + qi];
+                q[j].qx = f.x; q[j].qy = f.y; q[j].qz = f.z;
+                q[j].dot = a.q_idx[T.q0 + qi];
+            }
+            q[j].mf = INFINITY;
+            q[j].thr = MODE == NN_BAND ? band_thr : INFINITY;
+            q[j].best = INFINITY;
+            q[j].bidx = -1;
+            q[j].done = !q[j].live;
+        }
+        const f2_t qx01 = pk2(q[0].qx, q[1].qx), qy01 = pk2(q[0].qy, q[1].qy), qz01 = pk2(q[0].qz, q[1].qz);
+        const f2_t qx23 = pk2(q[2].qx, q[3].qx), qy23 = pk2(q[2].qy, q[3].qy), qz23 = pk2(q[2].qz, q[3].qz);
         for (long long rb = 0; rb < T.rn; rb += NN_R) {
             const int nr = (int)min((long long)NN_R, T.rn - rb);
             __syncthreads();
-            for (int k = threadIdx.x; k < nr; k += NN_T) sref[k] = a.r_f4[T.r0 + rb + k];
+            for (int k = threadIdx.x; k < nr; k += NN_T) {
+                const float4 r = a.r_f4[T.r0 + rb + k];
+                sA[k] = make_float4(r.x, r.x, r.y, r.y);
+                sB[k] = make_float2(r.z, r.z);
+            }
             __syncthreads();
-            if (!done) {
-                for (int k = 0; k < nr; ++k) {
-                    const float4 r4 = sref[k];
-                    const float dx = r4.x - qx, dy = r4.y - qy, dz = r4.z - qz;
-                    const float d2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, dx * dx));
-                    if (d2 <= thr) {
-                        const double* rp = d.dxyz + 3LL * a.r_idx[T.r0 + rb + k];
-                        const double e = exact_d2(rp, q64);
-                        if (MODE == NN_BAND) {
-                            if (e <= a.band_thr64) { done = true; best = e; break; }
-                        } else {
-                            if (e < best) { best = e; bidx = (int)(rb + k); }
-                            if (d2 < mf) { mf = d2; thr = nn_threshold(mf, E); }
-                        }
+            const bool all_done = q[0].done && q[1].done && q[2].done && q[3].done;
+            if (!all_done) {
+                for (int sb = 0; sb < nr; sb += NN_SUB) {
+                    const int n = min(NN_SUB, nr - sb);
+                    float m0 = INFINITY, m1 = INFINITY, m2 = INFINITY, m3 = INFINITY;
+#pragma unroll 4
+                    for (int k = sb; k < sb + n; ++k) {
+                        const float4 ra = sA[k];
+                        const float2 rz = sB[k];
+                        const f2_t rxx = pk2(ra.x, ra.y), ryy = pk2(ra.z, ra.w), rzz = pk2(rz.x, rz.y);
+                        f2_t dx = sub2(rxx, qx01), dy = sub2(ryy, qy01), dz = sub2(rzz, qz01);
+                        f2_t s01 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
+                        dx = sub2(rxx, qx23); dy = sub2(ryy, qy23); dz = sub2(rzz, qz23);
+                        f2_t s23 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
+                        float a0, a1, a2, a3;
+                        upk2(s01, a0, a1);
+                        upk2(s23, a2, a3);
+                        m0 = fminf(m0, a0); m1 = fminf(m1, a1); m2 = fminf(m2, a2); m3 = fminf(m3, a3);
                     }
+                    if (!q[0].done && m0 <= q[0].thr) nn_rescan<MODE>(d, a, T, q[0], sA, sB, sb, n, rb, E);
+                    if (!q[1].done && m1 <= q[1].thr) nn_rescan<MODE>(d, a, T, q[1], sA, sB, sb, n, rb, E);
+                    if (!q[2].done && m2 <= q[2].thr) nn_rescan<MODE>(d, a, T, q[2], sA, sB, sb, n, rb, E);
+                    if (!q[3].done && m3 <= q[3].thr) nn_rescan<MODE>(d, a, T, q[3], sA, sB, sb, n, rb, E);
                 }
             }
             if (MODE == NN_BAND) {
-                if (__syncthreads_and(done)) break;
+                if (__syncthreads_and(q[0].done && q[1].done && q[2].done && q[3].done)) break;
             }
         }
-        if (live) {
-            const long long o = T.q0 + qi;
-            if (MODE == NN_BAND) a.out_flag[o] = done ? 0 : 1;      // keep iff no reference within the band
+#pragma unroll
+        for (int j = 0; j < NN_Q; ++j) {
+            if (!q[j].live) continue;
+            const long long o = T.q0 + qb + (long long)j * NN_T;
+            if (MODE == NN_BAND) a.out_flag[o] = q[j].done ? 0 : 1;     // keep iff no reference within the band
             else {
-                a.out_d2[o] = best;
-                if (MODE == NN_ARGMIN) a.out_idx[o] = bidx;
+                a.out_d2[o] = q[j].best;
+                if (MODE == NN_ARGMIN) a.out_idx[o] = q[j].bidx;
             }
         }
     }
@@ -189,7 +260,7 @@ __global__ void k_nn_tiles(NNArgs a)
 {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < a.ntask; t += gridDim.x * blockDim.x) {
         const NNTask T = a.task[t];
-        a.tile_cnt[t] = (T.qn > 0 && (T.rn > 0 || a.band_mode)) ? (int)((T.qn + NN_T - 1) / NN_T) : 0;
+        a.tile_cnt[t] = (T.qn > 0 && (T.rn > 0 || a.band_mode)) ? (int)((T.qn + NN_TILE - 1) / NN_TILE) : 0;
     }
 }
 
@@ -198,7 +269,7 @@ void launch_nn(const Dev& d, NNArgs a, int mode, long long tile_cap, long long* 
     a.band_mode = mode == NN_BAND;
     k_nn_tiles<<<grid_for(a.ntask, 128), 128, 0, s>>>(a);
     scan_counts(a.tile_cnt, a.tile_off, a.ntask, scan_tmp, s);
-    const unsigned grid = grid_for(tile_cap, 1, 8);
+    const unsigned grid = grid_for(tile_cap, 1, 8);   // persistent: at most 8 tiles in flight per SM
     if (mode == NN_MIN) k_nn<NN_MIN><<<grid, NN_T, 0, s>>>(d, a);
     else if (mode == NN_ARGMIN) k_nn<NN_ARGMIN><<<grid, NN_T, 0, s>>>(d, a);
     else k_nn<NN_BAND><<<grid, NN_T, 0, s>>>(d, a);

@@ -153,9 +153,9 @@ __global__ void k_zero_int(int* p, long long n)
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = 0;
 }
 
+// d.ncell_scan must already hold the exclusive scan of d.ncell
 void launch_cells(const Dev& d, long long n_cells, long long* scan_tmp, cudaStream_t s)
 {
-    scan_counts(d.ncell, d.ncell_scan, d.B, scan_tmp, s);
     k_zero_int<<<grid_for(n_cells, 256), 256, 0, s>>>(d.cell_cnt, n_cells);
     k_zero_int<<<grid_for(n_cells, 256), 256, 0, s>>>(d.cell_fill, n_cells);
     k_cell_count<<<grid_for(d.N, 256), 256, 0, s>>>(d);
@@ -473,46 +473,6 @@ void launch_pairs(const Dev& d, bool emit, cudaStream_t s)
 // triple loop: probe placement over (i, j, k) with j, k neighbours of i,
 // natom_k > natom_j; probes ordered as all "+" then all "-" per complex
 // ---------------------------------------------------------------------------
-struct Triple {
-    bool valid, degenerate, kills;
-    V3 xk; double rk; int k;
-    V3 uik; double dik, swijk;
-};
-
-__device__ __forceinline__ Triple triple_test(const Dev& d, int g, V3 xi, double eri, int j, V3 xj, double erj,
-                                              const PairGeo& p, int8_t ati, int8_t atj, int kslot, long long off,
-                                              int K)
-{
-    Triple t;
-    t.valid = false; t.degenerate = false; t.kills = false;
-    if (kslot >= K) return t;
-    const double rp = d.st.rp;
-    int k = d.nb_id[off + kslot];
-    t.k = k;
-    if (k <= j) return t;
-    double4 ak = d.xyzr[k];
-    t.xk = v3(ak.x, ak.y, ak.z);
-    t.rk = ak.w;
-    double erk = ak.w + rp;
-    double djk = norm3(t.xk - xj);
-    if (!(djk < erj + erk)) return t;
-    t.dik = norm3(t.xk - xi);
-    if (!(t.dik < eri + erk)) return t;
-    if (ati <= 1 && atj <= 1 && d.atten[k] <= 1) return t;
-    t.valid = true;
-    t.uik = (t.xk - xi) / t.dik;
-    double dt = dot_alt(p.uij, t.uik);
-    double wijk = acos(dt < -1.0 ? -1.0 : (dt > 1.0 ? 1.0 : dt));   // np.clip keeps NaN
-    t.swijk = sin(wijk);
-    t.degenerate = (dt >= 1.0) || (dt <= -1.0) || (wijk <= 0.0) || (t.swijk <= 0.0);
-    if (t.degenerate) {
-        double dtijk2 = sq_seq(p.tij - t.xk);
-        double rkp2 = erk * erk - p.rij * p.rij;
-        t.kills = dtijk2 < rkp2;
-    }
-    return t;
-}
-
 // probe collision against atom1's neighbours except atom2 and atom3 (alt, <=)
 __device__ __forceinline__ bool probe_collides(const Dev& d, V3 pt, long long off, int K, int j, int k, double rp)
 {
@@ -526,26 +486,136 @@ __device__ __forceinline__ bool probe_collides(const Dev& d, V3 pt, long long of
     return false;
 }
 
+// Triple (i, j, k) validity of vec_third_loop (_core.py:1472-1494), cheapest
+// tests first: k after j, not all three blockers, then the two distance tests.
+struct TripleBase {
+    bool valid;
+    int k;
+    V3 xk; double erk, dik;
+};
+
+__device__ __forceinline__ TripleBase triple_base(const Dev& d, V3 xi, double eri, int j, V3 xj, double erj,
+                                                  int8_t ati, int8_t atj, int k)
+{
+    TripleBase t;
+    t.valid = false;
+    t.k = k;
+    if (k <= j) return t;
+    if (ati <= 1 && atj <= 1 && d.atten[k] <= 1) return t;
+    double4 ak = d.xyzr[k];
+    t.xk = v3(ak.x, ak.y, ak.z);
+    t.erk = ak.w + d.st.rp;
+    double djk = norm3(t.xk - xj);
+    if (!(djk < erj + t.erk)) return t;
+    t.dik = norm3(t.xk - xi);
+    if (!(t.dik < eri + t.erk)) return t;
+    t.valid = true;
+    return t;
+}
+
 static constexpr int TR_WARPS = 4;
+static constexpr int TR_QCAP = 256;   // queued (pair slot, k slot) triples per warp
+
+// probes of the queued triples, in queue order: "+" and "-" probes are
+// ballot-ordered into the atom's two probe ranges
+template <bool EMIT>
+__device__ __forceinline__ void triples_flush(const Dev& d, int g, V3 xi, double ri, double eri, long long off,
+                                              int K, const unsigned* queue, int qn, int& nplus, int& nminus,
+                                              long long pbase, long long mbase)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const double rp = d.st.rp;
+    for (int e0 = 0; e0 < qn; e0 += 32) {
+        const int e = e0 + lane;
+        bool okp = false, okm = false;
+        V3 pp, pm, up;
+        double h = 0.0;
+        int j = -1, k = -1;
+        if (e < qn) {
+            const unsigned ent = queue[e];
+            j = d.nb_id[off + (ent >> 16)];
+            k = d.nb_id[off + (ent & 0xffffu)];
+            const double4 aj = d.xyzr[j], ak = d.xyzr[k];
+            const V3 xj = v3(aj.x, aj.y, aj.z), xk = v3(ak.x, ak.y, ak.z);
+            const PairGeo p = pair_geo(xi, ri, xj, aj.w, rp);
+            const double erk = ak.w + rp;
+            const double dik = norm3(xk - xi);
+            const V3 uik = (xk - xi) / dik;
+            const double dt = dot_alt(p.uij, uik);
+            const double wijk = acos(dt < -1.0 ? -1.0 : (dt > 1.0 ? 1.0 : dt));   // np.clip keeps NaN
+            const double swijk = sin(wijk);
+            if (!((dt >= 1.0) || (dt <= -1.0) || (wijk <= 0.0) || (swijk <= 0.0))) {
+                const V3 uijk = cross3(p.uij, uik) / swijk;
+                const V3 utb = cross3(uijk, p.uij);
+                const double asymm = (eri * eri - erk * erk) / dik;
+                const V3 tik = (xi + xk) * 0.5 + uik * (asymm * 0.5);
+                const double dtb = dot_alt(uik, tik - p.tij);
+                const V3 bijk = p.tij + utb * (dtb / swijk);
+                const V3 bma = bijk - xi;
+                const double h2 = eri * eri - dot_alt(bma, bma);
+                if (h2 > 0.0) {
+                    h = sqrt(h2);
+                    up = uijk;
+                    pp = bijk + uijk * (h * 1.0);
+                    pm = bijk + uijk * (h * -1.0);
+                    okp = !probe_collides(d, pp, off, K, j, k, rp);
+                    okm = !probe_collides(d, pm, off, K, j, k, rp);
+                }
+            }
+        }
+        const unsigned bp = __ballot_sync(0xffffffffu, okp);
+        const unsigned bm = __ballot_sync(0xffffffffu, okm);
+        if (EMIT) {
+            if (okp) {
+                long long q = pbase + nplus + __popc(bp & lt);
+                if (q < d.probe_cap) {
+                    d.pa0[q] = g; d.pa1[q] = j; d.pa2[q] = k;
+                    d.ph[q] = h; st3(d.pxyz + 3 * q, pp); st3(d.palt + 3 * q, up * 1.0);
+                }
+            }
+            if (okm) {
+                long long q = mbase + nminus + __popc(bm & lt);
+                if (q < d.probe_cap) {
+                    d.pa0[q] = j; d.pa1[q] = g; d.pa2[q] = k;
+                    d.ph[q] = h; st3(d.pxyz + 3 * q, pm); st3(d.palt + 3 * q, up * -1.0);
+                }
+            }
+            if (okp || okm) { d.access[g] = 1; d.access[j] = 1; d.access[k] = 1; }
+        }
+        nplus += __popc(bp);
+        nminus += __popc(bm);
+    }
+}
 
 template <bool EMIT>
 __global__ void __launch_bounds__(TR_WARPS * 32) k_triples(Dev d)
 {
-    const int lane = threadIdx.x & 31;
+    __shared__ unsigned queue_s[TR_WARPS][TR_QCAP];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    const long long wid = blockIdx.x * (long long)TR_WARPS + (threadIdx.x >> 5);
+    unsigned* queue = queue_s[w];
+    const long long wid = blockIdx.x * (long long)TR_WARPS + w;
     const long long nw = (long long)gridDim.x * TR_WARPS;
     const double rp = d.st.rp;
     for (long long gg = wid; gg < d.N; gg += nw) {
         const int g = (int)gg;
         const int K = d.nnb[g];
         int nplus = 0, nminus = 0;
-        if (K > 1) {
-            double4 ai = d.xyzr[g];
+        const int8_t ati = d.atten[g];
+        const long long off = d.nb_off[g];
+        bool any_open = ati > 1;
+        if (K > 1 && !any_open) {
+            // every triple of an all-blocker neighbourhood is skipped (_core.py:1486-1494)
+            for (int kb = 0; kb < K && !any_open; kb += 32) {
+                const int ks = kb + lane;
+                any_open = __any_sync(0xffffffffu, ks < K && d.atten[d.nb_id[off + ks]] > 1);
+            }
+        }
+        if (K > 1 && any_open && K <= 0xffff) {
+            const double4 ai = d.xyzr[g];
             const V3 xi = v3(ai.x, ai.y, ai.z);
             const double eri = ai.w + rp;
-            const long long off = d.nb_off[g];
-            const int8_t ati = d.atten[g];
             long long pbase = 0, mbase = 0;
             if (EMIT) {
                 // probe layout per complex: [+mol0 | -mol0 | +mol1 | -mol1]
@@ -553,74 +623,91 @@ __global__ void __launch_bounds__(TR_WARPS * 32) k_triples(Dev d)
                 const Cplx C = d.cx[c];
                 const int s0 = C.a0, s1 = C.a0 + C.n0, e1 = C.a0 + C.n;
                 const int ms = d.mol[g] == 0 ? s0 : s1, me = d.mol[g] == 0 ? s1 : e1;
-                long long cbase = d.plus_off[s0] + d.minus_off[s0];
-                long long m0 = (d.plus_off[s1] - d.plus_off[s0]) + (d.minus_off[s1] - d.minus_off[s0]);
-                long long mb = cbase + (d.mol[g] == 0 ? 0 : m0);
+                const long long cbase = d.plus_off[s0] + d.minus_off[s0];
+                const long long m0 = (d.plus_off[s1] - d.plus_off[s0]) + (d.minus_off[s1] - d.minus_off[s0]);
+                const long long mb = cbase + (d.mol[g] == 0 ? 0 : m0);
                 pbase = mb + (d.plus_off[g] - d.plus_off[ms]);
                 mbase = mb + (d.plus_off[me] - d.plus_off[ms]) + (d.minus_off[g] - d.minus_off[ms]);
             }
+            int qn = 0;
             for (int ps = 0; ps < K; ++ps) {
                 const int j = d.nb_id[off + ps];
                 if (j <= g) continue;
-                double4 aj = d.xyzr[j];
+                const double4 aj = d.xyzr[j];
                 const V3 xj = v3(aj.x, aj.y, aj.z);
                 const PairGeo p = pair_geo(xi, ai.w, xj, aj.w, rp);
                 if (!p.ok) continue;
                 const double erj = aj.w + rp;
                 const int8_t atj = d.atten[j];
-                // pass 1: does a degenerate triple kill the whole pair?
+                // a degenerate triple (|uij.uik| >= 1) inside the torus kills the whole pair
+                // (_core.py:1524-1543); the others are queued in (pair, k) order
                 bool kill = false;
-                for (int kb = 0; kb < K; kb += 32) {
-                    Triple t = triple_test(d, g, xi, eri, j, xj, erj, p, ati, atj, kb + lane, off, K);
-                    kill |= __any_sync(0xffffffffu, t.valid && t.kills);
-                }
-                if (kill) continue;
-                // pass 2: probes
-                for (int kb = 0; kb < K; kb += 32) {
-                    Triple t = triple_test(d, g, xi, eri, j, xj, erj, p, ati, atj, kb + lane, off, K);
-                    bool okp = false, okm = false;
-                    V3 pp, pm, up; double h = 0;
-                    if (t.valid && !t.degenerate) {
-                        const double erk = t.rk + rp;
-                        V3 uijk = cross3(p.uij, t.uik) / t.swijk;
-                        V3 utb = cross3(uijk, p.uij);
-                        double asymm = (eri * eri - erk * erk) / t.dik;
-                        V3 tik = (xi + t.xk) * 0.5 + t.uik * (asymm * 0.5);
-                        double dtb = dot_alt(t.uik, tik - p.tij);
-                        V3 bijk = p.tij + utb * (dtb / t.swijk);
-                        V3 bma = bijk - xi;
-                        double h2 = eri * eri - dot_alt(bma, bma);
-                        if (h2 > 0.0) {
-                            h = sqrt(h2);
-                            up = uijk;
-                            pp = bijk + uijk * (h * 1.0);
-                            pm = bijk + uijk * (h * -1.0);
-                            okp = !probe_collides(d, pp, off, K, j, t.k, rp);
-                            okm = !probe_collides(d, pm, off, K, j, t.k, rp);
-                        }
-                    }
-                    unsigned bp = __ballot_sync(0xffffffffu, okp);
-                    unsigned bm = __ballot_sync(0xffffffffu, okm);
-                    if (EMIT) {
-                        if (okp) {
-                            long long q = pbase + nplus + __popc(bp & lt);
-                            if (q < d.probe_cap) {
-                                d.pa0[q] = g; d.pa1[q] = j; d.pa2[q] = t.k;
-                                d.ph[q] = h; st3(d.pxyz + 3 * q, pp); st3(d.palt + 3 * q, up * 1.0);
+                int nq = 0;
+                unsigned cand[4];
+                for (int kb = 0, r = 0; kb < K; kb += 32, ++r) {
+                    const int ks = kb + lane;
+                    bool c = false;
+                    if (ks < K) {
+                        const TripleBase t = triple_base(d, xi, eri, j, xj, erj, ati, atj, d.nb_id[off + ks]);
+                        if (t.valid) {
+                            const V3 uik = (t.xk - xi) / t.dik;
+                            const double dt = dot_alt(p.uij, uik);
+                            if (dt >= 1.0 || dt <= -1.0) {
+                                const double dtijk2 = sq_seq(p.tij - t.xk);
+                                const double rkp2 = t.erk * t.erk - p.rij * p.rij;
+                                kill |= dtijk2 < rkp2;
+                            } else {
+                                c = true;
                             }
                         }
-                        if (okm) {
-                            long long q = mbase + nminus + __popc(bm & lt);
-                            if (q < d.probe_cap) {
-                                d.pa0[q] = j; d.pa1[q] = g; d.pa2[q] = t.k;
-                                d.ph[q] = h; st3(d.pxyz + 3 * q, pm); st3(d.palt + 3 * q, up * -1.0);
+                    }
+                    const unsigned m = __ballot_sync(0xffffffffu, c);
+                    if (r < 4) cand[r] = m;
+                    nq += __popc(m);
+                }
+                if (__any_sync(0xffffffffu, kill)) continue;
+                if (nq == 0) continue;
+                if (qn + nq > TR_QCAP) {
+                    __syncwarp();
+                    triples_flush<EMIT>(d, g, xi, ai.w, eri, off, K, queue, qn, nplus, nminus, pbase, mbase);
+                    __syncwarp();
+                    qn = 0;
+                }
+                if (K <= 128 && nq <= TR_QCAP) {
+                    for (int r = 0; r * 32 < K; ++r) {
+                        const unsigned m = cand[r];
+                        if ((m >> lane) & 1u) queue[qn + __popc(m & lt)] = ((unsigned)ps << 16) | (unsigned)(r * 32 + lane);
+                        qn += __popc(m);
+                    }
+                } else {
+                    // long rows: recompute candidacy chunk by chunk, flushing as the queue fills
+                    for (int kb = 0; kb < K; kb += 32) {
+                        const int ks = kb + lane;
+                        bool c = false;
+                        if (ks < K) {
+                            const TripleBase t = triple_base(d, xi, eri, j, xj, erj, ati, atj, d.nb_id[off + ks]);
+                            if (t.valid) {
+                                const double dt = dot_alt(p.uij, (t.xk - xi) / t.dik);
+                                c = !(dt >= 1.0 || dt <= -1.0);
                             }
                         }
-                        if (okp || okm) { d.access[g] = 1; d.access[j] = 1; d.access[t.k] = 1; }
+                        const unsigned m = __ballot_sync(0xffffffffu, c);
+                        if (qn + 32 > TR_QCAP) {
+                            __syncwarp();
+                            triples_flush<EMIT>(d, g, xi, ai.w, eri, off, K, queue, qn, nplus, nminus, pbase, mbase);
+                            __syncwarp();
+                            qn = 0;
+                        }
+                        if (c) queue[qn + __popc(m & lt)] = ((unsigned)ps << 16) | (unsigned)ks;
+                        qn += __popc(m);
                     }
-                    nplus += __popc(bp);
-                    nminus += __popc(bm);
                 }
+                __syncwarp();
+            }
+            if (qn > 0) {
+                __syncwarp();
+                triples_flush<EMIT>(d, g, xi, ai.w, eri, off, K, queue, qn, nplus, nminus, pbase, mbase);
+                __syncwarp();
             }
         }
         if (!EMIT && lane == 0) { d.nplus[g] = nplus; d.nminus[g] = nminus; }
