@@ -28,6 +28,7 @@ EXPORTED = (
     "cms_export_probes", "cms_export_dots", "cms_export_trimmed", "cms_run_graph", "cms_kernel_launches",
     "cms_last_error", "cms_version", "cms_device_count", "cms_profile_stages", "cms_stage_name",
     "cms_graph_launch", "cms_graph_check", "cms_nn_work", "cms_transfer_bytes", "cms_fp32_peak",
+    "cms_nearest_dots",
 )
 
 
@@ -100,6 +101,7 @@ def load():
             "cms_nn_work": [_VP, _PI64],
             "cms_transfer_bytes": [_VP, _PI64, _PI64],
             "cms_fp32_peak": [_VP, ctypes.POINTER(ctypes.c_double)],
+            "cms_nearest_dots": [_VP, _VP, ctypes.c_int64, _VP, ctypes.c_int64, _VP, _VP, _I32],
         }
         for name, args in sig.items():
             f = getattr(lib, name)
@@ -213,6 +215,15 @@ class Context:
         n = ctypes.c_int32(0)
         self._check(self.lib.cms_profile_stages(self.h, _ptr(ms), 64, ctypes.byref(n)))
         return {self.lib.cms_stage_name(i).decode(): float(ms[i]) for i in range(n.value)}
+
+    def nearest_dots(self, query, ref):
+        """(min squared distance, first index) of each query point over the reference points."""
+        q = np.ascontiguousarray(query, dtype=np.float64).reshape(-1, 3)
+        r = np.ascontiguousarray(ref, dtype=np.float64).reshape(-1, 3)
+        d2 = np.empty(len(q)); idx = np.empty(len(q), np.int32)
+        self._check(self.lib.cms_nearest_dots(self.h, _ptr(q), len(q), _ptr(r), len(r), _ptr(d2), _ptr(idx),
+                                              CMS_HOST))
+        return d2, idx
 
     def fp32_peak(self):
         v = ctypes.c_double(0)

@@ -145,7 +145,9 @@ struct cms_ctx {
         S_R_FLAG, S_R_BUR_SCAN, S_R_BUR_IDX, S_R_BUR_F4, S_R_BUR_CM, S_R_ACC_IDX, S_R_ACC_F4, S_R_KEEP, S_R_TRIM_SCAN,
         S_R_TRIM_IDX, S_R_TRIM_F4, S_R_NN_D2, S_R_NN_IDX, S_R_VAL, S_R_OWN, S_R_ACNT, S_R_AFILL, S_R_AOFF, S_R_ASLOT,
         S_CM_TMP, S_SCAN_TMP, S_PER_ATOM_CMS, S_TOT_CMS, S_PER_ATOM_MAX, S_TOT_MAX, S_SC_SIDE, S_SC_OUT, S_TASKS,
-        S_TILE_CNT, S_TILE_OFF, S_SUMMARY, S_EXPORT, S_COUNT
+        S_TILE_CNT, S_TILE_OFF, S_SUMMARY, S_EXPORT,
+        S_NN_Q, S_NN_R, S_NN_QF4, S_NN_RF4, S_NN_PART, S_NN_BBOX, S_NN_TASK, S_NN_TCNT, S_NN_TOFF, S_NN_D2, S_NN_IDX,
+        S_COUNT
     };
 
     cms_ctx() : bufs(S_COUNT) {}
@@ -458,8 +460,9 @@ void enqueue_cms(cms_ctx* x)
     k_fill_d<<<grid1(x->cap_dot), 256, 0, s>>>(r.nn_d2, x->cap_dot, INFINITY);
     NNArgs a = nn_args(x, 0);
     a.q_f4 = r.bur_f4; a.q_idx = r.bur_idx; a.r_f4 = r.bur_f4; a.r_idx = r.bur_idx;
+    a.q_xyz = a.r_xyz = d.dxyz;
     a.out_d2 = r.nn_d2;
-    launch_nn(d, a, NN_MIN, tile_cap(x), tmp, s);
+    launch_nn(a, NN_MIN, tile_cap(x), tmp, s);
     mark(x, P_CMS_NN);
     launch_cms_weights(d, r, x->cap_dot, s);
     launch_per_atom_sum(d, r, x->cap_dot, x->get<double>(cms_ctx::S_PER_ATOM_CMS), tmp, s);
@@ -477,9 +480,10 @@ void enqueue_sc(cms_ctx* x)
     launch_tasks(d, r, 1, task + 2 * x->B, s);
     NNArgs a = nn_args(x, 1);
     a.q_f4 = r.bur_f4; a.q_idx = r.bur_idx; a.r_f4 = r.acc_f4; a.r_idx = r.acc_idx;
+    a.q_xyz = a.r_xyz = d.dxyz;
     a.out_flag = r.keep;
     a.band_thr64 = x->st.band * x->st.band;
-    launch_nn(d, a, NN_BAND, tile_cap(x), tmp, s);
+    launch_nn(a, NN_BAND, tile_cap(x), tmp, s);
     mark(x, P_SC_BAND_NN);
     launch_trim_compact(d, r, x->cap_dot, tmp, s);
     launch_tasks(d, r, 2, task + 4 * x->B, s);
@@ -487,8 +491,9 @@ void enqueue_sc(cms_ctx* x)
     k_fill_i<<<grid1(x->cap_dot), 256, 0, s>>>(r.nn_idx, x->cap_dot, -1);
     NNArgs b = nn_args(x, 2);
     b.q_f4 = r.trim_f4; b.q_idx = r.trim_idx; b.r_f4 = r.trim_f4; b.r_idx = r.trim_idx;
+    b.q_xyz = b.r_xyz = d.dxyz;
     b.out_d2 = r.nn_d2; b.out_idx = r.nn_idx;
-    launch_nn(d, b, NN_ARGMIN, tile_cap(x), tmp, s);
+    launch_nn(b, NN_ARGMIN, tile_cap(x), tmp, s);
     mark(x, P_SC_ARGMIN_NN);
     launch_sc_stats(d, r, task + 4 * x->B, x->get<double>(cms_ctx::S_SC_SIDE), x->get<double>(cms_ctx::S_SC_OUT), s);
     mark(x, P_SC_STATS);
@@ -1099,6 +1104,54 @@ cms_status cms_nn_work(cms_ctx* x, int64_t* pairs)
 }
 
 int64_t cms_kernel_launches(cms_ctx* x) { return x ? x->launches : -1; }
+
+cms_status cms_nearest_dots(cms_ctx* x, const double* query_xyz, int64_t n_query, const double* ref_xyz,
+                            int64_t n_ref, double* out_d2, int32_t* out_index, int32_t where)
+{
+    if (!x) return CMS_ERR_ARG;
+    if (n_query < 0 || n_ref <= 0 || (n_query > 0 && (!query_xyz || !out_d2)) || !ref_xyz)
+        return fail(x, CMS_ERR_ARG, "cms_nearest_dots: need n_ref > 0 and non-null point / output arrays");
+    if (n_query + n_ref >= (1LL << 31)) return fail(x, CMS_ERR_ARG, "cms_nearest_dots: too many points");
+    API_BEGIN
+    ck(cudaSetDevice(x->device), "cudaSetDevice");
+    if (n_query == 0) return CMS_OK;
+    cudaStream_t s = x->stream;
+    const double* q = query_xyz;
+    const double* r = ref_xyz;
+    if (where == CMS_HOST) {
+        double* dq = x->ensure<double>(cms_ctx::S_NN_Q, 3 * n_query);
+        double* dr = x->ensure<double>(cms_ctx::S_NN_R, 3 * n_ref);
+        ck(cudaMemcpyAsync(dq, query_xyz, sizeof(double) * 3 * n_query, cudaMemcpyHostToDevice, s), "upload");
+        ck(cudaMemcpyAsync(dr, ref_xyz, sizeof(double) * 3 * n_ref, cudaMemcpyHostToDevice, s), "upload");
+        q = dq;
+        r = dr;
+    }
+    const int pblocks = 256;
+    double* part = x->ensure<double>(cms_ctx::S_NN_PART, 6 * pblocks);
+    double* bbox = x->ensure<double>(cms_ctx::S_NN_BBOX, 8);
+    float4* qf = x->ensure<float4>(cms_ctx::S_NN_QF4, n_query);
+    float4* rf = x->ensure<float4>(cms_ctx::S_NN_RF4, n_ref);
+    NNTask* task = x->ensure<NNTask>(cms_ctx::S_NN_TASK, 1);
+    int* tcnt = x->ensure<int>(cms_ctx::S_NN_TCNT, 1);
+    long long* toff = x->ensure<long long>(cms_ctx::S_NN_TOFF, 2);
+    double* d2 = where == CMS_HOST ? x->ensure<double>(cms_ctx::S_NN_D2, n_query) : out_d2;
+    int* idx = where == CMS_HOST ? x->ensure<int>(cms_ctx::S_NN_IDX, n_query) : out_index;
+    if (!idx) idx = x->ensure<int>(cms_ctx::S_NN_IDX, n_query);
+    launch_points_setup(q, n_query, r, n_ref, part, pblocks, bbox, qf, rf, task, tcnt, toff, s);
+    NNArgs a{};
+    a.task = task; a.ntask = 1; a.tile_cnt = tcnt; a.tile_off = toff;
+    a.q_f4 = qf; a.q_idx = nullptr; a.r_f4 = rf; a.r_idx = nullptr;
+    a.q_xyz = q; a.r_xyz = r;
+    a.out_d2 = d2; a.out_idx = idx;
+    launch_nn_kernel(a, NN_ARGMIN, n_query / 512 + 2, s);
+    ck(cudaGetLastError(), "nearest-dot kernels");
+    if (where == CMS_HOST) {
+        ck(cudaMemcpyAsync(out_d2, d2, sizeof(double) * n_query, cudaMemcpyDeviceToHost, s), "copy out");
+        if (out_index) ck(cudaMemcpyAsync(out_index, idx, sizeof(int) * n_query, cudaMemcpyDeviceToHost, s), "copy out");
+        ck(cudaStreamSynchronize(s), "sync");
+    }
+    API_END
+}
 
 cms_status cms_fp32_peak(cms_ctx* x, double* tflops)
 {

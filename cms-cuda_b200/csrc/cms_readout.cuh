@@ -13,6 +13,7 @@ enum { NN_MIN = 0, NN_ARGMIN = 1, NN_BAND = 2 };
 // of the same complex, both as positions in packed lists
 struct NNTask {
     long long q0, qn, r0, rn;
+    double E;       // FP32 error scale: 2.5e-7 x the per-axis half-extent bounding both point sets
     int c;
 };
 
@@ -21,8 +22,9 @@ struct NNArgs {
     int ntask;
     int* tile_cnt;          // ntask
     long long* tile_off;    // ntask + 1
-    const float4* q_f4; const int* q_idx;
+    const float4* q_f4; const int* q_idx;       // packed FP32 points; index into q_xyz (null: identity)
     const float4* r_f4; const int* r_idx;
+    const double* q_xyz; const double* r_xyz;   // FP64 coordinates for the recheck
     double* out_d2; int* out_idx; int* out_flag;
     double band_thr64;      // band^2 (BAND mode)
     int band_mode;
@@ -43,7 +45,13 @@ struct Rd {
 
 void launch_split_buried(const Dev& d, const Rd& r, long long dot_cap, long long* scan_tmp, cudaStream_t s);
 void launch_tasks(const Dev& d, const Rd& r, int kind, NNTask* task, cudaStream_t s);
-void launch_nn(const Dev& d, NNArgs a, int mode, long long tile_cap, long long* scan_tmp, cudaStream_t s);
+void launch_nn(NNArgs a, int mode, long long tile_cap, long long* scan_tmp, cudaStream_t s);
+void launch_nn_tiles(NNArgs a, int mode, long long* scan_tmp, cudaStream_t s);
+void launch_nn_kernel(NNArgs a, int mode, long long tile_cap, cudaStream_t s);
+// standalone search helpers: bounding box of two point sets, FP32 packing, one task
+void launch_points_setup(const double* q, long long nq, const double* r, long long nr, double* partials,
+                         int partial_blocks, double* bbox, float4* q_f4, float4* r_f4, NNTask* task, int* tile_cnt,
+                         long long* tile_off, cudaStream_t s);
 void launch_cms_weights(const Dev& d, const Rd& r, long long cap, cudaStream_t s);
 void launch_area_values(const Dev& d, const Rd& r, long long cap, cudaStream_t s);
 void launch_per_atom_sum(const Dev& d, const Rd& r, long long cap, double* out, long long* scan_tmp, cudaStream_t s);

@@ -146,15 +146,15 @@ struct NNQ {
 // re-examine references [k0, k0+n) of the staged round for one query whose
 // block minimum fell under its threshold: FP32 filter, FP64 recheck in order
 template <int MODE>
-__device__ __forceinline__ void nn_rescan(const Dev& d, const NNArgs& a, const NNTask& T, NNQ& q,
-                                          const float4* sA, const float2* sB, int k0, int n, long long rb,
-                                          double E)
+__device__ __forceinline__ void nn_rescan(const NNArgs& a, const NNTask& T, NNQ& q, const float4* sA,
+                                          const float2* sB, int k0, int n, long long rb, double E)
 {
     for (int k = k0; k < k0 + n; ++k) {
         const float d2 = d2_f32(sA[k].x, sA[k].z, sB[k].x, q.qx, q.qy, q.qz);
         if (d2 <= q.thr) {
-            const double* rp = d.dxyz + 3LL * a.r_idx[T.r0 + rb + k];
-            const double e = exact_d2(rp, d.dxyz + 3LL * q.dot);
+            const long long rk = T.r0 + rb + k;
+            const double* rp = a.r_xyz + 3LL * (a.r_idx ? a.r_idx[rk] : rk);
+            const double e = exact_d2(rp, a.q_xyz + 3LL * q.dot);
             if (MODE == NN_BAND) {
                 if (e <= a.band_thr64) { q.done = true; q.best = e; return; }
             } else {
@@ -166,7 +166,7 @@ __device__ __forceinline__ void nn_rescan(const Dev& d, const NNArgs& a, const N
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(NN_T) k_nn(Dev d, NNArgs a)
+__global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
 {
     __shared__ float4 sA[NN_R];   // (x, x, y, y)
     __shared__ float2 sB[NN_R];   // (z, z)
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(NN_T) k_nn(Dev d, NNArgs a)
         }
         const NNTask T = a.task[lo];
         const long long qb = (tile - a.tile_off[lo]) * NN_TILE + threadIdx.x;
-        const double E = 2.5e-7 * d.cx[T.c].R;
+        const double E = T.E;
         float band_thr = INFINITY;
         if (MODE == NN_BAND) {
             double t = (sqrt(a.band_thr64) * (1.0 + 1e-6)) + E;
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(NN_T) k_nn(Dev d, NNArgs a)
             if (q[j].live) {
                 const float4 f = a.q_f4[T.q0 + qi];
                 q[j].qx = f.x; q[j].qy = f.y; q[j].qz = f.z;
-                q[j].dot = a.q_idx[T.q0 + qi];
+                q[j].dot = a.q_idx ? a.q_idx[T.q0 + qi] : (int)(T.q0 + qi);
             }
             q[j].mf = INFINITY;
             q[j].thr = MODE == NN_BAND ? band_thr : INFINITY;
@@ -233,10 +233,10 @@ __global__ void __launch_bounds__(NN_T) k_nn(Dev d, NNArgs a)
                         upk2(s23, a2, a3);
                         m0 = fminf(m0, a0); m1 = fminf(m1, a1); m2 = fminf(m2, a2); m3 = fminf(m3, a3);
                     }
-                    if (!q[0].done && m0 <= q[0].thr) nn_rescan<MODE>(d, a, T, q[0], sA, sB, sb, n, rb, E);
-                    if (!q[1].done && m1 <= q[1].thr) nn_rescan<MODE>(d, a, T, q[1], sA, sB, sb, n, rb, E);
-                    if (!q[2].done && m2 <= q[2].thr) nn_rescan<MODE>(d, a, T, q[2], sA, sB, sb, n, rb, E);
-                    if (!q[3].done && m3 <= q[3].thr) nn_rescan<MODE>(d, a, T, q[3], sA, sB, sb, n, rb, E);
+                    if (!q[0].done && m0 <= q[0].thr) nn_rescan<MODE>(a, T, q[0], sA, sB, sb, n, rb, E);
+                    if (!q[1].done && m1 <= q[1].thr) nn_rescan<MODE>(a, T, q[1], sA, sB, sb, n, rb, E);
+                    if (!q[2].done && m2 <= q[2].thr) nn_rescan<MODE>(a, T, q[2], sA, sB, sb, n, rb, E);
+                    if (!q[3].done && m3 <= q[3].thr) nn_rescan<MODE>(a, T, q[3], sA, sB, sb, n, rb, E);
                 }
             }
             if (MODE == NN_BAND) {
@@ -264,15 +264,99 @@ __global__ void k_nn_tiles(NNArgs a)
     }
 }
 
-void launch_nn(const Dev& d, NNArgs a, int mode, long long tile_cap, long long* scan_tmp, cudaStream_t s)
+void launch_nn_tiles(NNArgs a, int mode, long long* scan_tmp, cudaStream_t s)
 {
     a.band_mode = mode == NN_BAND;
     k_nn_tiles<<<grid_for(a.ntask, 128), 128, 0, s>>>(a);
     scan_counts(a.tile_cnt, a.tile_off, a.ntask, scan_tmp, s);
+}
+
+void launch_nn_kernel(NNArgs a, int mode, long long tile_cap, cudaStream_t s)
+{
+    a.band_mode = mode == NN_BAND;
     const unsigned grid = grid_for(tile_cap, 1, 8);   // persistent: at most 8 tiles in flight per SM
-    if (mode == NN_MIN) k_nn<NN_MIN><<<grid, NN_T, 0, s>>>(d, a);
-    else if (mode == NN_ARGMIN) k_nn<NN_ARGMIN><<<grid, NN_T, 0, s>>>(d, a);
-    else k_nn<NN_BAND><<<grid, NN_T, 0, s>>>(d, a);
+    if (mode == NN_MIN) k_nn<NN_MIN><<<grid, NN_T, 0, s>>>(a);
+    else if (mode == NN_ARGMIN) k_nn<NN_ARGMIN><<<grid, NN_T, 0, s>>>(a);
+    else k_nn<NN_BAND><<<grid, NN_T, 0, s>>>(a);
+}
+
+void launch_nn(NNArgs a, int mode, long long tile_cap, long long* scan_tmp, cudaStream_t s)
+{
+    launch_nn_tiles(a, mode, scan_tmp, s);
+    launch_nn_kernel(a, mode, tile_cap, s);
+}
+
+// ---------------------------------------------------------------------------
+// standalone nearest-dot search of two point sets (no batch state)
+// ---------------------------------------------------------------------------
+__global__ void k_points_bbox(const double* q, long long nq, const double* r, long long nr, double* partials)
+{
+    __shared__ double sh[6][32];
+    double v[6] = {INFINITY, INFINITY, INFINITY, INFINITY, INFINITY, INFINITY};   // min xyz, -max xyz
+    const long long n = nq + nr;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double* p = i < nq ? q + 3 * i : r + 3 * (i - nq);
+        for (int k = 0; k < 3; ++k) { v[k] = fmin(v[k], p[k]); v[3 + k] = fmin(v[3 + k], -p[k]); }
+    }
+    for (int k = 0; k < 6; ++k)
+        for (int o = 16; o > 0; o >>= 1) v[k] = fmin(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0) for (int k = 0; k < 6; ++k) sh[k][w] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 6; ++k) {
+            double m = sh[k][0];
+            for (int i = 1; i < nw; ++i) m = fmin(m, sh[k][i]);
+            partials[6 * blockIdx.x + k] = m;
+        }
+    }
+}
+
+// reduce the partial boxes, then the single task covering both sets
+__global__ void k_points_task(const double* partials, int nblocks, long long nq, long long nr, double* bbox,
+                              NNTask* task, int* tile_cnt, long long* tile_off)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double v[6];
+    for (int k = 0; k < 6; ++k) {
+        double m = INFINITY;
+        for (int b = 0; b < nblocks; ++b) m = fmin(m, partials[6 * b + k]);
+        v[k] = m;
+    }
+    double half = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        const double lo = v[k], hi = -v[3 + k];
+        bbox[k] = 0.5 * (lo + hi);
+        half = fmax(half, 0.5 * (hi - lo));
+    }
+    NNTask T;
+    T.q0 = 0; T.qn = nq; T.r0 = 0; T.rn = nr; T.c = 0;
+    T.E = 2.5e-7 * (half + 1.0);
+    task[0] = T;
+    const long long nt = (nq > 0 && nr > 0) ? (nq + NN_TILE - 1) / NN_TILE : 0;
+    tile_cnt[0] = (int)nt;
+    tile_off[0] = 0;
+    tile_off[1] = nt;
+}
+
+__global__ void k_points_pack(const double* q, long long nq, const double* r, long long nr, const double* bbox,
+                              float4* q_f4, float4* r_f4)
+{
+    const long long n = nq + nr;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double* p = i < nq ? q + 3 * i : r + 3 * (i - nq);
+        const float4 f = make_float4((float)(p[0] - bbox[0]), (float)(p[1] - bbox[1]), (float)(p[2] - bbox[2]), 0.f);
+        if (i < nq) q_f4[i] = f; else r_f4[i - nq] = f;
+    }
+}
+
+void launch_points_setup(const double* q, long long nq, const double* r, long long nr, double* partials,
+                         int partial_blocks, double* bbox, float4* q_f4, float4* r_f4, NNTask* task, int* tile_cnt,
+                         long long* tile_off, cudaStream_t s)
+{
+    k_points_bbox<<<partial_blocks, 256, 0, s>>>(q, nq, r, nr, partials);
+    k_points_task<<<1, 32, 0, s>>>(partials, partial_blocks, nq, nr, bbox, task, tile_cnt, tile_off);
+    k_points_pack<<<grid_for(nq + nr, 256), 256, 0, s>>>(q, nq, r, nr, bbox, q_f4, r_f4);
 }
 
 // ---------------------------------------------------------------------------
@@ -285,6 +369,7 @@ __global__ void k_tasks_cms(Dev d, Rd r, NNTask* task)
         const int c = t >> 1, m = t & 1, o = (c * 2) + (1 - m);
         NNTask T;
         T.c = c;
+        T.E = 2.5e-7 * d.cx[c].R;
         T.q0 = r.bur_scan[doff(d, t)];
         T.qn = r.bur_scan[doff(d, t + 1)] - T.q0;
         T.r0 = r.bur_scan[doff(d, o)];
@@ -300,6 +385,7 @@ __global__ void k_tasks_trim(Dev d, Rd r, NNTask* task)
         const long long ds = doff(d, t), de = doff(d, t + 1);
         NNTask T;
         T.c = t >> 1;
+        T.E = 2.5e-7 * d.cx[T.c].R;
         T.q0 = r.bur_scan[ds];
         T.qn = r.bur_scan[de] - T.q0;
         T.r0 = ds - r.bur_scan[ds];
@@ -315,6 +401,7 @@ __global__ void k_tasks_sc(Dev d, Rd r, NNTask* task)
         const int c = t >> 1, m = t & 1, o = (c * 2) + (1 - m);
         NNTask T;
         T.c = c;
+        T.E = 2.5e-7 * d.cx[c].R;
         T.q0 = r.trim_scan[r.bur_scan[doff(d, t)]];
         T.qn = r.trim_scan[r.bur_scan[doff(d, t + 1)]] - T.q0;
         T.r0 = r.trim_scan[r.bur_scan[doff(d, o)]];

@@ -134,6 +134,16 @@ cms_status cms_export_dots(cms_ctx* ctx, int32_t c, int32_t molecule, double* co
 /* local dot indices (within the molecule's dot array) of the SC trimmed dots */
 cms_status cms_export_trimmed(cms_ctx* ctx, int32_t c, int32_t molecule, int32_t* dot_index);
 
+/* Brute-force nearest dot: for each query point (n_query x 3 f64) the
+ * smallest squared distance to the reference points (n_ref x 3 f64) in
+ * scipy cdist 'sqeuclidean' order, and the first reference index attaining
+ * it -- cdist(ref, query).min(axis=0) / .argmin(axis=0), the primitive the
+ * reference calls min_sqdist (cms-cuda/_gpu_kernels.py:508-566).  FP32
+ * filter with an FP64 recheck, so both outputs equal the FP64 search's.
+ * out_index may be NULL.  Uses the context's workspace. */
+cms_status cms_nearest_dots(cms_ctx* ctx, const double* query_xyz, int64_t n_query, const double* ref_xyz,
+                            int64_t n_ref, double* out_d2, int32_t* out_index, int32_t where);
+
 /* Capture the whole pipeline (surfaces + CMS + SC) of the loaded batch shape
  * in a CUDA graph with the current capacities (run it once first), then
  * replay it; later cms_load_batch calls with the same B, N and offsets reuse
