@@ -28,7 +28,7 @@ EXPORTED = (
     "cms_export_probes", "cms_export_dots", "cms_export_trimmed", "cms_run_graph", "cms_kernel_launches",
     "cms_last_error", "cms_version", "cms_device_count", "cms_profile_stages", "cms_stage_name",
     "cms_graph_launch", "cms_graph_check", "cms_nn_work", "cms_transfer_bytes", "cms_fp32_peak",
-    "cms_nearest_dots",
+    "cms_nearest_dots", "cms_nearest_dots_noalloc",
 )
 
 

@@ -144,6 +144,19 @@ cms_status cms_export_trimmed(cms_ctx* ctx, int32_t c, int32_t molecule, int32_t
 cms_status cms_nearest_dots(cms_ctx* ctx, const double* query_xyz, int64_t n_query, const double* ref_xyz,
                             int64_t n_ref, double* out_d2, int32_t* out_index, int32_t where);
 
+/* Allocation-free variant of cms_nearest_dots, for callers that cannot
+ * allocate GPU memory (inside a stream capture or a framework that owns the
+ * allocator, real-time loops, hosted plugins).  This entry point has no
+ * counterpart in the reference.  query_xyz, ref_xyz, out_d2 and out_index
+ * (NULL: no indices) are device pointers; the work is enqueued on `stream`
+ * (NULL: the default stream) and no memory is allocated: the scratch is one
+ * fixed 32 MiB device array per GPU, so n_query + n_ref may not exceed
+ * 2,096,128 points (CMS_ERR_ARG otherwise, nothing launched).  The first call
+ * on a device looks up the scratch address (make it before any stream
+ * capture); calls that overlap on the GPU share the scratch and race. */
+cms_status cms_nearest_dots_noalloc(const double* query_xyz, int64_t n_query, const double* ref_xyz,
+                                    int64_t n_ref, double* out_d2, int32_t* out_index, void* stream);
+
 /* Capture the whole pipeline (surfaces + CMS + SC) of the loaded batch shape
  * in a CUDA graph with the current capacities (run it once first), then
  * replay it; later cms_load_batch calls with the same B, N and offsets reuse
