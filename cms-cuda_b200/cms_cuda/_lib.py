@@ -46,6 +46,7 @@ class ComplexInfo(ctypes.Structure):
         ("n_probes_plus", ctypes.c_int64 * 2), ("n_probes_minus", ctypes.c_int64 * 2),
         ("n_dots", ctypes.c_int64 * 2), ("n_trimmed", ctypes.c_int64 * 2),
         ("convex", ctypes.c_int64), ("toroidal", ctypes.c_int64), ("concave", ctypes.c_int64),
+        ("n_blocked", ctypes.c_int64 * 2), ("n_attended", ctypes.c_int64 * 2),
         ("status", ctypes.c_int32), ("coincident_i", ctypes.c_int32), ("coincident_j", ctypes.c_int32),
         ("radmax", ctypes.c_double),
     ]
@@ -304,6 +305,30 @@ class Context:
         idx = np.empty(n, np.int32)
         self._check(self.lib.cms_export_trimmed(self.h, int(c), int(m), _ptr(idx)))
         return idx[:info.n_trimmed[m]]
+
+
+# Contexts are expensive to create (stream, pinned staging, tens of device
+# buffers) and keep their workspace between runs, so calculators borrow them
+# from a per-thread, per-device pool and hand them back when released -- the
+# role CuPy's per-stream memory pool plays for the reference's GPU calculator.
+_pool = threading.local()
+
+
+def acquire_context(device=0):
+    free = getattr(_pool, "free", None)
+    if free is None:
+        free = _pool.free = {}
+    lst = free.setdefault(int(device), [])
+    return lst.pop() if lst else Context(device)
+
+
+def release_context(ctx, device=0):
+    free = getattr(_pool, "free", None)
+    if free is None:
+        free = _pool.free = {}
+    lst = free.setdefault(int(device), [])
+    if len(lst) < 4:
+        lst.append(ctx)
 
 
 def device_count():

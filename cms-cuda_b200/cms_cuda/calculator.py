@@ -142,6 +142,24 @@ class SimpleNeighborArray:
         return self._cap > 0
 
 
+class _Lease:
+    """
+    A pooled library context borrowed for one generated surface.  The
+    calculator and its ``run`` both hold the lease; the context goes back to
+    the pool when neither needs it any more.
+    """
+
+    def __init__(self, device):
+        self.device = device
+        self.ctx = _lib.acquire_context(device)
+
+    def __del__(self):
+        try:
+            _lib.release_context(self.ctx, self.device)
+        except Exception:
+            pass
+
+
 class _Run:
     """``calc.run``; device state is copied into host containers on first access."""
 
@@ -151,23 +169,78 @@ class _Run:
         self.radmax = 0.0
         self.results = RESULTS()
         self._host = {}
-        self._calc = None
+        self._state = None          # (lease, inputs, n, n0, sc_done) once a surface exists
         self.surfaces_generated = False
         self.surfaces_generated_all_atoms = None
 
     def __getattr__(self, name):
         if name in _Run._LAZY:
-            calc = self.__dict__.get("_calc")
             host = self.__dict__["_host"]
             if name not in host:
-                host[name] = calc._export(name) if calc is not None else _Run._empty(name, self)
+                st = self.__dict__.get("_state")
+                host[name] = _export(self, st, name) if st is not None else _Run._empty(name)
             return host[name]
         raise AttributeError(name)
 
     @staticmethod
-    def _empty(name, run):
+    def _empty(name):
         return {"atoms": AtomArray(0), "dots": [DotArray(), DotArray()], "trimmed_dots": [DotArray(), DotArray()],
                 "probes": ProbeArray(), "neighbor_array": None, "buried_array": None, "toroid_queue": []}[name]
+
+
+def _export(run, st, name):
+    """Host copy of one calc.run container from the device state of the run's surface."""
+    lease, (xyz, rad, dens, mol), n, n0, sc_done = st
+    ctx = lease.ctx
+    if name == "atoms":
+        a = AtomArray(n)
+        a.xyz, a.radius, a.density, a.molecule = xyz, rad, dens, mol
+        atten, access, _, _ = ctx.export_atoms(0, n)
+        a.atten, a.access = atten, access
+        return a
+    info = ctx.info(0)
+    if name in ("neighbor_array", "buried_array"):
+        nb_off, nb_id, bu_off, bu_id = ctx.export_neighbors(0, n, info)
+        off, ids = (nb_off, nb_id) if name == "neighbor_array" else (bu_off, bu_id)
+        cnt = np.diff(off).astype(np.int32)
+        K = max(int(cnt.max()) if len(cnt) and cnt.any() else 1, 1)
+        arr = SimpleNeighborArray(n, K)
+        rows = np.repeat(np.arange(n), cnt)
+        cols = np.arange(len(ids)) - np.repeat(off[:-1], cnt)
+        arr.natom[rows, cols] = ids
+        arr.radius[rows, cols] = rad[ids]
+        arr.xyz[rows, cols] = xyz[ids]
+        arr.nneighbors[:] = cnt
+        return arr
+    if name == "toroid_queue":
+        a1, a2, uij, tij, rij, bet = ctx.export_toroid(0, info)
+        return [(int(a1[k]), int(a2[k]), uij[k], tij[k], float(rij[k]), bool(bet[k])) for k in range(len(a1))]
+    if name == "probes":
+        a0, a1, a2, h, pt, alt = ctx.export_probes(0, info)
+        p = ProbeArray()
+        p.atom_idx_0, p.atom_idx_1, p.atom_idx_2, p.height, p.point_xyz, p.alt_xyz = a0, a1, a2, h, pt, alt
+        return p
+    if name == "dots":
+        out = []
+        for m in (0, 1):
+            d = DotArray()
+            d.coor_xyz, d.outnml_xyz, d.area, d.buried, d.type_, d.atom_idx = ctx.export_dots(0, m, info)
+            out.append(d)
+        return out
+    if name == "trimmed_dots":
+        if not sc_done[0]:
+            return [DotArray(), DotArray()]
+        dots = run.dots
+        out = []
+        for m in (0, 1):
+            idx = ctx.export_trimmed(0, m, info)
+            src = dots[m]
+            t = DotArray()
+            t.coor_xyz, t.outnml_xyz, t.area = src.coor_xyz[idx], src.outnml_xyz[idx], src.area[idx]
+            t.buried, t.type_, t.atom_idx = src.buried[idx], src.type_[idx], src.atom_idx[idx]
+            out.append(t)
+        return out
+    raise AttributeError(name)
 
 
 class MolecularSurfaceCalculator:
@@ -182,12 +255,13 @@ class MolecularSurfaceCalculator:
         self.settings.binwidth_dist = 0.02
         self.settings.binwidth_norm = 0.02
         self._device = device
-        self._ctx = None
         self.reset()
 
     # -- loading ---------------------------------------------------------------
     def reset(self):
+        # a previous run keeps its own lease (and so its device state)
         self.run = _Run()
+        self._lease = None
         self._xyz = []
         self._rad = []
         self._dens = []
@@ -195,7 +269,6 @@ class MolecularSurfaceCalculator:
         self._cms = None
         self._sc = None
         self._max = None
-        self._trim = None
 
     def add_binder_and_target(self, binder_xyz, binder_radii, target_xyz, target_radii):
         self.reset()
@@ -238,9 +311,9 @@ class MolecularSurfaceCalculator:
 
     # -- generation --------------------------------------------------------------
     def _context(self):
-        if self._ctx is None:
-            self._ctx = _lib.Context(self._device)
-        return self._ctx
+        if self._lease is None:
+            self._lease = _Lease(self._device)
+        return self._lease.ctx
 
     def _ensure_surfaces_generated(self, all_atoms=False):
         if self.run.surfaces_generated:
@@ -270,22 +343,18 @@ class MolecularSurfaceCalculator:
             raise RuntimeError("too many nearby low probes for one probe (limit 512)")
         self._n = len(rad)
         self._n0 = n0
-        self._inputs = (xyz, rad, dens, mol)
-        self._info = info
-        self.run._calc = self
+        self._sc_done = [False]
+        self.run._state = (self._lease, (xyz, rad, dens, mol), len(rad), n0, self._sc_done)
         self.run.radmax = np.float64(rad.max())
         r = self.run.results
         r.dots.convex += int(info.convex)
         r.dots.toroidal += int(info.toroidal)
         r.dots.concave += int(info.concave)
-        atten = self.run.atoms.atten
         for m in (0, 1):
-            sel = mol == m
-            if all_atoms:
-                r.surface[m].nBuriedAtoms += int(sel.sum())
-            else:
-                r.surface[m].nBlockedAtoms += int((atten[sel] == ATTEN_BLOCKER).sum())
-                r.surface[m].nBuriedAtoms += int((atten[sel] != ATTEN_BLOCKER).sum())
+            # assign_attention_numbers' counters (_core.py:1160-1193)
+            if not all_atoms:
+                r.surface[m].nBlockedAtoms += int(info.n_blocked[m])
+            r.surface[m].nBuriedAtoms += int(info.n_attended[m])
         self.run.surfaces_generated = True
         self.run.surfaces_generated_all_atoms = all_atoms
 
@@ -324,6 +393,7 @@ class MolecularSurfaceCalculator:
         self._ensure_surfaces_generated(all_atoms=False)
         if self._sc is None:
             self._sc = self._context().shape_complementarity()
+            self._sc_done[0] = True
             self.run._host.pop("trimmed_dots", None)
         sc, sides = self._sc
         res = self.run.results
@@ -347,66 +417,6 @@ class MolecularSurfaceCalculator:
         res.area = s2.trimmedArea
         res.valid = 1
         return res.sc, res.area, res.distance
-
-    # -- host mirror of calc.run ------------------------------------------------
-    def _export(self, name):
-        ctx = self._context()
-        n = self._n
-        xyz, rad, dens, mol = self._inputs
-        if name == "atoms":
-            a = AtomArray(n)
-            a.xyz, a.radius, a.density, a.molecule = xyz, rad, dens, mol
-            atten, access, nn, nb = ctx.export_atoms(0, n)
-            a.atten, a.access = atten, access
-            self._nn, self._nb = nn, nb
-            return a
-        if name in ("neighbor_array", "buried_array"):
-            info = ctx.info(0)
-            nb_off, nb_id, bu_off, bu_id = ctx.export_neighbors(0, n, info)
-            off, ids = (nb_off, nb_id) if name == "neighbor_array" else (bu_off, bu_id)
-            cnt = np.diff(off).astype(np.int32)
-            K = max(int(cnt.max()) if len(cnt) and cnt.any() else 1, 1)
-            arr = SimpleNeighborArray(n, K)
-            rows = np.repeat(np.arange(n), cnt)
-            cols = np.arange(len(ids)) - np.repeat(off[:-1], cnt)
-            arr.natom[rows, cols] = ids
-            arr.radius[rows, cols] = rad[ids]
-            arr.xyz[rows, cols] = xyz[ids]
-            arr.nneighbors[:] = cnt
-            return arr
-        if name == "toroid_queue":
-            info = ctx.info(0)
-            a1, a2, uij, tij, rij, bet = ctx.export_toroid(0, info)
-            return [(int(a1[k]), int(a2[k]), uij[k], tij[k], float(rij[k]), bool(bet[k])) for k in range(len(a1))]
-        if name == "probes":
-            info = ctx.info(0)
-            a0, a1, a2, h, pt, alt = ctx.export_probes(0, info)
-            p = ProbeArray()
-            p.atom_idx_0, p.atom_idx_1, p.atom_idx_2, p.height, p.point_xyz, p.alt_xyz = a0, a1, a2, h, pt, alt
-            return p
-        if name == "dots":
-            info = ctx.info(0)
-            out = []
-            for m in (0, 1):
-                d = DotArray()
-                d.coor_xyz, d.outnml_xyz, d.area, d.buried, d.type_, d.atom_idx = ctx.export_dots(0, m, info)
-                out.append(d)
-            return out
-        if name == "trimmed_dots":
-            if self._sc is None:
-                return [DotArray(), DotArray()]
-            info = ctx.info(0)
-            dots = self.run.dots
-            out = []
-            for m in (0, 1):
-                idx = ctx.export_trimmed(0, m, info)
-                src = dots[m]
-                t = DotArray()
-                t.coor_xyz, t.outnml_xyz, t.area = src.coor_xyz[idx], src.outnml_xyz[idx], src.area[idx]
-                t.buried, t.type_, t.atom_idx = src.buried[idx], src.type_[idx], src.atom_idx[idx]
-                out.append(t)
-            return out
-        raise AttributeError(name)
 
 
 MolecularSurfaceCalculatorGPU = MolecularSurfaceCalculator

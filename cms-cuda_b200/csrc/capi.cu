@@ -81,6 +81,79 @@ __global__ void k_export_toroid(Dev d, long long q0, long long n, double* out)
     }
 }
 
+// per-complex sizes, counters and status (one block per complex)
+__global__ void k_complex_info(Dev d, Rd r, int want_sc, cms_complex_info* out)
+{
+    __shared__ long long sh[6][32];
+    const int c = blockIdx.x;
+    const Cplx C = d.cx[c];
+    const int a0 = C.a0, s1 = C.a0 + C.n0, a1 = C.a0 + C.n;
+    long long v[6] = {1, 1, 0, 0, 0, 0};   // max nb, max bu, blocked0, blocked1, attended0, attended1
+    for (int g = a0 + threadIdx.x; g < a1; g += blockDim.x) {
+        v[0] = max(v[0], (long long)d.nnb[g]);
+        v[1] = max(v[1], (long long)d.nbur[g]);
+        const int m = g < s1 ? 0 : 1;
+        if (d.atten[g] == 1) ++v[2 + m]; else ++v[4 + m];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        v[0] = max(v[0], __shfl_xor_sync(0xffffffffu, v[0], o));
+        v[1] = max(v[1], __shfl_xor_sync(0xffffffffu, v[1], o));
+        for (int k = 2; k < 6; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0) for (int k = 0; k < 6; ++k) sh[k][w] = v[k];
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int i = 1; i < nw; ++i) {
+        v[0] = max(v[0], sh[0][i]);
+        v[1] = max(v[1], sh[1][i]);
+        for (int k = 2; k < 6; ++k) v[k] += sh[k][i];
+    }
+    cms_complex_info I;
+    memset(&I, 0, sizeof(I));
+    I.n_atoms = C.n;
+    I.n_binder = C.n0;
+    I.nb_entries = d.nb_off[a1] - d.nb_off[a0];
+    I.bu_entries = d.bu_off[a1] - d.bu_off[a0];
+    I.max_nb = v[0];
+    I.max_bu = v[1];
+    I.n_toroid = d.tor_off[a1] - d.tor_off[a0];
+    I.n_probes_plus[0] = d.plus_off[s1] - d.plus_off[a0];
+    I.n_probes_plus[1] = d.plus_off[a1] - d.plus_off[s1];
+    I.n_probes_minus[0] = d.minus_off[s1] - d.minus_off[a0];
+    I.n_probes_minus[1] = d.minus_off[a1] - d.minus_off[s1];
+    I.n_probes = I.n_probes_plus[0] + I.n_probes_plus[1] + I.n_probes_minus[0] + I.n_probes_minus[1];
+    long long cnt[4] = {0, 0, 0, 0};
+    for (int m = 0; m < 2; ++m) {
+        const long long ds = d.dot_off[2 * c + m], de = d.dot_off[2 * c + m + 1];
+        I.n_dots[m] = de - ds;
+        for (int t = 0; t < 4; ++t) {
+            const long long e = t < 3 ? d.seg[(c * 2 + m) * 4 + t + 1].dot0 : de;
+            cnt[t] += e - d.seg[(c * 2 + m) * 4 + t].dot0;
+        }
+        if (want_sc) {
+            const long long bs = r.bur_scan[ds], be = r.bur_scan[de];
+            I.n_trimmed[m] = r.trim_scan[be] - r.trim_scan[bs];
+        }
+        I.n_blocked[m] = v[2 + m];
+        I.n_attended[m] = v[4 + m];
+    }
+    I.convex = cnt[0];
+    I.toroidal = cnt[1] + cnt[2];
+    I.concave = cnt[3];
+    I.status = d.status[c];
+    const unsigned long long k = d.coin[c];
+    if (k != ~0ull) {
+        I.status |= ST_COINCIDENT;
+        I.coincident_i = (int32_t)(k >> 32);
+        I.coincident_j = (int32_t)(k & 0xffffffffu);
+    } else {
+        I.coincident_i = I.coincident_j = -1;
+    }
+    I.radmax = C.radmax;
+    out[c] = I;
+}
+
 // FP32 FMA throughput probe: 8 independent FMA chains per thread, the result
 // folded into one store so nothing is optimised away
 __global__ void __launch_bounds__(256) k_fp32_peak(float* out, int iters, float a, float b)
@@ -120,6 +193,8 @@ struct cms_ctx {
     std::vector<unsigned long long> h_coin;
     std::vector<Seg> h_seg;
     std::vector<double> h_radmax;
+    std::vector<cms_complex_info> h_info;   // per-complex info table of the last run
+    int info_state = 0;                      // 0 stale, 1 computed before SC, 2 with SC counts
     // graph
     cudaGraphExec_t gexec = nullptr;
     cudaGraph_t graph = nullptr;
@@ -146,7 +221,7 @@ struct cms_ctx {
         S_R_TRIM_IDX, S_R_TRIM_F4, S_R_NN_D2, S_R_NN_IDX, S_R_VAL, S_R_OWN, S_R_ACNT, S_R_AFILL, S_R_AOFF, S_R_ASLOT,
         S_CM_TMP, S_SCAN_TMP, S_PER_ATOM_CMS, S_TOT_CMS, S_PER_ATOM_MAX, S_TOT_MAX, S_SC_SIDE, S_SC_OUT, S_TASKS,
         S_TILE_CNT, S_TILE_OFF, S_SUMMARY, S_EXPORT,
-        S_NN_Q, S_NN_R, S_NN_QF4, S_NN_RF4, S_NN_PART, S_NN_BBOX, S_NN_TASK, S_NN_TCNT, S_NN_TOFF, S_NN_D2, S_NN_IDX,
+        S_NN_Q, S_NN_R, S_NN_QF4, S_NN_RF4, S_NN_PART, S_NN_BBOX, S_NN_TASK, S_NN_TCNT, S_NN_TOFF, S_NN_D2, S_NN_IDX, S_INFO,
         S_COUNT
     };
 
@@ -483,6 +558,7 @@ void enqueue_sc(cms_ctx* x)
     a.q_xyz = a.r_xyz = d.dxyz;
     a.out_flag = r.keep;
     a.band_thr64 = x->st.band * x->st.band;
+    a.hint_scan = r.bur_scan;
     launch_nn(a, NN_BAND, tile_cap(x), tmp, s);
     mark(x, P_SC_BAND_NN);
     launch_trim_compact(d, r, x->cap_dot, tmp, s);
@@ -536,6 +612,7 @@ void pull_host_state(cms_ctx* x)
     x->d2h_bytes += 8 * (long long)sizeof(long long) + (long long)B * (sizeof(int) + sizeof(unsigned long long) +
                     8 * sizeof(Seg) + sizeof(Cplx)) + (2LL * B + 1) * (long long)sizeof(long long);
     for (int k = 0; k < 6; ++k) x->tot[k] = x->pinned[k];
+    x->info_state = 0;
     x->h_radmax.resize(B);
     for (int c = 0; c < B; ++c) x->h_radmax[c] = cx[c].radmax;
     (void)N;
@@ -795,50 +872,18 @@ cms_status cms_complex_info_get(cms_ctx* x, int32_t c, cms_complex_info* info)
     if (!x || !info) return fail(x, CMS_ERR_ARG, "null argument");
     API_BEGIN
     check_complex(x, c);
-    cms_complex_info I;
-    std::memset(&I, 0, sizeof(I));
-    const long long a0 = x->h_off[c], a1 = x->h_off[c + 1], s1 = a0 + x->h_n0[c];
-    I.n_atoms = a1 - a0;
-    I.n_binder = x->h_n0[c];
-    I.nb_entries = host_ll(x, x->d.nb_off + a1) - host_ll(x, x->d.nb_off + a0);
-    I.bu_entries = host_ll(x, x->d.bu_off + a1) - host_ll(x, x->d.bu_off + a0);
-    std::vector<int> nn(I.n_atoms), nb(I.n_atoms);
-    ck(cudaMemcpy(nn.data(), x->d.nnb + a0, sizeof(int) * I.n_atoms, cudaMemcpyDeviceToHost), "copy");
-    ck(cudaMemcpy(nb.data(), x->d.nbur + a0, sizeof(int) * I.n_atoms, cudaMemcpyDeviceToHost), "copy");
-    I.max_nb = 1; I.max_bu = 1;
-    for (long long i = 0; i < I.n_atoms; ++i) { I.max_nb = std::max<int64_t>(I.max_nb, nn[i]); I.max_bu = std::max<int64_t>(I.max_bu, nb[i]); }
-    I.n_toroid = host_ll(x, x->d.tor_off + a1) - host_ll(x, x->d.tor_off + a0);
-    const long long p0 = host_ll(x, x->d.plus_off + a0), p1 = host_ll(x, x->d.plus_off + s1), p2 = host_ll(x, x->d.plus_off + a1);
-    const long long m0 = host_ll(x, x->d.minus_off + a0), m1 = host_ll(x, x->d.minus_off + s1), m2 = host_ll(x, x->d.minus_off + a1);
-    I.n_probes_plus[0] = p1 - p0; I.n_probes_plus[1] = p2 - p1;
-    I.n_probes_minus[0] = m1 - m0; I.n_probes_minus[1] = m2 - m1;
-    I.n_probes = (p2 - p0) + (m2 - m0);
-    for (int m = 0; m < 2; ++m) I.n_dots[m] = x->h_dot_off[2 * c + m + 1] - x->h_dot_off[2 * c + m];
-    long long cnt[4] = {0, 0, 0, 0};
-    for (int m = 0; m < 2; ++m)
-        for (int t = 0; t < 4; ++t) {
-            long long e = t < 3 ? x->h_seg[(c * 2 + m) * 4 + t + 1].dot0 : x->h_dot_off[2 * c + m + 1];
-            cnt[t] += e - x->h_seg[(c * 2 + m) * 4 + t].dot0;
-        }
-    I.convex = cnt[0]; I.toroidal = cnt[1] + cnt[2]; I.concave = cnt[3];
-    if (x->sc_ok) {
-        for (int m = 0; m < 2; ++m) {
-            long long ds = x->h_dot_off[2 * c + m], de = x->h_dot_off[2 * c + m + 1];
-            long long bs = host_ll(x, x->r.bur_scan + ds), be = host_ll(x, x->r.bur_scan + de);
-            I.n_trimmed[m] = host_ll(x, x->r.trim_scan + be) - host_ll(x, x->r.trim_scan + bs);
-        }
+    // the whole table is computed on the device once per run (one kernel, one copy)
+    const int want_sc = x->sc_ok ? 1 : 0;
+    if (x->info_state != (x->sc_ok ? 2 : 1)) {
+        cms_complex_info* dinfo = x->ensure<cms_complex_info>(cms_ctx::S_INFO, x->B);
+        k_complex_info<<<x->B, 256, 0, x->stream>>>(x->d, x->r, want_sc, dinfo);
+        x->h_info.resize(x->B);
+        ck(cudaMemcpyAsync(x->h_info.data(), dinfo, sizeof(cms_complex_info) * x->B, cudaMemcpyDeviceToHost,
+                           x->stream), "info");
+        ck(cudaStreamSynchronize(x->stream), "sync");
+        x->info_state = x->sc_ok ? 2 : 1;
     }
-    I.status = x->h_status[c];
-    unsigned long long k = x->h_coin[c];
-    if (k != ~0ull) {
-        I.status |= ST_COINCIDENT;
-        I.coincident_i = (int32_t)(k >> 32);
-        I.coincident_j = (int32_t)(k & 0xffffffffu);
-    } else {
-        I.coincident_i = I.coincident_j = -1;
-    }
-    I.radmax = x->h_radmax[c];
-    *info = I;
+    *info = x->h_info[c];
     API_END
 }
 

@@ -27,6 +27,10 @@ struct NNArgs {
     const double* q_xyz; const double* r_xyz;   // FP64 coordinates for the recheck
     double* out_d2; int* out_idx; int* out_flag;
     double band_thr64;      // band^2 (BAND mode)
+    // BAND mode scan order hint: references are the non-buried dots of the
+    // query's dot range, and hint_scan is the buried-dot exclusive scan, so
+    // dot - hint_scan[dot] is the reference position next to a query dot
+    const long long* hint_scan;
     int band_mode;
 };
 

@@ -91,17 +91,27 @@ void launch_split_buried(const Dev& d, const Rd& r, long long dot_cap, long long
 // ---------------------------------------------------------------------------
 // brute-force nearest-dot search, FP32 filter + FP64 recheck
 // ---------------------------------------------------------------------------
-// Error model (u = 2^-24): coordinates relative to the centre are within R of
-// it per axis.  For any pair, |sqrt(D32) - sqrt(D)| <= E + rho*sqrt(D) with
-// E = 3.53 u R and rho = 2.7 u (input rounding of both points, the rounded
-// difference and the three-term FP32 sum).  A reference that attains the
-// FP64 minimum therefore has sqrt(D32) <= (sqrt(m) + E)(1 + 3 rho) + E,
-// m = smallest D32 seen; the kernel rechecks everything under that bound.
-__device__ __forceinline__ float nn_threshold(float m, double E)
+// Formulation.  Each tile of queries is staged relative to its own centre c
+// (FP32): q' = q - c, r' = r - c, with rho bounding |q'| over the tile.  The
+// search minimises s(r) = |r'|^2 - 2 q'.r' (three FMAs per pair) and
+// d32 = s + |q'|^2 approximates the squared distance.  Error bound
+// (u = 2^-24; d the distance, so |r'| <= rho + d):
+//   FMA chain and |r'|^2      <= 5u((rho+d)^2 + 2 rho (rho+d))
+//   |q'|^2 and the final add  <= 3u rho^2 + u d^2-scale terms
+//   shifting by c in FP32     moves the distance by <= 2u(2 rho + d)
+//   the points' FP32 rounding relative to the task centre moves it by <= E0
+// so with t = rho + sqrt(D) + 1 the absolute error of d32 is at most
+//   eps(D) = 20 u t^2 + 2 (sqrt(D) + 1)(E0 + 4 u t) + (E0 + 4 u t)^2.
+// A reference attaining the FP64 minimum has d32 <= m + 2 eps(m) (m = the
+// smallest d32 seen); one within the band has d32 <= band^2 + eps(band^2).
+// Every reference under those thresholds is rechecked in FP64 in cdist order.
+__device__ __forceinline__ double nn_eps(double m, double rho, double E0)
 {
-    if (!(m < INFINITY)) return INFINITY;
-    double t = (sqrt((double)m) + E) * (1.0 + 1e-6) + E;
-    return __double2float_ru(t * t * (1.0 + 1e-6));
+    const double u = 5.9604644775390625e-08;
+    const double sm = sqrt(fmax(m, 0.0));
+    const double t = rho + sm + 1.0;
+    const double e = E0 + 4.0 * u * t;
+    return 20.0 * u * t * t + 2.0 * (sm + 1.0) * e + e * e;
 }
 
 __device__ __forceinline__ double exact_d2(const double* a, const double* b)
@@ -112,19 +122,22 @@ __device__ __forceinline__ double exact_d2(const double* a, const double* b)
 }
 
 // Packed FP32 pairs (Blackwell f32x2 arithmetic): one instruction does the
-// same IEEE round-to-nearest operation on two lanes, so the packed distances
-// equal the scalar ones bit for bit.
+// same IEEE round-to-nearest operation on two lanes, so packed results equal
+// the scalar ones bit for bit.
 typedef unsigned long long f2_t;
 __device__ __forceinline__ f2_t pk2(float a, float b) { f2_t r; asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b)); return r; }
 __device__ __forceinline__ void upk2(f2_t v, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
-__device__ __forceinline__ f2_t sub2(f2_t a, f2_t b) { f2_t r; asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b)); return r; }
-__device__ __forceinline__ f2_t mul2(f2_t a, f2_t b) { f2_t r; asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b)); return r; }
 __device__ __forceinline__ f2_t fma2(f2_t a, f2_t b, f2_t c) { f2_t r; asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c)); return r; }
 
-__device__ __forceinline__ float d2_f32(float rx, float ry, float rz, float qx, float qy, float qz)
+// s(r) for one query: |r|^2 - 2 q.r as three FMAs (the packed loop's order)
+__device__ __forceinline__ float nn_s(float qx2, float qy2, float qz2, float rx, float ry, float rz, float rr)
 {
-    const float dx = rx - qx, dy = ry - qy, dz = rz - qz;
-    return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, dx * dx));
+    return __fmaf_rn(qz2, rz, __fmaf_rn(qy2, ry, __fmaf_rn(qx2, rx, rr)));
+}
+
+__device__ __forceinline__ float nn_rr(float rx, float ry, float rz)
+{
+    return __fmaf_rn(rz, rz, __fmaf_rn(ry, ry, rx * rx));
 }
 
 static constexpr int NN_T = 128;              // threads per tile
@@ -135,31 +148,78 @@ static constexpr int NN_SUB = 32;             // references per threshold check
 
 // one query's state
 struct NNQ {
-    float qx, qy, qz;
-    int dot;            // dot index of the query (its FP64 coordinates are read on recheck)
-    float mf, thr;
+    float qx2, qy2, qz2;  // -2 q
+    double qq;            // |q|^2 (FP32 value, held in FP64)
+    int dot;              // index of the query point (FP64 coordinates read on recheck)
+    float ms;             // smallest s seen
+    float ts;             // s threshold: candidates have s <= ts (tile-relative)
     double best;
     int bidx;
     bool live, done;
 };
 
-// re-examine references [k0, k0+n) of the staged round for one query whose
-// block minimum fell under its threshold: FP32 filter, FP64 recheck in order
-template <int MODE>
-__device__ __forceinline__ void nn_rescan(const NNArgs& a, const NNTask& T, NNQ& q, const float4* sA,
-                                          const float2* sB, int k0, int n, long long rb, double E)
+struct NNTile {
+    float cx, cy, cz;     // tile centre
+    double rho, E0;       // bound on |q'|, FP32 rounding of the staged points
+};
+
+__device__ __forceinline__ float nn_s_threshold(const NNQ& q, const NNTile& t)
 {
-    for (int k = k0; k < k0 + n; ++k) {
-        const float d2 = d2_f32(sA[k].x, sA[k].z, sB[k].x, q.qx, q.qy, q.qz);
-        if (d2 <= q.thr) {
-            const long long rk = T.r0 + rb + k;
-            const double* rp = a.r_xyz + 3LL * (a.r_idx ? a.r_idx[rk] : rk);
-            const double e = exact_d2(rp, a.q_xyz + 3LL * q.dot);
-            if (MODE == NN_BAND) {
-                if (e <= a.band_thr64) { q.done = true; q.best = e; return; }
-            } else {
-                if (e < q.best) { q.best = e; q.bidx = (int)(rb + k); }
-                if (d2 < q.mf) { q.mf = d2; q.thr = nn_threshold(q.mf, E); }
+    if (!(q.ms < INFINITY)) return INFINITY;
+    const double m = (double)q.ms + q.qq;
+    const double th = m + 2.0 * nn_eps(m, t.rho, t.E0) * 1.01;
+    return __double2float_ru(th - q.qq);
+}
+
+// Re-examine a block of n (<= 32) staged references [k0, k0+n) for every
+// (lane, query) of the warp whose block minimum fell under its threshold.
+// The warp takes the flagged lanes one at a time and checks the block in
+// parallel, one reference per lane: FP32 filter against the lane's threshold
+// at block start (a superset of what a sequential scan would recheck), FP64
+// recheck in cdist order, then a warp reduction to the smallest FP64 value
+// and, on ties, the smallest reference index -- what an in-order scan keeps.
+template <int MODE>
+__device__ __forceinline__ void nn_rescan_warp(const NNArgs& a, const NNTask& T, NNQ& q, unsigned need,
+                                               const float4* sA, const float4* sB, int k0, int n, long long rb,
+                                               const NNTile& tl)
+{
+    const int lane = threadIdx.x & 31;
+    while (need) {
+        const int L = __ffs(need) - 1;
+        need &= need - 1;
+        const float qx2 = __shfl_sync(0xffffffffu, q.qx2, L);
+        const float qy2 = __shfl_sync(0xffffffffu, q.qy2, L);
+        const float qz2 = __shfl_sync(0xffffffffu, q.qz2, L);
+        const float ts = __shfl_sync(0xffffffffu, q.ts, L);
+        const int qdot = __shfl_sync(0xffffffffu, q.dot, L);
+        double e = INFINITY;
+        float sv = INFINITY;
+        int idx = 0x7fffffff;
+        if (lane < n) {
+            const int k = k0 + lane;
+            const float v = nn_s(qx2, qy2, qz2, sA[k].x, sA[k].z, sB[k].x, sB[k].z);
+            if (v <= ts) {
+                const long long rk = T.r0 + rb + k;
+                const double* rp = a.r_xyz + 3LL * (a.r_idx ? a.r_idx[rk] : rk);
+                e = exact_d2(rp, a.q_xyz + 3LL * qdot);
+                sv = v;
+                idx = (int)(rb + k);
+            }
+        }
+        if (MODE == NN_BAND) {
+            const bool hit = __any_sync(0xffffffffu, e <= a.band_thr64);
+            if (lane == L && hit) q.done = true;
+        } else {
+            for (int o = 16; o > 0; o >>= 1) {
+                const double e2 = __shfl_xor_sync(0xffffffffu, e, o);
+                const int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
+                const float v2 = __shfl_xor_sync(0xffffffffu, sv, o);
+                if (e2 < e || (e2 == e && i2 < idx)) { e = e2; idx = i2; }
+                sv = fminf(sv, v2);
+            }
+            if (lane == L) {
+                if (e < q.best) { q.best = e; q.bidx = idx; }
+                if (sv < q.ms) { q.ms = sv; q.ts = nn_s_threshold(q, tl); }
             }
         }
     }
@@ -169,7 +229,8 @@ template <int MODE>
 __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
 {
     __shared__ float4 sA[NN_R];   // (x, x, y, y)
-    __shared__ float2 sB[NN_R];   // (z, z)
+    __shared__ float4 sB[NN_R];   // (z, z, |r|^2, |r|^2)
+    const int lane = threadIdx.x & 31;
     const long long ntiles = a.tile_off[a.ntask];
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         int lo = 0, hi = a.ntask - 1;
@@ -179,42 +240,111 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
         }
         const NNTask T = a.task[lo];
         const long long qb = (tile - a.tile_off[lo]) * NN_TILE + threadIdx.x;
-        const double E = T.E;
-        float band_thr = INFINITY;
-        if (MODE == NN_BAND) {
-            double t = (sqrt(a.band_thr64) * (1.0 + 1e-6)) + E;
-            band_thr = __double2float_ru(t * t * (1.0 + 1e-6));
-        }
+        // queries of the tile, then the tile centre and radius
         NNQ q[NN_Q];
+        float qx[NN_Q], qy[NN_Q], qz[NN_Q];
+        float lo3[3] = {INFINITY, INFINITY, INFINITY}, hi3[3] = {-INFINITY, -INFINITY, -INFINITY};
 #pragma unroll
         for (int j = 0; j < NN_Q; ++j) {
             const long long qi = qb + (long long)j * NN_T;
             q[j].live = qi < T.qn;
-            q[j].qx = q[j].qy = q[j].qz = 0.f;
+            qx[j] = qy[j] = qz[j] = 0.f;
             q[j].dot = 0;
             if (q[j].live) {
                 const float4 f = a.q_f4[T.q0 + qi];
-                q[j].qx = f.x; q[j].qy = f.y; q[j].qz = f.z;
+                qx[j] = f.x; qy[j] = f.y; qz[j] = f.z;
                 q[j].dot = a.q_idx ? a.q_idx[T.q0 + qi] : (int)(T.q0 + qi);
+                lo3[0] = fminf(lo3[0], f.x); lo3[1] = fminf(lo3[1], f.y); lo3[2] = fminf(lo3[2], f.z);
+                hi3[0] = fmaxf(hi3[0], f.x); hi3[1] = fmaxf(hi3[1], f.y); hi3[2] = fmaxf(hi3[2], f.z);
             }
-            q[j].mf = INFINITY;
-            q[j].thr = MODE == NN_BAND ? band_thr : INFINITY;
+        }
+        __shared__ float sbox[6][NN_T / 32];
+        __shared__ double srho[NN_T / 32];
+        for (int k = 0; k < 3; ++k) {
+            for (int o = 16; o > 0; o >>= 1) {
+                lo3[k] = fminf(lo3[k], __shfl_xor_sync(0xffffffffu, lo3[k], o));
+                hi3[k] = fmaxf(hi3[k], __shfl_xor_sync(0xffffffffu, hi3[k], o));
+            }
+        }
+        if (lane == 0) for (int k = 0; k < 3; ++k) { sbox[k][threadIdx.x >> 5] = lo3[k]; sbox[3 + k][threadIdx.x >> 5] = hi3[k]; }
+        __syncthreads();
+        NNTile tl;
+        {
+            float c3[3];
+            for (int k = 0; k < 3; ++k) {
+                float l = sbox[k][0], h = sbox[3 + k][0];
+                for (int w = 1; w < NN_T / 32; ++w) { l = fminf(l, sbox[k][w]); h = fmaxf(h, sbox[3 + k][w]); }
+                c3[k] = (l <= h) ? 0.5f * (l + h) : 0.f;
+            }
+            tl.cx = c3[0]; tl.cy = c3[1]; tl.cz = c3[2];
+        }
+        double rho = 0.0;
+#pragma unroll
+        for (int j = 0; j < NN_Q; ++j) {
+            qx[j] -= tl.cx; qy[j] -= tl.cy; qz[j] -= tl.cz;
+            if (q[j].live) rho = fmax(rho, sqrt((double)qx[j] * qx[j] + (double)qy[j] * qy[j] + (double)qz[j] * qz[j]));
+        }
+        for (int o = 16; o > 0; o >>= 1) rho = fmax(rho, __shfl_xor_sync(0xffffffffu, rho, o));
+        if (lane == 0) srho[threadIdx.x >> 5] = rho;
+        __syncthreads();
+        for (int w = 0; w < NN_T / 32; ++w) rho = fmax(rho, srho[w]);
+        __syncthreads();
+        tl.rho = rho * (1.0 + 1e-6) + 1e-6;
+        tl.E0 = T.E;
+#pragma unroll
+        for (int j = 0; j < NN_Q; ++j) {
+            q[j].qx2 = -2.0f * qx[j]; q[j].qy2 = -2.0f * qy[j]; q[j].qz2 = -2.0f * qz[j];
+            q[j].qq = (double)nn_rr(qx[j], qy[j], qz[j]);
+            q[j].ms = INFINITY;
             q[j].best = INFINITY;
             q[j].bidx = -1;
             q[j].done = !q[j].live;
+            if (MODE == NN_BAND) {
+                const double t = a.band_thr64 + nn_eps(a.band_thr64, tl.rho, tl.E0) * 1.01;
+                q[j].ts = __double2float_ru(t - q[j].qq);
+            } else {
+                q[j].ts = INFINITY;
+                if (q[j].live && T.rn > 0) {
+                    // seed with reference 0 (the first index, so ties keep it)
+                    const long long r0 = a.r_idx ? a.r_idx[T.r0] : T.r0;
+                    const float4 f = a.r_f4[T.r0];
+                    const float rx = f.x - tl.cx, ry = f.y - tl.cy, rz = f.z - tl.cz;
+                    q[j].best = exact_d2(a.r_xyz + 3LL * r0, a.q_xyz + 3LL * q[j].dot);
+                    q[j].bidx = 0;
+                    q[j].ms = nn_s(q[j].qx2, q[j].qy2, q[j].qz2, rx, ry, rz, nn_rr(rx, ry, rz));
+                    q[j].ts = nn_s_threshold(q[j], tl);
+                }
+            }
         }
-        const f2_t qx01 = pk2(q[0].qx, q[1].qx), qy01 = pk2(q[0].qy, q[1].qy), qz01 = pk2(q[0].qz, q[1].qz);
-        const f2_t qx23 = pk2(q[2].qx, q[3].qx), qy23 = pk2(q[2].qy, q[3].qy), qz23 = pk2(q[2].qz, q[3].qz);
-        for (long long rb = 0; rb < T.rn; rb += NN_R) {
-            const int nr = (int)min((long long)NN_R, T.rn - rb);
+        const f2_t qx01 = pk2(q[0].qx2, q[1].qx2), qy01 = pk2(q[0].qy2, q[1].qy2), qz01 = pk2(q[0].qz2, q[1].qz2);
+        const f2_t qx23 = pk2(q[2].qx2, q[3].qx2), qy23 = pk2(q[2].qy2, q[3].qy2), qz23 = pk2(q[2].qz2, q[3].qz2);
+        // Order of the reference rounds.  The minimum searches go in index order
+        // (first index wins ties).  The band test only asks whether ANY reference
+        // is within the band, so it starts at the references that sit next to the
+        // tile's first query in dot order (usually its own surface patch) and
+        // wraps around: every pair is still examined unless a hit ends the scan.
+        long long rb_start = 0;
+        if (MODE == NN_BAND && a.hint_scan && T.rn > NN_R) {
+            const long long first = T.q0 + (tile - a.tile_off[lo]) * NN_TILE;
+            const long long dot = a.q_idx ? a.q_idx[first] : first;
+            const long long pos = (dot - a.hint_scan[dot]) - T.r0 - NN_R / 2;
+            rb_start = pos < 0 ? 0 : (pos >= T.rn ? T.rn - 1 : pos);
+        }
+        for (long long seen = 0; seen < T.rn;) {
+            const long long rb = (rb_start + seen) % T.rn;
+            const int nr = (int)min(min((long long)NN_R, T.rn - seen), T.rn - rb);
+            seen += nr;
             __syncthreads();
             for (int k = threadIdx.x; k < nr; k += NN_T) {
                 const float4 r = a.r_f4[T.r0 + rb + k];
-                sA[k] = make_float4(r.x, r.x, r.y, r.y);
-                sB[k] = make_float2(r.z, r.z);
+                const float rx = r.x - tl.cx, ry = r.y - tl.cy, rz = r.z - tl.cz;
+                const float rr = nn_rr(rx, ry, rz);
+                sA[k] = make_float4(rx, rx, ry, ry);
+                sB[k] = make_float4(rz, rz, rr, rr);
             }
             __syncthreads();
-            const bool all_done = q[0].done && q[1].done && q[2].done && q[3].done;
+            // warp-uniform: the block loop below uses full-warp ballots and shuffles
+            const bool all_done = __all_sync(0xffffffffu, q[0].done && q[1].done && q[2].done && q[3].done);
             if (!all_done) {
                 for (int sb = 0; sb < nr; sb += NN_SUB) {
                     const int n = min(NN_SUB, nr - sb);
@@ -222,27 +352,31 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
 #pragma unroll 4
                     for (int k = sb; k < sb + n; ++k) {
                         const float4 ra = sA[k];
-                        const float2 rz = sB[k];
-                        const f2_t rxx = pk2(ra.x, ra.y), ryy = pk2(ra.z, ra.w), rzz = pk2(rz.x, rz.y);
-                        f2_t dx = sub2(rxx, qx01), dy = sub2(ryy, qy01), dz = sub2(rzz, qz01);
-                        f2_t s01 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
-                        dx = sub2(rxx, qx23); dy = sub2(ryy, qy23); dz = sub2(rzz, qz23);
-                        f2_t s23 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
+                        const float4 rb4 = sB[k];
+                        const f2_t rxx = pk2(ra.x, ra.y), ryy = pk2(ra.z, ra.w);
+                        const f2_t rzz = pk2(rb4.x, rb4.y), rrr = pk2(rb4.z, rb4.w);
+                        const f2_t s01 = fma2(qz01, rzz, fma2(qy01, ryy, fma2(qx01, rxx, rrr)));
+                        const f2_t s23 = fma2(qz23, rzz, fma2(qy23, ryy, fma2(qx23, rxx, rrr)));
                         float a0, a1, a2, a3;
                         upk2(s01, a0, a1);
                         upk2(s23, a2, a3);
                         m0 = fminf(m0, a0); m1 = fminf(m1, a1); m2 = fminf(m2, a2); m3 = fminf(m3, a3);
                     }
-                    if (!q[0].done && m0 <= q[0].thr) nn_rescan<MODE>(a, T, q[0], sA, sB, sb, n, rb, E);
-                    if (!q[1].done && m1 <= q[1].thr) nn_rescan<MODE>(a, T, q[1], sA, sB, sb, n, rb, E);
-                    if (!q[2].done && m2 <= q[2].thr) nn_rescan<MODE>(a, T, q[2], sA, sB, sb, n, rb, E);
-                    if (!q[3].done && m3 <= q[3].thr) nn_rescan<MODE>(a, T, q[3], sA, sB, sb, n, rb, E);
+                    const unsigned n0 = __ballot_sync(0xffffffffu, !q[0].done && m0 <= q[0].ts);
+                    const unsigned n1 = __ballot_sync(0xffffffffu, !q[1].done && m1 <= q[1].ts);
+                    const unsigned n2 = __ballot_sync(0xffffffffu, !q[2].done && m2 <= q[2].ts);
+                    const unsigned n3 = __ballot_sync(0xffffffffu, !q[3].done && m3 <= q[3].ts);
+                    if (n0) nn_rescan_warp<MODE>(a, T, q[0], n0, sA, sB, sb, n, rb, tl);
+                    if (n1) nn_rescan_warp<MODE>(a, T, q[1], n1, sA, sB, sb, n, rb, tl);
+                    if (n2) nn_rescan_warp<MODE>(a, T, q[2], n2, sA, sB, sb, n, rb, tl);
+                    if (n3) nn_rescan_warp<MODE>(a, T, q[3], n3, sA, sB, sb, n, rb, tl);
                 }
             }
             if (MODE == NN_BAND) {
                 if (__syncthreads_and(q[0].done && q[1].done && q[2].done && q[3].done)) break;
             }
         }
+        (void)lane;
 #pragma unroll
         for (int j = 0; j < NN_Q; ++j) {
             if (!q[j].live) continue;
@@ -622,7 +756,6 @@ __global__ void k_sc_stats(Dev d, Rd r, const NNTask* task, double* out)
     __shared__ double sh[32];
     __shared__ long long shl[64];
     const int t = blockIdx.x;
-    const int c = t >> 1, m = t & 1;
     const long long ds = doff(d, t), de = doff(d, t + 1);
     const long long bs = r.bur_scan[ds], be = r.bur_scan[de];
     // trimmed area: sum of areas of kept buried dots

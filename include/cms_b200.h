@@ -68,6 +68,8 @@ typedef struct {
     int64_t n_dots[2];                    /* dots per molecule */
     int64_t n_trimmed[2];                 /* SC trimmed dots per molecule (after cms_shape_complementarity) */
     int64_t convex, toroidal, concave;    /* results.dots counters */
+    int64_t n_blocked[2];                 /* atoms with attention 1 (blockers) per molecule */
+    int64_t n_attended[2];                /* atoms with attention 5 per molecule (results nBuriedAtoms) */
     int32_t status;                       /* per-complex status bits */
     int32_t coincident_i, coincident_j;   /* first coincident pair (local indices) or -1 */
     double radmax;
