@@ -326,7 +326,7 @@ def run_ours(args):
                 "config": {"workload": WORKLOAD, "complexes_per_gpu": B, "atoms_per_gpu": N,
                            "parallelism": f"replicas x{world} (independent complexes per GPU)",
                            "l2": "inputs larger than L2 (9M atoms), no flush",
-                           "nn_search": "FP32 filter + FP64 recheck, brute force",
+                           "nn_search": "FP32 filter + FP64 recheck over every pair not excluded by a proven box-distance bound",
                            "grad": "not included"},
                 "e2e": e2e, "gpu_launches": launches * args.steps, "clocks": clocks,
                 "complex_status_nonzero": int(sum(1 for s in statuses if s))}

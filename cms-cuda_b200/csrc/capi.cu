@@ -220,8 +220,9 @@ struct cms_ctx {
         S_R_FLAG, S_R_BUR_SCAN, S_R_BUR_IDX, S_R_BUR_F4, S_R_BUR_CM, S_R_ACC_IDX, S_R_ACC_F4, S_R_KEEP, S_R_TRIM_SCAN,
         S_R_TRIM_IDX, S_R_TRIM_F4, S_R_NN_D2, S_R_NN_IDX, S_R_VAL, S_R_OWN, S_R_ACNT, S_R_AFILL, S_R_AOFF, S_R_ASLOT,
         S_CM_TMP, S_SCAN_TMP, S_PER_ATOM_CMS, S_TOT_CMS, S_PER_ATOM_MAX, S_TOT_MAX, S_SC_SIDE, S_SC_OUT, S_TASKS,
-        S_TILE_CNT, S_TILE_OFF, S_SUMMARY, S_EXPORT,
-        S_NN_Q, S_NN_R, S_NN_QF4, S_NN_RF4, S_NN_PART, S_NN_BBOX, S_NN_TASK, S_NN_TCNT, S_NN_TOFF, S_NN_D2, S_NN_IDX, S_INFO,
+        S_TILE_CNT, S_TILE_OFF, S_ROUND_CNT, S_ROUND_OFF, S_BOX_ROUND, S_BOX_BLK, S_SUMMARY, S_EXPORT,
+        S_NN_Q, S_NN_R, S_NN_QF4, S_NN_RF4, S_NN_PART, S_NN_BBOX, S_NN_TASK, S_NN_TCNT, S_NN_TOFF, S_NN_RCNT, S_NN_ROFF,
+        S_NN_BOXR, S_NN_BOXB, S_NN_D2, S_NN_IDX, S_INFO,
         S_COUNT
     };
 
@@ -323,6 +324,8 @@ void bind_batch(cms_ctx* x)
     x->ensure<NNTask>(cms_ctx::S_TASKS, 3 * 2 * B);
     x->ensure<int>(cms_ctx::S_TILE_CNT, 2 * B);
     x->ensure<long long>(cms_ctx::S_TILE_OFF, 2 * B + 1);
+    x->ensure<int>(cms_ctx::S_ROUND_CNT, 2 * B);
+    x->ensure<long long>(cms_ctx::S_ROUND_OFF, 2 * B + 1);
     x->ensure<long long>(cms_ctx::S_SUMMARY, 8);
 }
 
@@ -386,6 +389,10 @@ void bind_caps(cms_ctx* x)
     r.val = x->ensure<double>(cms_ctx::S_R_VAL, D);
     r.own = x->ensure<int>(cms_ctx::S_R_OWN, D);
     r.aslot = x->ensure<int>(cms_ctx::S_R_ASLOT, D);
+    // search boxes: every search's references are a subset of the dots
+    const long long rounds = nn_round_cap(D, 2LL * x->B);
+    x->ensure<float4>(cms_ctx::S_BOX_ROUND, 2 * rounds);
+    x->ensure<float4>(cms_ctx::S_BOX_BLK, 2 * rounds * (NN_ROUND / 32));
     long long mx = std::max({x->N + 1, x->cap_cells + 1, x->cap_tor + 1, x->cap_probe + 1, D + 1, 2LL * x->B + 2});
     x->ensure<long long>(cms_ctx::S_SCAN_TMP, scan_tmp_elems(mx) + 8);
 }
@@ -519,6 +526,11 @@ NNArgs nn_args(cms_ctx* x, int kind)
     a.ntask = 2 * x->B;
     a.tile_cnt = x->get<int>(cms_ctx::S_TILE_CNT);
     a.tile_off = x->get<long long>(cms_ctx::S_TILE_OFF);
+    a.round_cnt = x->get<int>(cms_ctx::S_ROUND_CNT);
+    a.round_off = x->get<long long>(cms_ctx::S_ROUND_OFF);
+    a.box_round = x->get<float4>(cms_ctx::S_BOX_ROUND);
+    a.box_blk = x->get<float4>(cms_ctx::S_BOX_BLK);
+    a.round_cap = nn_round_cap(x->cap_dot, 2LL * x->B);
     return a;
 }
 
@@ -558,7 +570,6 @@ void enqueue_sc(cms_ctx* x)
     a.q_xyz = a.r_xyz = d.dxyz;
     a.out_flag = r.keep;
     a.band_thr64 = x->st.band * x->st.band;
-    a.hint_scan = r.bur_scan;
     launch_nn(a, NN_BAND, tile_cap(x), tmp, s);
     mark(x, P_SC_BAND_NN);
     launch_trim_compact(d, r, x->cap_dot, tmp, s);
@@ -1179,12 +1190,18 @@ cms_status cms_nearest_dots(cms_ctx* x, const double* query_xyz, int64_t n_query
     NNTask* task = x->ensure<NNTask>(cms_ctx::S_NN_TASK, 1);
     int* tcnt = x->ensure<int>(cms_ctx::S_NN_TCNT, 1);
     long long* toff = x->ensure<long long>(cms_ctx::S_NN_TOFF, 2);
+    int* rcnt = x->ensure<int>(cms_ctx::S_NN_RCNT, 1);
+    long long* roff = x->ensure<long long>(cms_ctx::S_NN_ROFF, 2);
+    const long long rounds = nn_round_cap(n_ref, 1);
+    float4* boxr = x->ensure<float4>(cms_ctx::S_NN_BOXR, 2 * rounds);
+    float4* boxb = x->ensure<float4>(cms_ctx::S_NN_BOXB, 2 * rounds * (NN_ROUND / 32));
     double* d2 = where == CMS_HOST ? x->ensure<double>(cms_ctx::S_NN_D2, n_query) : out_d2;
     int* idx = where == CMS_HOST ? x->ensure<int>(cms_ctx::S_NN_IDX, n_query) : out_index;
     if (!idx) idx = x->ensure<int>(cms_ctx::S_NN_IDX, n_query);
-    launch_points_setup(q, n_query, r, n_ref, part, pblocks, bbox, qf, rf, task, tcnt, toff, s);
+    launch_points_setup(q, n_query, r, n_ref, part, pblocks, bbox, qf, rf, task, tcnt, toff, rcnt, roff, s);
     NNArgs a{};
     a.task = task; a.ntask = 1; a.tile_cnt = tcnt; a.tile_off = toff;
+    a.round_cnt = rcnt; a.round_off = roff; a.box_round = boxr; a.box_blk = boxb; a.round_cap = rounds;
     a.q_f4 = qf; a.q_idx = nullptr; a.r_f4 = rf; a.r_idx = nullptr;
     a.q_xyz = q; a.r_xyz = r;
     a.out_d2 = d2; a.out_idx = idx;

@@ -6,6 +6,11 @@ namespace cms {
 
 enum { NN_MIN = 0, NN_ARGMIN = 1, NN_BAND = 2 };
 
+// references per round of the nearest-dot search; a search's box arrays
+// hold ceil(references / NN_ROUND) rounds per task
+static constexpr int NN_ROUND = 1024;
+static inline long long nn_round_cap(long long refs, long long ntask) { return refs / NN_ROUND + ntask + 1; }
+
 #define SC_SIDE_FIELDS 7   // d_mean, d_median, s_mean, s_median, trimmedArea, nTrimmedDots, nAllDots
 #define SC_FIELDS 5        // sc, area, distance, d_mean (surface 2), s_mean (surface 2)
 
@@ -27,10 +32,13 @@ struct NNArgs {
     const double* q_xyz; const double* r_xyz;   // FP64 coordinates for the recheck
     double* out_d2; int* out_idx; int* out_flag;
     double band_thr64;      // band^2 (BAND mode)
-    // BAND mode scan order hint: references are the non-buried dots of the
-    // query's dot range, and hint_scan is the buried-dot exclusive scan, so
-    // dot - hint_scan[dot] is the reference position next to a query dot
-    const long long* hint_scan;
+    // rounds of NN_ROUND references per task and their bounding boxes (lo, hi):
+    // box_round 2 per round, box_blk 2 per 32-reference block (32 per round)
+    int* round_cnt;         // ntask
+    long long* round_off;   // ntask + 1
+    float4* box_round;
+    float4* box_blk;
+    long long round_cap;    // rounds the box arrays hold
     int band_mode;
 };
 
@@ -55,7 +63,7 @@ void launch_nn_kernel(NNArgs a, int mode, long long tile_cap, cudaStream_t s);
 // standalone search helpers: bounding box of two point sets, FP32 packing, one task
 void launch_points_setup(const double* q, long long nq, const double* r, long long nr, double* partials,
                          int partial_blocks, double* bbox, float4* q_f4, float4* r_f4, NNTask* task, int* tile_cnt,
-                         long long* tile_off, cudaStream_t s);
+                         long long* tile_off, int* round_cnt, long long* round_off, cudaStream_t s);
 void launch_cms_weights(const Dev& d, const Rd& r, long long cap, cudaStream_t s);
 void launch_area_values(const Dev& d, const Rd& r, long long cap, cudaStream_t s);
 void launch_per_atom_sum(const Dev& d, const Rd& r, long long cap, double* out, long long* scan_tmp, cudaStream_t s);

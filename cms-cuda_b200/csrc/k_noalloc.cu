@@ -8,8 +8,9 @@
 // applications that own every device allocation.  This entry point gives
 // them the same search as cms_nearest_dots without any allocation: the caller
 // passes device pointers for inputs and outputs, and the search's scratch
-// (the bounding-box partials, the search task and the FP32-packed copies of
-// both point sets) lives in one fixed file-scope device array.
+// (the bounding-box partials, the search task, the FP32-packed copies of
+// both point sets and the boxes of the reference blocks) lives in one fixed
+// file-scope device array.
 //
 // Contract:
 //  - scratch is CMS_NOALLOC_SCRATCH_BYTES (32 MiB) per device, allocated when
@@ -34,9 +35,17 @@ using namespace cms;
 
 #define CMS_NOALLOC_SCRATCH_BYTES (32u << 20)
 #define CMS_NOALLOC_HEADER_BYTES (16u << 10)
-#define CMS_NOALLOC_MAX_POINTS ((CMS_NOALLOC_SCRATCH_BYTES - CMS_NOALLOC_HEADER_BYTES) / 16u)
+// 1920 x 1024 points: 16 bytes each when packed, plus the reference boxes
+// (66 float4 per round of NN_ROUND references, at most MAX/NN_ROUND + 2 rounds)
+#define CMS_NOALLOC_MAX_POINTS (1920u * 1024u)
+#define CMS_NOALLOC_MAX_ROUNDS (CMS_NOALLOC_MAX_POINTS / NN_ROUND + 2u)
+#define CMS_NOALLOC_BOX_F4 (2u + 2u * (NN_ROUND / 32))
 #define CMS_NOALLOC_PARTIAL_BLOCKS 256
 #define CMS_NOALLOC_MAX_DEVICES 64
+
+static_assert(CMS_NOALLOC_HEADER_BYTES + 16ull * CMS_NOALLOC_BOX_F4 * CMS_NOALLOC_MAX_ROUNDS +
+                  16ull * CMS_NOALLOC_MAX_POINTS <= CMS_NOALLOC_SCRATCH_BYTES,
+              "no-alloc scratch layout exceeds the array");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[CMS_NOALLOC_SCRATCH_BYTES];
 
@@ -79,12 +88,19 @@ extern "C" cms_status cms_nearest_dots_noalloc(const double* query_xyz, int64_t 
     NNTask* task = (NNTask*)(bbox + 8);
     int* tile_cnt = (int*)(task + 1);
     long long* tile_off = (long long*)(tile_cnt + 4);
-    float4* q_f4 = (float4*)(base + CMS_NOALLOC_HEADER_BYTES);
+    int* round_cnt = (int*)(tile_off + 2);
+    long long* round_off = (long long*)(round_cnt + 4);
+    // after the header: the round boxes, the block boxes, then the packed points
+    float4* box_round = (float4*)(base + CMS_NOALLOC_HEADER_BYTES);
+    float4* box_blk = box_round + 2u * CMS_NOALLOC_MAX_ROUNDS;
+    float4* q_f4 = box_round + CMS_NOALLOC_BOX_F4 * CMS_NOALLOC_MAX_ROUNDS;
     float4* r_f4 = q_f4 + n_query;
     launch_points_setup(query_xyz, n_query, ref_xyz, n_ref, partials, CMS_NOALLOC_PARTIAL_BLOCKS, bbox, q_f4, r_f4,
-                        task, tile_cnt, tile_off, s);
+                        task, tile_cnt, tile_off, round_cnt, round_off, s);
     NNArgs a{};
     a.task = task; a.ntask = 1; a.tile_cnt = tile_cnt; a.tile_off = tile_off;
+    a.round_cnt = round_cnt; a.round_off = round_off; a.box_round = box_round; a.box_blk = box_blk;
+    a.round_cap = CMS_NOALLOC_MAX_ROUNDS;
     a.q_f4 = q_f4; a.q_idx = nullptr; a.r_f4 = r_f4; a.r_idx = nullptr;
     a.q_xyz = query_xyz; a.r_xyz = ref_xyz;
     a.out_d2 = out_d2; a.out_idx = out_index;

@@ -141,47 +141,88 @@ __device__ __forceinline__ float nn_rr(float rx, float ry, float rz)
 }
 
 static constexpr int NN_T = 128;              // threads per tile
+static constexpr int NN_W = NN_T / 32;        // warps per tile
 static constexpr int NN_Q = 4;                // queries per thread (two packed pairs)
+static constexpr int NN_WQ = 32 * NN_Q;       // consecutive queries per warp
 static constexpr int NN_TILE = NN_T * NN_Q;   // queries per tile
-static constexpr int NN_R = 1024;             // references staged per round
-static constexpr int NN_SUB = 32;             // references per threshold check
+static constexpr int NN_BLK = 32;             // references per block (one bounding box)
+static constexpr int NN_R = NN_ROUND;         // references per round (staged together)
+static constexpr int NN_RB = NN_R / NN_BLK;   // blocks per round
+static constexpr int NN_SORT = 512;           // rounds of a task visited nearest first (more: index order)
 
 // one query's state
 struct NNQ {
-    float qx2, qy2, qz2;  // -2 q
-    double qq;            // |q|^2 (FP32 value, held in FP64)
+    float qx2, qy2, qz2;  // -2 q'
+    double qq;            // |q'|^2 (FP32 value, held in FP64)
     int dot;              // index of the query point (FP64 coordinates read on recheck)
-    float ms;             // smallest s seen
-    float ts;             // s threshold: candidates have s <= ts (tile-relative)
+    float ms, ms2;        // smallest block minimum of s; smallest among the other blocks
+    int mb;               // block holding ms
+    float ts;             // s threshold: candidates have s <= ts
+    float cth;            // cull threshold on the squared box distance
     double best;
     int bidx;
     bool live, done;
 };
 
+// Per-tile constants.  Box culling: a reference at squared distance L from
+// the query in the staged FP32 frame has d32 >= L - eps(L) >= L (1 - B) - A,
+// with eps(D) <= A + B D from the bound above (expand t^2 and sqrt(D)).
+// A block whose box lies farther than (th + A) / (1 - B) from a query holds
+// no candidate for a d32 threshold th.
 struct NNTile {
     float cx, cy, cz;     // tile centre
     double rho, E0;       // bound on |q'|, FP32 rounding of the staged points
+    double A, cull;       // cull threshold = (th + A) * cull
 };
 
-__device__ __forceinline__ float nn_s_threshold(const NNQ& q, const NNTile& t)
+__device__ __forceinline__ NNTile nn_tile(float cx, float cy, float cz, double half_diag, double E0)
 {
-    if (!(q.ms < INFINITY)) return INFINITY;
-    const double m = (double)q.ms + q.qq;
-    const double th = m + 2.0 * nn_eps(m, t.rho, t.E0) * 1.01;
-    return __double2float_ru(th - q.qq);
+    const double u = 5.9604644775390625e-08;
+    NNTile t;
+    t.cx = cx; t.cy = cy; t.cz = cz;
+    // |q - c| <= half diagonal of the box, plus the rounding of c and of q - c
+    const double cn = fabs((double)cx) + fabs((double)cy) + fabs((double)cz);
+    t.rho = (half_diag + 1e-6 * (cn + 1.0)) * (1.0 + 1e-6);
+    t.E0 = E0;
+    const double e0 = E0 + 4.0 * u * (t.rho + 1.0);
+    t.A = 40.0 * u * (t.rho + 1.0) * (t.rho + 1.0) + 3.0 * e0 + 4.0 * u + 2.0 * e0 * e0;
+    const double B = 52.0 * u + e0 + 32.0 * u * u;
+    t.cull = (1.0 + 1e-6) / (1.0 - B);
+    return t;
 }
 
-// Re-examine a block of n (<= 32) staged references [k0, k0+n) for every
-// (lane, query) of the warp whose block minimum fell under its threshold.
-// The warp takes the flagged lanes one at a time and checks the block in
-// parallel, one reference per lane: FP32 filter against the lane's threshold
-// at block start (a superset of what a sequential scan would recheck), FP64
-// recheck in cdist order, then a warp reduction to the smallest FP64 value
-// and, on ties, the smallest reference index -- what an in-order scan keeps.
-template <int MODE>
-__device__ __forceinline__ void nn_rescan_warp(const NNArgs& a, const NNTask& T, NNQ& q, unsigned need,
-                                               const float4* sA, const float4* sB, int k0, int n, long long rb,
-                                               const NNTile& tl)
+// d32 threshold for the minimum searches: m + 2 eps(m), m = smallest d32 seen
+__device__ __forceinline__ double nn_min_th(float ms, double qq, const NNTile& t)
+{
+    const double m = (double)ms + qq;
+    return m + 2.0 * nn_eps(m, t.rho, t.E0) * 1.01;
+}
+
+__device__ __forceinline__ float nn_cull_th(double th, const NNTile& t)
+{
+    return __double2float_ru((th + t.A) * t.cull);
+}
+
+// squared distance between two boxes (0 when they overlap); an empty box
+// (lo = +inf, hi = -inf) is infinitely far from everything
+__device__ __forceinline__ float box_gap2(float lx, float ly, float lz, float hx, float hy, float hz, float4 blo, float4 bhi)
+{
+    const float gx = fmaxf(fmaxf(blo.x - hx, lx - bhi.x), 0.f);
+    const float gy = fmaxf(fmaxf(blo.y - hy, ly - bhi.y), 0.f);
+    const float gz = fmaxf(fmaxf(blo.z - hz, lz - bhi.z), 0.f);
+    return gx * gx + gy * gy + gz * gz;
+}
+
+// the FP32 box distance is within a few ulps of the exact one: scale it down
+// before comparing against a cull threshold
+__device__ __forceinline__ bool box_far(float g2, float cth) { return g2 * 0.999999f > cth; }
+
+// BAND mode: re-examine a block of n (<= 32) staged references [k0, k0+n) for
+// every (lane, query) of the warp whose block minimum fell under its
+// threshold.  The warp takes the flagged lanes one at a time and checks the
+// block in parallel, one reference per lane, FP32 filter then FP64 test.
+__device__ __forceinline__ void nn_band_warp(const NNArgs& a, const NNTask& T, NNQ& q, unsigned need,
+                                             const float4* sA, const float4* sB, int k0, int n, long long rb)
 {
     const int lane = threadIdx.x & 31;
     while (need) {
@@ -192,45 +233,100 @@ __device__ __forceinline__ void nn_rescan_warp(const NNArgs& a, const NNTask& T,
         const float qz2 = __shfl_sync(0xffffffffu, q.qz2, L);
         const float ts = __shfl_sync(0xffffffffu, q.ts, L);
         const int qdot = __shfl_sync(0xffffffffu, q.dot, L);
-        double e = INFINITY;
-        float sv = INFINITY;
-        int idx = 0x7fffffff;
+        bool hit = false;
         if (lane < n) {
             const int k = k0 + lane;
             const float v = nn_s(qx2, qy2, qz2, sA[k].x, sA[k].z, sB[k].x, sB[k].z);
             if (v <= ts) {
                 const long long rk = T.r0 + rb + k;
                 const double* rp = a.r_xyz + 3LL * (a.r_idx ? a.r_idx[rk] : rk);
-                e = exact_d2(rp, a.q_xyz + 3LL * qdot);
-                sv = v;
-                idx = (int)(rb + k);
+                hit = exact_d2(rp, a.q_xyz + 3LL * qdot) <= a.band_thr64;
             }
         }
-        if (MODE == NN_BAND) {
-            const bool hit = __any_sync(0xffffffffu, e <= a.band_thr64);
-            if (lane == L && hit) q.done = true;
-        } else {
-            for (int o = 16; o > 0; o >>= 1) {
-                const double e2 = __shfl_xor_sync(0xffffffffu, e, o);
-                const int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
-                const float v2 = __shfl_xor_sync(0xffffffffu, sv, o);
-                if (e2 < e || (e2 == e && i2 < idx)) { e = e2; idx = i2; }
-                sv = fminf(sv, v2);
-            }
-            if (lane == L) {
-                if (e < q.best) { q.best = e; q.bidx = idx; }
-                if (sv < q.ms) { q.ms = sv; q.ts = nn_s_threshold(q, tl); }
-            }
-        }
+        if (__any_sync(0xffffffffu, hit) && lane == L) q.done = true;
     }
 }
 
+// FP32 filter + FP64 recheck of one reference for a minimum search
+__device__ __forceinline__ void nn_recheck(const NNArgs& a, const NNTask& T, const NNTile& tl, float qx2, float qy2,
+                                           float qz2, float ts, int qdot, long long k, double& best, int& bidx)
+{
+    const float4 r = a.r_f4[T.r0 + k];
+    const float rx = r.x - tl.cx, ry = r.y - tl.cy, rz = r.z - tl.cz;
+    const float v = nn_s(qx2, qy2, qz2, rx, ry, rz, nn_rr(rx, ry, rz));
+    if (v <= ts) {
+        const long long rk = T.r0 + k;
+        const double e = exact_d2(a.r_xyz + 3LL * (a.r_idx ? a.r_idx[rk] : rk), a.q_xyz + 3LL * qdot);
+        if (e < best || (e == best && (int)k < bidx)) { best = e; bidx = (int)k; }
+    }
+}
+
+// Minimum searches, rare case: candidates may sit in more than one block.
+// The warp rechecks every reference of the task for each flagged lane,
+// skipping blocks whose box is beyond the lane's cull threshold, and keeps
+// the smallest FP64 value with the smallest index.
+__device__ __forceinline__ void nn_full_warp(const NNArgs& a, const NNTask& T, const NNTile& tl, long long ro, int nrt,
+                                             NNQ& q, unsigned need, long long qbase)
+{
+    const int lane = threadIdx.x & 31;
+    const long long nblk = (long long)nrt * NN_RB;
+    while (need) {
+        const int L = __ffs(need) - 1;
+        need &= need - 1;
+        const float qx2 = __shfl_sync(0xffffffffu, q.qx2, L);
+        const float qy2 = __shfl_sync(0xffffffffu, q.qy2, L);
+        const float qz2 = __shfl_sync(0xffffffffu, q.qz2, L);
+        const float ts = __shfl_sync(0xffffffffu, q.ts, L);
+        const float cth = __shfl_sync(0xffffffffu, q.cth, L);
+        const int qdot = __shfl_sync(0xffffffffu, q.dot, L);
+        const float4 qf = a.q_f4[qbase + L];
+        double best = INFINITY;
+        int bidx = 0x7fffffff;
+        for (long long blk0 = 0; blk0 < nblk; blk0 += 32) {
+            const long long blk = blk0 + lane;
+            bool want = false;
+            if (blk < nblk) {
+                const float4 lo = a.box_blk[2 * (ro * NN_RB + blk)], hi = a.box_blk[2 * (ro * NN_RB + blk) + 1];
+                want = !box_far(box_gap2(qf.x, qf.y, qf.z, qf.x, qf.y, qf.z, lo, hi), cth);
+            }
+            unsigned wb = __ballot_sync(0xffffffffu, want);
+            while (wb) {
+                const int b = __ffs(wb) - 1;
+                wb &= wb - 1;
+                const long long k = (blk0 + b) * NN_BLK + lane;
+                if (k < T.rn) nn_recheck(a, T, tl, qx2, qy2, qz2, ts, qdot, k, best, bidx);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double e2 = __shfl_xor_sync(0xffffffffu, best, o);
+            const int i2 = __shfl_xor_sync(0xffffffffu, bidx, o);
+            if (e2 < best || (e2 == best && i2 < bidx)) { best = e2; bidx = i2; }
+        }
+        if (lane == L) { q.best = best; q.bidx = bidx; }
+    }
+}
+
+// Nearest-dot search over tiles of NN_TILE queries.  Each warp owns 128
+// consecutive queries (4 per lane, two packed pairs).  The task's references
+// come in rounds of NN_R, visited in order of their box distance to the
+// tile's box; a round is staged in shared memory only when some warp's query
+// box is within its cull threshold, and each warp skips the 32-reference
+// blocks whose box is beyond it.  The minimum searches keep, per query, the
+// smallest block minimum of s, the block holding it and the smallest minimum
+// of the other blocks; after the scan, the FP64 recheck covers that one block
+// when no other block can hold a candidate (the usual case) and every block
+// otherwise.  The band search stops a query at its first FP64 hit and a tile
+// once every query has one or no round is left within reach.
 template <int MODE>
 __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
 {
     __shared__ float4 sA[NN_R];   // (x, x, y, y)
     __shared__ float4 sB[NN_R];   // (z, z, |r|^2, |r|^2)
-    const int lane = threadIdx.x & 31;
+    __shared__ float4 sBox[2 * NN_RB];
+    __shared__ float sKey[NN_SORT];
+    __shared__ short sOrd[NN_SORT];
+    __shared__ float sWbox[6][NN_W];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const long long ntiles = a.tile_off[a.ntask];
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         int lo = 0, hi = a.ntask - 1;
@@ -239,102 +335,106 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
             if (a.tile_off[mid] <= tile) lo = mid; else hi = mid - 1;
         }
         const NNTask T = a.task[lo];
-        const long long qb = (tile - a.tile_off[lo]) * NN_TILE + threadIdx.x;
-        // queries of the tile, then the tile centre and radius
+        const long long ro = a.round_off[lo];
+        const int nrt = a.round_cnt[lo];
+        if (ro + nrt > a.round_cap) continue;     // over capacity: the run is flagged and redone
+        const long long qw = (tile - a.tile_off[lo]) * NN_TILE + (long long)wid * NN_WQ;
+
+        // queries and the warp's box
         NNQ q[NN_Q];
-        float qx[NN_Q], qy[NN_Q], qz[NN_Q];
-        float lo3[3] = {INFINITY, INFINITY, INFINITY}, hi3[3] = {-INFINITY, -INFINITY, -INFINITY};
+        float qpx[NN_Q], qpy[NN_Q], qpz[NN_Q];
+        float wl[3] = {INFINITY, INFINITY, INFINITY}, wh[3] = {-INFINITY, -INFINITY, -INFINITY};
 #pragma unroll
         for (int j = 0; j < NN_Q; ++j) {
-            const long long qi = qb + (long long)j * NN_T;
+            const long long qi = qw + j * 32 + lane;
             q[j].live = qi < T.qn;
-            qx[j] = qy[j] = qz[j] = 0.f;
+            qpx[j] = qpy[j] = qpz[j] = 0.f;
             q[j].dot = 0;
             if (q[j].live) {
                 const float4 f = a.q_f4[T.q0 + qi];
-                qx[j] = f.x; qy[j] = f.y; qz[j] = f.z;
+                qpx[j] = f.x; qpy[j] = f.y; qpz[j] = f.z;
                 q[j].dot = a.q_idx ? a.q_idx[T.q0 + qi] : (int)(T.q0 + qi);
-                lo3[0] = fminf(lo3[0], f.x); lo3[1] = fminf(lo3[1], f.y); lo3[2] = fminf(lo3[2], f.z);
-                hi3[0] = fmaxf(hi3[0], f.x); hi3[1] = fmaxf(hi3[1], f.y); hi3[2] = fmaxf(hi3[2], f.z);
+                wl[0] = fminf(wl[0], f.x); wl[1] = fminf(wl[1], f.y); wl[2] = fminf(wl[2], f.z);
+                wh[0] = fmaxf(wh[0], f.x); wh[1] = fmaxf(wh[1], f.y); wh[2] = fmaxf(wh[2], f.z);
             }
         }
-        __shared__ float sbox[6][NN_T / 32];
-        __shared__ double srho[NN_T / 32];
+#pragma unroll
         for (int k = 0; k < 3; ++k) {
             for (int o = 16; o > 0; o >>= 1) {
-                lo3[k] = fminf(lo3[k], __shfl_xor_sync(0xffffffffu, lo3[k], o));
-                hi3[k] = fmaxf(hi3[k], __shfl_xor_sync(0xffffffffu, hi3[k], o));
+                wl[k] = fminf(wl[k], __shfl_xor_sync(0xffffffffu, wl[k], o));
+                wh[k] = fmaxf(wh[k], __shfl_xor_sync(0xffffffffu, wh[k], o));
             }
         }
-        if (lane == 0) for (int k = 0; k < 3; ++k) { sbox[k][threadIdx.x >> 5] = lo3[k]; sbox[3 + k][threadIdx.x >> 5] = hi3[k]; }
+        if (lane == 0) for (int k = 0; k < 3; ++k) { sWbox[k][wid] = wl[k]; sWbox[3 + k][wid] = wh[k]; }
         __syncthreads();
+        // the tile's box, centre and constants
+        float tb[6];
+        for (int k = 0; k < 3; ++k) {
+            float l = sWbox[k][0], h = sWbox[3 + k][0];
+            for (int w = 1; w < NN_W; ++w) { l = fminf(l, sWbox[k][w]); h = fmaxf(h, sWbox[3 + k][w]); }
+            tb[k] = l; tb[3 + k] = h;
+        }
         NNTile tl;
         {
-            float c3[3];
-            for (int k = 0; k < 3; ++k) {
-                float l = sbox[k][0], h = sbox[3 + k][0];
-                for (int w = 1; w < NN_T / 32; ++w) { l = fminf(l, sbox[k][w]); h = fmaxf(h, sbox[3 + k][w]); }
-                c3[k] = (l <= h) ? 0.5f * (l + h) : 0.f;
-            }
-            tl.cx = c3[0]; tl.cy = c3[1]; tl.cz = c3[2];
+            const float cx = 0.5f * (tb[0] + tb[3]), cy = 0.5f * (tb[1] + tb[4]), cz = 0.5f * (tb[2] + tb[5]);
+            const double ex = (double)tb[3] - tb[0], ey = (double)tb[4] - tb[1], ez = (double)tb[5] - tb[2];
+            tl = nn_tile(cx, cy, cz, 0.5 * sqrt(ex * ex + ey * ey + ez * ez), T.E);
         }
-        double rho = 0.0;
+        const double band_th = MODE == NN_BAND ? a.band_thr64 + nn_eps(a.band_thr64, tl.rho, tl.E0) * 1.01 : 0.0;
+        const float band_cth = MODE == NN_BAND ? nn_cull_th(band_th, tl) : 0.f;
+        float cthw = -INFINITY;        // warp cull threshold: max over its open queries
 #pragma unroll
         for (int j = 0; j < NN_Q; ++j) {
-            qx[j] -= tl.cx; qy[j] -= tl.cy; qz[j] -= tl.cz;
-            if (q[j].live) rho = fmax(rho, sqrt((double)qx[j] * qx[j] + (double)qy[j] * qy[j] + (double)qz[j] * qz[j]));
-        }
-        for (int o = 16; o > 0; o >>= 1) rho = fmax(rho, __shfl_xor_sync(0xffffffffu, rho, o));
-        if (lane == 0) srho[threadIdx.x >> 5] = rho;
-        __syncthreads();
-        for (int w = 0; w < NN_T / 32; ++w) rho = fmax(rho, srho[w]);
-        __syncthreads();
-        tl.rho = rho * (1.0 + 1e-6) + 1e-6;
-        tl.E0 = T.E;
-#pragma unroll
-        for (int j = 0; j < NN_Q; ++j) {
-            q[j].qx2 = -2.0f * qx[j]; q[j].qy2 = -2.0f * qy[j]; q[j].qz2 = -2.0f * qz[j];
-            q[j].qq = (double)nn_rr(qx[j], qy[j], qz[j]);
-            q[j].ms = INFINITY;
-            q[j].best = INFINITY;
-            q[j].bidx = -1;
+            const float x = qpx[j] - tl.cx, y = qpy[j] - tl.cy, z = qpz[j] - tl.cz;
+            q[j].qx2 = -2.0f * x; q[j].qy2 = -2.0f * y; q[j].qz2 = -2.0f * z;
+            q[j].qq = (double)nn_rr(x, y, z);
+            q[j].ms = INFINITY; q[j].ms2 = INFINITY; q[j].mb = -1;
+            q[j].best = INFINITY; q[j].bidx = -1;
             q[j].done = !q[j].live;
             if (MODE == NN_BAND) {
-                const double t = a.band_thr64 + nn_eps(a.band_thr64, tl.rho, tl.E0) * 1.01;
-                q[j].ts = __double2float_ru(t - q[j].qq);
+                q[j].ts = __double2float_ru(band_th - q[j].qq);
+                q[j].cth = band_cth;
             } else {
                 q[j].ts = INFINITY;
-                if (q[j].live && T.rn > 0) {
-                    // seed with reference 0 (the first index, so ties keep it)
-                    const long long r0 = a.r_idx ? a.r_idx[T.r0] : T.r0;
-                    const float4 f = a.r_f4[T.r0];
-                    const float rx = f.x - tl.cx, ry = f.y - tl.cy, rz = f.z - tl.cz;
-                    q[j].best = exact_d2(a.r_xyz + 3LL * r0, a.q_xyz + 3LL * q[j].dot);
-                    q[j].bidx = 0;
-                    q[j].ms = nn_s(q[j].qx2, q[j].qy2, q[j].qz2, rx, ry, rz, nn_rr(rx, ry, rz));
-                    q[j].ts = nn_s_threshold(q[j], tl);
-                }
+                q[j].cth = INFINITY;
             }
+            if (!q[j].done) cthw = fmaxf(cthw, q[j].cth);
         }
+        for (int o = 16; o > 0; o >>= 1) cthw = fmaxf(cthw, __shfl_xor_sync(0xffffffffu, cthw, o));
         const f2_t qx01 = pk2(q[0].qx2, q[1].qx2), qy01 = pk2(q[0].qy2, q[1].qy2), qz01 = pk2(q[0].qz2, q[1].qz2);
         const f2_t qx23 = pk2(q[2].qx2, q[3].qx2), qy23 = pk2(q[2].qy2, q[3].qy2), qz23 = pk2(q[2].qz2, q[3].qz2);
-        // Order of the reference rounds.  The minimum searches go in index order
-        // (first index wins ties).  The band test only asks whether ANY reference
-        // is within the band, so it starts at the references that sit next to the
-        // tile's first query in dot order (usually its own surface patch) and
-        // wraps around: every pair is still examined unless a hit ends the scan.
-        long long rb_start = 0;
-        if (MODE == NN_BAND && a.hint_scan && T.rn > NN_R) {
-            const long long first = T.q0 + (tile - a.tile_off[lo]) * NN_TILE;
-            const long long dot = a.q_idx ? a.q_idx[first] : first;
-            const long long pos = (dot - a.hint_scan[dot]) - T.r0 - NN_R / 2;
-            rb_start = pos < 0 ? 0 : (pos >= T.rn ? T.rn - 1 : pos);
-        }
-        for (long long seen = 0; seen < T.rn;) {
-            const long long rb = (rb_start + seen) % T.rn;
-            const int nr = (int)min(min((long long)NN_R, T.rn - seen), T.rn - rb);
-            seen += nr;
+
+        // visiting order of the rounds: nearest to the tile's box first
+        const bool sorted = nrt <= NN_SORT;
+        if (sorted) {
+            for (int i = threadIdx.x; i < nrt; i += NN_T)
+                sKey[i] = box_gap2(tb[0], tb[1], tb[2], tb[3], tb[4], tb[5], a.box_round[2 * (ro + i)],
+                                   a.box_round[2 * (ro + i) + 1]);
             __syncthreads();
+            for (int i = threadIdx.x; i < nrt; i += NN_T) {
+                const float ki = sKey[i];
+                int rank = 0;
+                for (int j2 = 0; j2 < nrt; ++j2) {
+                    const float kj = sKey[j2];
+                    rank += (kj < ki || (kj == ki && j2 < i)) ? 1 : 0;
+                }
+                sOrd[rank] = (short)i;
+            }
+            __syncthreads();
+        }
+
+        for (int kr = 0; kr < nrt; ++kr) {
+            const int i = sorted ? sOrd[kr] : kr;
+            const float4 rlo = a.box_round[2 * (ro + i)], rhi = a.box_round[2 * (ro + i) + 1];
+            const bool open = cthw > -INFINITY;
+            const bool need = open && !box_far(box_gap2(wl[0], wl[1], wl[2], wh[0], wh[1], wh[2], rlo, rhi), cthw);
+            if (!__syncthreads_or(need)) {
+                // every later round is at least as far from the tile's box
+                if (sorted && !__syncthreads_or(open && !box_far(sKey[i], cthw))) break;
+                continue;
+            }
+            const long long rb = (long long)i * NN_R;
+            const int nr = (int)min((long long)NN_R, T.rn - rb);
             for (int k = threadIdx.x; k < nr; k += NN_T) {
                 const float4 r = a.r_f4[T.r0 + rb + k];
                 const float rx = r.x - tl.cx, ry = r.y - tl.cy, rz = r.z - tl.cz;
@@ -342,12 +442,15 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
                 sA[k] = make_float4(rx, rx, ry, ry);
                 sB[k] = make_float4(rz, rz, rr, rr);
             }
+            for (int k = threadIdx.x; k < 2 * NN_RB; k += NN_T) sBox[k] = a.box_blk[2 * (ro + i) * NN_RB + k];
             __syncthreads();
-            // warp-uniform: the block loop below uses full-warp ballots and shuffles
-            const bool all_done = __all_sync(0xffffffffu, q[0].done && q[1].done && q[2].done && q[3].done);
-            if (!all_done) {
-                for (int sb = 0; sb < nr; sb += NN_SUB) {
-                    const int n = min(NN_SUB, nr - sb);
+            if (need) {
+                for (int b = 0; b < NN_RB; ++b) {
+                    const int sb = b * NN_BLK;
+                    if (sb >= nr) break;
+                    if (box_far(box_gap2(wl[0], wl[1], wl[2], wh[0], wh[1], wh[2], sBox[2 * b], sBox[2 * b + 1]), cthw))
+                        continue;
+                    const int n = min(NN_BLK, nr - sb);
                     float m0 = INFINITY, m1 = INFINITY, m2 = INFINITY, m3 = INFINITY;
 #pragma unroll 4
                     for (int k = sb; k < sb + n; ++k) {
@@ -362,31 +465,77 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
                         upk2(s23, a2, a3);
                         m0 = fminf(m0, a0); m1 = fminf(m1, a1); m2 = fminf(m2, a2); m3 = fminf(m3, a3);
                     }
-                    const unsigned n0 = __ballot_sync(0xffffffffu, !q[0].done && m0 <= q[0].ts);
-                    const unsigned n1 = __ballot_sync(0xffffffffu, !q[1].done && m1 <= q[1].ts);
-                    const unsigned n2 = __ballot_sync(0xffffffffu, !q[2].done && m2 <= q[2].ts);
-                    const unsigned n3 = __ballot_sync(0xffffffffu, !q[3].done && m3 <= q[3].ts);
-                    if (n0) nn_rescan_warp<MODE>(a, T, q[0], n0, sA, sB, sb, n, rb, tl);
-                    if (n1) nn_rescan_warp<MODE>(a, T, q[1], n1, sA, sB, sb, n, rb, tl);
-                    if (n2) nn_rescan_warp<MODE>(a, T, q[2], n2, sA, sB, sb, n, rb, tl);
-                    if (n3) nn_rescan_warp<MODE>(a, T, q[3], n3, sA, sB, sb, n, rb, tl);
+                    if (MODE == NN_BAND) {
+                        const unsigned n0 = __ballot_sync(0xffffffffu, !q[0].done && m0 <= q[0].ts);
+                        const unsigned n1 = __ballot_sync(0xffffffffu, !q[1].done && m1 <= q[1].ts);
+                        const unsigned n2 = __ballot_sync(0xffffffffu, !q[2].done && m2 <= q[2].ts);
+                        const unsigned n3 = __ballot_sync(0xffffffffu, !q[3].done && m3 <= q[3].ts);
+                        if (n0) nn_band_warp(a, T, q[0], n0, sA, sB, sb, n, rb);
+                        if (n1) nn_band_warp(a, T, q[1], n1, sA, sB, sb, n, rb);
+                        if (n2) nn_band_warp(a, T, q[2], n2, sA, sB, sb, n, rb);
+                        if (n3) nn_band_warp(a, T, q[3], n3, sA, sB, sb, n, rb);
+                    } else {
+                        const int blk = i * NN_RB + b;
+                        const float mv[NN_Q] = {m0, m1, m2, m3};
+#pragma unroll
+                        for (int j = 0; j < NN_Q; ++j) {
+                            if (mv[j] < q[j].ms) { q[j].ms2 = q[j].ms; q[j].ms = mv[j]; q[j].mb = blk; }
+                            else q[j].ms2 = fminf(q[j].ms2, mv[j]);
+                        }
+                    }
                 }
-            }
-            if (MODE == NN_BAND) {
-                if (__syncthreads_and(q[0].done && q[1].done && q[2].done && q[3].done)) break;
+                // thresholds for the next rounds
+                float c = -INFINITY;
+#pragma unroll
+                for (int j = 0; j < NN_Q; ++j) {
+                    if (MODE != NN_BAND && q[j].live && q[j].ms < INFINITY)
+                        q[j].cth = nn_cull_th(nn_min_th(q[j].ms, q[j].qq, tl), tl);
+                    if (!q[j].done) c = fmaxf(c, q[j].cth);
+                }
+                for (int o = 16; o > 0; o >>= 1) c = fmaxf(c, __shfl_xor_sync(0xffffffffu, c, o));
+                cthw = c;
             }
         }
-        (void)lane;
+
+        if (MODE != NN_BAND) {
+            // FP64 recheck: the best block alone when no other block can hold a candidate
+            bool full[NN_Q];
+#pragma unroll
+            for (int j = 0; j < NN_Q; ++j) {
+                full[j] = false;
+                if (!q[j].live || !(q[j].ms < INFINITY)) continue;
+                const double th = nn_min_th(q[j].ms, q[j].qq, tl);
+                q[j].ts = __double2float_ru(th - q[j].qq);
+                q[j].cth = nn_cull_th(th, tl);
+                if (q[j].ms2 > q[j].ts) {
+                    const long long k0 = (long long)q[j].mb * NN_BLK;
+                    const long long k1 = min(k0 + NN_BLK, T.rn);
+                    double best = INFINITY;
+                    int bidx = 0x7fffffff;
+                    for (long long k = k0; k < k1; ++k)
+                        nn_recheck(a, T, tl, q[j].qx2, q[j].qy2, q[j].qz2, q[j].ts, q[j].dot, k, best, bidx);
+                    q[j].best = best; q[j].bidx = bidx;
+                } else {
+                    full[j] = true;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < NN_Q; ++j) {
+                const unsigned nf = __ballot_sync(0xffffffffu, full[j]);
+                if (nf) nn_full_warp(a, T, tl, ro, nrt, q[j], nf, T.q0 + qw + j * 32);
+            }
+        }
 #pragma unroll
         for (int j = 0; j < NN_Q; ++j) {
             if (!q[j].live) continue;
-            const long long o = T.q0 + qb + (long long)j * NN_T;
+            const long long o = T.q0 + qw + j * 32 + lane;
             if (MODE == NN_BAND) a.out_flag[o] = q[j].done ? 0 : 1;     // keep iff no reference within the band
             else {
                 a.out_d2[o] = q[j].best;
                 if (MODE == NN_ARGMIN) a.out_idx[o] = q[j].bidx;
             }
         }
+        __syncthreads();
     }
 }
 
@@ -394,7 +543,45 @@ __global__ void k_nn_tiles(NNArgs a)
 {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < a.ntask; t += gridDim.x * blockDim.x) {
         const NNTask T = a.task[t];
-        a.tile_cnt[t] = (T.qn > 0 && (T.rn > 0 || a.band_mode)) ? (int)((T.qn + NN_TILE - 1) / NN_TILE) : 0;
+        const bool on = T.qn > 0 && (T.rn > 0 || a.band_mode);
+        a.tile_cnt[t] = on ? (int)((T.qn + NN_TILE - 1) / NN_TILE) : 0;
+        a.round_cnt[t] = on ? (int)((T.rn + NN_R - 1) / NN_R) : 0;
+    }
+}
+
+// one warp per round: the box of each 32-reference block (lane b) and of the round
+__global__ void k_nn_boxes(NNArgs a)
+{
+    const long long nround = min(a.round_off[a.ntask], a.round_cap);
+    const int lane = threadIdx.x & 31;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long g = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; g < nround; g += nw) {
+        int lo = 0, hi = a.ntask - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (a.round_off[mid] <= g) lo = mid; else hi = mid - 1;
+        }
+        const NNTask T = a.task[lo];
+        const long long k0 = (g - a.round_off[lo]) * NN_R + (long long)lane * NN_BLK;
+        const long long k1 = min(k0 + NN_BLK, T.rn);
+        float l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (long long k = k0; k < k1; ++k) {
+            const float4 p = a.r_f4[T.r0 + k];
+            l[0] = fminf(l[0], p.x); l[1] = fminf(l[1], p.y); l[2] = fminf(l[2], p.z);
+            h[0] = fmaxf(h[0], p.x); h[1] = fmaxf(h[1], p.y); h[2] = fmaxf(h[2], p.z);
+        }
+        a.box_blk[2 * (g * NN_RB + lane)] = make_float4(l[0], l[1], l[2], 0.f);
+        a.box_blk[2 * (g * NN_RB + lane) + 1] = make_float4(h[0], h[1], h[2], 0.f);
+        for (int k = 0; k < 3; ++k) {
+            for (int o = 16; o > 0; o >>= 1) {
+                l[k] = fminf(l[k], __shfl_xor_sync(0xffffffffu, l[k], o));
+                h[k] = fmaxf(h[k], __shfl_xor_sync(0xffffffffu, h[k], o));
+            }
+        }
+        if (lane == 0) {
+            a.box_round[2 * g] = make_float4(l[0], l[1], l[2], 0.f);
+            a.box_round[2 * g + 1] = make_float4(h[0], h[1], h[2], 0.f);
+        }
     }
 }
 
@@ -403,12 +590,15 @@ void launch_nn_tiles(NNArgs a, int mode, long long* scan_tmp, cudaStream_t s)
     a.band_mode = mode == NN_BAND;
     k_nn_tiles<<<grid_for(a.ntask, 128), 128, 0, s>>>(a);
     scan_counts(a.tile_cnt, a.tile_off, a.ntask, scan_tmp, s);
+    scan_counts(a.round_cnt, a.round_off, a.ntask, scan_tmp, s);
 }
 
 void launch_nn_kernel(NNArgs a, int mode, long long tile_cap, cudaStream_t s)
 {
     a.band_mode = mode == NN_BAND;
-    const unsigned grid = grid_for(tile_cap, 1, 8);   // persistent: at most 8 tiles in flight per SM
+    k_nn_boxes<<<grid_for(a.round_cap * 32, 256), 256, 0, s>>>(a);
+    // one tile per CTA; CTAs past the tile count exit at once
+    const unsigned grid = (unsigned)(tile_cap < 1 ? 1 : (tile_cap > 0x7fffffffLL ? 0x7fffffffLL : tile_cap));
     if (mode == NN_MIN) k_nn<NN_MIN><<<grid, NN_T, 0, s>>>(a);
     else if (mode == NN_ARGMIN) k_nn<NN_ARGMIN><<<grid, NN_T, 0, s>>>(a);
     else k_nn<NN_BAND><<<grid, NN_T, 0, s>>>(a);
@@ -448,7 +638,7 @@ __global__ void k_points_bbox(const double* q, long long nq, const double* r, lo
 
 // reduce the partial boxes, then the single task covering both sets
 __global__ void k_points_task(const double* partials, int nblocks, long long nq, long long nr, double* bbox,
-                              NNTask* task, int* tile_cnt, long long* tile_off)
+                              NNTask* task, int* tile_cnt, long long* tile_off, int* round_cnt, long long* round_off)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double v[6];
@@ -471,6 +661,10 @@ __global__ void k_points_task(const double* partials, int nblocks, long long nq,
     tile_cnt[0] = (int)nt;
     tile_off[0] = 0;
     tile_off[1] = nt;
+    const long long nrd = nt > 0 ? (nr + NN_R - 1) / NN_R : 0;
+    round_cnt[0] = (int)nrd;
+    round_off[0] = 0;
+    round_off[1] = nrd;
 }
 
 __global__ void k_points_pack(const double* q, long long nq, const double* r, long long nr, const double* bbox,
@@ -486,10 +680,11 @@ __global__ void k_points_pack(const double* q, long long nq, const double* r, lo
 
 void launch_points_setup(const double* q, long long nq, const double* r, long long nr, double* partials,
                          int partial_blocks, double* bbox, float4* q_f4, float4* r_f4, NNTask* task, int* tile_cnt,
-                         long long* tile_off, cudaStream_t s)
+                         long long* tile_off, int* round_cnt, long long* round_off, cudaStream_t s)
 {
     k_points_bbox<<<partial_blocks, 256, 0, s>>>(q, nq, r, nr, partials);
-    k_points_task<<<1, 32, 0, s>>>(partials, partial_blocks, nq, nr, bbox, task, tile_cnt, tile_off);
+    k_points_task<<<1, 32, 0, s>>>(partials, partial_blocks, nq, nr, bbox, task, tile_cnt, tile_off, round_cnt,
+                                   round_off);
     k_points_pack<<<grid_for(nq + nr, 256), 256, 0, s>>>(q, nq, r, nr, bbox, q_f4, r_f4);
 }
 

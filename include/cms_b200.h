@@ -153,7 +153,7 @@ cms_status cms_nearest_dots(cms_ctx* ctx, const double* query_xyz, int64_t n_que
  * (NULL: no indices) are device pointers; the work is enqueued on `stream`
  * (NULL: the default stream) and no memory is allocated: the scratch is one
  * fixed 32 MiB device array per GPU, so n_query + n_ref may not exceed
- * 2,096,128 points (CMS_ERR_ARG otherwise, nothing launched).  The first call
+ * 1,966,080 points (CMS_ERR_ARG otherwise, nothing launched).  The first call
  * on a device looks up the scratch address (make it before any stream
  * capture); calls that overlap on the GPU share the scratch and race. */
 cms_status cms_nearest_dots_noalloc(const double* query_xyz, int64_t n_query, const double* ref_xyz,

@@ -19,7 +19,7 @@ from parity import exact
 
 pytestmark = pytest.mark.gpu
 
-MAX_POINTS = 2096128
+MAX_POINTS = 1920 * 1024
 
 
 def _lib():
