@@ -44,8 +44,8 @@ __device__ __forceinline__ int8_t buried_test(const Dev& d, int owner, V3 pcen)
     return 0;
 }
 
-__device__ __forceinline__ void write_dot(const Dev& d, long long q, V3 pt, V3 pcen, double area, int owner,
-                                          int type, int unit, int sub)
+__device__ __forceinline__ void write_dot_b(const Dev& d, long long q, V3 pt, V3 pcen, double area, int owner,
+                                            int type, int unit, int sub, int8_t bur)
 {
     if (q >= d.dot_cap) return;
     const double rp = d.st.rp;
@@ -53,11 +53,18 @@ __device__ __forceinline__ void write_dot(const Dev& d, long long q, V3 pt, V3 p
     st3(d.dxyz + 3 * q, pt);
     st3(d.dnml + 3 * q, nml);
     d.darea[q] = area;
-    d.dbur[q] = buried_test(d, owner, pcen);
+    d.dbur[q] = bur;
     d.dtype[q] = (int8_t)type;
     d.datom[q] = owner;
     d.dunit[q] = unit;
     d.dsub[q] = sub;
+}
+
+__device__ __forceinline__ void write_dot(const Dev& d, long long q, V3 pt, V3 pcen, double area, int owner,
+                                          int type, int unit, int sub)
+{
+    if (q >= d.dot_cap) return;
+    write_dot_b(d, q, pt, pcen, area, owner, type, unit, sub, buried_test(d, owner, pcen));
 }
 
 __device__ __forceinline__ long long unit_base(const Dev& d, int c, int m, int t, long long unit_scan)
@@ -214,6 +221,24 @@ void launch_convex(const Dev& d, bool emit, cudaStream_t s)
 // ---------------------------------------------------------------------------
 // toroidal dots: one warp per toroid pair, lanes over torus points
 // ---------------------------------------------------------------------------
+// Every torus point of a pair lies on one circle (centre tij, axis uij,
+// radius rij), and so does the probe centre of each of its arc dots.  Before
+// the points, the warp keeps the atoms whose sphere (radius r + rp) can reach
+// that circle: atom i's neighbours for the collision test and, when emitting,
+// the buried partners of i and j for the burial test.  The others fail those
+// tests at every point of the circle (a 1e-4 A margin covers the rounding of
+// the points), so the tests give the reference's results on the short lists.
+// The burial test depends on the probe centre alone, so each torus point
+// takes it once per arc instead of once per dot.
+//
+// A torus circle has few points (often under a dozen), so a warp takes
+// TO_PAIRS pairs at a time and spreads their points over its lanes; when
+// emitting, the dots of the 32 points of a chunk are spread over the lanes
+// again, so consecutive lanes write consecutive dots.
+static constexpr int TO_WARPS = 4;
+static constexpr int TO_PAIRS = 16;   // toroid pairs per warp batch
+static constexpr int TO_POOL = 512;   // pruned atom ids per warp batch (past it: the full lists are scanned)
+
 struct TorPair {
     int i, j;
     V3 xi, xj, uij, tij;
@@ -261,28 +286,92 @@ __device__ __forceinline__ TorPair tor_pair(const Dev& d, long long q)
     return T;
 }
 
+// Compact into out[] (room for cap ids) the atoms ids[s, e) other than
+// `skip` whose sphere of radius r + rp may reach the torus circle of T; -1
+// when they do not fit (the caller then scans the full list).  A non-finite
+// distance keeps the atom.
+__device__ __forceinline__ int tor_prune(const Dev& d, const TorPair& T, const int* ids, long long s, long long e,
+                                         int skip, int* out, int cap)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const double rp = d.st.rp;
+    int n = 0;
+    for (long long b = s; b < e; b += 32) {
+        const long long k = b + lane;
+        bool keep = false;
+        int id = -1;
+        if (k < e) {
+            id = ids[k];
+            if (id != skip) {
+                const double4 a = d.xyzr[id];
+                const V3 v = v3(a.x, a.y, a.z) - T.tij;
+                const double h = dot_seq(v, T.uij);
+                const double rho = sqrt(fmax(sq_seq(v) - h * h, 0.0));
+                const double dr = rho - T.rij;
+                const double t = a.w + rp + 1e-4;
+                keep = !(h * h + dr * dr > t * t);
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        const int pos = n + __popc(m & lt);
+        if (keep && pos < cap) out[pos] = id;
+        n += __popc(m);
+    }
+    __syncwarp();
+    return n > cap ? -1 : n;
+}
+
 struct TorPoint {
     V3 pij, pi, pj, axis, pqi, pqj;
     bool valid;    // survives the neighbour collision test (gives access)
     bool arcs;     // also passes the angle test (generates dots)
 };
 
-__device__ __forceinline__ TorPoint tor_point(const Dev& d, const TorPair& T, int s)
+// atom i's neighbours except atom j, strict <
+__device__ __forceinline__ bool tor_collides(const Dev& d, const TorPair& T, V3 pij, const int* near, int nnear)
+{
+    const double rp = d.st.rp;
+    if (nnear >= 0) {
+        for (int k = 0; k < nnear; ++k) {
+            const double4 b = d.xyzr[near[k]];
+            const double t = b.w + rp;
+            if (sq_alt(pij - v3(b.x, b.y, b.z)) < t * t) return true;
+        }
+        return false;
+    }
+    const long long off = d.nb_off[T.i];
+    const int K = d.nnb[T.i];
+    for (int k = 0; k < K; ++k) {
+        const int n = d.nb_id[off + k];
+        if (n == T.j) continue;
+        const double4 b = d.xyzr[n];
+        const double t = b.w + rp;
+        if (sq_alt(pij - v3(b.x, b.y, b.z)) < t * t) return true;
+    }
+    return false;
+}
+
+// burial of a probe centre on the torus circle: buried_test on the pruned list
+__device__ __forceinline__ int8_t tor_buried(const Dev& d, int owner, V3 pcen, const int* near, int nnear)
+{
+    if (nnear < 0) return buried_test(d, owner, pcen);
+    const double rp = d.st.rp;
+    for (int k = 0; k < nnear; ++k) {
+        const double4 b = d.xyzr[near[k]];
+        const double t = b.w + rp;
+        if (sq_seq(v3(b.x, b.y, b.z) - pcen) <= t * t) return 1;
+    }
+    return 0;
+}
+
+__device__ __forceinline__ TorPoint tor_point(const Dev& d, const TorPair& T, int s, const int* near, int nnear)
 {
     TorPoint P;
     const double rp = d.st.rp;
     P.pij = subdiv_point(T.tij, T.rij, T.fx, T.fy, T.dtor, s);
-    P.valid = true;
+    P.valid = !tor_collides(d, T, P.pij, near, nnear);
     P.arcs = false;
-    const long long off = d.nb_off[T.i];
-    const int K = d.nnb[T.i];
-    for (int k = 0; k < K; ++k) {                         // atom1's neighbours except atom2, strict <
-        int n = d.nb_id[off + k];
-        if (n == T.j) continue;
-        double4 b = d.xyzr[n];
-        double t = b.w + rp;
-        if (sq_alt(P.pij - v3(b.x, b.y, b.z)) < t * t) { P.valid = false; break; }
-    }
     if (!P.valid) return P;
     P.pi = (T.xi - P.pij) / T.eri;
     P.pj = (T.xj - P.pij) / T.erj;
@@ -327,8 +416,17 @@ __device__ __forceinline__ Arc tor_arc(const TorPair& T, const TorPoint& P, V3 x
     return A;
 }
 
-__device__ __forceinline__ int arc_count(const TorPair& T, const TorPoint& P, const Arc& A, double rp)
+__device__ __forceinline__ bool fin3(V3 v) { return isfinite(v.x) && isfinite(v.y) && isfinite(v.z); }
+
+// Dots of an arc whose area is a number.  With every input finite and rij
+// non-zero the points and areas are finite, so all A.n dots count.
+__device__ __forceinline__ int arc_count(const TorPair& T, const TorPoint& P, const Arc& A, double rp, bool& fast)
 {
+    if (A.n <= 0) return 0;
+    if (isfinite(A.ps) && isfinite(T.ts) && isfinite(T.rij) && T.rij != 0.0 && isfinite(T.darc) && isfinite(rp) &&
+        fin3(P.pij) && fin3(A.x) && fin3(A.y) && fin3(T.tij) && fin3(T.uij))
+        return A.n;
+    fast = false;
     int c = 0;
     for (int t = 0; t < A.n; ++t) {
         V3 pt = subdiv_point(P.pij, rp, A.x, A.y, T.darc, t);
@@ -338,14 +436,14 @@ __device__ __forceinline__ int arc_count(const TorPair& T, const TorPoint& P, co
 }
 
 __device__ __forceinline__ void arc_emit(const Dev& d, const TorPair& T, const TorPoint& P, const Arc& A, double rp,
-                                         long long q0, int owner, long long unit, int s, int arcbit)
+                                         long long q0, int owner, long long unit, int s, int arcbit, int8_t bur)
 {
     int c = 0;
     for (int t = 0; t < A.n; ++t) {
         V3 pt = subdiv_point(P.pij, rp, A.x, A.y, T.darc, t);
         double area = tor_area(T, A.ps, pt);
         if (isnan(area)) continue;
-        write_dot(d, q0 + c, pt, P.pij, area, owner, 2, (int)unit, (s << 16) | arcbit | t);
+        write_dot_b(d, q0 + c, pt, P.pij, area, owner, 2, (int)unit, (s << 16) | arcbit | t, bur);
         ++c;
     }
 }
@@ -362,60 +460,182 @@ __device__ __forceinline__ int warp_excl_scan(int v, int& total)
     return x - v;
 }
 
-static constexpr int TO_WARPS = 4;
+// one lane's arc, staged for the spread-out dot loop
+struct TorArcS {
+    V3 p, x, y;
+    double ps;
+    long long pos;     // dot index of the arc's first dot
+    int k, s, bur;     // pair slot in the batch, torus point, burial of its probe centre
+};
+
+// Emit the dots of the warp's arcs (c dots for this lane's arc, e its
+// exclusive scan, tot the warp's total), one dot per lane per step.  Every
+// arc here took the finite path, so its dots are 0 .. c-1 in order.
+__device__ __forceinline__ void tor_emit_spread(const Dev& d, TorArcS* S, int* X, const TorPair* tps, long long q0,
+                                                int c, int e, int tot, V3 pij, const Arc& A, long long pos, int k,
+                                                int s, int8_t bur, int arcbit)
+{
+    const int lane = threadIdx.x & 31;
+    const double rp = d.st.rp;
+    __syncwarp();
+    if (c > 0) {
+        TorArcS& a = S[lane];
+        a.p = pij; a.x = A.x; a.y = A.y; a.ps = A.ps; a.pos = pos; a.k = k; a.s = s; a.bur = bur;
+    }
+    X[lane] = e;
+    if (lane == 31) X[32] = e + c;
+    __syncwarp();
+    for (int g = lane; g < tot; g += 32) {
+        int lo = 0, hi = 31;                  // the lane whose dots cover g: largest o with X[o] <= g
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (X[mid] <= g) lo = mid; else hi = mid - 1;
+        }
+        const TorArcS& a = S[lo];
+        const TorPair& T = tps[a.k];
+        const int t = g - X[lo];
+        const V3 pt = subdiv_point(a.p, rp, a.x, a.y, T.darc, t);
+        write_dot_b(d, a.pos + t, pt, a.p, tor_area(T, a.ps, pt), arcbit ? T.j : T.i, 2, (int)(q0 + a.k),
+                    (a.s << 16) | arcbit | t, (int8_t)a.bur);
+    }
+}
 
 template <bool EMIT>
 __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
 {
-    const int lane = threadIdx.x & 31;
+    __shared__ TorPair tp[TO_WARPS][TO_PAIRS];
+    __shared__ int pool[TO_WARPS][TO_POOL];
+    __shared__ int pst[TO_WARPS][TO_PAIRS + 1];             // exclusive scan of torus points per pair
+    __shared__ int l_off[TO_WARPS][3][TO_PAIRS];            // pruned lists: neighbours of i, partners of i, of j
+    __shared__ int l_cnt[TO_WARPS][3][TO_PAIRS];
+    __shared__ int run[TO_WARPS][2][TO_PAIRS];              // arc dots of each pair before the current chunk
+    __shared__ int hasf[TO_WARPS][TO_PAIRS];
+    __shared__ unsigned char arcf[TO_WARPS][TO_PAIRS];      // bit 0: arc 1 dots, bit 1: arc 2 dots
+    __shared__ long long base[EMIT ? TO_WARPS : 1][2][TO_PAIRS];
+    __shared__ TorArcS arcs[EMIT ? TO_WARPS : 1][32];
+    __shared__ int arcx[EMIT ? TO_WARPS : 1][33];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int we = EMIT ? w : 0;
     const double rp = d.st.rp;
     const long long NT = min(d.tor_off[d.N], d.tor_cap);
-    const long long wid = blockIdx.x * (long long)TO_WARPS + (threadIdx.x >> 5);
-    const long long nw = (long long)gridDim.x * TO_WARPS;
-    for (long long q = wid; q < NT; q += nw) {
-        const TorPair T = tor_pair(d, q);
-        const bool arc1 = d.atten[T.i] >= 2, arc2 = d.atten[T.j] >= 2;
-        long long b1 = 0, b2 = 0;
-        if (EMIT) {
-            const int c = d.cplx[T.i], m = d.mol[T.i];
-            b1 = unit_base(d, c, m, 1, d.tor1_off[q]);
-            b2 = unit_base(d, c, m, 2, d.tor2_off[q]);
+    const long long nbatch = (NT + TO_PAIRS - 1) / TO_PAIRS;
+    for (long long bt = blockIdx.x * (long long)TO_WARPS + w; bt < nbatch; bt += (long long)gridDim.x * TO_WARPS) {
+        const long long q0 = bt * TO_PAIRS;
+        const int np = (int)min((long long)TO_PAIRS, NT - q0);
+        __syncwarp();
+        int ns = 0;
+        if (lane < np) {
+            const TorPair T = tor_pair(d, q0 + lane);
+            tp[w][lane] = T;
+            ns = T.ns;
+            run[w][0][lane] = 0; run[w][1][lane] = 0;
+            hasf[w][lane] = 0;
+            arcf[w][lane] = (unsigned char)((d.atten[T.i] >= 2 ? 1 : 0) | (d.atten[T.j] >= 2 ? 2 : 0));
+            if (EMIT) {
+                const int c = d.cplx[T.i], m = d.mol[T.i];
+                base[we][0][lane] = unit_base(d, c, m, 1, d.tor1_off[q0 + lane]);
+                base[we][1][lane] = unit_base(d, c, m, 2, d.tor2_off[q0 + lane]);
+            }
         }
-        int n1 = 0, n2 = 0;
-        bool has = false;
-        for (int s0 = 0; s0 < T.ns; s0 += 32) {
-            const int s = s0 + lane;
+        int tot;
+        const int ex = warp_excl_scan(ns, tot);
+        if (lane < np) pst[w][lane] = ex;
+        if (lane == 0) pst[w][np] = tot;
+        __syncwarp();
+        // pruned lists of the batch's pairs
+        int used = 0;
+        for (int k = 0; k < np; ++k) {
+            const TorPair& T = tp[w][k];
+            int c = tor_prune(d, T, d.nb_id, d.nb_off[T.i], d.nb_off[T.i] + d.nnb[T.i], T.j, pool[w] + used,
+                              TO_POOL - used);
+            if (lane == 0) { l_off[w][0][k] = used; l_cnt[w][0][k] = c; }
+            if (c > 0) used += c;
+            if (EMIT) {
+                const int af = arcf[w][k];
+                c = (af & 1) ? tor_prune(d, T, d.bu_id, d.bu_off[T.i], d.bu_off[T.i + 1], -1, pool[w] + used,
+                                         TO_POOL - used) : 0;
+                if (lane == 0) { l_off[w][1][k] = used; l_cnt[w][1][k] = c; }
+                if (c > 0) used += c;
+                c = (af & 2) ? tor_prune(d, T, d.bu_id, d.bu_off[T.j], d.bu_off[T.j + 1], -1, pool[w] + used,
+                                         TO_POOL - used) : 0;
+                if (lane == 0) { l_off[w][2][k] = used; l_cnt[w][2][k] = c; }
+                if (c > 0) used += c;
+            }
+        }
+        __syncwarp();
+        // torus points, 32 at a time; lanes of one pair are contiguous
+        for (int c0 = 0; c0 < tot; c0 += 32) {
+            const int g = c0 + lane;
+            const bool on = g < tot;
+            int k = 0;
+            if (on) {
+                int lo = 0, hi = np - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (pst[w][mid] <= g) lo = mid; else hi = mid - 1;
+                }
+                k = lo;
+            }
+            const TorPair& T = tp[w][k];
+            const int s = on ? g - pst[w][k] : 0;
             int c1 = 0, c2 = 0;
-            bool valid = false;
+            bool valid = false, fast = true;
             TorPoint P;
             Arc A1, A2;
-            if (s < T.ns) {
-                P = tor_point(d, T, s);
+            if (on) {
+                P = tor_point(d, T, s, pool[w] + l_off[w][0][k], l_cnt[w][0][k]);
                 valid = P.valid;
                 if (P.arcs) {
-                    if (arc1) { A1 = tor_arc(T, P, P.pi, P.pqi, rp); c1 = arc_count(T, P, A1, rp); }
-                    if (arc2) { A2 = tor_arc(T, P, P.pqj, P.pj, rp); c2 = arc_count(T, P, A2, rp); }
+                    const int af = arcf[w][k];
+                    if (af & 1) { A1 = tor_arc(T, P, P.pi, P.pqi, rp); c1 = arc_count(T, P, A1, rp, fast); }
+                    if (af & 2) { A2 = tor_arc(T, P, P.pqj, P.pj, rp); c2 = arc_count(T, P, A2, rp, fast); }
                 }
             }
-            has |= __any_sync(0xffffffffu, valid);
+            const int first = on ? max(pst[w][k] - c0, 0) : lane;
+            const int knext = __shfl_down_sync(0xffffffffu, k, 1);
+            const int onnext = __shfl_down_sync(0xffffffffu, on ? 1 : 0, 1);
+            const bool last = on && (lane == 31 || !onnext || knext != k);
             int t1, t2;
-            int e1 = warp_excl_scan(c1, t1);
-            int e2 = warp_excl_scan(c2, t2);
+            const int e1 = warp_excl_scan(c1, t1), e2 = warp_excl_scan(c2, t2);
+            const int f1 = __shfl_sync(0xffffffffu, e1, first), f2 = __shfl_sync(0xffffffffu, e2, first);
+            const unsigned vm = __ballot_sync(0xffffffffu, valid);
             if (EMIT) {
-                if (c1) arc_emit(d, T, P, A1, rp, b1 + n1 + e1, T.i, q, s, 0);
-                if (c2) arc_emit(d, T, P, A2, rp, b2 + n2 + e2, T.j, q, s, 1 << 15);
+                const long long pos1 = on ? base[we][0][k] + run[w][0][k] + (e1 - f1) : 0;
+                const long long pos2 = on ? base[we][1][k] + run[w][1][k] + (e2 - f2) : 0;
+                int8_t bur1 = 0, bur2 = 0;
+                if (c1) bur1 = tor_buried(d, T.i, P.pij, pool[w] + l_off[w][1][k], l_cnt[w][1][k]);
+                if (c2) bur2 = tor_buried(d, T.j, P.pij, pool[w] + l_off[w][2][k], l_cnt[w][2][k]);
+                if (__all_sync(0xffffffffu, fast)) {
+                    if (t1) tor_emit_spread(d, arcs[we], arcx[we], tp[w], q0, c1, e1, t1, P.pij, A1, pos1, k, s, bur1, 0);
+                    if (t2) tor_emit_spread(d, arcs[we], arcx[we], tp[w], q0, c2, e2, t2, P.pij, A2, pos2, k, s, bur2,
+                                            1 << 15);
+                } else {
+                    if (c1) arc_emit(d, T, P, A1, rp, pos1, T.i, q0 + k, s, 0, bur1);
+                    if (c2) arc_emit(d, T, P, A2, rp, pos2, T.j, q0 + k, s, 1 << 15, bur2);
+                }
             }
-            n1 += t1;
-            n2 += t2;
+            __syncwarp();
+            if (last) {
+                run[w][0][k] += (e1 + c1) - f1;
+                run[w][1][k] += (e2 + c2) - f2;
+                const unsigned seg = ((2u << lane) - 1u) & ~((1u << first) - 1u);
+                if (vm & seg) hasf[w][k] = 1;
+            }
+            __syncwarp();
         }
-        if (!EMIT && lane == 0) { d.tor1_cnt[q] = n1; d.tor2_cnt[q] = n2; d.tor_has[q] = has ? 1 : 0; }
+        if (!EMIT && lane < np) {
+            d.tor1_cnt[q0 + lane] = run[w][0][lane];
+            d.tor2_cnt[q0 + lane] = run[w][1][lane];
+            d.tor_has[q0 + lane] = (int8_t)hasf[w][lane];
+        }
     }
 }
 
 void launch_toroidal(const Dev& d, long long tor_grid, bool emit, cudaStream_t s)
 {
-    if (emit) k_toroidal<true><<<grid_for(tor_grid, TO_WARPS), TO_WARPS * 32, 0, s>>>(d);
-    else k_toroidal<false><<<grid_for(tor_grid, TO_WARPS), TO_WARPS * 32, 0, s>>>(d);
+    const long long batches = (tor_grid + TO_PAIRS - 1) / TO_PAIRS;
+    if (emit) k_toroidal<true><<<grid_for(batches, TO_WARPS), TO_WARPS * 32, 0, s>>>(d);
+    else k_toroidal<false><<<grid_for(batches, TO_WARPS), TO_WARPS * 32, 0, s>>>(d);
 }
 
 // ---------------------------------------------------------------------------
@@ -519,7 +739,16 @@ __global__ void __launch_bounds__(CC_WARPS * 32) k_concave(Dev d)
         lat_prefix(L, ncs[w], nl);
         const int total = nl > 0 ? L.start[nl] : 0;
         long long base = 0;
-        if (EMIT) base = unit_base(d, c, d.mol[ia[0]], 3, d.conc_off[p]);
+        // burial depends on the probe centre and the owner: one test per atom of the probe
+        int8_t bur3[3] = {0, 0, 0};
+        if (EMIT) {
+            base = unit_base(d, c, d.mol[ia[0]], 3, d.conc_off[p]);
+            if (d.conc_cnt[p] > 0) {
+                int8_t bk = 0;
+                if (lane < 3) bk = buried_test(d, lane == 0 ? ia[0] : (lane == 1 ? ia[1] : ia[2]), pijk);
+                for (int k = 0; k < 3; ++k) bur3[k] = (int8_t)__shfl_sync(0xffffffffu, (int)bk, k);
+            }
+        }
         int kept = 0;
         for (int t0 = 0; t0 < total; t0 += 32) {
             const int t = t0 + lane;
@@ -552,7 +781,9 @@ __global__ void __launch_bounds__(CC_WARPS * 32) k_concave(Dev d)
                 }
             }
             const unsigned m = __ballot_sync(0xffffffffu, keep);
-            if (EMIT && keep) write_dot(d, base + kept + __popc(m & lt), pts, pijk, L.area[l], ia[mc], 3, (int)p, (l << 16) | i);
+            if (EMIT && keep)
+                write_dot_b(d, base + kept + __popc(m & lt), pts, pijk, L.area[l], ia[mc], 3, (int)p, (l << 16) | i,
+                            mc == 0 ? bur3[0] : (mc == 1 ? bur3[1] : bur3[2]));
             kept += __popc(m);
         }
         if (!EMIT && lane == 0) d.conc_cnt[p] = kept;
