@@ -16,6 +16,7 @@
 // (probe, latitude, point).  Each unit's dots start at
 // seg.dot0 + (unit scan - seg.scan0); inside a unit a warp orders its dots
 // with ballots.
+#include "cms_circle.cuh"
 #include "cms_kernels.cuh"
 
 namespace cms {
@@ -227,7 +228,8 @@ void launch_convex(const Dev& d, bool emit, cudaStream_t s)
 // that circle: atom i's neighbours for the collision test and, when emitting,
 // the buried partners of i and j for the burial test.  The others fail those
 // tests at every point of the circle (a 1e-4 A margin covers the rounding of
-// the points), so the tests give the reference's results on the short lists.
+// the points), so the tests give the reference's results on the short lists
+// (cms_circle.cuh).
 // The burial test depends on the probe centre alone, so each torus point
 // takes it once per arc instead of once per dot.
 //
@@ -286,40 +288,11 @@ __device__ __forceinline__ TorPair tor_pair(const Dev& d, long long q)
     return T;
 }
 
-// Compact into out[] (room for cap ids) the atoms ids[s, e) other than
-// `skip` whose sphere of radius r + rp may reach the torus circle of T; -1
-// when they do not fit (the caller then scans the full list).  A non-finite
-// distance keeps the atom.
+// atoms of ids[s, e) other than `skip` that may reach the torus circle of T
 __device__ __forceinline__ int tor_prune(const Dev& d, const TorPair& T, const int* ids, long long s, long long e,
                                          int skip, int* out, int cap)
 {
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    const double rp = d.st.rp;
-    int n = 0;
-    for (long long b = s; b < e; b += 32) {
-        const long long k = b + lane;
-        bool keep = false;
-        int id = -1;
-        if (k < e) {
-            id = ids[k];
-            if (id != skip) {
-                const double4 a = d.xyzr[id];
-                const V3 v = v3(a.x, a.y, a.z) - T.tij;
-                const double h = dot_seq(v, T.uij);
-                const double rho = sqrt(fmax(sq_seq(v) - h * h, 0.0));
-                const double dr = rho - T.rij;
-                const double t = a.w + rp + 1e-4;
-                keep = !(h * h + dr * dr > t * t);
-            }
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, keep);
-        const int pos = n + __popc(m & lt);
-        if (keep && pos < cap) out[pos] = id;
-        n += __popc(m);
-    }
-    __syncwarp();
-    return n > cap ? -1 : n;
+    return circle_prune(d, T.tij, T.uij, T.rij, ids, s, e, skip, out, cap);
 }
 
 struct TorPoint {

@@ -513,7 +513,7 @@ __device__ __forceinline__ TripleBase triple_base(const Dev& d, V3 xi, double er
     return t;
 }
 
-static constexpr int TR_WARPS = 4;
+static constexpr int TR_WARPS = 2;
 static constexpr int TR_QCAP = 256;   // queued (pair slot, k slot) triples per warp
 
 // probes of the queued triples, in queue order: "+" and "-" probes are
@@ -588,10 +588,211 @@ __device__ __forceinline__ void triples_flush(const Dev& d, int g, V3 xi, double
     }
 }
 
+// Rows of up to TR_KC neighbours run from shared memory: the row's
+// coordinates and radii, and per neighbour k the distance dik = |xk - xi| and
+// unit vector uik = (xk - xi) / dik, which every pair (i, j) of the row
+// reuses.  Queued pairs keep their geometry for the probe pass.
+static constexpr int TR_KC = 128;
+static constexpr int TR_PQ = 32;      // queued pairs per probe pass
+
+struct TrRow {
+    double x[TR_KC], y[TR_KC], z[TR_KC], r[TR_KC];
+    double ux[TR_KC], uy[TR_KC], uz[TR_KC], dk[TR_KC];
+    int id[TR_KC];
+    int8_t at[TR_KC];
+};
+
+struct TrPairC { V3 uij, tij; int ps; };
+
+// norm3(v) < T, skipping the square root when the squared comparison settles
+// it: with a 1e-12 relative margin on T^2 the rounded root lies on the same side
+__device__ __forceinline__ bool norm_lt(V3 v, double T)
+{
+    const double s = dot_seq(v, v);
+    const double T2 = T * T;
+    if (s < T2 * (1.0 - 1e-12)) return true;
+    if (s > T2 * (1.0 + 1e-12)) return false;
+    return sqrt(s) < T;
+}
+
+// triple_base on the cached row: k after j, not all three blockers, the two distance tests
+__device__ __forceinline__ bool triple_ok_c(const TrRow& R, int ks, int j, V3 xj, double erj, double eri,
+                                            int8_t ati, int8_t atj, double rp)
+{
+    if (R.id[ks] <= j) return false;
+    if (ati <= 1 && atj <= 1 && R.at[ks] <= 1) return false;
+    const double erk = R.r[ks] + rp;
+    if (!norm_lt(v3(R.x[ks], R.y[ks], R.z[ks]) - xj, erj + erk)) return false;
+    return R.dk[ks] < eri + erk;
+}
+
+__device__ __forceinline__ bool probe_collides_c(const TrRow& R, int K, V3 pt, int j, int k, double rp)
+{
+    for (int s = 0; s < K; ++s) {
+        const int n = R.id[s];
+        if (n == j || n == k) continue;
+        const double t = R.r[s] + rp;
+        if (sq_alt(pt - v3(R.x[s], R.y[s], R.z[s])) <= t * t) return true;
+    }
+    return false;
+}
+
 template <bool EMIT>
+__device__ __forceinline__ void triples_flush_c(const Dev& d, int g, V3 xi, double eri, const TrRow& R, int K,
+                                                const unsigned* queue, const TrPairC* pq, int qn, int& nplus,
+                                                int& nminus, long long pbase, long long mbase)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const double rp = d.st.rp;
+    for (int e0 = 0; e0 < qn; e0 += 32) {
+        const int e = e0 + lane;
+        bool okp = false, okm = false;
+        V3 pp, pm, up;
+        double h = 0.0;
+        int j = -1, k = -1;
+        if (e < qn) {
+            const unsigned ent = queue[e];
+            const TrPairC& P = pq[ent >> 16];
+            const int ks = (int)(ent & 0xffffu);
+            j = R.id[P.ps];
+            k = R.id[ks];
+            const V3 xk = v3(R.x[ks], R.y[ks], R.z[ks]);
+            const double erk = R.r[ks] + rp;
+            const double dik = R.dk[ks];
+            const V3 uik = v3(R.ux[ks], R.uy[ks], R.uz[ks]);
+            const double dt = dot_alt(P.uij, uik);
+            const double wijk = acos(dt < -1.0 ? -1.0 : (dt > 1.0 ? 1.0 : dt));   // np.clip keeps NaN
+            const double swijk = sin(wijk);
+            if (!((dt >= 1.0) || (dt <= -1.0) || (wijk <= 0.0) || (swijk <= 0.0))) {
+                const V3 uijk = cross3(P.uij, uik) / swijk;
+                const V3 utb = cross3(uijk, P.uij);
+                const double asymm = (eri * eri - erk * erk) / dik;
+                const V3 tik = (xi + xk) * 0.5 + uik * (asymm * 0.5);
+                const double dtb = dot_alt(uik, tik - P.tij);
+                const V3 bijk = P.tij + utb * (dtb / swijk);
+                const V3 bma = bijk - xi;
+                const double h2 = eri * eri - dot_alt(bma, bma);
+                if (h2 > 0.0) {
+                    h = sqrt(h2);
+                    up = uijk;
+                    pp = bijk + uijk * (h * 1.0);
+                    pm = bijk + uijk * (h * -1.0);
+                    okp = !probe_collides_c(R, K, pp, j, k, rp);
+                    okm = !probe_collides_c(R, K, pm, j, k, rp);
+                }
+            }
+        }
+        const unsigned bp = __ballot_sync(0xffffffffu, okp);
+        const unsigned bm = __ballot_sync(0xffffffffu, okm);
+        if (EMIT) {
+            if (okp) {
+                long long q = pbase + nplus + __popc(bp & lt);
+                if (q < d.probe_cap) {
+                    d.pa0[q] = g; d.pa1[q] = j; d.pa2[q] = k;
+                    d.ph[q] = h; st3(d.pxyz + 3 * q, pp); st3(d.palt + 3 * q, up * 1.0);
+                }
+            }
+            if (okm) {
+                long long q = mbase + nminus + __popc(bm & lt);
+                if (q < d.probe_cap) {
+                    d.pa0[q] = j; d.pa1[q] = g; d.pa2[q] = k;
+                    d.ph[q] = h; st3(d.pxyz + 3 * q, pm); st3(d.palt + 3 * q, up * -1.0);
+                }
+            }
+            if (okp || okm) { d.access[g] = 1; d.access[j] = 1; d.access[k] = 1; }
+        }
+        nplus += __popc(bp);
+        nminus += __popc(bm);
+    }
+}
+
+// the triple loop of one atom whose row fits the cache (K <= TR_KC)
+template <bool EMIT>
+__device__ __forceinline__ void triples_row_c(const Dev& d, int g, int K, long long off, V3 xi, double ri, double eri,
+                                              int8_t ati, TrRow& R, unsigned* queue, TrPairC* pq, int& nplus,
+                                              int& nminus, long long pbase, long long mbase)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const double rp = d.st.rp;
+    for (int s = lane; s < K; s += 32) {
+        const int id = d.nb_id[off + s];
+        const double4 a = d.xyzr[id];
+        R.x[s] = a.x; R.y[s] = a.y; R.z[s] = a.z; R.r[s] = a.w;
+        R.id[s] = id;
+        R.at[s] = d.atten[id];
+        const V3 v = v3(a.x, a.y, a.z) - xi;
+        const double dk = norm3(v);
+        const V3 u = v / dk;
+        R.dk[s] = dk; R.ux[s] = u.x; R.uy[s] = u.y; R.uz[s] = u.z;
+    }
+    __syncwarp();
+    int qn = 0, npq = 0;
+    for (int ps = 0; ps < K; ++ps) {
+        const int j = R.id[ps];
+        if (j <= g) continue;
+        const V3 xj = v3(R.x[ps], R.y[ps], R.z[ps]);
+        const PairGeo p = pair_geo(xi, ri, xj, R.r[ps], rp);
+        if (!p.ok) continue;
+        const double erj = R.r[ps] + rp;
+        const int8_t atj = R.at[ps];
+        // a degenerate triple (|uij.uik| >= 1) inside the torus kills the whole pair
+        // (_core.py:1524-1543); the others are queued in (pair, k) order
+        bool kill = false;
+        int nq = 0;
+        unsigned cand[TR_KC / 32];
+#pragma unroll
+        for (int r = 0; r < TR_KC / 32; ++r) {
+            const int ks = r * 32 + lane;
+            bool c = false;
+            if (ks < K && triple_ok_c(R, ks, j, xj, erj, eri, ati, atj, rp)) {
+                const double dt = dot_alt(p.uij, v3(R.ux[ks], R.uy[ks], R.uz[ks]));
+                if (dt >= 1.0 || dt <= -1.0) {
+                    const double erk = R.r[ks] + rp;
+                    const double dtijk2 = sq_seq(p.tij - v3(R.x[ks], R.y[ks], R.z[ks]));
+                    const double rkp2 = erk * erk - p.rij * p.rij;
+                    kill |= dtijk2 < rkp2;
+                } else {
+                    c = true;
+                }
+            }
+            cand[r] = __ballot_sync(0xffffffffu, c);
+            nq += __popc(cand[r]);
+        }
+        if (__any_sync(0xffffffffu, kill)) continue;
+        if (nq == 0) continue;
+        if (qn + nq > TR_QCAP || npq == TR_PQ) {
+            __syncwarp();
+            triples_flush_c<EMIT>(d, g, xi, eri, R, K, queue, pq, qn, nplus, nminus, pbase, mbase);
+            __syncwarp();
+            qn = 0; npq = 0;
+        }
+        if (lane == 0) pq[npq] = TrPairC{p.uij, p.tij, ps};
+        const unsigned slot = (unsigned)npq << 16;
+        ++npq;
+#pragma unroll
+        for (int r = 0; r < TR_KC / 32; ++r) {
+            const unsigned m = cand[r];
+            if ((m >> lane) & 1u) queue[qn + __popc(m & lt)] = slot | (unsigned)(r * 32 + lane);
+            qn += __popc(m);
+        }
+        __syncwarp();
+    }
+    if (qn > 0) {
+        __syncwarp();
+        triples_flush_c<EMIT>(d, g, xi, eri, R, K, queue, pq, qn, nplus, nminus, pbase, mbase);
+    }
+    __syncwarp();
+}
+
+// LONG = false: atoms whose neighbour row fits the cache; true: the others
+template <bool EMIT, bool LONG>
 __global__ void __launch_bounds__(TR_WARPS * 32) k_triples(Dev d)
 {
     __shared__ unsigned queue_s[TR_WARPS][TR_QCAP];
+    __shared__ TrRow rows_s[LONG ? 1 : TR_WARPS];
+    __shared__ TrPairC pq_s[LONG ? 1 : TR_WARPS][TR_PQ];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     unsigned* queue = queue_s[w];
@@ -601,6 +802,7 @@ __global__ void __launch_bounds__(TR_WARPS * 32) k_triples(Dev d)
     for (long long gg = wid; gg < d.N; gg += nw) {
         const int g = (int)gg;
         const int K = d.nnb[g];
+        if (LONG != (K > TR_KC)) continue;
         int nplus = 0, nminus = 0;
         const int8_t ati = d.atten[g];
         const long long off = d.nb_off[g];
@@ -628,6 +830,12 @@ __global__ void __launch_bounds__(TR_WARPS * 32) k_triples(Dev d)
                 const long long mb = cbase + (d.mol[g] == 0 ? 0 : m0);
                 pbase = mb + (d.plus_off[g] - d.plus_off[ms]);
                 mbase = mb + (d.plus_off[me] - d.plus_off[ms]) + (d.minus_off[g] - d.minus_off[ms]);
+            }
+            if (!LONG) {
+                triples_row_c<EMIT>(d, g, K, off, xi, ai.w, eri, ati, rows_s[w], queue, pq_s[w], nplus, nminus,
+                                    pbase, mbase);
+                if (!EMIT && lane == 0) { d.nplus[g] = nplus; d.nminus[g] = nminus; }
+                continue;
             }
             int qn = 0;
             for (int ps = 0; ps < K; ++ps) {
@@ -716,8 +924,14 @@ __global__ void __launch_bounds__(TR_WARPS * 32) k_triples(Dev d)
 
 void launch_triples(const Dev& d, bool emit, cudaStream_t s)
 {
-    if (emit) k_triples<true><<<grid_for(d.N, TR_WARPS), TR_WARPS * 32, 0, s>>>(d);
-    else k_triples<false><<<grid_for(d.N, TR_WARPS), TR_WARPS * 32, 0, s>>>(d);
+    const unsigned g = grid_for(d.N, TR_WARPS, 32);
+    if (emit) {
+        k_triples<true, false><<<g, TR_WARPS * 32, 0, s>>>(d);
+        k_triples<true, true><<<g, TR_WARPS * 32, 0, s>>>(d);
+    } else {
+        k_triples<false, false><<<g, TR_WARPS * 32, 0, s>>>(d);
+        k_triples<false, true><<<g, TR_WARPS * 32, 0, s>>>(d);
+    }
 }
 
 // ---------------------------------------------------------------------------
