@@ -63,9 +63,10 @@ __global__ void k_setup(Dev d, int* ncell)
         } else {
             double lo[3] = {v[0], v[1], v[2]}, hi[3] = {-v[3], -v[4], -v[5]};
             C.radmax = -v[6];
-            double cut = 2.0 * fmax(C.radmax, 0.0) + 2.0 * fmax(rp, 0.0);
-            if (!d.all_atoms && d.st.sep > cut) cut = d.st.sep;
-            double h = fmax(cut, 1e-3) * (1.0 + 1e-6) + 1e-6;
+            // cells of half the longest neighbour bridge (2 radmax + 2 rp); the
+            // scans below visit every cell that meets their search ball
+            const double cut = 2.0 * fmax(C.radmax, 0.0) + 2.0 * fmax(rp, 0.0);
+            double h = fmax(fmax(0.5 * cut, d.all_atoms ? 0.0 : d.st.sep / 6.0), 0.1) * (1.0 + 1e-6) + 1e-6;
             long long nc;
             for (;;) {
                 nc = 1;
@@ -164,49 +165,125 @@ void launch_cells(const Dev& d, long long n_cells, long long* scan_tmp, cudaStre
     k_cell_sort<<<grid_for(n_cells, 128), 128, 0, s>>>(d, n_cells);
 }
 
-// visit every atom in the 27 cells around atom g's cell
-template <class F>
-__device__ __forceinline__ void for_near_atoms(const Dev& d, int g, int c, F&& f)
+// ---------------------------------------------------------------------------
+// Ball scan: a warp visits every atom in the cells that meet the ball of
+// radius `range` around atom g (a superset of the atoms within range).  The
+// cells of one (x, y) column that meet the ball are contiguous in cell_atom,
+// so the warp lays the columns end to end and hands one atom to each lane;
+// f(j) is called by all 32 lanes together, j = -1 past the end.  Cell
+// bounds get a 1e-9 A margin over the rounding of the cell assignment.
+// ---------------------------------------------------------------------------
+static constexpr int NB_WARPS = 4;
+
+__device__ __forceinline__ double slab_gap(double x, double lo, double hi)
 {
+    return fmax(fmax(lo - x, x - hi), 0.0);
+}
+
+__device__ __forceinline__ int warp_scan_excl(int v, int& total)
+{
+    const int lane = threadIdx.x & 31;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    total = __shfl_sync(0xffffffffu, x, 31);
+    return x - v;
+}
+
+struct BallScratch {
+    int pre[33];
+    long long beg[32];
+};
+
+template <class F>
+__device__ __forceinline__ void scan_ball(const Dev& d, int g, int c, double range, BallScratch& S, F&& f)
+{
+    const int lane = threadIdx.x & 31;
     const Cplx& C = d.cx[c];
+    const double4 a = d.xyzr[g];
     int x, y, z;
     atom_cell(d, g, c, x, y, z);
+    const double re = range * (1.0 + 1e-9) + 1e-9;
+    const double rc = fmin(ceil(re / C.h), 1e6);
+    const int R = (int)rc;
+    const int x0 = max(x - R, 0), x1 = min(x + R, C.dims[0] - 1);
+    const int y0 = max(y - R, 0), y1 = min(y + R, C.dims[1] - 1);
+    const int ny = y1 - y0 + 1;
+    const int ncol = (x1 - x0 + 1) * ny;
     const long long c0 = d.ncell_scan[c];
-    for (int ix = max(x - 1, 0); ix <= min(x + 1, C.dims[0] - 1); ++ix)
-        for (int iy = max(y - 1, 0); iy <= min(y + 1, C.dims[1] - 1); ++iy)
-            for (int iz = max(z - 1, 0); iz <= min(z + 1, C.dims[2] - 1); ++iz) {
-                long long cell = c0 + ((long long)ix * C.dims[1] + iy) * C.dims[2] + iz;
-                long long s = d.cell_start[cell], e = d.cell_start[cell + 1];
-                for (long long p = s; p < e; ++p) f(d.cell_atom[p]);
+    for (int cb = 0; cb < ncol; cb += 32) {
+        const int col = cb + lane;
+        long long s = 0;
+        int len = 0;
+        if (col < ncol) {
+            const int ix = x0 + col / ny, iy = y0 + col % ny;
+            const double gx = slab_gap(a.x, C.org[0] + ix * C.h, C.org[0] + (ix + 1) * C.h) - 1e-9;
+            const double gy = slab_gap(a.y, C.org[1] + iy * C.h, C.org[1] + (iy + 1) * C.h) - 1e-9;
+            const double gx2 = gx > 0.0 ? gx * gx : 0.0, gy2 = gy > 0.0 ? gy * gy : 0.0;
+            const double rem = re * re - (gx2 + gy2);
+            if (rem >= 0.0) {
+                const double dz = sqrt(rem) + 1e-9;
+                const int z0 = cell_coord(a.z - dz, C.org[2], C.h, C.dims[2]);
+                const int z1 = cell_coord(a.z + dz, C.org[2], C.h, C.dims[2]);
+                const long long base = c0 + ((long long)ix * C.dims[1] + iy) * C.dims[2];
+                s = d.cell_start[base + z0];
+                len = (int)(d.cell_start[base + z1 + 1] - s);
             }
+        }
+        int tot;
+        const int ex = warp_scan_excl(len, tot);
+        __syncwarp();
+        S.pre[lane] = ex;
+        S.beg[lane] = s;
+        if (lane == 31) S.pre[32] = tot;
+        __syncwarp();
+        for (int b = 0; b < tot; b += 32) {
+            const int i = b + lane;
+            int j = -1;
+            if (i < tot) {
+                int lo = 0, hi = 31;          // column holding i: largest k with pre[k] <= i
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (S.pre[mid] <= i) lo = mid; else hi = mid - 1;
+                }
+                j = d.cell_atom[S.beg[lo] + (i - S.pre[lo])];
+            }
+            f(j);
+        }
+    }
+    __syncwarp();
 }
 
 // ---------------------------------------------------------------------------
 // attention numbers: blocker (1) when the closest atom of the other molecule
 // is at least `sep` away, else 5; every atom gets 5 in all-atoms mode
 // ---------------------------------------------------------------------------
-__global__ void k_attention(Dev d)
+__global__ void __launch_bounds__(NB_WARPS * 32) k_attention(Dev d)
 {
-    for (long long gg = blockIdx.x * (long long)blockDim.x + threadIdx.x; gg < d.N; gg += (long long)gridDim.x * blockDim.x) {
+    __shared__ BallScratch sc[NB_WARPS];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long wid = blockIdx.x * (long long)NB_WARPS + w;
+    const long long nw = (long long)gridDim.x * NB_WARPS;
+    for (long long gg = wid; gg < d.N; gg += nw) {
         const int g = (int)gg;
-        if (d.all_atoms) { d.atten[g] = 5; continue; }
+        if (d.all_atoms) { if (lane == 0) d.atten[g] = 5; continue; }
         const int c = d.cplx[g];
         const V3 xi = atom_xyz(d, g);
         const int8_t mi = d.mol[g];
         double best = INFINITY;
-        for_near_atoms(d, g, c, [&](int j) {
-            if (d.mol[j] != mi) {
-                double d2 = sq_seq(xi - atom_xyz(d, j));
-                best = fmin(best, d2);
-            }
+        scan_ball(d, g, c, d.st.sep, sc[w], [&](int j) {
+            if (j >= 0 && d.mol[j] != mi) best = fmin(best, sq_seq(xi - atom_xyz(d, j)));
         });
-        d.atten[g] = (sqrt(best) >= d.st.sep) ? 1 : 5;
+        for (int o = 16; o > 0; o >>= 1) best = fmin(best, __shfl_xor_sync(0xffffffffu, best, o));
+        if (lane == 0) d.atten[g] = (sqrt(best) >= d.st.sep) ? 1 : 5;
     }
 }
 
 void launch_attention(const Dev& d, cudaStream_t s)
 {
-    k_attention<<<grid_for(d.N, 128), 128, 0, s>>>(d);
+    k_attention<<<grid_for(d.N, NB_WARPS), NB_WARPS * 32, 0, s>>>(d);
 }
 
 // ---------------------------------------------------------------------------
@@ -216,32 +293,13 @@ void launch_attention(const Dev& d, cudaStream_t s)
 //   coincident: same molecule, j != i, d2 <= 1e-4 (first pair reported)
 // rows sorted by (d2, j) (neighbours) and by j (buried partners)
 // ---------------------------------------------------------------------------
-static constexpr int NB_WARPS = 4;
 static constexpr int NB_CAP = 256;
 
-struct NearScan {
-    // warp-cooperative walk over the 27 cells; calls f(j, valid) with all 32 lanes
-    template <class F>
-    __device__ __forceinline__ static void run(const Dev& d, int g, int c, F&& f)
-    {
-        const Cplx& C = d.cx[c];
-        int x, y, z;
-        atom_cell(d, g, c, x, y, z);
-        const long long c0 = d.ncell_scan[c];
-        const int lane = threadIdx.x & 31;
-        for (int ix = max(x - 1, 0); ix <= min(x + 1, C.dims[0] - 1); ++ix)
-            for (int iy = max(y - 1, 0); iy <= min(y + 1, C.dims[1] - 1); ++iy)
-                for (int iz = max(z - 1, 0); iz <= min(z + 1, C.dims[2] - 1); ++iz) {
-                    long long cell = c0 + ((long long)ix * C.dims[1] + iy) * C.dims[2] + iz;
-                    long long s = d.cell_start[cell], e = d.cell_start[cell + 1];
-                    for (long long b = s; b < e; b += 32) {
-                        long long p = b + lane;
-                        int j = p < e ? d.cell_atom[p] : -1;
-                        f(j);
-                    }
-                }
-    }
-};
+// every partner of atom g lies within ri + radmax + 2 rp
+__device__ __forceinline__ double nb_range(const Dev& d, int c, double ri)
+{
+    return ri + fmax(d.cx[c].radmax, 0.0) + 2.0 * d.st.rp;
+}
 
 __device__ __forceinline__ void classify(const Dev& d, int g, V3 xi, double ri, int8_t mi, int j,
                                          bool& is_nb, bool& is_bur, bool& coin, double& d2)
@@ -264,8 +322,9 @@ __device__ __forceinline__ void classify(const Dev& d, int g, V3 xi, double ri, 
 
 __global__ void __launch_bounds__(NB_WARPS * 32) k_nb_count(Dev d)
 {
-    const int lane = threadIdx.x & 31;
-    const long long wid = blockIdx.x * (long long)NB_WARPS + (threadIdx.x >> 5);
+    __shared__ BallScratch sc[NB_WARPS];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long wid = blockIdx.x * (long long)NB_WARPS + w;
     const long long nw = (long long)gridDim.x * NB_WARPS;
     for (long long gg = wid; gg < d.N; gg += nw) {
         const int g = (int)gg;
@@ -274,7 +333,7 @@ __global__ void __launch_bounds__(NB_WARPS * 32) k_nb_count(Dev d)
         const V3 xi = v3(ai.x, ai.y, ai.z);
         const int8_t mi = d.mol[g];
         int nn = 0, nb = 0;
-        NearScan::run(d, g, c, [&](int j) {
+        scan_ball(d, g, c, nb_range(d, c, ai.w), sc[w], [&](int j) {
             bool is_nb, is_bur, coin; double d2;
             classify(d, g, xi, ai.w, mi, j, is_nb, is_bur, coin, d2);
             nn += __popc(__ballot_sync(0xffffffffu, is_nb));
@@ -298,10 +357,14 @@ void launch_neighbor_count(const Dev& d, cudaStream_t s)
     k_nb_count<<<grid_for(d.N, NB_WARPS), NB_WARPS * 32, 0, s>>>(d);
 }
 
+// one scan gathers both lists unsorted; neighbours are then placed by their
+// (d2, j) rank and buried partners by their atom index
 __global__ void __launch_bounds__(NB_WARPS * 32) k_nb_emit(Dev d, int* __restrict__ tmp_id)
 {
+    __shared__ BallScratch sc[NB_WARPS];
     __shared__ double sd2[NB_WARPS][NB_CAP];
     __shared__ int sid[NB_WARPS][NB_CAP];
+    __shared__ int sbid[NB_WARPS][NB_CAP];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     const long long wid = blockIdx.x * (long long)NB_WARPS + w;
@@ -314,63 +377,53 @@ __global__ void __launch_bounds__(NB_WARPS * 32) k_nb_emit(Dev d, int* __restric
         const int8_t mi = d.mol[g];
         const int K = d.nnb[g];
         const long long off = d.nb_off[g];
-        if (off + K > d.nb_cap || d.bu_off[g] + d.nbur[g] > d.bu_cap) {
+        const int KB = d.nbur[g];
+        const long long boff = d.bu_off[g];
+        if (off + K > d.nb_cap || boff + KB > d.bu_cap) {
             if (lane == 0) atomicOr(&d.status[c], ST_OVERFLOW);
             continue;
         }
-        const bool in_sh = K <= NB_CAP;
-        // ---- neighbours: gather unsorted, then place each by its rank ----
-        int cnt = 0;
-        NearScan::run(d, g, c, [&](int j) {
+        const bool in_sh = K <= NB_CAP, b_sh = KB <= NB_CAP;
+        int cnt = 0, bcnt = 0;
+        scan_ball(d, g, c, nb_range(d, c, ai.w), sc[w], [&](int j) {
             bool is_nb, is_bur, coin; double d2;
             classify(d, g, xi, ai.w, mi, j, is_nb, is_bur, coin, d2);
-            unsigned m = __ballot_sync(0xffffffffu, is_nb);
+            const unsigned m = __ballot_sync(0xffffffffu, is_nb);
             if (is_nb) {
-                int pos = cnt + __popc(m & lt);
+                const int pos = cnt + __popc(m & lt);
                 if (pos < K) {
                     if (in_sh) { sd2[w][pos] = d2; sid[w][pos] = j; }
                     else { d.nb_d2[off + pos] = d2; tmp_id[off + pos] = j; }
                 }
             }
             cnt += __popc(m);
+            const unsigned mb = __ballot_sync(0xffffffffu, is_bur);
+            if (is_bur) {
+                const int pos = bcnt + __popc(mb & lt);
+                if (pos < KB) {
+                    if (b_sh) sbid[w][pos] = j;
+                    else d.bu_id[boff + pos] = j;
+                }
+            }
+            bcnt += __popc(mb);
         });
         __syncwarp();
         for (int e = lane; e < K; e += 32) {
-            double ke = in_sh ? sd2[w][e] : d.nb_d2[off + e];
-            int je = in_sh ? sid[w][e] : tmp_id[off + e];
+            const double ke = in_sh ? sd2[w][e] : d.nb_d2[off + e];
+            const int je = in_sh ? sid[w][e] : tmp_id[off + e];
             int rank = 0;
             for (int f = 0; f < K; ++f) {
-                double kf = in_sh ? sd2[w][f] : d.nb_d2[off + f];
-                int jf = in_sh ? sid[w][f] : tmp_id[off + f];
+                const double kf = in_sh ? sd2[w][f] : d.nb_d2[off + f];
+                const int jf = in_sh ? sid[w][f] : tmp_id[off + f];
                 rank += (kf < ke || (kf == ke && jf < je)) ? 1 : 0;
             }
             d.nb_id[off + rank] = je;
         }
-        __syncwarp();
-        // ---- buried partners: ascending atom index ----
-        const int KB = d.nbur[g];
-        const long long boff = d.bu_off[g];
-        const bool b_sh = KB <= NB_CAP;
-        cnt = 0;
-        NearScan::run(d, g, c, [&](int j) {
-            bool is_nb, is_bur, coin; double d2;
-            classify(d, g, xi, ai.w, mi, j, is_nb, is_bur, coin, d2);
-            unsigned m = __ballot_sync(0xffffffffu, is_bur);
-            if (is_bur) {
-                int pos = cnt + __popc(m & lt);
-                if (pos < KB) {
-                    if (b_sh) sid[w][pos] = j;
-                    else d.bu_id[boff + pos] = j;
-                }
-            }
-            cnt += __popc(m);
-        });
-        __syncwarp();
         if (b_sh) {
             for (int e = lane; e < KB; e += 32) {
-                int je = sid[w][e];
+                const int je = sbid[w][e];
                 int rank = 0;
-                for (int f = 0; f < KB; ++f) rank += sid[w][f] < je ? 1 : 0;
+                for (int f = 0; f < KB; ++f) rank += sbid[w][f] < je ? 1 : 0;
                 d.bu_id[boff + rank] = je;
             }
         } else if (lane == 0) {
