@@ -26,6 +26,7 @@ struct Cplx {
     double ctr[3], R;           // centre and half-extent bounding every dot
     double radmax;
     long long cell0;            // first global cell
+    double mlo[2][3], mhi[2][3];  // bounding box of each molecule's atom centres
 };
 
 // dot segment bookkeeping: for complex c, molecule m and dot type t

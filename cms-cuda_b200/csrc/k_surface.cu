@@ -33,26 +33,35 @@ __global__ void k_setup(Dev d, int* ncell)
 {
     const int c = blockIdx.x;
     const int a0 = d.atom_off[c], a1 = d.atom_off[c + 1];
-    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-    double rmax = -INFINITY;
+    // per molecule: min xyz, -max xyz; then -max radius over both
+    double v[13];
+    for (int k = 0; k < 13; ++k) v[k] = INFINITY;
     for (int g = a0 + threadIdx.x; g < a1; g += blockDim.x) {
         double4 a = d.xyzr[g];
-        mn[0] = fmin(mn[0], a.x); mn[1] = fmin(mn[1], a.y); mn[2] = fmin(mn[2], a.z);
-        mx[0] = fmax(mx[0], a.x); mx[1] = fmax(mx[1], a.y); mx[2] = fmax(mx[2], a.z);
-        rmax = fmax(rmax, a.w);
+        const int m = (g - a0) < d.n0[c] ? 0 : 1;
+        double* b = v + 6 * m;
+        b[0] = fmin(b[0], a.x); b[1] = fmin(b[1], a.y); b[2] = fmin(b[2], a.z);
+        b[3] = fmin(b[3], -a.x); b[4] = fmin(b[4], -a.y); b[5] = fmin(b[5], -a.z);
+        v[12] = fmin(v[12], -a.w);
         d.cplx[g] = c;
-        d.mol[g] = (g - a0) < d.n0[c] ? 0 : 1;
+        d.mol[g] = (int8_t)m;
     }
-    __shared__ double sh[7][32];
-    double v[7] = {mn[0], mn[1], mn[2], -mx[0], -mx[1], -mx[2], -rmax};
-    for (int k = 0; k < 7; ++k)
+    __shared__ double sh[13][32];
+    for (int k = 0; k < 13; ++k)
         for (int o = 16; o > 0; o >>= 1) v[k] = fmin(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (lane == 0) for (int k = 0; k < 7; ++k) sh[k][w] = v[k];
+    if (lane == 0) for (int k = 0; k < 13; ++k) sh[k][w] = v[k];
     __syncthreads();
     if (threadIdx.x == 0) {
-        for (int k = 0; k < 7; ++k) { double m = sh[k][0]; for (int i = 1; i < nw; ++i) m = fmin(m, sh[k][i]); v[k] = m; }
+        for (int k = 0; k < 13; ++k) { double m = sh[k][0]; for (int i = 1; i < nw; ++i) m = fmin(m, sh[k][i]); v[k] = m; }
         Cplx C;
+        for (int m = 0; m < 2; ++m)
+            for (int k = 0; k < 3; ++k) { C.mlo[m][k] = v[6 * m + k]; C.mhi[m][k] = -v[6 * m + 3 + k]; }
+        // whole-complex box and radius in the layout used below
+        double u[7];
+        for (int k = 0; k < 3; ++k) { u[k] = fmin(v[k], v[6 + k]); u[3 + k] = fmin(v[3 + k], v[9 + k]); }
+        u[6] = v[12];
+        for (int k = 0; k < 7; ++k) v[k] = u[k];
         C.a0 = a0; C.n = a1 - a0; C.n0 = d.n0[c];
         const double rp = d.st.rp;
         if (C.n <= 0) {
@@ -272,6 +281,16 @@ __global__ void __launch_bounds__(NB_WARPS * 32) k_attention(Dev d)
         const int c = d.cplx[g];
         const V3 xi = atom_xyz(d, g);
         const int8_t mi = d.mol[g];
+        // farther than sep (plus a margin) from the other molecule's box: no atom within sep
+        {
+            const Cplx& C = d.cx[c];
+            const int o = 1 - mi;
+            const double gx = slab_gap(xi.x, C.mlo[o][0], C.mhi[o][0]);
+            const double gy = slab_gap(xi.y, C.mlo[o][1], C.mhi[o][1]);
+            const double gz = slab_gap(xi.z, C.mlo[o][2], C.mhi[o][2]);
+            const double se = d.st.sep * (1.0 + 1e-9) + 1e-9;
+            if (gx * gx + gy * gy + gz * gz > se * se) { if (lane == 0) d.atten[g] = 1; continue; }
+        }
         double best = INFINITY;
         scan_ball(d, g, c, d.st.sep, sc[w], [&](int j) {
             if (j >= 0 && d.mol[j] != mi) best = fmin(best, sq_seq(xi - atom_xyz(d, j)));
