@@ -448,8 +448,15 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
                 for (int b = 0; b < NN_RB; ++b) {
                     const int sb = b * NN_BLK;
                     if (sb >= nr) break;
-                    if (box_far(box_gap2(wl[0], wl[1], wl[2], wh[0], wh[1], wh[2], sBox[2 * b], sBox[2 * b + 1]), cthw))
-                        continue;
+                    const float4 blo = sBox[2 * b], bhi = sBox[2 * b + 1];
+                    if (box_far(box_gap2(wl[0], wl[1], wl[2], wh[0], wh[1], wh[2], blo, bhi), cthw)) continue;
+                    // each lane's open queries against the block's box
+                    bool lane_need = false;
+#pragma unroll
+                    for (int j = 0; j < NN_Q; ++j)
+                        lane_need |= !q[j].done &&
+                                     !box_far(box_gap2(qpx[j], qpy[j], qpz[j], qpx[j], qpy[j], qpz[j], blo, bhi), q[j].cth);
+                    if (!__any_sync(0xffffffffu, lane_need)) continue;
                     const int n = min(NN_BLK, nr - sb);
                     float m0 = INFINITY, m1 = INFINITY, m2 = INFINITY, m3 = INFINITY;
 #pragma unroll 4
@@ -494,6 +501,24 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
                 }
                 for (int o = 16; o > 0; o >>= 1) c = fmaxf(c, __shfl_xor_sync(0xffffffffu, c, o));
                 cthw = c;
+                if (MODE == NN_BAND) {
+                    // the warp's box shrinks to its open queries
+                    float l3[3] = {INFINITY, INFINITY, INFINITY}, h3[3] = {-INFINITY, -INFINITY, -INFINITY};
+#pragma unroll
+                    for (int j = 0; j < NN_Q; ++j) {
+                        if (q[j].done) continue;
+                        l3[0] = fminf(l3[0], qpx[j]); l3[1] = fminf(l3[1], qpy[j]); l3[2] = fminf(l3[2], qpz[j]);
+                        h3[0] = fmaxf(h3[0], qpx[j]); h3[1] = fmaxf(h3[1], qpy[j]); h3[2] = fmaxf(h3[2], qpz[j]);
+                    }
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        for (int o = 16; o > 0; o >>= 1) {
+                            l3[k] = fminf(l3[k], __shfl_xor_sync(0xffffffffu, l3[k], o));
+                            h3[k] = fmaxf(h3[k], __shfl_xor_sync(0xffffffffu, h3[k], o));
+                        }
+                        wl[k] = l3[k]; wh[k] = h3[k];
+                    }
+                }
             }
         }
 
