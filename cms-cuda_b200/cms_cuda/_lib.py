@@ -28,7 +28,8 @@ EXPORTED = (
     "cms_export_probes", "cms_export_dots", "cms_export_trimmed", "cms_run_graph", "cms_kernel_launches",
     "cms_last_error", "cms_version", "cms_device_count", "cms_profile_stages", "cms_stage_name",
     "cms_graph_launch", "cms_graph_check", "cms_nn_work", "cms_transfer_bytes", "cms_fp32_peak",
-    "cms_nearest_dots", "cms_nearest_dots_noalloc",
+    "cms_nearest_dots", "cms_nearest_dots_noalloc", "cms_contact_ms_backward", "cms_set_backward",
+    "cms_set_grad_total", "cms_grad_xyz", "cms_recompute_dots",
 )
 
 
@@ -103,6 +104,11 @@ def load():
             "cms_transfer_bytes": [_VP, _PI64, _PI64],
             "cms_fp32_peak": [_VP, ctypes.POINTER(ctypes.c_double)],
             "cms_nearest_dots": [_VP, _VP, ctypes.c_int64, _VP, ctypes.c_int64, _VP, _VP, _I32],
+            "cms_contact_ms_backward": [_VP, _I32, _VP, _VP, _I32],
+            "cms_set_backward": [_VP, _I32, _I32],
+            "cms_set_grad_total": [_VP, _VP, _I32],
+            "cms_grad_xyz": [_VP, _VP, _I32],
+            "cms_recompute_dots": [_VP, _I32, _I32, _VP, _VP],
         }
         for name, args in sig.items():
             f = getattr(lib, name)
@@ -241,6 +247,41 @@ class Context:
         totals = np.empty(2 * self.B, dtype=np.float64)
         self._check(self.lib.cms_contact_ms(self.h, _ptr(per_atom), _ptr(totals), CMS_HOST))
         return per_atom, totals.reshape(self.B, 2)
+
+    def contact_ms_backward(self, target_side=True, grad_total=None):
+        """d(sum_c grad_total[c] * CMS_c)/d(xyz) (N x 3) for one side, dot topology held fixed."""
+        g = None if grad_total is None else np.ascontiguousarray(grad_total, dtype=np.float64)
+        if g is not None and g.shape != (self.B,):
+            raise ValueError(f"grad_total must have shape ({self.B},)")
+        out = np.empty((self.N, 3), dtype=np.float64)
+        self._check(self.lib.cms_contact_ms_backward(self.h, 1 if target_side else 0, _ptr(g), _ptr(out), CMS_HOST))
+        return out
+
+    def contact_ms_backward_device(self, target_side, grad_total_ptr, grad_xyz_ptr):
+        """Device-pointer variant: grad_total (B) and grad_xyz (N x 3) are device buffers."""
+        self._check(self.lib.cms_contact_ms_backward(self.h, 1 if target_side else 0, ctypes.c_void_p(grad_total_ptr),
+                                                     ctypes.c_void_p(grad_xyz_ptr), CMS_DEVICE))
+
+    def set_backward(self, enable=True, target_side=True):
+        """Include the gradient of one side's CMS in the captured pipeline (upstream ones)."""
+        self._check(self.lib.cms_set_backward(self.h, 1 if enable else 0, 1 if target_side else 0))
+
+    def set_grad_total(self, grad_total):
+        g = np.ascontiguousarray(grad_total, dtype=np.float64)
+        self._check(self.lib.cms_set_grad_total(self.h, _ptr(g), CMS_HOST))
+
+    def grad_xyz(self):
+        out = np.empty((self.N, 3), dtype=np.float64)
+        self._check(self.lib.cms_grad_xyz(self.h, _ptr(out), CMS_HOST))
+        return out
+
+    def recompute_dots(self, c, m, info):
+        """Dots of complex c, molecule m recomputed by the adjoint's geometry (self-check)."""
+        n = max(info.n_dots[m], 1)
+        coor = np.empty((n, 3)); area = np.empty(n)
+        self._check(self.lib.cms_recompute_dots(self.h, int(c), int(m), _ptr(coor), _ptr(area)))
+        k = info.n_dots[m]
+        return coor[:k], area[:k]
 
     def max_contact_ms(self):
         per_atom = np.empty(self.N, dtype=np.float64)

@@ -198,7 +198,10 @@ struct cms_ctx {
     // graph
     cudaGraphExec_t gexec = nullptr;
     cudaGraph_t graph = nullptr;
-    long long graph_key[3] = {-1, -1, -1};
+    long long graph_key[4] = {-1, -1, -1, -1};
+    // gradient of one side's CMS (cms_set_backward / cms_contact_ms_backward)
+    int bwd_enabled = 0, bwd_side = 1;
+    bool bwd_ok = false;
     long long launches = -1;
     std::string err;
     // stage timing: an event after each pipeline stage when profiling
@@ -223,6 +226,8 @@ struct cms_ctx {
         S_TILE_CNT, S_TILE_OFF, S_ROUND_CNT, S_ROUND_OFF, S_BOX_ROUND, S_BOX_BLK, S_SUMMARY, S_EXPORT,
         S_NN_Q, S_NN_R, S_NN_QF4, S_NN_RF4, S_NN_PART, S_NN_BBOX, S_NN_TASK, S_NN_TCNT, S_NN_TOFF, S_NN_RCNT, S_NN_ROFF,
         S_NN_BOXR, S_NN_BOXB, S_NN_D2, S_NN_IDX, S_INFO,
+        S_CMS_IDX, S_ADJ_A, S_ADJ_REFDOT, S_ADJ_REFVEC, S_ADJ_RCNT, S_ADJ_RFILL, S_ADJ_ROFF, S_ADJ_RSLOT,
+        S_ADJ_GCONV, S_ADJ_GTOR, S_ADJ_GCONC, S_ADJ_GTOT, S_ADJ_GRAD, S_RECOMP_XYZ, S_RECOMP_AREA,
         S_COUNT
     };
 
@@ -386,6 +391,7 @@ void bind_caps(cms_ctx* x)
     r.trim_f4 = x->ensure<float4>(cms_ctx::S_R_TRIM_F4, D);
     r.nn_d2 = x->ensure<double>(cms_ctx::S_R_NN_D2, D);
     r.nn_idx = x->ensure<int>(cms_ctx::S_R_NN_IDX, D);
+    x->ensure<int>(cms_ctx::S_CMS_IDX, D);
     r.val = x->ensure<double>(cms_ctx::S_R_VAL, D);
     r.own = x->ensure<int>(cms_ctx::S_R_OWN, D);
     r.aslot = x->ensure<int>(cms_ctx::S_R_ASLOT, D);
@@ -409,7 +415,7 @@ long long* scan_tmp(cms_ctx* x) { return x->get<long long>(cms_ctx::S_SCAN_TMP);
 enum Stage {
     P_CELLS, P_ATTENTION, P_NB_COUNT, P_NB_EMIT, P_PAIRS, P_TRIPLES_COUNT, P_TRIPLES_EMIT, P_CONVEX_COUNT,
     P_TOROIDAL_COUNT, P_CONCAVE_COUNT, P_LAYOUT, P_CONVEX_EMIT, P_TOROIDAL_EMIT, P_CONCAVE_EMIT, P_SPLIT,
-    P_CMS_NN, P_CMS_SUM, P_SC_BAND_NN, P_SC_ARGMIN_NN, P_SC_STATS, P_MAX_SUM, P_NSTAGES
+    P_CMS_NN, P_CMS_SUM, P_SC_BAND_NN, P_SC_ARGMIN_NN, P_SC_STATS, P_MAX_SUM, P_BACKWARD, P_NSTAGES
 };
 
 void mark(cms_ctx* x, int stage)
@@ -549,7 +555,8 @@ void enqueue_cms(cms_ctx* x)
     a.q_f4 = r.bur_f4; a.q_idx = r.bur_idx; a.r_f4 = r.bur_f4; a.r_idx = r.bur_idx;
     a.q_xyz = a.r_xyz = d.dxyz;
     a.out_d2 = r.nn_d2;
-    launch_nn(a, NN_MIN, tile_cap(x), tmp, s);
+    a.out_idx = x->get<int>(cms_ctx::S_CMS_IDX);       // kept for the adjoint
+    launch_nn(a, NN_ARGMIN, tile_cap(x), tmp, s);
     mark(x, P_CMS_NN);
     launch_cms_weights(d, r, x->cap_dot, s);
     launch_per_atom_sum(d, r, x->cap_dot, x->get<double>(cms_ctx::S_PER_ATOM_CMS), tmp, s);
@@ -594,6 +601,47 @@ void enqueue_max(cms_ctx* x)
     launch_area_values(d, r, x->cap_dot, s);
     launch_per_atom_sum(d, r, x->cap_dot, x->get<double>(cms_ctx::S_PER_ATOM_MAX), scan_tmp(x), s);
     launch_atom_totals(d, x->get<double>(cms_ctx::S_PER_ATOM_MAX), x->get<double>(cms_ctx::S_TOT_MAX), s);
+}
+
+// adjoint buffers, sized to the current capacities
+AdjBuf bind_adj(cms_ctx* x)
+{
+    const long long D = x->cap_dot;
+    AdjBuf a{};
+    a.A = x->ensure<double4>(cms_ctx::S_ADJ_A, D);
+    a.cms_idx = x->get<int>(cms_ctx::S_CMS_IDX);
+    a.ref_dot = x->ensure<int>(cms_ctx::S_ADJ_REFDOT, D);
+    a.ref_vec = x->ensure<double4>(cms_ctx::S_ADJ_REFVEC, D);
+    a.rcnt = x->ensure<int>(cms_ctx::S_ADJ_RCNT, D);
+    a.rfill = x->ensure<int>(cms_ctx::S_ADJ_RFILL, D);
+    a.roff = x->ensure<long long>(cms_ctx::S_ADJ_ROFF, D + 1);
+    a.rslot = x->ensure<int>(cms_ctx::S_ADJ_RSLOT, D);
+    a.gconv = x->ensure<double>(cms_ctx::S_ADJ_GCONV, 6 * x->N);
+    a.gtor = x->ensure<double>(cms_ctx::S_ADJ_GTOR, 6 * std::max(x->cap_tor, 1LL));
+    a.gconc = x->ensure<double>(cms_ctx::S_ADJ_GCONC, 9 * std::max(x->cap_probe, 1LL));
+    a.gtot = x->ensure<double>(cms_ctx::S_ADJ_GTOT, x->B);
+    x->ensure<double>(cms_ctx::S_ADJ_GRAD, 3 * x->N);
+    return a;
+}
+
+void enqueue_backward(cms_ctx* x)
+{
+    const AdjBuf a = bind_adj(x);
+    launch_adjoint(x->d, x->r, a, x->get<NNTask>(cms_ctx::S_TASKS), x->bwd_side,
+                   x->get<double>(cms_ctx::S_ADJ_GRAD), scan_tmp(x), x->stream);
+    mark(x, P_BACKWARD);
+}
+
+void fill_gtot(cms_ctx* x, const double* g, int where)
+{
+    double* dst = x->ensure<double>(cms_ctx::S_ADJ_GTOT, x->B);
+    if (g) {
+        if (where == CMS_HOST) x->h2d_bytes += 8LL * x->B;
+        ck(cudaMemcpyAsync(dst, g, sizeof(double) * x->B,
+                           where == CMS_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, x->stream), "grad");
+    } else {
+        k_fill_d<<<grid1(x->B), 256, 0, x->stream>>>(dst, x->B, 1.0);
+    }
 }
 
 void enqueue_summary(cms_ctx* x)
@@ -811,8 +859,11 @@ cms_status cms_load_batch(cms_ctx* x, int32_t B, const int64_t* atom_off, const 
     ck(cudaGetLastError(), "pack");
     if (where == CMS_HOST) ck(cudaStreamSynchronize(s), "sync");   // host buffers may be released after return
     x->have_batch = true;
-    x->surf_ok = x->cms_ok = x->sc_ok = x->max_ok = false;
-    if (!same_shape) x->graph_key[0] = -1;
+    x->surf_ok = x->cms_ok = x->sc_ok = x->max_ok = x->bwd_ok = false;
+    if (!same_shape) {
+        x->graph_key[0] = -1;
+        if (x->bwd_enabled) fill_gtot(x, nullptr, CMS_DEVICE);    // upstream gradients of ones
+    }
     API_END
 }
 
@@ -1049,19 +1100,21 @@ namespace {
 void capture_graph(cms_ctx* x)
 {
     if (x->cap_dot == 0) run_sized_surface(x, 0);       // size every buffer once
-    const long long key[3] = {x->B, x->N, x->cap_dot};
+    const long long key[4] = {x->B, x->N, x->cap_dot, x->bwd_enabled ? 1 + x->bwd_side : 0};
     if (x->gexec && std::memcmp(key, x->graph_key, sizeof(key)) == 0) return;
     if (x->gexec) { cudaGraphExecDestroy(x->gexec); x->gexec = nullptr; }
     if (x->graph) { cudaGraphDestroy(x->graph); x->graph = nullptr; }
     x->d.all_atoms = 0;
     set_settings_dev(x);
     bind_caps(x);
+    if (x->bwd_enabled) bind_adj(x);                    // allocate before capture
     ck(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     try {
         enqueue_surface(x, false);
         enqueue_split(x);
         enqueue_cms(x);
         enqueue_sc(x);
+        if (x->bwd_enabled) enqueue_backward(x);
         enqueue_summary(x);
     } catch (...) {
         cudaGraph_t g = nullptr;
@@ -1090,6 +1143,7 @@ void mark_graph_results(cms_ctx* x)
     x->surf_ok = true;
     x->surf_all_atoms = 0;
     x->cms_ok = x->sc_ok = true;
+    x->bwd_ok = x->bwd_enabled != 0;
     x->max_ok = false;
 }
 
@@ -1111,6 +1165,7 @@ cms_status cms_run_graph(cms_ctx* x)
         run_sized_surface(x, 0);
         enqueue_cms(x);
         enqueue_sc(x);
+        if (x->bwd_enabled) enqueue_backward(x);
         enqueue_summary(x);
         pull_host_state(x);
         x->graph_key[0] = -1;
@@ -1252,7 +1307,7 @@ cms_status cms_transfer_bytes(cms_ctx* x, int64_t* h2d, int64_t* d2h)
 static const char* k_stage_names[P_NSTAGES] = {
     "cells", "attention", "neighbor_count", "neighbor_emit", "pairs", "triples_count", "triples_emit",
     "convex_count", "toroidal_count", "concave_count", "layout", "convex_emit", "toroidal_emit", "concave_emit",
-    "split_buried", "cms_nn", "cms_sum", "sc_band_nn", "sc_argmin_nn", "sc_stats", "max_sum"};
+    "split_buried", "cms_nn", "cms_sum", "sc_band_nn", "sc_argmin_nn", "sc_stats", "max_sum", "cms_backward"};
 
 const char* cms_stage_name(int32_t stage)
 {
@@ -1269,12 +1324,14 @@ cms_status cms_profile_stages(cms_ctx* x, double* ms, int32_t cap, int32_t* n_st
     x->d.all_atoms = 0;
     set_settings_dev(x);
     bind_caps(x);
+    if (x->bwd_enabled) bind_adj(x);
     x->profiling = true;
     try {
         enqueue_surface(x, false);
         enqueue_split(x);
         enqueue_cms(x);
         enqueue_sc(x);
+        if (x->bwd_enabled) enqueue_backward(x);
         enqueue_summary(x);
     } catch (...) {
         x->profiling = false;
@@ -1295,7 +1352,80 @@ cms_status cms_profile_stages(cms_ctx* x, double* ms, int32_t cap, int32_t* n_st
     if (n_stages) *n_stages = P_NSTAGES;
     pull_host_state(x);
     x->surf_ok = x->cms_ok = x->sc_ok = true;
+    x->bwd_ok = x->bwd_enabled != 0;
     x->max_ok = false;
+    API_END
+}
+
+cms_status cms_set_backward(cms_ctx* x, int32_t enable, int32_t target_side)
+{
+    if (!x) return CMS_ERR_ARG;
+    API_BEGIN
+    x->bwd_enabled = enable ? 1 : 0;
+    x->bwd_side = target_side ? 1 : 0;
+    x->bwd_ok = false;
+    if (x->have_batch) {
+        ck(cudaSetDevice(x->device), "cudaSetDevice");
+        fill_gtot(x, nullptr, CMS_DEVICE);
+    }
+    API_END
+}
+
+cms_status cms_set_grad_total(cms_ctx* x, const double* grad_total, int32_t where)
+{
+    if (!x || !grad_total) return fail(x, CMS_ERR_ARG, "null argument");
+    API_BEGIN
+    if (!x->have_batch) throw Fail{CMS_ERR_STATE, "no batch loaded"};
+    ck(cudaSetDevice(x->device), "cudaSetDevice");
+    fill_gtot(x, grad_total, where);
+    API_END
+}
+
+cms_status cms_contact_ms_backward(cms_ctx* x, int32_t target_side, const double* grad_total, double* grad_xyz,
+                                   int32_t where)
+{
+    if (!x || !grad_xyz) return fail(x, CMS_ERR_ARG, "null argument");
+    API_BEGIN
+    need_surface(x);
+    ck(cudaSetDevice(x->device), "cudaSetDevice");
+    if (!x->cms_ok) {
+        enqueue_cms(x);
+        ck(cudaGetLastError(), "cms kernels");
+        x->cms_ok = true;
+    }
+    x->bwd_side = target_side ? 1 : 0;
+    fill_gtot(x, grad_total, where);
+    enqueue_backward(x);
+    ck(cudaGetLastError(), "adjoint kernels");
+    x->bwd_ok = true;
+    copy_out(x, grad_xyz, x->get<double>(cms_ctx::S_ADJ_GRAD), sizeof(double) * 3 * x->N, where);
+    API_END
+}
+
+cms_status cms_grad_xyz(cms_ctx* x, double* grad_xyz, int32_t where)
+{
+    if (!x || !grad_xyz) return fail(x, CMS_ERR_ARG, "null argument");
+    API_BEGIN
+    if (!x->bwd_ok) throw Fail{CMS_ERR_STATE, "no gradient computed (enable cms_set_backward before the run)"};
+    copy_out(x, grad_xyz, x->get<double>(cms_ctx::S_ADJ_GRAD), sizeof(double) * 3 * x->N, where);
+    API_END
+}
+
+cms_status cms_recompute_dots(cms_ctx* x, int32_t c, int32_t molecule, double* coor, double* area)
+{
+    if (!x || !coor || !area || molecule < 0 || molecule > 1) return fail(x, CMS_ERR_ARG, "bad argument");
+    API_BEGIN
+    check_complex(x, c);
+    ck(cudaSetDevice(x->device), "cudaSetDevice");
+    double* rx = x->ensure<double>(cms_ctx::S_RECOMP_XYZ, 3 * x->cap_dot);
+    double* ra = x->ensure<double>(cms_ctx::S_RECOMP_AREA, x->cap_dot);
+    launch_recompute(x->d, rx, ra, x->stream);
+    ck(cudaGetLastError(), "recompute");
+    const long long b = x->h_dot_off[2 * c + molecule], e = x->h_dot_off[2 * c + molecule + 1];
+    if (e > b) {
+        copy_out(x, coor, rx + 3 * b, sizeof(double) * 3 * (e - b), CMS_HOST);
+        copy_out(x, area, ra + b, sizeof(double) * (e - b), CMS_HOST);
+    }
     API_END
 }
 

@@ -55,6 +55,24 @@ struct Rd {
     int* aslot;                                 // D
 };
 
+// adjoint of the contact molecular surface (k_adjoint.cu); capacity D = dot
+// capacity unless noted
+struct AdjBuf {
+    double4* A;            // per dot: (dCMS/dp, dCMS/darea)
+    int* cms_idx;          // per buried entry: nearest reference position of the CMS search
+    int* ref_dot;          // per buried entry: the reference dot its query picked (-1: none)
+    double4* ref_vec;      // per buried entry: contribution to that reference dot's position
+    int* rcnt; int* rfill; long long* roff; int* rslot;   // D, D, D + 1, D
+    double* gconv;         // 6 per atom: convex unit contributions (atom, frame atom)
+    double* gtor;          // 6 per toroid pair: (atom 1, atom 2)
+    double* gconc;         // 9 per probe: (atom 0, atom 1, atom 2)
+    const double* gtot;    // per complex: upstream gradient of the side's CMS
+};
+
+void launch_adjoint(const Dev& d, const Rd& r, const AdjBuf& a, const NNTask* cms_task, int side, double* grad,
+                    long long* scan_tmp, cudaStream_t s);
+void launch_recompute(const Dev& d, double* xyz, double* area, cudaStream_t s);
+
 void launch_split_buried(const Dev& d, const Rd& r, long long dot_cap, long long* scan_tmp, cudaStream_t s);
 void launch_tasks(const Dev& d, const Rd& r, int kind, NNTask* task, cudaStream_t s);
 void launch_nn(NNArgs a, int mode, long long tile_cap, long long* scan_tmp, cudaStream_t s);

@@ -1,0 +1,715 @@
+// FP64 adjoint of the contact molecular surface: d(sum_c g_c CMS_c)/d(xyz)
+// with the dot topology held fixed.
+//
+// CMS of one side of a complex (cms-cuda/_core.py:946-1004) is
+//   sum over the side's buried dots q of  area_q * exp(-w |p_q - p_r(q)|^2)
+// where r(q) is the nearest buried dot of the other side (first index on
+// ties).  Holding the topology fixed means keeping which dots exist, their
+// burial, their (latitude, point) / (torus point, arc point) indices, every
+// branch of the construction and r(q); positions and areas then are smooth
+// functions of the atom coordinates:
+//   convex dot of atom i      -- coordinates of i and of its first neighbour
+//                                (the frame atom), _core.py:1646-1840
+//   toroidal dot of pair i, j -- coordinates of i and j, _core.py:1847-2067
+//   concave dot of a probe    -- coordinates of its three atoms, through the
+//                                probe solve of _core.py:1445-1643 and the
+//                                cap construction of _core.py:2069-2333
+//
+// Passes:
+//   1. per query dot: the adjoints of its area and position, and the
+//      contribution to its nearest dot's position;
+//   2. per reference dot: the sum of the contributions from the queries that
+//      picked it, in query order (counting sort by reference dot);
+//   3. per unit (atom / toroid pair / probe) holding a dot with a non-zero
+//      adjoint: the unit's geometry in forward-mode duals (6 or 9 tangents,
+//      cms_dual.cuh), the Jacobian-transpose products summed over its dots in
+//      dot order, one 3-vector per atom of the unit;
+//   4. per atom: the unit contributions gathered in a fixed order.
+// Every sum has a fixed order, so the gradient is deterministic.
+//
+// The same unit code run on plain doubles recomputes the dots; that recompute
+// must equal the surface kernels' output bit for bit, which ties the
+// differentiated formula to the generated surface.
+#include "cms_dual.cuh"
+#include "cms_readout.cuh"
+
+namespace cms {
+
+static constexpr int SM_COUNT_ADJ = 148;
+
+static inline unsigned grid_adj(long long items, int per_block)
+{
+    long long b = (items + per_block - 1) / per_block;
+    const long long cap = (long long)SM_COUNT_ADJ * 16;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (unsigned)b;
+}
+
+__device__ __forceinline__ long long adj_doff(const Dev& d, long long i) { return min(d.dot_off[i], d.dot_cap); }
+
+__device__ __forceinline__ long long adj_unit_base(const Dev& d, int c, int m, int t, long long unit_scan)
+{
+    const Seg s = d.seg[(c * 2 + m) * 4 + t];
+    return s.dot0 + (unit_scan - s.scan0);
+}
+
+// ---------------------------------------------------------------------------
+// unit geometry, templated on double / Dn<K>
+// ---------------------------------------------------------------------------
+template <class T> struct DotV { TV3<T> p; T area; };
+
+// convex unit of atom g with frame atom n0 (k_convex in k_dots.cu)
+template <class T> struct ConvexU {
+    TV3<T> xi, north, ylat, fx, fy;
+    T cs;
+    double ri, dl, dens;
+    int nl;
+};
+
+template <class T>
+__device__ __forceinline__ ConvexU<T> convex_unit(const Dev& d, int g, const TV3<T>& xi, const TV3<T>& xn, double ri,
+                                                  double rj)
+{
+    ConvexU<T> U;
+    const double rp = d.st.rp;
+    const double eri = ri + rp;
+    U.xi = xi; U.ri = ri; U.dens = d.dens[g];
+    U.north = tnormalize(xi - xn);
+    const TV3<T>& n = U.north;
+    TV3<T> vt = tv3<T>(n.y * n.y + n.z * n.z, n.x * n.x + n.z * n.z, n.x * n.x + n.y * n.y);
+    vt = tnormalize(vt);
+    if (fabs(val(tdot_seq(vt, n))) > 0.99) vt = tconst<T>(v3(1.0, 0.0, 0.0));
+    const TV3<T> eq = tnormalize(tcross(n, vt));
+    const TV3<T> vql = tcross(eq, n);
+    TV3<T> south = tconst<T>(v3(0.0, 0.0, -1.0));
+    {
+        const double erj = rj + rp;
+        const T dij = tnorm(xn - xi);
+        const TV3<T> uij = (xn - xi) / dij;
+        const T asymm = (eri * eri - erj * erj) / dij;
+        const TV3<T> tij = ((xi + xn) * 0.5) + uij * (asymm * 0.5);
+        const T far_sq = (eri + erj) * (eri + erj) - dij * dij;
+        const double rd = ri - rj;
+        const T contain_sq = dij * dij - rd * rd;
+        if (val(far_sq) > 0.0 && val(contain_sq) > 0.0) {
+            const T rij = ((0.5 * dsqrt(far_sq)) * dsqrt(contain_sq)) / dij;
+            const TV3<T> pij = tij + vql * rij;
+            south = (pij - xi) / eri;
+        }
+    }
+    const T ang = tarc_angle(eq, n, south, U.ylat);
+    U.dl = subdiv_delta(U.dens, ri);
+    U.nl = subdiv_count(U.dl, val(ang));
+    U.cs = tsubdiv_ps(ri, ang, U.nl);
+    tcircle_frame(n, U.fx, U.fy);
+    return U;
+}
+
+template <class T> struct LatU { TV3<T> cen; T rad, delta, area; };
+
+template <class T>
+__device__ __forceinline__ LatU<T> convex_lat(const ConvexU<T>& U, int l)
+{
+    LatU<T> L;
+    const TV3<T> lat = tsubdiv_point(tconst<T>(v3(0.0, 0.0, 0.0)), U.ri, U.north, U.ylat, U.dl, l);
+    const T dt = tdot_seq(lat, U.north);
+    L.cen = U.xi + U.north * dt;
+    const T rsq = U.ri * U.ri - dt * dt;
+    L.rad = val(rsq) > 0.0 ? dsqrt(rsq) : lift<T>(0.0);
+    L.delta = lift<T>(0.0);
+    L.area = lift<T>(0.0);
+    if (val(L.rad) > 0.0) {
+        L.delta = tsubdiv_delta(U.dens, L.rad);
+        const int nc = subdiv_count(val(L.delta), CMS_TWO_PI);
+        const T ps = nc > 0 ? (L.rad * CMS_TWO_PI) / (double)nc : lift<T>(0.0);
+        L.area = ps * U.cs;
+    }
+    return L;
+}
+
+// toroidal unit of pair (i, j) (tor_pair / tor_point / tor_arc / tor_area in k_dots.cu)
+template <class T> struct TorU {
+    TV3<T> xi, xj, uij, tij, fx, fy;
+    T rij, ts, dtor;
+    double eri, erj, darc;
+    bool between;
+};
+
+template <class T>
+__device__ __forceinline__ TorU<T> tor_unit(const Dev& d, int i, int j, const TV3<T>& xi, const TV3<T>& xj)
+{
+    TorU<T> U;
+    const double rp = d.st.rp;
+    const double ri = d.xyzr[i].w, rj = d.xyzr[j].w;
+    U.xi = xi; U.xj = xj;
+    const TV3<T> diff = xj - xi;
+    const T dij_sq = tdot_alt(diff, diff);
+    const T dij = dsqrt(dij_sq);
+    U.eri = ri + rp; U.erj = rj + rp;
+    const T asymm = (U.eri * U.eri - U.erj * U.erj) / dij;
+    U.between = fabs(val(asymm)) < val(dij);
+    U.uij = diff / dij;
+    U.tij = ((xi + xj) * 0.5) + U.uij * (asymm * 0.5);
+    const T far_sq = (U.eri + U.erj) * (U.eri + U.erj) - dij_sq;
+    const double rd = ri - rj;
+    const T cont_sq = dij_sq - rd * rd;
+    U.rij = ((0.5 * dsqrt(far_sq)) * dsqrt(cont_sq)) / dij;
+    const double density = (d.dens[i] + d.dens[j]) * 0.5;
+    const T rci = (U.rij * ri) / U.eri;
+    const T rcj = (U.rij * rj) / U.erj;
+    const T rbt = U.rij - rp;
+    const T rb = val(rbt) < 0.0 ? lift<T>(0.0) : rbt;
+    const T rs = ((rci + 2.0 * rb) + rcj) * 0.25;
+    const T e = rs / U.rij;
+    const T edens = (e * e) * density;
+    tcircle_frame(U.uij, U.fx, U.fy);
+    U.dtor = 1.0 / (dsqrt(edens) * U.rij);
+    const int ns = subdiv_count(val(U.dtor), CMS_TWO_PI);
+    U.ts = tsubdiv_ps(U.rij, lift<T>(CMS_TWO_PI), ns);
+    U.darc = subdiv_delta(density, rp);
+    return U;
+}
+
+// one arc of torus point s: start x, frame y, per-point length ps
+template <class T> struct TorArcU { TV3<T> pij, x, y; T ps; };
+
+template <class T>
+__device__ __forceinline__ TorArcU<T> tor_point_arc(const Dev& d, const TorU<T>& U, int s, bool arc2)
+{
+    const double rp = d.st.rp;
+    TorArcU<T> A;
+    A.pij = tsubdiv_point(U.tij, U.rij, U.fx, U.fy, U.dtor, s);
+    const TV3<T> pi = (U.xi - A.pij) / U.eri;
+    const TV3<T> pj = (U.xj - A.pij) / U.erj;
+    const TV3<T> axis = tnormalize(tcross(pi, pj));
+    const T dtq = rp * rp - U.rij * U.rij;
+    TV3<T> pqi, pqj;
+    if (val(dtq) > 0.0 && U.between) {
+        const T dtq_s = dsqrt(dtq);
+        const TV3<T> qij = U.tij - U.uij * dtq_s;
+        pqi = (qij - A.pij) / rp;
+        pqj = tconst<T>(v3(0.0, 0.0, 0.0));
+    } else {
+        const TV3<T> mid = tnormalize(pi + pj);
+        pqi = mid;
+        pqj = mid;
+    }
+    const TV3<T> x = arc2 ? pqj : pi;
+    const TV3<T> v = arc2 ? pj : pqi;
+    A.x = x;
+    const T ang = tarc_angle(axis, x, v, A.y);
+    const int n = subdiv_count(U.darc, val(ang));
+    A.ps = tsubdiv_ps(rp, ang, n);
+    return A;
+}
+
+template <class T>
+__device__ __forceinline__ DotV<T> tor_dot(const Dev& d, const TorU<T>& U, const TorArcU<T>& A, int t)
+{
+    DotV<T> D;
+    D.p = tsubdiv_point(A.pij, d.st.rp, A.x, A.y, U.darc, t);
+    const TV3<T> vec = D.p - U.tij;
+    const T dt = tdot_seq(vec, U.uij);
+    const T d2 = tdot_seq(vec, vec) - dt * dt;
+    const T dist = val(d2) < 0.0 ? lift<T>(0.0) : dsqrt(d2);
+    D.area = ((A.ps * U.ts) * dist) / U.rij;
+    return D;
+}
+
+// probe solve of the triple loop (triples_flush in k_surface.cu): the probe
+// of sign sg (+1 / -1) over atoms i, j, k and its direction (alt = sg * uijk)
+template <class T>
+__device__ __forceinline__ void probe_solve(const Dev& d, const TV3<T>& xi, double ri, const TV3<T>& xj, double rj,
+                                            const TV3<T>& xk, double rk, double sg, TV3<T>& pijk, TV3<T>& alt)
+{
+    const double rp = d.st.rp;
+    const double eri = ri + rp, erj = rj + rp, erk = rk + rp;
+    const TV3<T> diff = xj - xi;
+    const T dij_sq = tdot_alt(diff, diff);
+    const T dij = dsqrt(dij_sq);
+    const T asymm_j = (eri * eri - erj * erj) / dij;
+    const TV3<T> uij = diff / dij;
+    const TV3<T> tij = ((xi + xj) * 0.5) + uij * (asymm_j * 0.5);
+    const TV3<T> vk = xk - xi;
+    const T dik = tnorm(vk);
+    const TV3<T> uik = vk / dik;
+    const T dt = tdot_alt(uij, uik);
+    const T dtc = val(dt) < -1.0 ? lift<T>(-1.0) : (val(dt) > 1.0 ? lift<T>(1.0) : dt);
+    const T wijk = dacos(dtc);
+    const T swijk = dsin(wijk);
+    const TV3<T> uijk = tcross(uij, uik) / swijk;
+    const TV3<T> utb = tcross(uijk, uij);
+    const T asymm = (eri * eri - erk * erk) / dik;
+    const TV3<T> tik = (xi + xk) * 0.5 + uik * (asymm * 0.5);
+    const T dtb = tdot_alt(uik, tik - tij);
+    const TV3<T> bijk = tij + utb * (dtb / swijk);
+    const TV3<T> bma = bijk - xi;
+    const T h2 = eri * eri - tdot_alt(bma, bma);
+    const T h = dsqrt(h2);
+    pijk = bijk + uijk * (h * sg);
+    alt = uijk * sg;
+}
+
+// concave unit of a probe (k_concave in k_dots.cu)
+template <class T> struct ConcU {
+    TV3<T> pijk, south, vtop, ylat, fx, fy;
+    T cs;
+    double density, dl;
+    int nl;
+};
+
+template <class T>
+__device__ __forceinline__ ConcU<T> conc_unit(const Dev& d, const TV3<T>* xa, const int* ia, const TV3<T>& pijk,
+                                              const TV3<T>& uijk)
+{
+    ConcU<T> U;
+    const double rp = d.st.rp;
+    U.pijk = pijk;
+    U.density = ((d.dens[ia[0]] + d.dens[ia[1]]) + d.dens[ia[2]]) / 3.0;
+    TV3<T> vp[3];
+    for (int k = 0; k < 3; ++k) vp[k] = tnormalize(xa[k] - pijk);
+    double dts[3];
+    for (int k = 0; k < 3; ++k) dts[k] = val(tdot_seq(uijk, vp[k]));
+    int mm = 0;                                   // np.argmax: first maximum, NaN wins
+    if (!isnan(dts[0])) {
+        for (int k = 1; k < 3; ++k) {
+            if (isnan(dts[k])) { mm = k; break; }
+            if (dts[k] > dts[mm]) mm = k;
+        }
+    }
+    U.south = -uijk;
+    U.vtop = vp[mm];
+    const TV3<T> axis = tnormalize(tcross(U.vtop, U.south));
+    const T ang = tarc_angle(axis, U.vtop, U.south, U.ylat);
+    U.dl = subdiv_delta(U.density, rp);
+    U.nl = subdiv_count(U.dl, val(ang));
+    U.cs = tsubdiv_ps(rp, ang, U.nl);
+    tcircle_frame(U.south, U.fx, U.fy);
+    return U;
+}
+
+template <class T>
+__device__ __forceinline__ LatU<T> conc_lat(const Dev& d, const ConcU<T>& U, int l)
+{
+    const double rp = d.st.rp, rp2 = rp * rp;
+    LatU<T> L;
+    const TV3<T> lat = tsubdiv_point(tconst<T>(v3(0.0, 0.0, 0.0)), rp, U.vtop, U.ylat, U.dl, l);
+    const T dt = tdot_seq(lat, U.south);
+    L.cen = U.south * dt;
+    const T rsq = rp2 - dt * dt;
+    L.rad = dsqrt(val(rsq) < 0.0 ? lift<T>(0.0) : rsq);
+    L.delta = lift<T>(0.0);
+    L.area = lift<T>(0.0);
+    if (val(L.rad) > 0.0) {
+        L.delta = tsubdiv_delta(U.density, L.rad);
+        const int nc = subdiv_count(val(L.delta), CMS_TWO_PI);
+        const T ps = nc > 0 ? (L.rad * CMS_TWO_PI) / (double)nc : lift<T>(0.0);
+        L.area = ps * U.cs;
+    }
+    return L;
+}
+
+// the sign of probe p and the index of its triple's atom i among (a0, a1, a2):
+// probes are laid out per complex as [+mol0 | -mol0 | +mol1 | -mol1]
+__device__ __forceinline__ bool probe_is_plus(const Dev& d, long long p, int a0)
+{
+    const int c = d.cplx[a0];
+    const Cplx C = d.cx[c];
+    const int s0 = C.a0, s1 = C.a0 + C.n0, e1 = C.a0 + C.n;
+    const int m = d.mol[a0];
+    const int ms = m == 0 ? s0 : s1, me = m == 0 ? s1 : e1;
+    const long long cbase = d.plus_off[s0] + d.minus_off[s0];
+    const long long m0 = (d.plus_off[s1] - d.plus_off[s0]) + (d.minus_off[s1] - d.minus_off[s0]);
+    const long long mb = cbase + (m == 0 ? 0 : m0);
+    return p < mb + (d.plus_off[me] - d.plus_off[ms]);
+}
+
+// ---------------------------------------------------------------------------
+// per-unit drivers: f.want(dot) selects dots, f.take(dot, DotV) consumes them
+// ---------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ TV3<T> atom_t(const Dev& d, int a, int k0);
+
+template <>
+__device__ __forceinline__ TV3<double> atom_t<double>(const Dev& d, int a, int)
+{
+    const double4 x = d.xyzr[a];
+    return tv3<double>(x.x, x.y, x.z);
+}
+
+template <int K>
+__device__ __forceinline__ TV3<Dn<K>> atom_dn(const Dev& d, int a, int k0)
+{
+    const double4 x = d.xyzr[a];
+    return tv3<Dn<K>>(dn_var<K>(x.x, k0), dn_var<K>(x.y, k0 + 1), dn_var<K>(x.z, k0 + 2));
+}
+
+template <> __device__ __forceinline__ TV3<Dn<6>> atom_t<Dn<6>>(const Dev& d, int a, int k0) { return atom_dn<6>(d, a, k0); }
+template <> __device__ __forceinline__ TV3<Dn<9>> atom_t<Dn<9>>(const Dev& d, int a, int k0) { return atom_dn<9>(d, a, k0); }
+
+template <class T, class F>
+__device__ __forceinline__ void convex_unit_dots(const Dev& d, int g, F& f)
+{
+    const long long base = adj_unit_base(d, d.cplx[g], d.mol[g], 0, d.conv_off[g]);
+    const int cnt = d.conv_cnt[g];
+    const int n0 = d.nb_id[d.nb_off[g]];
+    const ConvexU<T> U = convex_unit<T>(d, g, atom_t<T>(d, g, 0), atom_t<T>(d, n0, 3), d.xyzr[g].w, d.xyzr[n0].w);
+    int cur = -1;
+    LatU<T> L;
+    for (long long q = base; q < base + cnt; ++q) {
+        if (q >= d.dot_cap || !f.want(q)) continue;
+        const int sub = d.dsub[q];
+        const int l = sub >> 16, i = sub & 0xffff;
+        if (l != cur) { L = convex_lat(U, l); cur = l; }
+        DotV<T> D;
+        D.p = tsubdiv_point(L.cen, L.rad, U.fx, U.fy, L.delta, i);
+        D.area = L.area;
+        f.take(q, D);
+    }
+}
+
+template <class T, class F>
+__device__ __forceinline__ void tor_unit_dots(const Dev& d, long long qp, F& f)
+{
+    const int i = d.tor_i[qp], j = d.tor_j[qp];
+    const int c = d.cplx[i], m = d.mol[i];
+    const TorU<T> U = tor_unit<T>(d, i, j, atom_t<T>(d, i, 0), atom_t<T>(d, j, 3));
+    for (int arc = 0; arc < 2; ++arc) {
+        const long long base = adj_unit_base(d, c, m, 1 + arc, arc ? d.tor2_off[qp] : d.tor1_off[qp]);
+        const int cnt = arc ? d.tor2_cnt[qp] : d.tor1_cnt[qp];
+        int cur = -1;
+        TorArcU<T> A;
+        for (long long q = base; q < base + cnt; ++q) {
+            if (q >= d.dot_cap || !f.want(q)) continue;
+            const int sub = d.dsub[q];
+            const int s = sub >> 16, t = sub & 0x7fff;
+            if (s != cur) { A = tor_point_arc(d, U, s, arc == 1); cur = s; }
+            f.take(q, tor_dot(d, U, A, t));
+        }
+    }
+}
+
+template <class T, class F>
+__device__ __forceinline__ void conc_unit_dots(const Dev& d, long long p, F& f)
+{
+    const int ia[3] = {d.pa0[p], d.pa1[p], d.pa2[p]};
+    TV3<T> xa[3];
+    for (int k = 0; k < 3; ++k) xa[k] = atom_t<T>(d, ia[k], 3 * k);
+    const bool plus = probe_is_plus(d, p, ia[0]);
+    // the triple's (i, j): (a0, a1) for a "+" probe, (a1, a0) for a "-" probe
+    const int si = plus ? 0 : 1, sj = plus ? 1 : 0;
+    TV3<T> pijk, uijk;
+    probe_solve<T>(d, xa[si], d.xyzr[ia[si]].w, xa[sj], d.xyzr[ia[sj]].w, xa[2], d.xyzr[ia[2]].w, plus ? 1.0 : -1.0,
+                   pijk, uijk);
+    const ConcU<T> U = conc_unit<T>(d, xa, ia, pijk, uijk);
+    const int c = d.cplx[ia[0]];
+    const long long base = adj_unit_base(d, c, d.mol[ia[0]], 3, d.conc_off[p]);
+    const int cnt = d.conc_cnt[p];
+    int cur = -1;
+    LatU<T> L;
+    for (long long q = base; q < base + cnt; ++q) {
+        if (q >= d.dot_cap || !f.want(q)) continue;
+        const int sub = d.dsub[q];
+        const int l = sub >> 16, i = sub & 0xffff;
+        if (l != cur) { L = conc_lat(d, U, l); cur = l; }
+        DotV<T> D;
+        D.p = tsubdiv_point(L.cen, L.rad, U.fx, U.fy, L.delta, i) + U.pijk;
+        D.area = L.area;
+        f.take(q, D);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// recompute (plain doubles): positions and areas of every dot
+// ---------------------------------------------------------------------------
+struct RecomputeF {
+    double* xyz; double* area;
+    __device__ bool want(long long) const { return true; }
+    __device__ void take(long long q, const DotV<double>& D)
+    {
+        xyz[3 * q] = D.p.x; xyz[3 * q + 1] = D.p.y; xyz[3 * q + 2] = D.p.z;
+        area[q] = D.area;
+    }
+};
+
+__global__ void k_recompute(Dev d, double* xyz, double* area)
+{
+    RecomputeF f{xyz, area};
+    const long long NT = min(d.tor_off[d.N], d.tor_cap);
+    const long long NP = min(d.plus_off[d.N] + d.minus_off[d.N], d.probe_cap);
+    const long long total = d.N + NT + NP;
+    for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < total; u += (long long)gridDim.x * blockDim.x) {
+        if (u < d.N) {
+            if (d.conv_cnt[u] > 0) convex_unit_dots<double>(d, (int)u, f);
+        } else if (u < d.N + NT) {
+            tor_unit_dots<double>(d, u - d.N, f);
+        } else {
+            conc_unit_dots<double>(d, u - d.N - NT, f);
+        }
+    }
+}
+
+void launch_recompute(const Dev& d, double* xyz, double* area, cudaStream_t s)
+{
+    k_recompute<<<grid_adj((long long)d.N + d.tor_cap + d.probe_cap, 128), 128, 0, s>>>(d, xyz, area);
+}
+
+// ---------------------------------------------------------------------------
+// adjoint
+// ---------------------------------------------------------------------------
+// pass 1: query dots of `side`; A = (d/dp, d/darea) per dot
+__global__ void k_adj_queries(Dev d, Rd r, AdjBuf a, const NNTask* task, int side)
+{
+    const long long NB = r.bur_scan[adj_doff(d, 2LL * d.B)];
+    const double w = d.st.weight;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < NB; k += (long long)gridDim.x * blockDim.x) {
+        a.ref_dot[k] = -1;
+        const int cm = r.bur_cm[k];
+        if ((cm & 1) != side) continue;
+        const NNTask T = task[cm];
+        const int idx = a.cms_idx[k];
+        if (T.rn <= 0 || idx < 0 || idx >= T.rn) continue;
+        const int q = r.bur_idx[k];
+        const int rd = r.bur_idx[T.r0 + idx];
+        const double g = a.gtot[cm >> 1];
+        const double* pq = d.dxyz + 3LL * q;
+        const double* pr = d.dxyz + 3LL * rd;
+        // cdist(ref, query) order, as the search computed it
+        const double dx = pr[0] - pq[0], dy = pr[1] - pq[1], dz = pr[2] - pq[2];
+        const double d2 = (dx * dx + dy * dy) + dz * dz;
+        const double e = exp((-d2) * w);
+        const double area = d.darea[q];
+        // d(area e)/dp_q = area e (-w) 2 (p_q - p_r) = area e 2w (p_r - p_q)
+        const double s = g * area * e * 2.0 * w;
+        a.A[q] = make_double4(s * dx, s * dy, s * dz, g * e);
+        a.ref_dot[k] = rd;
+        a.ref_vec[k] = make_double4(-s * dx, -s * dy, -s * dz, 0.0);
+    }
+}
+
+// pass 2: reference contributions, counting sort by reference dot
+__global__ void k_adj_ref_count(Dev d, Rd r, AdjBuf a)
+{
+    const long long NB = r.bur_scan[adj_doff(d, 2LL * d.B)];
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < NB; k += (long long)gridDim.x * blockDim.x) {
+        const int rd = a.ref_dot[k];
+        if (rd >= 0) atomicAdd(&a.rcnt[rd], 1);
+    }
+}
+
+__global__ void k_adj_ref_fill(Dev d, Rd r, AdjBuf a)
+{
+    const long long NB = r.bur_scan[adj_doff(d, 2LL * d.B)];
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < NB; k += (long long)gridDim.x * blockDim.x) {
+        const int rd = a.ref_dot[k];
+        if (rd >= 0) a.rslot[a.roff[rd] + atomicAdd(&a.rfill[rd], 1)] = (int)k;
+    }
+}
+
+__global__ void k_adj_ref_sum(Dev d, AdjBuf a, long long cap)
+{
+    const long long D = adj_doff(d, 2LL * d.B);
+    for (long long rd = blockIdx.x * (long long)blockDim.x + threadIdx.x; rd < D && rd < cap;
+         rd += (long long)gridDim.x * blockDim.x) {
+        const int n = a.rcnt[rd];
+        if (n == 0) continue;
+        int* s = a.rslot + a.roff[rd];
+        for (int i = 1; i < n; ++i) {          // query order
+            const int v = s[i];
+            int k = i - 1;
+            while (k >= 0 && s[k] > v) { s[k + 1] = s[k]; --k; }
+            s[k + 1] = v;
+        }
+        double x = 0.0, y = 0.0, z = 0.0;
+        for (int i = 0; i < n; ++i) {
+            const double4 v = a.ref_vec[s[i]];
+            x += v.x; y += v.y; z += v.z;
+        }
+        const double4 o = a.A[rd];
+        a.A[rd] = make_double4(o.x + x, o.y + y, o.z + z, o.w);
+    }
+}
+
+// pass 3: units; J^T A summed over the unit's dots in dot order
+template <int K>
+struct AdjF {
+    const double4* A;
+    double g[K];
+    __device__ bool want(long long q) const
+    {
+        const double4 v = A[q];
+        return v.x != 0.0 || v.y != 0.0 || v.z != 0.0 || v.w != 0.0;
+    }
+    __device__ void take(long long q, const DotV<Dn<K>>& D)
+    {
+        const double4 v = A[q];
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            g[k] += ((v.x * D.p.x.d[k] + v.y * D.p.y.d[k]) + v.z * D.p.z.d[k]) + v.w * D.area.d[k];
+    }
+};
+
+__device__ __forceinline__ bool any_adj(const AdjBuf& a, long long base, int cnt, long long cap)
+{
+    for (long long q = base; q < base + cnt && q < cap; ++q) {
+        const double4 v = a.A[q];
+        if (v.x != 0.0 || v.y != 0.0 || v.z != 0.0 || v.w != 0.0) return true;
+    }
+    return false;
+}
+
+__global__ void k_adj_convex(Dev d, AdjBuf a)
+{
+    for (long long gg = blockIdx.x * (long long)blockDim.x + threadIdx.x; gg < d.N; gg += (long long)gridDim.x * blockDim.x) {
+        const int g = (int)gg;
+        double* out = a.gconv + 6 * gg;
+        AdjF<6> f;
+        f.A = a.A;
+        for (int k = 0; k < 6; ++k) f.g[k] = 0.0;
+        const int cnt = d.conv_cnt[g];
+        if (cnt > 0) {
+            const long long base = adj_unit_base(d, d.cplx[g], d.mol[g], 0, d.conv_off[g]);
+            if (any_adj(a, base, cnt, d.dot_cap)) convex_unit_dots<Dn<6>>(d, g, f);
+        }
+        for (int k = 0; k < 6; ++k) out[k] = f.g[k];
+    }
+}
+
+__global__ void k_adj_toroidal(Dev d, AdjBuf a)
+{
+    const long long NT = min(d.tor_off[d.N], d.tor_cap);
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < NT; q += (long long)gridDim.x * blockDim.x) {
+        double* out = a.gtor + 6 * q;
+        AdjF<6> f;
+        f.A = a.A;
+        for (int k = 0; k < 6; ++k) f.g[k] = 0.0;
+        const int i = d.tor_i[q];
+        const int c = d.cplx[i], m = d.mol[i];
+        const bool act = any_adj(a, adj_unit_base(d, c, m, 1, d.tor1_off[q]), d.tor1_cnt[q], d.dot_cap) ||
+                         any_adj(a, adj_unit_base(d, c, m, 2, d.tor2_off[q]), d.tor2_cnt[q], d.dot_cap);
+        if (act) tor_unit_dots<Dn<6>>(d, q, f);
+        for (int k = 0; k < 6; ++k) out[k] = f.g[k];
+    }
+}
+
+__global__ void k_adj_concave(Dev d, AdjBuf a)
+{
+    const long long NP = min(d.plus_off[d.N] + d.minus_off[d.N], d.probe_cap);
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < NP; p += (long long)gridDim.x * blockDim.x) {
+        double* out = a.gconc + 9 * p;
+        AdjF<9> f;
+        f.A = a.A;
+        for (int k = 0; k < 9; ++k) f.g[k] = 0.0;
+        const int cnt = d.conc_cnt[p];
+        if (cnt > 0) {
+            const int a0 = d.pa0[p];
+            if (any_adj(a, adj_unit_base(d, d.cplx[a0], d.mol[a0], 3, d.conc_off[p]), cnt, d.dot_cap))
+                conc_unit_dots<Dn<9>>(d, p, f);
+        }
+        for (int k = 0; k < 9; ++k) out[k] = f.g[k];
+    }
+}
+
+// probe range of atom g's triples: "+" probes [pb, pb + nplus), "-" probes [mb, mb + nminus)
+__device__ __forceinline__ void atom_probe_ranges(const Dev& d, int g, long long& pb, long long& pe, long long& mb,
+                                                  long long& me)
+{
+    const int c = d.cplx[g];
+    const Cplx C = d.cx[c];
+    const int s0 = C.a0, s1 = C.a0 + C.n0, e1 = C.a0 + C.n;
+    const int ms = d.mol[g] == 0 ? s0 : s1, mend = d.mol[g] == 0 ? s1 : e1;
+    const long long cbase = d.plus_off[s0] + d.minus_off[s0];
+    const long long m0 = (d.plus_off[s1] - d.plus_off[s0]) + (d.minus_off[s1] - d.minus_off[s0]);
+    const long long blk = cbase + (d.mol[g] == 0 ? 0 : m0);
+    pb = blk + (d.plus_off[g] - d.plus_off[ms]);
+    pe = pb + (d.plus_off[g + 1] - d.plus_off[g]);
+    mb = blk + (d.plus_off[mend] - d.plus_off[ms]) + (d.minus_off[g] - d.minus_off[ms]);
+    me = mb + (d.minus_off[g + 1] - d.minus_off[g]);
+}
+
+__device__ __forceinline__ void add_probe_range(const Dev& d, const AdjBuf& a, int atom, long long b, long long e,
+                                                double& x, double& y, double& z)
+{
+    for (long long p = b; p < e && p < d.probe_cap; ++p) {
+        const int ia[3] = {d.pa0[p], d.pa1[p], d.pa2[p]};
+        for (int s = 0; s < 3; ++s) {
+            if (ia[s] != atom) continue;
+            const double* v = a.gconc + 9 * p + 3 * s;
+            x += v[0]; y += v[1]; z += v[2];
+        }
+    }
+}
+
+// pass 4: per atom, in a fixed order: its convex unit, convex units framed by
+// it, its pairs as i, pairs with it as j, probes of its own triples and of
+// its lower-index neighbours' triples
+__global__ void k_adj_gather(Dev d, AdjBuf a, double* grad)
+{
+    for (long long aa = blockIdx.x * (long long)blockDim.x + threadIdx.x; aa < d.N; aa += (long long)gridDim.x * blockDim.x) {
+        const int at = (int)aa;
+        double x = a.gconv[6 * aa], y = a.gconv[6 * aa + 1], z = a.gconv[6 * aa + 2];
+        const long long off = d.nb_off[at];
+        const int K = d.nnb[at];
+        for (int s = 0; s < K; ++s) {
+            const int g = d.nb_id[off + s];
+            if (d.nnb[g] > 0 && d.nb_id[d.nb_off[g]] == at) {
+                const double* v = a.gconv + 6LL * g + 3;
+                x += v[0]; y += v[1]; z += v[2];
+            }
+        }
+        const long long NT = min(d.tor_off[d.N], d.tor_cap);
+        for (long long q = d.tor_off[at]; q < d.tor_off[at + 1] && q < NT; ++q) {
+            const double* v = a.gtor + 6 * q;
+            x += v[0]; y += v[1]; z += v[2];
+        }
+        for (int s = 0; s < K; ++s) {
+            const int i = d.nb_id[off + s];
+            if (i >= at) continue;
+            for (long long q = d.tor_off[i]; q < d.tor_off[i + 1] && q < NT; ++q) {
+                if (d.tor_j[q] != at) continue;
+                const double* v = a.gtor + 6 * q + 3;
+                x += v[0]; y += v[1]; z += v[2];
+            }
+        }
+        long long pb, pe, mb, me;
+        atom_probe_ranges(d, at, pb, pe, mb, me);
+        add_probe_range(d, a, at, pb, pe, x, y, z);
+        add_probe_range(d, a, at, mb, me, x, y, z);
+        for (int s = 0; s < K; ++s) {
+            const int g = d.nb_id[off + s];
+            if (g >= at) continue;
+            atom_probe_ranges(d, g, pb, pe, mb, me);
+            add_probe_range(d, a, at, pb, pe, x, y, z);
+            add_probe_range(d, a, at, mb, me, x, y, z);
+        }
+        grad[3 * aa] = x; grad[3 * aa + 1] = y; grad[3 * aa + 2] = z;
+    }
+}
+
+__global__ void k_adj_zero(AdjBuf a, long long dcap)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < dcap; i += (long long)gridDim.x * blockDim.x) {
+        a.A[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+        a.rcnt[i] = 0;
+        a.rfill[i] = 0;
+    }
+}
+
+void launch_adjoint(const Dev& d, const Rd& r, const AdjBuf& a, const NNTask* cms_task, int side, double* grad,
+                    long long* scan_tmp, cudaStream_t s)
+{
+    const long long D = d.dot_cap;
+    k_adj_zero<<<grid_adj(D, 256), 256, 0, s>>>(a, D);
+    k_adj_queries<<<grid_adj(D, 256), 256, 0, s>>>(d, r, a, cms_task, side);
+    k_adj_ref_count<<<grid_adj(D, 256), 256, 0, s>>>(d, r, a);
+    scan_counts(a.rcnt, a.roff, D, scan_tmp, s);
+    k_adj_ref_fill<<<grid_adj(D, 256), 256, 0, s>>>(d, r, a);
+    k_adj_ref_sum<<<grid_adj(D, 256), 256, 0, s>>>(d, a, D);
+    k_adj_convex<<<grid_adj(d.N, 64), 64, 0, s>>>(d, a);
+    k_adj_toroidal<<<grid_adj(d.tor_cap, 64), 64, 0, s>>>(d, a);
+    k_adj_concave<<<grid_adj(d.probe_cap, 64), 64, 0, s>>>(d, a);
+    k_adj_gather<<<grid_adj(d.N, 128), 128, 0, s>>>(d, a, grad);
+}
+
+}  // namespace cms

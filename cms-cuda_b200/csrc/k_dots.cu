@@ -107,7 +107,7 @@ __device__ __forceinline__ void lat_prefix(LatTable& L, const int* nc, int nl)
 }
 
 template <bool EMIT>
-__global__ void __launch_bounds__(CV_WARPS * 32) k_convex(Dev d)
+__global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 5 : 6) k_convex(Dev d)
 {
     __shared__ LatTable tab[CV_WARPS];
     __shared__ int ncs[CV_WARPS][CMS_MAX_SUBDIV];
@@ -617,7 +617,7 @@ void launch_toroidal(const Dev& d, long long tor_grid, bool emit, cudaStream_t s
 static constexpr int CC_WARPS = 4;
 
 template <bool EMIT>
-__global__ void __launch_bounds__(CC_WARPS * 32) k_concave(Dev d)
+__global__ void __launch_bounds__(CC_WARPS * 32, EMIT ? 4 : 1) k_concave(Dev d)
 {
     __shared__ LatTable tab[CC_WARPS];
     __shared__ int ncs[CC_WARPS][CMS_MAX_SUBDIV];

@@ -860,7 +860,7 @@ __device__ __forceinline__ void triples_row_c(const Dev& d, int g, int K, long l
 
 // LONG = false: atoms whose neighbour row fits the cache; true: the others
 template <bool EMIT, bool LONG>
-__global__ void __launch_bounds__(TR_WARPS * 32) k_triples(Dev d)
+__global__ void __launch_bounds__(TR_WARPS * 32, EMIT ? 8 : 1) k_triples(Dev d)
 {
     __shared__ unsigned queue_s[TR_WARPS][TR_QCAP];
     __shared__ TrRow rows_s[LONG ? 1 : TR_WARPS];

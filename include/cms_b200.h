@@ -105,6 +105,31 @@ cms_status cms_generate_surfaces(cms_ctx* ctx, int32_t all_atoms);
  * (_core.py:946-1004) for target_side True and False. */
 cms_status cms_contact_ms(cms_ctx* ctx, double* per_atom, double* totals, int32_t where);
 
+/* Gradient of sum_c grad_total[c] * CMS_c (one side: target_side 1 = the
+ * target-side CMS, 0 = the binder side) with respect to every atom's
+ * coordinates, grad_xyz (N x 3), with the dot topology of the last surface
+ * generation held fixed (which dots exist, their burial, subdivision indices,
+ * construction branches and each query's nearest dot).  grad_total (B) NULL
+ * means all ones.  Runs the CMS readout first when needed.  The reference has
+ * no gradient; this is the adjoint of calc_contact_molecular_surface
+ * (_core.py:946-1004) through the dot construction (_core.py:1646-2333). */
+cms_status cms_contact_ms_backward(cms_ctx* ctx, int32_t target_side, const double* grad_total, double* grad_xyz,
+                                   int32_t where);
+
+/* Include the gradient of one side's CMS in the captured pipeline
+ * (cms_run_graph / cms_graph_launch); upstream gradients are all ones until
+ * cms_set_grad_total (device or host, B values) replaces them, and
+ * cms_grad_xyz reads the last result.  No reference counterpart. */
+cms_status cms_set_backward(cms_ctx* ctx, int32_t enable, int32_t target_side);
+cms_status cms_set_grad_total(cms_ctx* ctx, const double* grad_total, int32_t where);
+cms_status cms_grad_xyz(cms_ctx* ctx, double* grad_xyz, int32_t where);
+
+/* Self-check of the adjoint's formula: the positions (n x 3) and areas (n) of
+ * complex c's dots of one molecule recomputed from the atoms and the stored
+ * dot topology by the adjoint's geometry code on plain doubles, in
+ * cms_export_dots order.  Equal bit for bit to the generated dots. */
+cms_status cms_recompute_dots(cms_ctx* ctx, int32_t c, int32_t molecule, double* coor, double* area);
+
 /* Maximum possible CMS (per-atom dot area of molecule 0, surface generated
  * with all_atoms = 1).  per_atom (N; molecule-0 atoms), totals (B).
  * Replaces calc_max_possible_contact_molecular_surface (_core.py:1007-1034). */
