@@ -29,7 +29,7 @@ EXPORTED = (
     "cms_last_error", "cms_version", "cms_device_count", "cms_profile_stages", "cms_stage_name",
     "cms_graph_launch", "cms_graph_check", "cms_nn_work", "cms_transfer_bytes", "cms_fp32_peak",
     "cms_nearest_dots", "cms_nearest_dots_noalloc", "cms_contact_ms_backward", "cms_set_backward",
-    "cms_set_grad_total", "cms_grad_xyz", "cms_recompute_dots",
+    "cms_set_grad_total", "cms_grad_xyz", "cms_recompute_dots", "cms_export_dot_units",
 )
 
 
@@ -109,6 +109,7 @@ def load():
             "cms_set_grad_total": [_VP, _VP, _I32],
             "cms_grad_xyz": [_VP, _VP, _I32],
             "cms_recompute_dots": [_VP, _I32, _I32, _VP, _VP],
+            "cms_export_dot_units": [_VP, _I32, _I32, _VP, _VP],
         }
         for name, args in sig.items():
             f = getattr(lib, name)
@@ -340,6 +341,14 @@ class Context:
                                              _ptr(typ), _ptr(atom)))
         k = info.n_dots[m]
         return coor[:k], nml[:k], area[:k], bur[:k], typ[:k], atom[:k]
+
+    def export_dot_units(self, c, m, info):
+        """(unit, sub) construction indices of complex c's dots of molecule m."""
+        n = max(info.n_dots[m], 1)
+        unit = np.empty(n, np.int32); sub = np.empty(n, np.int32)
+        self._check(self.lib.cms_export_dot_units(self.h, int(c), int(m), _ptr(unit), _ptr(sub)))
+        k = info.n_dots[m]
+        return unit[:k], sub[:k]
 
     def export_trimmed(self, c, m, info):
         n = max(info.n_trimmed[m], 1)

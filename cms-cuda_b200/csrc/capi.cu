@@ -1076,6 +1076,45 @@ cms_status cms_export_dots(cms_ctx* x, int32_t c, int32_t molecule, double* coor
     API_END
 }
 
+cms_status cms_export_dot_units(cms_ctx* x, int32_t c, int32_t molecule, int32_t* unit, int32_t* sub)
+{
+    if (!x) return CMS_ERR_ARG;
+    API_BEGIN
+    check_complex(x, c);
+    if (molecule != 0 && molecule != 1) throw Fail{CMS_ERR_ARG, "molecule must be 0 or 1"};
+    const long long ds = x->h_dot_off[2 * c + molecule], n = x->h_dot_off[2 * c + molecule + 1] - ds;
+    if (n <= 0) return CMS_OK;
+    std::vector<int> u(n), sb(n);
+    std::vector<int8_t> ty(n);
+    ck(cudaMemcpy(u.data(), x->d.dunit + ds, sizeof(int) * n, cudaMemcpyDeviceToHost), "copy");
+    ck(cudaMemcpy(sb.data(), x->d.dsub + ds, sizeof(int) * n, cudaMemcpyDeviceToHost), "copy");
+    ck(cudaMemcpy(ty.data(), x->d.dtype + ds, n, cudaMemcpyDeviceToHost), "copy");
+    cms_complex_info I;
+    cms_status st = cms_complex_info_get(x, c, &I);
+    if (st != CMS_OK) return st;
+    const long long at0 = x->h_off[c];
+    const long long q0 = host_ll(x, x->d.tor_off + at0);
+    const long long p0 = host_ll(x, x->d.plus_off + at0) + host_ll(x, x->d.minus_off + at0);
+    // probes: device blocks [+mol0 | -mol0 | +mol1 | -mol1] -> cms_export_probes order [+mol0 | +mol1 | -mol0 | -mol1]
+    const long long pp0 = I.n_probes_plus[0], pm0 = I.n_probes_minus[0], pp1 = I.n_probes_plus[1];
+    const long long dev_start[4] = {0, pp0, pp0 + pm0, pp0 + pm0 + pp1};
+    const long long ref_start[4] = {0, pp0 + pp1, pp0, pp0 + pp1 + pm0};
+    for (long long i = 0; i < n; ++i) {
+        long long v = u[i];
+        if (ty[i] == 1) v -= at0;
+        else if (ty[i] == 2) v -= q0;
+        else {
+            const long long pl = v - p0;
+            int b = 3;
+            while (b > 0 && pl < dev_start[b]) --b;
+            v = ref_start[b] + (pl - dev_start[b]);
+        }
+        if (unit) unit[i] = (int32_t)v;
+        if (sub) sub[i] = sb[i];
+    }
+    API_END
+}
+
 cms_status cms_export_trimmed(cms_ctx* x, int32_t c, int32_t molecule, int32_t* dot_index)
 {
     if (!x) return CMS_ERR_ARG;

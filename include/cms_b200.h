@@ -158,6 +158,15 @@ cms_status cms_export_probes(cms_ctx* ctx, int32_t c, int32_t* a0, int32_t* a1, 
                              double* point, double* alt);
 cms_status cms_export_dots(cms_ctx* ctx, int32_t c, int32_t molecule, double* coor, double* outnml, double* area,
                            int8_t* buried, int8_t* type, int32_t* atom_idx);
+/* Construction indices of complex c's dots of one molecule, in
+ * cms_export_dots order: unit = the generating atom (convex dots), toroid
+ * pair (toroidal, cms_export_toroid order) or probe (concave,
+ * cms_export_probes order); sub = (latitude << 16) | point for convex and
+ * concave dots, (torus point << 16) | (arc 2 ? 1 << 15 : 0) | arc point for
+ * toroidal dots.  The reference keeps no such indices; they define the dot
+ * topology the gradient holds fixed. */
+cms_status cms_export_dot_units(cms_ctx* ctx, int32_t c, int32_t molecule, int32_t* unit, int32_t* sub);
+
 /* local dot indices (within the molecule's dot array) of the SC trimmed dots */
 cms_status cms_export_trimmed(cms_ctx* ctx, int32_t c, int32_t molecule, int32_t* dot_index);
 

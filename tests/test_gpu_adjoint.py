@@ -185,3 +185,30 @@ def test_torch_function():
     g = ctx.contact_ms_backward(True, np.array([3.0]))
     exact("torch binder gradient", b.grad.cpu().numpy(), g[:len(br)])
     exact("torch target gradient", t.grad.cpu().numpy(), g[len(br):])
+
+
+@pytest.mark.parametrize("name,side", [("golden_pkl", 1), ("synth_small_s7", 1), ("synth_small_s7", 0),
+                                       ("sc_example_pdb", 1)])
+def test_gradient_matches_torch_autograd(name, side):
+    """The adjoint against torch FP64 autograd of the same fixed-topology formula."""
+    import torch
+    import torch_cms_formula as F
+    c = load_case(name)
+    ctx = _ctx()
+    X, R, off, nb = _load(ctx, [c])
+    ctx.generate(all_atoms=False)
+    _, totals = ctx.contact_ms(per_atom=False)
+    grad = ctx.contact_ms_backward(target_side=bool(side))
+    topo = F.topology(ctx, 0)
+    Xt = torch.tensor(X, dtype=torch.float64, requires_grad=True)
+    for m in (0, 1):
+        p, a = F.dots(Xt, R, topo["dens"], 1.7, topo, m)
+        assert np.abs(p.detach().numpy() - topo["dots"][m]["coor"]).max() < 1e-9
+        assert np.abs(a.detach().numpy() - topo["dots"][m]["area"]).max() < 1e-9
+    cms = F.contact_ms(Xt, R, 1.7, 0.5, topo, side)
+    assert abs(float(cms.detach()) - totals[0, side]) <= 1e-10 * max(1.0, abs(totals[0, side]))
+    cms.backward()
+    ref = Xt.grad.numpy()
+    scale = max(1.0, np.abs(ref).max())
+    err = np.abs(ref - grad).max() / scale
+    assert err < 1e-9, f"{name} side {side}: adjoint vs torch autograd, max scaled difference {err:.3g}"
