@@ -146,7 +146,7 @@ def cpu_baseline_single(batch, k):
     atoms = int(np.mean([batch.atom_off[c + 1] - batch.atom_off[c] for c in idx]))
     return {"value": len(idx) / tot, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"{len(idx)} complexes of the batch (sizes at the 20-80th percentile, mean {atoms} atoms), "
-                      f"CMS both sides + SC, one process, {tot:.1f} s"}
+                      f"CMS both sides + SC, one process, {tot:.1f} s (the reference has no gradient)"}
 
 
 def run_reference(args):
@@ -255,10 +255,11 @@ def run_ours(args):
     stream = torch.cuda.Stream(device=dev)
     ctx = _lib.Context(local, stream=stream.cuda_stream)
     ctx.load_batch(batch.atom_off, batch.n_binder, xyz_np, rad_np)
+    ctx.set_backward(True, target_side=True)         # each step: surfaces, CMS, SC and d(CMS)/d(xyz)
     ctx.run_graph()                                  # sizes the workspace, captures, replays once
     infos = [ctx.info(c) for c in range(B)]
     statuses = [i.status for i in infos]
-    totals = {"atoms": N, "nb_entries": sum(i.nb_entries for i in infos), "bu_entries": sum(i.bu_entries for i in infos),
+    surf = {"atoms": N, "nb_entries": sum(i.nb_entries for i in infos), "bu_entries": sum(i.bu_entries for i in infos),
               "probes": sum(i.n_probes for i in infos), "toroids": sum(i.n_toroid for i in infos),
               "convex": sum(i.convex for i in infos), "toroidal": sum(i.toroidal for i in infos),
               "concave": sum(i.concave for i in infos)}
@@ -292,6 +293,7 @@ def run_ours(args):
     value = world * B / (ms_max * 1e-3)
     _, totals = ctx.contact_ms(per_atom=False)
     sc, _ = ctx.shape_complementarity()
+    grad_dev = ctx.grad_xyz()
 
     extras = {}
     if rank == 0 and world == 1 and not args.no_extras:
@@ -301,8 +303,8 @@ def run_ours(args):
         pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
         if os.path.exists(pk):
             peaks = json.load(open(pk))
-        extras["roofline"] = stage_roofline(stages, work, totals, peaks, fp32)
-        extras["surface_totals"] = totals
+        extras["roofline"] = stage_roofline(stages, work, surf, peaks, fp32)
+        extras["surface_totals"] = surf
         extras["stages_ms"] = {k: round(v, 3) for k, v in stages.items()}
         extras["nn_work"] = work
     del ctx
@@ -312,19 +314,20 @@ def run_ours(args):
     from cms_cuda.batch import BatchCalculator
     bc = BatchCalculator(local)
     bc.load(batch.atom_off, batch.n_binder, xyz_np, rad_np)
-    r = bc.run(graph=True)
+    r = bc.run(graph=True, grad=True)
     for _ in range(args.warmup):
         bc.load(batch.atom_off, batch.n_binder, xyz_np, rad_np)
-        r = bc.run(graph=True)
+        r = bc.run(graph=True, grad=True)
     h0, d0 = bc.ctx.transfer_bytes()
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         bc.load(batch.atom_off, batch.n_binder, xyz_np, rad_np)
-        r = bc.run(graph=True)
+        r = bc.run(graph=True, grad=True)
     e2e_s = (time.perf_counter() - t0) / args.steps
     h1, d1 = bc.ctx.transfer_bytes()
-    same = bool(np.array_equal(r.cms, totals[:, 1]) and np.array_equal(r.sc, sc[:, 0]))
+    same = bool(np.array_equal(r.cms, totals[:, 1]) and np.array_equal(r.sc, sc[:, 0]) and
+                np.array_equal(r.grad, grad_dev))
     del bc
     e2e_t = torch.tensor([e2e_s], device=dev)
     if world > 1:
@@ -339,7 +342,7 @@ def run_ours(args):
         for c in idx[:2]:
             m = MolecularSurfaceCalculator(local)
             m.add_binder_and_target(*batch.complex(c))
-            m.CalcLoaded(); m.CalcLoadedSC()
+            m.CalcLoaded(); m.CalcLoadedSC(); m.calc_contact_molecular_surface_gradient(True)
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         plain_match = True
@@ -348,9 +351,12 @@ def run_ours(args):
             m.add_binder_and_target(*batch.complex(c))
             cms, _ = m.CalcLoaded()
             s = m.CalcLoadedSC()
-            plain_match &= (cms == totals[c, 1]) and (s[0] == sc[c, 0])
+            g = m.calc_contact_molecular_surface_gradient(True)
+            a0, a1 = int(batch.atom_off[c]), int(batch.atom_off[c + 1])
+            plain_match &= (cms == totals[c, 1]) and (s[0] == sc[c, 0]) and bool(np.array_equal(g, grad_dev[a0:a1]))
         plain = len(idx) / (time.perf_counter() - t0)
-        extras["plain_gpu"] = {"value": plain, "unit": UNIT, "sample": f"first {len(idx)} complexes, one per call",
+        extras["plain_gpu"] = {"value": plain, "unit": UNIT,
+                               "sample": f"first {len(idx)} complexes, one per call (CMS, SC, gradient)",
                                "results_match_batched": bool(plain_match)}
         extras["batched_vs_plain"] = value / plain
         extras["cpu_baseline"] = cpu_baseline_single(batch, args.cpu_sample)
@@ -363,7 +369,8 @@ def run_ours(args):
                            "parallelism": f"replicas x{world} (independent complexes per GPU)",
                            "l2": "inputs larger than L2 (9M atoms), no flush",
                            "nn_search": "FP32 filter + FP64 recheck over every pair not excluded by a proven box-distance bound",
-                           "grad": "not included"},
+                           "grad": "included: d(target-side CMS)/d(xyz) of binder and target atoms, FP64 adjoint "
+                                   "with the dot topology fixed, in every step"},
                 "e2e": e2e, "gpu_launches": launches * args.steps, "clocks": clocks,
                 "complex_status_nonzero": int(sum(1 for s in statuses if s))}
         line.update(extras)

@@ -17,8 +17,9 @@ from . import _lib
 class BatchResult:
     """Per-complex outputs of one batched run."""
 
-    def __init__(self, totals, sc, sides, per_atom=None):
+    def __init__(self, totals, sc, sides, per_atom=None, grad=None):
         self.cms = totals[:, 1].copy()              # target side (calculate_contact_ms)
+        self.grad = grad                            # d(target-side CMS)/d(xyz) (N x 3) when requested
         self.cms_binder = totals[:, 0].copy()
         self.sc = sc[:, 0].copy()
         self.sc_area = sc[:, 1].copy()
@@ -39,6 +40,7 @@ class BatchCalculator:
         if settings is not None:
             self.ctx.set_settings(settings)
         self._settings = settings
+        self._grad = False
 
     def set_settings(self, settings):
         self.ctx.set_settings(settings)
@@ -47,15 +49,25 @@ class BatchCalculator:
     def load(self, atom_off, n_binder, xyz, radius, density=None):
         self.ctx.load_batch(atom_off, n_binder, xyz, radius, density)
 
-    def run(self, graph=True, per_atom=False):
-        """Surfaces + CMS (both sides) + SC of every loaded complex."""
+    def run(self, graph=True, per_atom=False, grad=False):
+        """
+        Surfaces + CMS (both sides) + SC of every loaded complex; with
+        grad=True also d(target-side CMS)/d(xyz) of every atom (in the
+        captured graph when graph=True).
+        """
         if graph:
+            if grad != self._grad:
+                self.ctx.set_backward(grad, target_side=True)
+                self._grad = grad
             self.ctx.run_graph()
         else:
             self.ctx.generate(all_atoms=False)
         pa, totals = self.ctx.contact_ms(per_atom=per_atom)
         sc, sides = self.ctx.shape_complementarity()
-        return BatchResult(totals, sc, sides, pa if per_atom else None)
+        g = None
+        if grad:
+            g = self.ctx.grad_xyz() if graph else self.ctx.contact_ms_backward(target_side=True)
+        return BatchResult(totals, sc, sides, pa if per_atom else None, g)
 
     def statuses(self):
         return np.array([self.ctx.info(c).status for c in range(self.ctx.B)], dtype=np.int32)

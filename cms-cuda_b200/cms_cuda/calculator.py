@@ -382,6 +382,18 @@ class MolecularSurfaceCalculator:
             return float(totals[0, 1]), per_atom[n0:self._n].copy()
         return float(totals[0, 0]), per_atom[:n0].copy()
 
+    def calc_contact_molecular_surface_gradient(self, target_side=True):
+        """
+        d(CMS)/d(xyz) of every loaded atom (N x 3, in AddMolecule order:
+        binder rows, then target rows) for the target-side (or binder-side)
+        CMS, with the generated dot topology held fixed.  The reference has
+        no gradient; this is the FP64 adjoint of calc_contact_molecular_surface.
+        """
+        self._ensure_surfaces_generated(all_atoms=False)
+        if self._cms is None:
+            self.calc_contact_molecular_surface(target_side)
+        return self._context().contact_ms_backward(target_side=target_side)
+
     def calc_max_possible_contact_molecular_surface(self, target_side=True):
         if self._max is None:
             self._max = self._context().max_contact_ms()

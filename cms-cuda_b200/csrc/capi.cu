@@ -228,6 +228,8 @@ struct cms_ctx {
         S_NN_BOXR, S_NN_BOXB, S_NN_D2, S_NN_IDX, S_INFO,
         S_CMS_IDX, S_ADJ_A, S_ADJ_REFDOT, S_ADJ_REFVEC, S_ADJ_RCNT, S_ADJ_RFILL, S_ADJ_ROFF, S_ADJ_RSLOT,
         S_ADJ_GCONV, S_ADJ_GTOR, S_ADJ_GCONC, S_ADJ_GTOT, S_ADJ_GRAD, S_RECOMP_XYZ, S_RECOMP_AREA,
+        S_ADJ_ACT_CONV, S_ADJ_ACT_TOR, S_ADJ_ACT_CONC, S_ADJ_ACT_ATOM, S_ADJ_LIST_CONV, S_ADJ_LIST_TOR,
+        S_ADJ_LIST_CONC, S_ADJ_NACT,
         S_COUNT
     };
 
@@ -610,7 +612,7 @@ AdjBuf bind_adj(cms_ctx* x)
     AdjBuf a{};
     a.A = x->ensure<double4>(cms_ctx::S_ADJ_A, D);
     a.cms_idx = x->get<int>(cms_ctx::S_CMS_IDX);
-    a.ref_dot = x->ensure<int>(cms_ctx::S_ADJ_REFDOT, D);
+    a.ref_ent = x->ensure<int>(cms_ctx::S_ADJ_REFDOT, D);
     a.ref_vec = x->ensure<double4>(cms_ctx::S_ADJ_REFVEC, D);
     a.rcnt = x->ensure<int>(cms_ctx::S_ADJ_RCNT, D);
     a.rfill = x->ensure<int>(cms_ctx::S_ADJ_RFILL, D);
@@ -620,6 +622,15 @@ AdjBuf bind_adj(cms_ctx* x)
     a.gtor = x->ensure<double>(cms_ctx::S_ADJ_GTOR, 6 * std::max(x->cap_tor, 1LL));
     a.gconc = x->ensure<double>(cms_ctx::S_ADJ_GCONC, 9 * std::max(x->cap_probe, 1LL));
     a.gtot = x->ensure<double>(cms_ctx::S_ADJ_GTOT, x->B);
+    const long long T = std::max(x->cap_tor, 1LL), P = std::max(x->cap_probe, 1LL);
+    a.act_conv = x->ensure<int8_t>(cms_ctx::S_ADJ_ACT_CONV, x->N);
+    a.act_tor = x->ensure<int8_t>(cms_ctx::S_ADJ_ACT_TOR, T);
+    a.act_conc = x->ensure<int8_t>(cms_ctx::S_ADJ_ACT_CONC, P);
+    a.act_atom = x->ensure<int8_t>(cms_ctx::S_ADJ_ACT_ATOM, x->N);
+    a.list_conv = x->ensure<int>(cms_ctx::S_ADJ_LIST_CONV, x->N);
+    a.list_tor = x->ensure<int>(cms_ctx::S_ADJ_LIST_TOR, T);
+    a.list_conc = x->ensure<int>(cms_ctx::S_ADJ_LIST_CONC, P);
+    a.nact = x->ensure<int>(cms_ctx::S_ADJ_NACT, 4);
     x->ensure<double>(cms_ctx::S_ADJ_GRAD, 3 * x->N);
     return a;
 }

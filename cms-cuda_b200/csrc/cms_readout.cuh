@@ -60,12 +60,16 @@ struct Rd {
 struct AdjBuf {
     double4* A;            // per dot: (dCMS/dp, dCMS/darea)
     int* cms_idx;          // per buried entry: nearest reference position of the CMS search
-    int* ref_dot;          // per buried entry: the reference dot its query picked (-1: none)
+    int* ref_ent;          // per buried entry: the buried entry of the reference its query picked (-1: none)
     double4* ref_vec;      // per buried entry: contribution to that reference dot's position
-    int* rcnt; int* rfill; long long* roff; int* rslot;   // D, D, D + 1, D
+    int* rcnt; int* rfill; long long* roff; int* rslot;   // per buried entry (capacity D), roff D + 1
     double* gconv;         // 6 per atom: convex unit contributions (atom, frame atom)
     double* gtor;          // 6 per toroid pair: (atom 1, atom 2)
     double* gconc;         // 9 per probe: (atom 0, atom 1, atom 2)
+    int8_t* act_conv; int8_t* act_tor; int8_t* act_conc;   // units holding a dot with a non-zero adjoint
+    int8_t* act_atom;      // atoms of active units
+    int* list_conv; int* list_tor; int* list_conc;         // active units
+    int* nact;             // 3 counters
     const double* gtot;    // per complex: upstream gradient of the side's CMS
 };
 

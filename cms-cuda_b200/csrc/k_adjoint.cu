@@ -31,6 +31,8 @@
 // must equal the surface kernels' output bit for bit, which ties the
 // differentiated formula to the generated surface.
 #include "cms_dual.cuh"
+#include <algorithm>
+
 #include "cms_readout.cuh"
 
 namespace cms {
@@ -328,33 +330,33 @@ __device__ __forceinline__ bool probe_is_plus(const Dev& d, long long p, int a0)
 // ---------------------------------------------------------------------------
 // per-unit drivers: f.want(dot) selects dots, f.take(dot, DotV) consumes them
 // ---------------------------------------------------------------------------
-template <class T>
-__device__ __forceinline__ TV3<T> atom_t(const Dev& d, int a, int k0);
+// Seeds of the atom coordinates: Plain (doubles), Lane (one tangent: the
+// coordinate 3 * slot + axis equal to the lane's k gets derivative 1)
+struct SeedPlain {
+    __device__ TV3<double> atom(const Dev& d, int a, int) const
+    {
+        const double4 x = d.xyzr[a];
+        return tv3<double>(x.x, x.y, x.z);
+    }
+};
 
-template <>
-__device__ __forceinline__ TV3<double> atom_t<double>(const Dev& d, int a, int)
-{
-    const double4 x = d.xyzr[a];
-    return tv3<double>(x.x, x.y, x.z);
-}
+struct SeedLane {
+    int k;
+    __device__ TV3<Dn<1>> atom(const Dev& d, int a, int slot) const
+    {
+        const double4 x = d.xyzr[a];
+        return tv3<Dn<1>>(dn_var<1>(x.x, k == 3 * slot ? 0 : -1), dn_var<1>(x.y, k == 3 * slot + 1 ? 0 : -1),
+                          dn_var<1>(x.z, k == 3 * slot + 2 ? 0 : -1));
+    }
+};
 
-template <int K>
-__device__ __forceinline__ TV3<Dn<K>> atom_dn(const Dev& d, int a, int k0)
-{
-    const double4 x = d.xyzr[a];
-    return tv3<Dn<K>>(dn_var<K>(x.x, k0), dn_var<K>(x.y, k0 + 1), dn_var<K>(x.z, k0 + 2));
-}
-
-template <> __device__ __forceinline__ TV3<Dn<6>> atom_t<Dn<6>>(const Dev& d, int a, int k0) { return atom_dn<6>(d, a, k0); }
-template <> __device__ __forceinline__ TV3<Dn<9>> atom_t<Dn<9>>(const Dev& d, int a, int k0) { return atom_dn<9>(d, a, k0); }
-
-template <class T, class F>
-__device__ __forceinline__ void convex_unit_dots(const Dev& d, int g, F& f)
+template <class T, class S, class F>
+__device__ __forceinline__ void convex_unit_dots(const Dev& d, int g, const S& seed, F& f)
 {
     const long long base = adj_unit_base(d, d.cplx[g], d.mol[g], 0, d.conv_off[g]);
     const int cnt = d.conv_cnt[g];
     const int n0 = d.nb_id[d.nb_off[g]];
-    const ConvexU<T> U = convex_unit<T>(d, g, atom_t<T>(d, g, 0), atom_t<T>(d, n0, 3), d.xyzr[g].w, d.xyzr[n0].w);
+    const ConvexU<T> U = convex_unit<T>(d, g, seed.atom(d, g, 0), seed.atom(d, n0, 1), d.xyzr[g].w, d.xyzr[n0].w);
     int cur = -1;
     LatU<T> L;
     for (long long q = base; q < base + cnt; ++q) {
@@ -369,12 +371,12 @@ __device__ __forceinline__ void convex_unit_dots(const Dev& d, int g, F& f)
     }
 }
 
-template <class T, class F>
-__device__ __forceinline__ void tor_unit_dots(const Dev& d, long long qp, F& f)
+template <class T, class S, class F>
+__device__ __forceinline__ void tor_unit_dots(const Dev& d, long long qp, const S& seed, F& f)
 {
     const int i = d.tor_i[qp], j = d.tor_j[qp];
     const int c = d.cplx[i], m = d.mol[i];
-    const TorU<T> U = tor_unit<T>(d, i, j, atom_t<T>(d, i, 0), atom_t<T>(d, j, 3));
+    const TorU<T> U = tor_unit<T>(d, i, j, seed.atom(d, i, 0), seed.atom(d, j, 1));
     for (int arc = 0; arc < 2; ++arc) {
         const long long base = adj_unit_base(d, c, m, 1 + arc, arc ? d.tor2_off[qp] : d.tor1_off[qp]);
         const int cnt = arc ? d.tor2_cnt[qp] : d.tor1_cnt[qp];
@@ -390,12 +392,12 @@ __device__ __forceinline__ void tor_unit_dots(const Dev& d, long long qp, F& f)
     }
 }
 
-template <class T, class F>
-__device__ __forceinline__ void conc_unit_dots(const Dev& d, long long p, F& f)
+template <class T, class S, class F>
+__device__ __forceinline__ void conc_unit_dots(const Dev& d, long long p, const S& seed, F& f)
 {
     const int ia[3] = {d.pa0[p], d.pa1[p], d.pa2[p]};
     TV3<T> xa[3];
-    for (int k = 0; k < 3; ++k) xa[k] = atom_t<T>(d, ia[k], 3 * k);
+    for (int k = 0; k < 3; ++k) xa[k] = seed.atom(d, ia[k], k);
     const bool plus = probe_is_plus(d, p, ia[0]);
     // the triple's (i, j): (a0, a1) for a "+" probe, (a1, a0) for a "-" probe
     const int si = plus ? 0 : 1, sj = plus ? 1 : 0;
@@ -436,16 +438,17 @@ struct RecomputeF {
 __global__ void k_recompute(Dev d, double* xyz, double* area)
 {
     RecomputeF f{xyz, area};
+    const SeedPlain seed;
     const long long NT = min(d.tor_off[d.N], d.tor_cap);
     const long long NP = min(d.plus_off[d.N] + d.minus_off[d.N], d.probe_cap);
     const long long total = d.N + NT + NP;
     for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < total; u += (long long)gridDim.x * blockDim.x) {
         if (u < d.N) {
-            if (d.conv_cnt[u] > 0) convex_unit_dots<double>(d, (int)u, f);
+            if (d.conv_cnt[u] > 0) convex_unit_dots<double>(d, (int)u, seed, f);
         } else if (u < d.N + NT) {
-            tor_unit_dots<double>(d, u - d.N, f);
+            tor_unit_dots<double>(d, u - d.N, seed, f);
         } else {
-            conc_unit_dots<double>(d, u - d.N - NT, f);
+            conc_unit_dots<double>(d, u - d.N - NT, seed, f);
         }
     }
 }
@@ -458,20 +461,30 @@ void launch_recompute(const Dev& d, double* xyz, double* area, cudaStream_t s)
 // ---------------------------------------------------------------------------
 // adjoint
 // ---------------------------------------------------------------------------
+// a dot with a non-zero adjoint makes its unit active
+__device__ __forceinline__ void mark_unit(const Dev& d, const AdjBuf& a, int dot)
+{
+    const int t = d.dtype[dot], u = d.dunit[dot];
+    if (t == 1) a.act_conv[u] = 1;
+    else if (t == 2) a.act_tor[u] = 1;
+    else a.act_conc[u] = 1;
+}
+
 // pass 1: query dots of `side`; A = (d/dp, d/darea) per dot
 __global__ void k_adj_queries(Dev d, Rd r, AdjBuf a, const NNTask* task, int side)
 {
     const long long NB = r.bur_scan[adj_doff(d, 2LL * d.B)];
     const double w = d.st.weight;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < NB; k += (long long)gridDim.x * blockDim.x) {
-        a.ref_dot[k] = -1;
+        a.ref_ent[k] = -1;
         const int cm = r.bur_cm[k];
         if ((cm & 1) != side) continue;
         const NNTask T = task[cm];
         const int idx = a.cms_idx[k];
         if (T.rn <= 0 || idx < 0 || idx >= T.rn) continue;
         const int q = r.bur_idx[k];
-        const int rd = r.bur_idx[T.r0 + idx];
+        const long long re = T.r0 + idx;            // the reference's buried entry
+        const int rd = r.bur_idx[re];
         const double g = a.gtot[cm >> 1];
         const double* pq = d.dxyz + 3LL * q;
         const double* pr = d.dxyz + 3LL * rd;
@@ -483,18 +496,19 @@ __global__ void k_adj_queries(Dev d, Rd r, AdjBuf a, const NNTask* task, int sid
         // d(area e)/dp_q = area e (-w) 2 (p_q - p_r) = area e 2w (p_r - p_q)
         const double s = g * area * e * 2.0 * w;
         a.A[q] = make_double4(s * dx, s * dy, s * dz, g * e);
-        a.ref_dot[k] = rd;
+        mark_unit(d, a, q);
+        a.ref_ent[k] = (int)re;
         a.ref_vec[k] = make_double4(-s * dx, -s * dy, -s * dz, 0.0);
     }
 }
 
-// pass 2: reference contributions, counting sort by reference dot
+// pass 2: reference contributions, counting sort by the reference's buried entry
 __global__ void k_adj_ref_count(Dev d, Rd r, AdjBuf a)
 {
     const long long NB = r.bur_scan[adj_doff(d, 2LL * d.B)];
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < NB; k += (long long)gridDim.x * blockDim.x) {
-        const int rd = a.ref_dot[k];
-        if (rd >= 0) atomicAdd(&a.rcnt[rd], 1);
+        const int re = a.ref_ent[k];
+        if (re >= 0) atomicAdd(&a.rcnt[re], 1);
     }
 }
 
@@ -502,19 +516,18 @@ __global__ void k_adj_ref_fill(Dev d, Rd r, AdjBuf a)
 {
     const long long NB = r.bur_scan[adj_doff(d, 2LL * d.B)];
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < NB; k += (long long)gridDim.x * blockDim.x) {
-        const int rd = a.ref_dot[k];
-        if (rd >= 0) a.rslot[a.roff[rd] + atomicAdd(&a.rfill[rd], 1)] = (int)k;
+        const int re = a.ref_ent[k];
+        if (re >= 0) a.rslot[a.roff[re] + atomicAdd(&a.rfill[re], 1)] = (int)k;
     }
 }
 
-__global__ void k_adj_ref_sum(Dev d, AdjBuf a, long long cap)
+__global__ void k_adj_ref_sum(Dev d, Rd r, AdjBuf a)
 {
-    const long long D = adj_doff(d, 2LL * d.B);
-    for (long long rd = blockIdx.x * (long long)blockDim.x + threadIdx.x; rd < D && rd < cap;
-         rd += (long long)gridDim.x * blockDim.x) {
-        const int n = a.rcnt[rd];
+    const long long NB = r.bur_scan[adj_doff(d, 2LL * d.B)];
+    for (long long re = blockIdx.x * (long long)blockDim.x + threadIdx.x; re < NB; re += (long long)gridDim.x * blockDim.x) {
+        const int n = a.rcnt[re];
         if (n == 0) continue;
-        int* s = a.rslot + a.roff[rd];
+        int* s = a.rslot + a.roff[re];
         for (int i = 1; i < n; ++i) {          // query order
             const int v = s[i];
             int k = i - 1;
@@ -526,92 +539,81 @@ __global__ void k_adj_ref_sum(Dev d, AdjBuf a, long long cap)
             const double4 v = a.ref_vec[s[i]];
             x += v.x; y += v.y; z += v.z;
         }
+        const int rd = r.bur_idx[re];
         const double4 o = a.A[rd];
         a.A[rd] = make_double4(o.x + x, o.y + y, o.z + z, o.w);
+        mark_unit(d, a, rd);
     }
 }
 
-// pass 3: units; J^T A summed over the unit's dots in dot order
-template <int K>
-struct AdjF {
+// active units of each kind, in any order (each unit owns its output slots)
+__global__ void k_adj_collect(Dev d, AdjBuf a)
+{
+    const long long NT = min(d.tor_off[d.N], d.tor_cap);
+    const long long NP = min(d.plus_off[d.N] + d.minus_off[d.N], d.probe_cap);
+    const long long total = d.N + NT + NP;
+    for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < total; u += (long long)gridDim.x * blockDim.x) {
+        if (u < d.N) {
+            if (a.act_conv[u]) a.list_conv[atomicAdd(&a.nact[0], 1)] = (int)u;
+        } else if (u < d.N + NT) {
+            if (a.act_tor[u - d.N]) a.list_tor[atomicAdd(&a.nact[1], 1)] = (int)(u - d.N);
+        } else {
+            if (a.act_conc[u - d.N - NT]) a.list_conc[atomicAdd(&a.nact[2], 1)] = (int)(u - d.N - NT);
+        }
+    }
+}
+
+// pass 3: per active unit, one lane per coordinate of its atoms (K lanes);
+// lane k accumulates sum over the unit's dots of A . d(dot)/d(coordinate k)
+struct AdjLaneF {
     const double4* A;
-    double g[K];
+    double g;
     __device__ bool want(long long q) const
     {
         const double4 v = A[q];
         return v.x != 0.0 || v.y != 0.0 || v.z != 0.0 || v.w != 0.0;
     }
-    __device__ void take(long long q, const DotV<Dn<K>>& D)
+    __device__ void take(long long q, const DotV<Dn<1>>& D)
     {
         const double4 v = A[q];
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-            g[k] += ((v.x * D.p.x.d[k] + v.y * D.p.y.d[k]) + v.z * D.p.z.d[k]) + v.w * D.area.d[k];
+        g += ((v.x * D.p.x.d[0] + v.y * D.p.y.d[0]) + v.z * D.p.z.d[0]) + v.w * D.area.d[0];
     }
 };
 
-__device__ __forceinline__ bool any_adj(const AdjBuf& a, long long base, int cnt, long long cap)
+template <int KIND>
+__global__ void k_adj_units(Dev d, AdjBuf a)
 {
-    for (long long q = base; q < base + cnt && q < cap; ++q) {
-        const double4 v = a.A[q];
-        if (v.x != 0.0 || v.y != 0.0 || v.z != 0.0 || v.w != 0.0) return true;
-    }
-    return false;
-}
-
-__global__ void k_adj_convex(Dev d, AdjBuf a)
-{
-    for (long long gg = blockIdx.x * (long long)blockDim.x + threadIdx.x; gg < d.N; gg += (long long)gridDim.x * blockDim.x) {
-        const int g = (int)gg;
-        double* out = a.gconv + 6 * gg;
-        AdjF<6> f;
-        f.A = a.A;
-        for (int k = 0; k < 6; ++k) f.g[k] = 0.0;
-        const int cnt = d.conv_cnt[g];
-        if (cnt > 0) {
-            const long long base = adj_unit_base(d, d.cplx[g], d.mol[g], 0, d.conv_off[g]);
-            if (any_adj(a, base, cnt, d.dot_cap)) convex_unit_dots<Dn<6>>(d, g, f);
+    constexpr int K = KIND == 2 ? 9 : 6;       // coordinates of the unit's atoms
+    constexpr int G = 32 / K;                  // units per warp
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / K, k = lane % K;
+    const int* list = KIND == 0 ? a.list_conv : (KIND == 1 ? a.list_tor : a.list_conc);
+    const long long n = a.nact[KIND];
+    const long long wid = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long base = wid * G; base < n; base += nw * G) {
+        const long long e = base + grp;
+        if (grp >= G || e >= n) continue;
+        const int u = list[e];
+        AdjLaneF f{a.A, 0.0};
+        const SeedLane seed{k};
+        if (KIND == 0) {
+            convex_unit_dots<Dn<1>>(d, u, seed, f);
+            a.gconv[6LL * u + k] = f.g;
+            if (k == 0) { a.act_atom[u] = 1; a.act_atom[d.nb_id[d.nb_off[u]]] = 1; }
+        } else if (KIND == 1) {
+            tor_unit_dots<Dn<1>>(d, u, seed, f);
+            a.gtor[6LL * u + k] = f.g;
+            if (k == 0) { a.act_atom[d.tor_i[u]] = 1; a.act_atom[d.tor_j[u]] = 1; }
+        } else {
+            conc_unit_dots<Dn<1>>(d, u, seed, f);
+            a.gconc[9LL * u + k] = f.g;
+            if (k == 0) { a.act_atom[d.pa0[u]] = 1; a.act_atom[d.pa1[u]] = 1; a.act_atom[d.pa2[u]] = 1; }
         }
-        for (int k = 0; k < 6; ++k) out[k] = f.g[k];
     }
 }
 
-__global__ void k_adj_toroidal(Dev d, AdjBuf a)
-{
-    const long long NT = min(d.tor_off[d.N], d.tor_cap);
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < NT; q += (long long)gridDim.x * blockDim.x) {
-        double* out = a.gtor + 6 * q;
-        AdjF<6> f;
-        f.A = a.A;
-        for (int k = 0; k < 6; ++k) f.g[k] = 0.0;
-        const int i = d.tor_i[q];
-        const int c = d.cplx[i], m = d.mol[i];
-        const bool act = any_adj(a, adj_unit_base(d, c, m, 1, d.tor1_off[q]), d.tor1_cnt[q], d.dot_cap) ||
-                         any_adj(a, adj_unit_base(d, c, m, 2, d.tor2_off[q]), d.tor2_cnt[q], d.dot_cap);
-        if (act) tor_unit_dots<Dn<6>>(d, q, f);
-        for (int k = 0; k < 6; ++k) out[k] = f.g[k];
-    }
-}
-
-__global__ void k_adj_concave(Dev d, AdjBuf a)
-{
-    const long long NP = min(d.plus_off[d.N] + d.minus_off[d.N], d.probe_cap);
-    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < NP; p += (long long)gridDim.x * blockDim.x) {
-        double* out = a.gconc + 9 * p;
-        AdjF<9> f;
-        f.A = a.A;
-        for (int k = 0; k < 9; ++k) f.g[k] = 0.0;
-        const int cnt = d.conc_cnt[p];
-        if (cnt > 0) {
-            const int a0 = d.pa0[p];
-            if (any_adj(a, adj_unit_base(d, d.cplx[a0], d.mol[a0], 3, d.conc_off[p]), cnt, d.dot_cap))
-                conc_unit_dots<Dn<9>>(d, p, f);
-        }
-        for (int k = 0; k < 9; ++k) out[k] = f.g[k];
-    }
-}
-
-// probe range of atom g's triples: "+" probes [pb, pb + nplus), "-" probes [mb, mb + nminus)
+// probe range of atom g's triples: "+" probes [pb, pe), "-" probes [mb, me)
 __device__ __forceinline__ void atom_probe_ranges(const Dev& d, int g, long long& pb, long long& pe, long long& mb,
                                                   long long& me)
 {
@@ -632,6 +634,7 @@ __device__ __forceinline__ void add_probe_range(const Dev& d, const AdjBuf& a, i
                                                 double& x, double& y, double& z)
 {
     for (long long p = b; p < e && p < d.probe_cap; ++p) {
+        if (!a.act_conc[p]) continue;
         const int ia[3] = {d.pa0[p], d.pa1[p], d.pa2[p]};
         for (int s = 0; s < 3; ++s) {
             if (ia[s] != atom) continue;
@@ -641,58 +644,70 @@ __device__ __forceinline__ void add_probe_range(const Dev& d, const AdjBuf& a, i
     }
 }
 
-// pass 4: per atom, in a fixed order: its convex unit, convex units framed by
-// it, its pairs as i, pairs with it as j, probes of its own triples and of
-// its lower-index neighbours' triples
+// pass 4: per atom of an active unit, in a fixed order: its convex unit,
+// convex units framed by it, its pairs as i, pairs with it as j, probes of
+// its own triples and of its lower-index neighbours' triples
 __global__ void k_adj_gather(Dev d, AdjBuf a, double* grad)
 {
     for (long long aa = blockIdx.x * (long long)blockDim.x + threadIdx.x; aa < d.N; aa += (long long)gridDim.x * blockDim.x) {
         const int at = (int)aa;
-        double x = a.gconv[6 * aa], y = a.gconv[6 * aa + 1], z = a.gconv[6 * aa + 2];
-        const long long off = d.nb_off[at];
-        const int K = d.nnb[at];
-        for (int s = 0; s < K; ++s) {
-            const int g = d.nb_id[off + s];
-            if (d.nnb[g] > 0 && d.nb_id[d.nb_off[g]] == at) {
-                const double* v = a.gconv + 6LL * g + 3;
+        double x = 0.0, y = 0.0, z = 0.0;
+        if (a.act_atom[at]) {
+            if (a.act_conv[at]) { x = a.gconv[6 * aa]; y = a.gconv[6 * aa + 1]; z = a.gconv[6 * aa + 2]; }
+            const long long off = d.nb_off[at];
+            const int K = d.nnb[at];
+            for (int s = 0; s < K; ++s) {
+                const int g = d.nb_id[off + s];
+                if (a.act_conv[g] && d.nb_id[d.nb_off[g]] == at) {
+                    const double* v = a.gconv + 6LL * g + 3;
+                    x += v[0]; y += v[1]; z += v[2];
+                }
+            }
+            const long long NT = min(d.tor_off[d.N], d.tor_cap);
+            for (long long q = d.tor_off[at]; q < d.tor_off[at + 1] && q < NT; ++q) {
+                if (!a.act_tor[q]) continue;
+                const double* v = a.gtor + 6 * q;
                 x += v[0]; y += v[1]; z += v[2];
             }
-        }
-        const long long NT = min(d.tor_off[d.N], d.tor_cap);
-        for (long long q = d.tor_off[at]; q < d.tor_off[at + 1] && q < NT; ++q) {
-            const double* v = a.gtor + 6 * q;
-            x += v[0]; y += v[1]; z += v[2];
-        }
-        for (int s = 0; s < K; ++s) {
-            const int i = d.nb_id[off + s];
-            if (i >= at) continue;
-            for (long long q = d.tor_off[i]; q < d.tor_off[i + 1] && q < NT; ++q) {
-                if (d.tor_j[q] != at) continue;
-                const double* v = a.gtor + 6 * q + 3;
-                x += v[0]; y += v[1]; z += v[2];
+            for (int s = 0; s < K; ++s) {
+                const int i = d.nb_id[off + s];
+                if (i >= at) continue;
+                for (long long q = d.tor_off[i]; q < d.tor_off[i + 1] && q < NT; ++q) {
+                    if (d.tor_j[q] != at || !a.act_tor[q]) continue;
+                    const double* v = a.gtor + 6 * q + 3;
+                    x += v[0]; y += v[1]; z += v[2];
+                }
             }
-        }
-        long long pb, pe, mb, me;
-        atom_probe_ranges(d, at, pb, pe, mb, me);
-        add_probe_range(d, a, at, pb, pe, x, y, z);
-        add_probe_range(d, a, at, mb, me, x, y, z);
-        for (int s = 0; s < K; ++s) {
-            const int g = d.nb_id[off + s];
-            if (g >= at) continue;
-            atom_probe_ranges(d, g, pb, pe, mb, me);
+            long long pb, pe, mb, me;
+            atom_probe_ranges(d, at, pb, pe, mb, me);
             add_probe_range(d, a, at, pb, pe, x, y, z);
             add_probe_range(d, a, at, mb, me, x, y, z);
+            for (int s = 0; s < K; ++s) {
+                const int g = d.nb_id[off + s];
+                if (g >= at) continue;
+                atom_probe_ranges(d, g, pb, pe, mb, me);
+                add_probe_range(d, a, at, pb, pe, x, y, z);
+                add_probe_range(d, a, at, mb, me, x, y, z);
+            }
         }
         grad[3 * aa] = x; grad[3 * aa + 1] = y; grad[3 * aa + 2] = z;
     }
 }
 
-__global__ void k_adj_zero(AdjBuf a, long long dcap)
+__global__ void k_adj_zero(Dev d, AdjBuf a, long long dcap)
 {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < dcap; i += (long long)gridDim.x * blockDim.x) {
-        a.A[i] = make_double4(0.0, 0.0, 0.0, 0.0);
-        a.rcnt[i] = 0;
-        a.rfill[i] = 0;
+    const long long nf = (long long)d.N + d.tor_cap + d.probe_cap;
+    const long long n = max(dcap, nf);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        if (i < dcap) {
+            a.A[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+            a.rcnt[i] = 0;
+            a.rfill[i] = 0;
+        }
+        if (i < d.N) { a.act_conv[i] = 0; a.act_atom[i] = 0; }
+        if (i < d.tor_cap) a.act_tor[i] = 0;
+        if (i < d.probe_cap) a.act_conc[i] = 0;
+        if (i < 3) a.nact[i] = 0;
     }
 }
 
@@ -700,15 +715,16 @@ void launch_adjoint(const Dev& d, const Rd& r, const AdjBuf& a, const NNTask* cm
                     long long* scan_tmp, cudaStream_t s)
 {
     const long long D = d.dot_cap;
-    k_adj_zero<<<grid_adj(D, 256), 256, 0, s>>>(a, D);
+    k_adj_zero<<<grid_adj(std::max(D, (long long)d.N + d.tor_cap + d.probe_cap), 256), 256, 0, s>>>(d, a, D);
     k_adj_queries<<<grid_adj(D, 256), 256, 0, s>>>(d, r, a, cms_task, side);
     k_adj_ref_count<<<grid_adj(D, 256), 256, 0, s>>>(d, r, a);
     scan_counts(a.rcnt, a.roff, D, scan_tmp, s);
     k_adj_ref_fill<<<grid_adj(D, 256), 256, 0, s>>>(d, r, a);
-    k_adj_ref_sum<<<grid_adj(D, 256), 256, 0, s>>>(d, a, D);
-    k_adj_convex<<<grid_adj(d.N, 64), 64, 0, s>>>(d, a);
-    k_adj_toroidal<<<grid_adj(d.tor_cap, 64), 64, 0, s>>>(d, a);
-    k_adj_concave<<<grid_adj(d.probe_cap, 64), 64, 0, s>>>(d, a);
+    k_adj_ref_sum<<<grid_adj(D, 256), 256, 0, s>>>(d, r, a);
+    k_adj_collect<<<grid_adj((long long)d.N + d.tor_cap + d.probe_cap, 256), 256, 0, s>>>(d, a);
+    k_adj_units<0><<<grid_adj(d.N, 128), 128, 0, s>>>(d, a);
+    k_adj_units<1><<<grid_adj(d.tor_cap, 128), 128, 0, s>>>(d, a);
+    k_adj_units<2><<<grid_adj(d.probe_cap, 128), 128, 0, s>>>(d, a);
     k_adj_gather<<<grid_adj(d.N, 128), 128, 0, s>>>(d, a, grad);
 }
 
