@@ -213,6 +213,27 @@ def stage_bytes(name, t):
     return table.get(name)
 
 
+# DRAM traffic per unit of work (dram__bytes_read.sum + dram__bytes_write.sum of
+# one launch, ncu on the 256-complex batch of this generator, divided by that
+# batch's units); scaled by the units of the measured batch
+TRAFFIC_PER_UNIT = {
+    "toroidal_emit": (369.3e6 / 5021616, "toroidal"),      # per toroidal dot
+    "triples_count": (96.95e6 / 558670, "atoms"),          # per atom
+    "triples_emit": (106.8e6 / 558670, "atoms"),
+    "cms_nn": (174.2e6 / 2750610, "cms_queries"),          # per query dot
+    "sc_band_nn": (380.9e6 / 2750610, "band_queries"),
+}
+
+
+def stage_traffic(name, totals, work):
+    t = TRAFFIC_PER_UNIT.get(name)
+    if t is None:
+        return None
+    per, unit = t
+    n = totals.get(unit, work.get(unit))
+    return None if n is None else per * n
+
+
 def stage_roofline(stages, work, totals, peaks, fp32_peak):
     """Roofline of the most expensive stage: the nearest-dot search against the
     measured FP32 throughput (8 FLOP per pair), a surface stage against the
@@ -223,13 +244,14 @@ def stage_roofline(stages, work, totals, peaks, fp32_peak):
     if name in nn:
         achieved = 8.0 * nn[name] / (ms * 1e-3) / 1e12
         return {"bound": "fp32", "kernel": f"k_nn ({name})", "achieved": achieved, "peak": fp32_peak,
-                "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None, "ms": ms,
+                "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": stage_traffic(name, totals, work), "ms": ms,
                 "peak_source": "measured FP32 FMA throughput of this GPU (cms_fp32_peak, in this run)"}
     hbm = peaks.get("hbm_gbs")
     nbytes = stage_bytes(name, totals)
     achieved = nbytes / (ms * 1e-3) / 1e9 if nbytes is not None else None
     return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": (achieved / hbm) if (achieved is not None and hbm) else None, "traffic": None, "ms": ms,
+            "frac": (achieved / hbm) if (achieved is not None and hbm) else None,
+            "traffic": stage_traffic(name, totals, work), "ms": ms,
             "algorithmic_bytes": nbytes,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm else None,
             "note": "FP64 geometry: the stage is bound by FP64 issue latency, not HBM (ncu summaries under profiles/)"}
@@ -265,6 +287,8 @@ def run_ours(args):
               "concave": sum(i.concave for i in infos)}
     work = ctx.nn_work()
     launches = ctx.kernel_launches()
+    free_b, total_b = torch.cuda.mem_get_info(dev)
+    device_gb = (total_b - free_b) / 1e9             # whole GPU in use while the context holds its workspace
 
     # ---- device throughput: graph replays with inputs resident -------------
     for _ in range(args.warmup):
@@ -305,6 +329,7 @@ def run_ours(args):
             peaks = json.load(open(pk))
         extras["roofline"] = stage_roofline(stages, work, surf, peaks, fp32)
         extras["surface_totals"] = surf
+        extras["device_memory_gb"] = round(device_gb, 1)
         extras["stages_ms"] = {k: round(v, 3) for k, v in stages.items()}
         extras["nn_work"] = work
     del ctx
