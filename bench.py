@@ -287,6 +287,10 @@ def run_ours(args):
               "concave": sum(i.concave for i in infos)}
     work = ctx.nn_work()
     launches = ctx.kernel_launches()
+    tv, tms = ctx.nn_variants()
+    autotune = {stage: {"shape": _lib.NN_VARIANT_NAMES[tv[k]],
+                        "ms": {_lib.NN_VARIANT_NAMES[v]: round(float(tms[k, v]), 3) for v in range(4)}}
+                for k, stage in enumerate(("cms_nn", "sc_band_nn", "sc_argmin_nn"))}
     free_b, total_b = torch.cuda.mem_get_info(dev)
     device_gb = (total_b - free_b) / 1e9             # whole GPU in use while the context holds its workspace
 
@@ -396,7 +400,7 @@ def run_ours(args):
                            "nn_search": "FP32 filter + FP64 recheck over every pair not excluded by a proven box-distance bound",
                            "grad": "included: d(target-side CMS)/d(xyz) of binder and target atoms, FP64 adjoint "
                                    "with the dot topology fixed, in every step"},
-                "e2e": e2e, "gpu_launches": launches * args.steps, "clocks": clocks,
+                "e2e": e2e, "gpu_launches": launches * args.steps, "clocks": clocks, "autotune": autotune,
                 "complex_status_nonzero": int(sum(1 for s in statuses if s))}
         line.update(extras)
         print(json.dumps(line), flush=True)

@@ -30,7 +30,10 @@ EXPORTED = (
     "cms_graph_launch", "cms_graph_check", "cms_nn_work", "cms_transfer_bytes", "cms_fp32_peak",
     "cms_nearest_dots", "cms_nearest_dots_noalloc", "cms_contact_ms_backward", "cms_set_backward",
     "cms_set_grad_total", "cms_grad_xyz", "cms_recompute_dots", "cms_export_dot_units",
+    "cms_set_nn_variants", "cms_get_nn_variants", "cms_set_autotune",
 )
+
+NN_VARIANT_NAMES = ("q4 r1024", "q4 r512", "q2 r1024", "q2 r512")
 
 
 class Settings(ctypes.Structure):
@@ -110,6 +113,9 @@ def load():
             "cms_grad_xyz": [_VP, _VP, _I32],
             "cms_recompute_dots": [_VP, _I32, _I32, _VP, _VP],
             "cms_export_dot_units": [_VP, _I32, _I32, _VP, _VP],
+            "cms_set_nn_variants": [_VP, _VP],
+            "cms_get_nn_variants": [_VP, _VP, _VP],
+            "cms_set_autotune": [_VP, _I32],
         }
         for name, args in sig.items():
             f = getattr(lib, name)
@@ -207,6 +213,21 @@ class Context:
 
     def graph_check(self):
         self._check(self.lib.cms_graph_check(self.h))
+
+    def set_nn_variants(self, variants):
+        """Force the three search shapes (CMS, SC band, SC argmin); turns the autotuner off."""
+        v = np.ascontiguousarray(variants, dtype=np.int32)
+        self._check(self.lib.cms_set_nn_variants(self.h, _ptr(v)))
+
+    def set_autotune(self, enable=True):
+        self._check(self.lib.cms_set_autotune(self.h, 1 if enable else 0))
+
+    def nn_variants(self):
+        """(chosen shape per search, measured ms per search and shape) of the autotuner."""
+        v = np.zeros(3, np.int32)
+        ms = np.zeros(12)
+        self._check(self.lib.cms_get_nn_variants(self.h, _ptr(v), _ptr(ms)))
+        return v.tolist(), ms.reshape(3, 4)
 
     def nn_work(self):
         w = np.zeros(6, dtype=np.int64)

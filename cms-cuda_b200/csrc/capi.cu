@@ -199,9 +199,16 @@ struct cms_ctx {
     cudaGraphExec_t gexec = nullptr;
     cudaGraph_t graph = nullptr;
     long long graph_key[4] = {-1, -1, -1, -1};
+    long long graph_vk = -1;                 // search shapes the graph was captured with
     // gradient of one side's CMS (cms_set_backward / cms_contact_ms_backward)
     int bwd_enabled = 0, bwd_side = 1;
     bool bwd_ok = false;
+    // nearest-dot search shapes per stage (CMS, SC band, SC argmin), chosen by
+    // the autotuner for each batch shape (or forced by cms_set_nn_variants)
+    int nn_var[3] = {0, 0, 0};
+    bool autotune = true;
+    long long tune_key[3] = {-1, -1, -1};
+    double tune_ms[3][NN_VARIANTS] = {};
     long long launches = -1;
     std::string err;
     // stage timing: an event after each pipeline stage when profiling
@@ -558,7 +565,7 @@ void enqueue_cms(cms_ctx* x)
     a.q_xyz = a.r_xyz = d.dxyz;
     a.out_d2 = r.nn_d2;
     a.out_idx = x->get<int>(cms_ctx::S_CMS_IDX);       // kept for the adjoint
-    launch_nn(a, NN_ARGMIN, tile_cap(x), tmp, s);
+    launch_nn(a, NN_ARGMIN, x->nn_var[0], tile_cap(x), tmp, s);
     mark(x, P_CMS_NN);
     launch_cms_weights(d, r, x->cap_dot, s);
     launch_per_atom_sum(d, r, x->cap_dot, x->get<double>(cms_ctx::S_PER_ATOM_CMS), tmp, s);
@@ -579,7 +586,7 @@ void enqueue_sc(cms_ctx* x)
     a.q_xyz = a.r_xyz = d.dxyz;
     a.out_flag = r.keep;
     a.band_thr64 = x->st.band * x->st.band;
-    launch_nn(a, NN_BAND, tile_cap(x), tmp, s);
+    launch_nn(a, NN_BAND, x->nn_var[1], tile_cap(x), tmp, s);
     mark(x, P_SC_BAND_NN);
     launch_trim_compact(d, r, x->cap_dot, tmp, s);
     launch_tasks(d, r, 2, task + 4 * x->B, s);
@@ -589,7 +596,7 @@ void enqueue_sc(cms_ctx* x)
     b.q_f4 = r.trim_f4; b.q_idx = r.trim_idx; b.r_f4 = r.trim_f4; b.r_idx = r.trim_idx;
     b.q_xyz = b.r_xyz = d.dxyz;
     b.out_d2 = r.nn_d2; b.out_idx = r.nn_idx;
-    launch_nn(b, NN_ARGMIN, tile_cap(x), tmp, s);
+    launch_nn(b, NN_ARGMIN, x->nn_var[2], tile_cap(x), tmp, s);
     mark(x, P_SC_ARGMIN_NN);
     launch_sc_stats(d, r, task + 4 * x->B, x->get<double>(cms_ctx::S_SC_SIDE), x->get<double>(cms_ctx::S_SC_OUT), s);
     mark(x, P_SC_STATS);
@@ -1146,12 +1153,73 @@ cms_status cms_export_trimmed(cms_ctx* x, int32_t c, int32_t molecule, int32_t* 
 
 namespace {
 
+// milliseconds per stage from the profiling marks (the events are released)
+void take_stage_times(cms_ctx* x, double* ms, int cap)
+{
+    ck(cudaStreamSynchronize(x->stream), "sync");
+    for (int i = 0; i < cap; ++i) ms[i] = 0.0;
+    for (size_t k = 1; k < x->marks.size(); ++k) {
+        float t = 0.f;
+        ck(cudaEventElapsedTime(&t, x->marks[k - 1], x->marks[k]), "elapsed");
+        const int id = x->mark_ids[k];
+        if (id >= 0 && id < cap) ms[id] += t;
+    }
+    for (auto e : x->marks) cudaEventDestroy(e);
+    x->marks.clear();
+    x->mark_ids.clear();
+}
+
+// Autotuner: with the surfaces of the loaded batch in place, run the CMS and
+// SC readouts once per search shape (each stage timed with events), twice
+// over, and keep the fastest shape per stage.  All shapes give the same
+// results, so the choice only changes speed.
+void autotune_nn(cms_ctx* x)
+{
+    const long long key[3] = {x->B, x->N, x->cap_dot};
+    if (!x->autotune || std::memcmp(key, x->tune_key, sizeof(key)) == 0) return;
+    static const int stage[3] = {P_CMS_NN, P_SC_BAND_NN, P_SC_ARGMIN_NN};
+    for (int k = 0; k < 3; ++k)
+        for (int v = 0; v < NN_VARIANTS; ++v) x->tune_ms[k][v] = INFINITY;
+    double ms[P_NSTAGES];
+    for (int rep = 0; rep < 2; ++rep) {
+        for (int v = 0; v < NN_VARIANTS; ++v) {
+            for (int k = 0; k < 3; ++k) x->nn_var[k] = v;
+            x->profiling = true;
+            try {
+                mark(x, -1);
+                enqueue_cms(x);
+                enqueue_sc(x);
+            } catch (...) {
+                x->profiling = false;
+                throw;
+            }
+            x->profiling = false;
+            take_stage_times(x, ms, P_NSTAGES);
+            for (int k = 0; k < 3; ++k) x->tune_ms[k][v] = std::min(x->tune_ms[k][v], ms[stage[k]]);
+        }
+    }
+    for (int k = 0; k < 3; ++k) {
+        int best = 0;
+        for (int v = 1; v < NN_VARIANTS; ++v)
+            if (x->tune_ms[k][v] < x->tune_ms[k][best]) best = v;
+        x->nn_var[k] = best;
+    }
+    std::memcpy(x->tune_key, key, sizeof(key));
+    x->cms_ok = x->sc_ok = true;
+}
+
 // capture the whole batched pipeline into a CUDA graph for the current shape
 void capture_graph(cms_ctx* x)
 {
-    if (x->cap_dot == 0) run_sized_surface(x, 0);       // size every buffer once
+    const long long shape[2] = {x->B, x->N};
+    const bool new_shape = x->cap_dot == 0 || std::memcmp(shape, x->tune_key, sizeof(shape)) != 0;
+    if (new_shape && (x->cap_dot == 0 || x->autotune)) {
+        run_sized_surface(x, 0);                         // size every buffer for this batch
+        autotune_nn(x);                                  // pick the search shapes on it
+    }
     const long long key[4] = {x->B, x->N, x->cap_dot, x->bwd_enabled ? 1 + x->bwd_side : 0};
-    if (x->gexec && std::memcmp(key, x->graph_key, sizeof(key)) == 0) return;
+    const long long vk = (x->nn_var[0] << 8) | (x->nn_var[1] << 4) | x->nn_var[2];
+    if (x->gexec && std::memcmp(key, x->graph_key, sizeof(key)) == 0 && vk == x->graph_vk) return;
     if (x->gexec) { cudaGraphExecDestroy(x->gexec); x->gexec = nullptr; }
     if (x->graph) { cudaGraphDestroy(x->graph); x->graph = nullptr; }
     x->d.all_atoms = 0;
@@ -1186,6 +1254,7 @@ void capture_graph(cms_ctx* x)
     }
     x->launches = kernels;
     std::memcpy(x->graph_key, key, sizeof(key));
+    x->graph_vk = vk;
 }
 
 void mark_graph_results(cms_ctx* x)
@@ -1310,7 +1379,7 @@ cms_status cms_nearest_dots(cms_ctx* x, const double* query_xyz, int64_t n_query
     a.q_f4 = qf; a.q_idx = nullptr; a.r_f4 = rf; a.r_idx = nullptr;
     a.q_xyz = q; a.r_xyz = r;
     a.out_d2 = d2; a.out_idx = idx;
-    launch_nn_kernel(a, NN_ARGMIN, n_query / 512 + 2, s);
+    launch_nn_kernel(a, NN_ARGMIN, 0, n_query / 512 + 2, s);
     ck(cudaGetLastError(), "nearest-dot kernels");
     if (where == CMS_HOST) {
         ck(cudaMemcpyAsync(out_d2, d2, sizeof(double) * n_query, cudaMemcpyDeviceToHost, s), "copy out");
@@ -1388,23 +1457,42 @@ cms_status cms_profile_stages(cms_ctx* x, double* ms, int32_t cap, int32_t* n_st
         throw;
     }
     x->profiling = false;
-    ck(cudaStreamSynchronize(x->stream), "sync");
-    for (int i = 0; i < cap; ++i) ms[i] = 0.0;
-    for (size_t k = 1; k < x->marks.size(); ++k) {
-        float t = 0.f;
-        ck(cudaEventElapsedTime(&t, x->marks[k - 1], x->marks[k]), "elapsed");
-        int id = x->mark_ids[k];
-        if (id >= 0 && id < cap) ms[id] += t;
-    }
-    for (auto e : x->marks) cudaEventDestroy(e);
-    x->marks.clear();
-    x->mark_ids.clear();
+    take_stage_times(x, ms, cap);
     if (n_stages) *n_stages = P_NSTAGES;
     pull_host_state(x);
     x->surf_ok = x->cms_ok = x->sc_ok = true;
     x->bwd_ok = x->bwd_enabled != 0;
     x->max_ok = false;
     API_END
+}
+
+cms_status cms_set_nn_variants(cms_ctx* x, const int32_t* variants)
+{
+    if (!x || !variants) return fail(x, CMS_ERR_ARG, "null argument");
+    for (int k = 0; k < 3; ++k)
+        if (variants[k] < 0 || variants[k] >= NN_VARIANTS) return fail(x, CMS_ERR_ARG, "search shape out of range");
+    for (int k = 0; k < 3; ++k) x->nn_var[k] = variants[k];
+    x->autotune = false;
+    x->cms_ok = x->sc_ok = false;
+    return CMS_OK;
+}
+
+cms_status cms_set_autotune(cms_ctx* x, int32_t enable)
+{
+    if (!x) return CMS_ERR_ARG;
+    x->autotune = enable != 0;
+    if (x->autotune) x->tune_key[0] = -1;
+    return CMS_OK;
+}
+
+cms_status cms_get_nn_variants(cms_ctx* x, int32_t* variants, double* tune_ms)
+{
+    if (!x || !variants) return fail(x, CMS_ERR_ARG, "null argument");
+    for (int k = 0; k < 3; ++k) variants[k] = x->nn_var[k];
+    if (tune_ms)
+        for (int k = 0; k < 3; ++k)
+            for (int v = 0; v < NN_VARIANTS; ++v) tune_ms[k * NN_VARIANTS + v] = x->tune_ms[k][v];
+    return CMS_OK;
 }
 
 cms_status cms_set_backward(cms_ctx* x, int32_t enable, int32_t target_side)

@@ -6,9 +6,11 @@ namespace cms {
 
 enum { NN_MIN = 0, NN_ARGMIN = 1, NN_BAND = 2 };
 
-// references per round of the nearest-dot search; a search's box arrays
-// hold ceil(references / NN_ROUND) rounds per task
-static constexpr int NN_ROUND = 1024;
+// references per sub-round of the nearest-dot search (the granularity of the
+// round boxes); a search's box arrays hold ceil(references / NN_ROUND)
+// sub-rounds per task
+static constexpr int NN_ROUND = 512;
+static constexpr int NN_VARIANTS = 4;        // tunable search shapes (k_readout.cu)
 static inline long long nn_round_cap(long long refs, long long ntask) { return refs / NN_ROUND + ntask + 1; }
 
 #define SC_SIDE_FIELDS 7   // d_mean, d_median, s_mean, s_median, trimmedArea, nTrimmedDots, nAllDots
@@ -40,6 +42,7 @@ struct NNArgs {
     float4* box_blk;
     long long round_cap;    // rounds the box arrays hold
     int band_mode;
+    int tile_q;             // queries per tile of the launched variant
 };
 
 // readout workspace, capacity = dot capacity unless noted
@@ -79,9 +82,9 @@ void launch_recompute(const Dev& d, double* xyz, double* area, cudaStream_t s);
 
 void launch_split_buried(const Dev& d, const Rd& r, long long dot_cap, long long* scan_tmp, cudaStream_t s);
 void launch_tasks(const Dev& d, const Rd& r, int kind, NNTask* task, cudaStream_t s);
-void launch_nn(NNArgs a, int mode, long long tile_cap, long long* scan_tmp, cudaStream_t s);
-void launch_nn_tiles(NNArgs a, int mode, long long* scan_tmp, cudaStream_t s);
-void launch_nn_kernel(NNArgs a, int mode, long long tile_cap, cudaStream_t s);
+void launch_nn(NNArgs a, int mode, int variant, long long tile_cap, long long* scan_tmp, cudaStream_t s);
+void launch_nn_tiles(NNArgs a, int mode, int variant, long long* scan_tmp, cudaStream_t s);
+void launch_nn_kernel(NNArgs a, int mode, int variant, long long tile_cap, cudaStream_t s);
 // standalone search helpers: bounding box of two point sets, FP32 packing, one task
 void launch_points_setup(const double* q, long long nq, const double* r, long long nr, double* partials,
                          int partial_blocks, double* bbox, float4* q_f4, float4* r_f4, NNTask* task, int* tile_cnt,

@@ -35,9 +35,9 @@ using namespace cms;
 
 #define CMS_NOALLOC_SCRATCH_BYTES (32u << 20)
 #define CMS_NOALLOC_HEADER_BYTES (16u << 10)
-// 1920 x 1024 points: 16 bytes each when packed, plus the reference boxes
-// (66 float4 per round of NN_ROUND references, at most MAX/NN_ROUND + 2 rounds)
-#define CMS_NOALLOC_MAX_POINTS (1920u * 1024u)
+// 3836 x 512 points: 16 bytes each when packed, plus the reference boxes
+// (34 float4 per sub-round of NN_ROUND references, at most MAX/NN_ROUND + 2 sub-rounds)
+#define CMS_NOALLOC_MAX_POINTS (3836u * 512u)
 #define CMS_NOALLOC_MAX_ROUNDS (CMS_NOALLOC_MAX_POINTS / NN_ROUND + 2u)
 #define CMS_NOALLOC_BOX_F4 (2u + 2u * (NN_ROUND / 32))
 #define CMS_NOALLOC_PARTIAL_BLOCKS 256
@@ -104,6 +104,6 @@ extern "C" cms_status cms_nearest_dots_noalloc(const double* query_xyz, int64_t 
     a.q_f4 = q_f4; a.q_idx = nullptr; a.r_f4 = r_f4; a.r_idx = nullptr;
     a.q_xyz = query_xyz; a.r_xyz = ref_xyz;
     a.out_d2 = out_d2; a.out_idx = out_index;
-    launch_nn_kernel(a, out_index ? NN_ARGMIN : NN_MIN, n_query / 512 + 2, s);
+    launch_nn_kernel(a, out_index ? NN_ARGMIN : NN_MIN, 0, n_query / 512 + 2, s);
     return cudaGetLastError() == cudaSuccess ? CMS_OK : CMS_ERR_CUDA;
 }

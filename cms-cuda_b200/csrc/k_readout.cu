@@ -142,13 +142,17 @@ __device__ __forceinline__ float nn_rr(float rx, float ry, float rz)
 
 static constexpr int NN_T = 128;              // threads per tile
 static constexpr int NN_W = NN_T / 32;        // warps per tile
-static constexpr int NN_Q = 4;                // queries per thread (two packed pairs)
-static constexpr int NN_WQ = 32 * NN_Q;       // consecutive queries per warp
-static constexpr int NN_TILE = NN_T * NN_Q;   // queries per tile
 static constexpr int NN_BLK = 32;             // references per block (one bounding box)
-static constexpr int NN_R = NN_ROUND;         // references per round (staged together)
-static constexpr int NN_RB = NN_R / NN_BLK;   // blocks per round
+static constexpr int NN_SR = NN_ROUND;        // references per sub-round (one bounding box)
+static constexpr int NN_SRB = NN_SR / NN_BLK; // blocks per sub-round
 static constexpr int NN_SORT = 512;           // rounds of a task visited nearest first (more: index order)
+static constexpr int NN_TILE = NN_T * 4;      // queries per tile of the default variant (standalone searches)
+
+// Tunable shapes: queries per thread Q (2 or 4: tiles of 256 or 512 queries)
+// and sub-rounds per staged round (1 or 2: 512 or 1024 references).  Every
+// variant computes the same exact result; the autotuner picks per stage.
+__host__ __device__ constexpr int nn_var_q(int v) { return (v & 2) ? 2 : 4; }
+__host__ __device__ constexpr int nn_var_sub(int v) { return (v & 1) ? 1 : 2; }
 
 // one query's state
 struct NNQ {
@@ -265,11 +269,11 @@ __device__ __forceinline__ void nn_recheck(const NNArgs& a, const NNTask& T, con
 // The warp rechecks every reference of the task for each flagged lane,
 // skipping blocks whose box is beyond the lane's cull threshold, and keeps
 // the smallest FP64 value with the smallest index.
-__device__ __forceinline__ void nn_full_warp(const NNArgs& a, const NNTask& T, const NNTile& tl, long long ro, int nrt,
+__device__ __forceinline__ void nn_full_warp(const NNArgs& a, const NNTask& T, const NNTile& tl, long long ro, int nsr,
                                              NNQ& q, unsigned need, long long qbase)
 {
     const int lane = threadIdx.x & 31;
-    const long long nblk = (long long)nrt * NN_RB;
+    const long long nblk = (long long)nsr * NN_SRB;
     while (need) {
         const int L = __ffs(need) - 1;
         need &= need - 1;
@@ -286,7 +290,7 @@ __device__ __forceinline__ void nn_full_warp(const NNArgs& a, const NNTask& T, c
             const long long blk = blk0 + lane;
             bool want = false;
             if (blk < nblk) {
-                const float4 lo = a.box_blk[2 * (ro * NN_RB + blk)], hi = a.box_blk[2 * (ro * NN_RB + blk) + 1];
+                const float4 lo = a.box_blk[2 * (ro * NN_SRB + blk)], hi = a.box_blk[2 * (ro * NN_SRB + blk) + 1];
                 want = !box_far(box_gap2(qf.x, qf.y, qf.z, qf.x, qf.y, qf.z, lo, hi), cth);
             }
             unsigned wb = __ballot_sync(0xffffffffu, want);
@@ -306,9 +310,24 @@ __device__ __forceinline__ void nn_full_warp(const NNArgs& a, const NNTask& T, c
     }
 }
 
-// Nearest-dot search over tiles of NN_TILE queries.  Each warp owns 128
-// consecutive queries (4 per lane, two packed pairs).  The task's references
-// come in rounds of NN_R, visited in order of their box distance to the
+// box of round i (SUB sub-rounds) of a task whose sub-rounds start at ro
+template <int SUB>
+__device__ __forceinline__ void nn_round_box(const NNArgs& a, long long ro, int nsr, int i, float4& lo, float4& hi)
+{
+    lo = a.box_round[2 * (ro + (long long)i * SUB)];
+    hi = a.box_round[2 * (ro + (long long)i * SUB) + 1];
+#pragma unroll
+    for (int s = 1; s < SUB; ++s) {
+        if ((long long)i * SUB + s >= nsr) break;
+        const float4 l2 = a.box_round[2 * (ro + (long long)i * SUB + s)], h2 = a.box_round[2 * (ro + (long long)i * SUB + s) + 1];
+        lo = make_float4(fminf(lo.x, l2.x), fminf(lo.y, l2.y), fminf(lo.z, l2.z), 0.f);
+        hi = make_float4(fmaxf(hi.x, h2.x), fmaxf(hi.y, h2.y), fmaxf(hi.z, h2.z), 0.f);
+    }
+}
+
+// Nearest-dot search over tiles of 128 * Q queries.  Each warp owns 32 * Q
+// consecutive queries (Q per lane, Q / 2 packed pairs).  The task's references
+// come in rounds of SUB * 512, visited in order of their box distance to the
 // tile's box; a round is staged in shared memory only when some warp's query
 // box is within its cull threshold, and each warp skips the 32-reference
 // blocks whose box is beyond it.  The minimum searches keep, per query, the
@@ -317,12 +336,17 @@ __device__ __forceinline__ void nn_full_warp(const NNArgs& a, const NNTask& T, c
 // when no other block can hold a candidate (the usual case) and every block
 // otherwise.  The band search stops a query at its first FP64 hit and a tile
 // once every query has one or no round is left within reach.
-template <int MODE>
+template <int MODE, int Q, int SUB>
 __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
 {
-    __shared__ float4 sA[NN_R];   // (x, x, y, y)
-    __shared__ float4 sB[NN_R];   // (z, z, |r|^2, |r|^2)
-    __shared__ float4 sBox[2 * NN_RB];
+    constexpr int P = Q / 2;                  // packed query pairs per lane
+    constexpr int WQ = 32 * Q;                // queries per warp
+    constexpr int TILE = NN_T * Q;            // queries per tile
+    constexpr int RR = SUB * NN_SR;           // references per round
+    constexpr int RB = RR / NN_BLK;           // blocks per round
+    __shared__ float4 sA[RR];     // (x, x, y, y)
+    __shared__ float4 sB[RR];     // (z, z, |r|^2, |r|^2)
+    __shared__ float4 sBox[2 * RB];
     __shared__ float sKey[NN_SORT];
     __shared__ short sOrd[NN_SORT];
     __shared__ float sWbox[6][NN_W];
@@ -335,17 +359,18 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
             if (a.tile_off[mid] <= tile) lo = mid; else hi = mid - 1;
         }
         const NNTask T = a.task[lo];
-        const long long ro = a.round_off[lo];
-        const int nrt = a.round_cnt[lo];
-        if (ro + nrt > a.round_cap) continue;     // over capacity: the run is flagged and redone
-        const long long qw = (tile - a.tile_off[lo]) * NN_TILE + (long long)wid * NN_WQ;
+        const long long ro = a.round_off[lo];     // first sub-round of the task
+        const int nsr = a.round_cnt[lo];          // sub-rounds of the task
+        if (ro + nsr > a.round_cap) continue;     // over capacity: the run is flagged and redone
+        const int nrt = (nsr + SUB - 1) / SUB;    // rounds
+        const long long qw = (tile - a.tile_off[lo]) * TILE + (long long)wid * WQ;
 
         // queries and the warp's box
-        NNQ q[NN_Q];
-        float qpx[NN_Q], qpy[NN_Q], qpz[NN_Q];
+        NNQ q[Q];
+        float qpx[Q], qpy[Q], qpz[Q];
         float wl[3] = {INFINITY, INFINITY, INFINITY}, wh[3] = {-INFINITY, -INFINITY, -INFINITY};
 #pragma unroll
-        for (int j = 0; j < NN_Q; ++j) {
+        for (int j = 0; j < Q; ++j) {
             const long long qi = qw + j * 32 + lane;
             q[j].live = qi < T.qn;
             qpx[j] = qpy[j] = qpz[j] = 0.f;
@@ -384,7 +409,7 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
         const float band_cth = MODE == NN_BAND ? nn_cull_th(band_th, tl) : 0.f;
         float cthw = -INFINITY;        // warp cull threshold: max over its open queries
 #pragma unroll
-        for (int j = 0; j < NN_Q; ++j) {
+        for (int j = 0; j < Q; ++j) {
             const float x = qpx[j] - tl.cx, y = qpy[j] - tl.cy, z = qpz[j] - tl.cz;
             q[j].qx2 = -2.0f * x; q[j].qy2 = -2.0f * y; q[j].qz2 = -2.0f * z;
             q[j].qq = (double)nn_rr(x, y, z);
@@ -401,15 +426,22 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
             if (!q[j].done) cthw = fmaxf(cthw, q[j].cth);
         }
         for (int o = 16; o > 0; o >>= 1) cthw = fmaxf(cthw, __shfl_xor_sync(0xffffffffu, cthw, o));
-        const f2_t qx01 = pk2(q[0].qx2, q[1].qx2), qy01 = pk2(q[0].qy2, q[1].qy2), qz01 = pk2(q[0].qz2, q[1].qz2);
-        const f2_t qx23 = pk2(q[2].qx2, q[3].qx2), qy23 = pk2(q[2].qy2, q[3].qy2), qz23 = pk2(q[2].qz2, q[3].qz2);
+        f2_t qxp[P], qyp[P], qzp[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            qxp[p] = pk2(q[2 * p].qx2, q[2 * p + 1].qx2);
+            qyp[p] = pk2(q[2 * p].qy2, q[2 * p + 1].qy2);
+            qzp[p] = pk2(q[2 * p].qz2, q[2 * p + 1].qz2);
+        }
 
         // visiting order of the rounds: nearest to the tile's box first
         const bool sorted = nrt <= NN_SORT;
         if (sorted) {
-            for (int i = threadIdx.x; i < nrt; i += NN_T)
-                sKey[i] = box_gap2(tb[0], tb[1], tb[2], tb[3], tb[4], tb[5], a.box_round[2 * (ro + i)],
-                                   a.box_round[2 * (ro + i) + 1]);
+            for (int i = threadIdx.x; i < nrt; i += NN_T) {
+                float4 rlo, rhi;
+                nn_round_box<SUB>(a, ro, nsr, i, rlo, rhi);
+                sKey[i] = box_gap2(tb[0], tb[1], tb[2], tb[3], tb[4], tb[5], rlo, rhi);
+            }
             __syncthreads();
             for (int i = threadIdx.x; i < nrt; i += NN_T) {
                 const float ki = sKey[i];
@@ -425,7 +457,8 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
 
         for (int kr = 0; kr < nrt; ++kr) {
             const int i = sorted ? sOrd[kr] : kr;
-            const float4 rlo = a.box_round[2 * (ro + i)], rhi = a.box_round[2 * (ro + i) + 1];
+            float4 rlo, rhi;
+            nn_round_box<SUB>(a, ro, nsr, i, rlo, rhi);
             const bool open = cthw > -INFINITY;
             const bool need = open && !box_far(box_gap2(wl[0], wl[1], wl[2], wh[0], wh[1], wh[2], rlo, rhi), cthw);
             if (!__syncthreads_or(need)) {
@@ -433,8 +466,8 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
                 if (sorted && !__syncthreads_or(open && !box_far(sKey[i], cthw))) break;
                 continue;
             }
-            const long long rb = (long long)i * NN_R;
-            const int nr = (int)min((long long)NN_R, T.rn - rb);
+            const long long rb = (long long)i * RR;
+            const int nr = (int)min((long long)RR, T.rn - rb);
             for (int k = threadIdx.x; k < nr; k += NN_T) {
                 const float4 r = a.r_f4[T.r0 + rb + k];
                 const float rx = r.x - tl.cx, ry = r.y - tl.cy, rz = r.z - tl.cz;
@@ -442,10 +475,15 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
                 sA[k] = make_float4(rx, rx, ry, ry);
                 sB[k] = make_float4(rz, rz, rr, rr);
             }
-            for (int k = threadIdx.x; k < 2 * NN_RB; k += NN_T) sBox[k] = a.box_blk[2 * (ro + i) * NN_RB + k];
+            for (int k = threadIdx.x; k < 2 * RB; k += NN_T) {
+                // blocks of a missing second sub-round (odd sub-round count) are never reached: nr stops first
+                const bool have = (long long)i * SUB + k / (2 * NN_SRB) < nsr;
+                sBox[k] = have ? a.box_blk[2 * (ro + (long long)i * SUB) * NN_SRB + k]
+                               : make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+            }
             __syncthreads();
             if (need) {
-                for (int b = 0; b < NN_RB; ++b) {
+                for (int b = 0; b < RB; ++b) {
                     const int sb = b * NN_BLK;
                     if (sb >= nr) break;
                     const float4 blo = sBox[2 * b], bhi = sBox[2 * b + 1];
@@ -453,39 +491,39 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
                     // each lane's open queries against the block's box
                     bool lane_need = false;
 #pragma unroll
-                    for (int j = 0; j < NN_Q; ++j)
+                    for (int j = 0; j < Q; ++j)
                         lane_need |= !q[j].done &&
                                      !box_far(box_gap2(qpx[j], qpy[j], qpz[j], qpx[j], qpy[j], qpz[j], blo, bhi), q[j].cth);
                     if (!__any_sync(0xffffffffu, lane_need)) continue;
                     const int n = min(NN_BLK, nr - sb);
-                    float m0 = INFINITY, m1 = INFINITY, m2 = INFINITY, m3 = INFINITY;
+                    float mv[Q];
+#pragma unroll
+                    for (int j = 0; j < Q; ++j) mv[j] = INFINITY;
 #pragma unroll 4
                     for (int k = sb; k < sb + n; ++k) {
                         const float4 ra = sA[k];
                         const float4 rb4 = sB[k];
                         const f2_t rxx = pk2(ra.x, ra.y), ryy = pk2(ra.z, ra.w);
                         const f2_t rzz = pk2(rb4.x, rb4.y), rrr = pk2(rb4.z, rb4.w);
-                        const f2_t s01 = fma2(qz01, rzz, fma2(qy01, ryy, fma2(qx01, rxx, rrr)));
-                        const f2_t s23 = fma2(qz23, rzz, fma2(qy23, ryy, fma2(qx23, rxx, rrr)));
-                        float a0, a1, a2, a3;
-                        upk2(s01, a0, a1);
-                        upk2(s23, a2, a3);
-                        m0 = fminf(m0, a0); m1 = fminf(m1, a1); m2 = fminf(m2, a2); m3 = fminf(m3, a3);
+#pragma unroll
+                        for (int p = 0; p < P; ++p) {
+                            const f2_t sv = fma2(qzp[p], rzz, fma2(qyp[p], ryy, fma2(qxp[p], rxx, rrr)));
+                            float a0, a1;
+                            upk2(sv, a0, a1);
+                            mv[2 * p] = fminf(mv[2 * p], a0);
+                            mv[2 * p + 1] = fminf(mv[2 * p + 1], a1);
+                        }
                     }
                     if (MODE == NN_BAND) {
-                        const unsigned n0 = __ballot_sync(0xffffffffu, !q[0].done && m0 <= q[0].ts);
-                        const unsigned n1 = __ballot_sync(0xffffffffu, !q[1].done && m1 <= q[1].ts);
-                        const unsigned n2 = __ballot_sync(0xffffffffu, !q[2].done && m2 <= q[2].ts);
-                        const unsigned n3 = __ballot_sync(0xffffffffu, !q[3].done && m3 <= q[3].ts);
-                        if (n0) nn_band_warp(a, T, q[0], n0, sA, sB, sb, n, rb);
-                        if (n1) nn_band_warp(a, T, q[1], n1, sA, sB, sb, n, rb);
-                        if (n2) nn_band_warp(a, T, q[2], n2, sA, sB, sb, n, rb);
-                        if (n3) nn_band_warp(a, T, q[3], n3, sA, sB, sb, n, rb);
-                    } else {
-                        const int blk = i * NN_RB + b;
-                        const float mv[NN_Q] = {m0, m1, m2, m3};
 #pragma unroll
-                        for (int j = 0; j < NN_Q; ++j) {
+                        for (int j = 0; j < Q; ++j) {
+                            const unsigned nj = __ballot_sync(0xffffffffu, !q[j].done && mv[j] <= q[j].ts);
+                            if (nj) nn_band_warp(a, T, q[j], nj, sA, sB, sb, n, rb);
+                        }
+                    } else {
+                        const int blk = i * RB + b;
+#pragma unroll
+                        for (int j = 0; j < Q; ++j) {
                             if (mv[j] < q[j].ms) { q[j].ms2 = q[j].ms; q[j].ms = mv[j]; q[j].mb = blk; }
                             else q[j].ms2 = fminf(q[j].ms2, mv[j]);
                         }
@@ -494,7 +532,7 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
                 // thresholds for the next rounds
                 float c = -INFINITY;
 #pragma unroll
-                for (int j = 0; j < NN_Q; ++j) {
+                for (int j = 0; j < Q; ++j) {
                     if (MODE != NN_BAND && q[j].live && q[j].ms < INFINITY)
                         q[j].cth = nn_cull_th(nn_min_th(q[j].ms, q[j].qq, tl), tl);
                     if (!q[j].done) c = fmaxf(c, q[j].cth);
@@ -505,7 +543,7 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
                     // the warp's box shrinks to its open queries
                     float l3[3] = {INFINITY, INFINITY, INFINITY}, h3[3] = {-INFINITY, -INFINITY, -INFINITY};
 #pragma unroll
-                    for (int j = 0; j < NN_Q; ++j) {
+                    for (int j = 0; j < Q; ++j) {
                         if (q[j].done) continue;
                         l3[0] = fminf(l3[0], qpx[j]); l3[1] = fminf(l3[1], qpy[j]); l3[2] = fminf(l3[2], qpz[j]);
                         h3[0] = fmaxf(h3[0], qpx[j]); h3[1] = fmaxf(h3[1], qpy[j]); h3[2] = fmaxf(h3[2], qpz[j]);
@@ -524,9 +562,9 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
 
         if (MODE != NN_BAND) {
             // FP64 recheck: the best block alone when no other block can hold a candidate
-            bool full[NN_Q];
+            bool full[Q];
 #pragma unroll
-            for (int j = 0; j < NN_Q; ++j) {
+            for (int j = 0; j < Q; ++j) {
                 full[j] = false;
                 if (!q[j].live || !(q[j].ms < INFINITY)) continue;
                 const double th = nn_min_th(q[j].ms, q[j].qq, tl);
@@ -545,13 +583,13 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
                 }
             }
 #pragma unroll
-            for (int j = 0; j < NN_Q; ++j) {
+            for (int j = 0; j < Q; ++j) {
                 const unsigned nf = __ballot_sync(0xffffffffu, full[j]);
-                if (nf) nn_full_warp(a, T, tl, ro, nrt, q[j], nf, T.q0 + qw + j * 32);
+                if (nf) nn_full_warp(a, T, tl, ro, nsr, q[j], nf, T.q0 + qw + j * 32);
             }
         }
 #pragma unroll
-        for (int j = 0; j < NN_Q; ++j) {
+        for (int j = 0; j < Q; ++j) {
             if (!q[j].live) continue;
             const long long o = T.q0 + qw + j * 32 + lane;
             if (MODE == NN_BAND) a.out_flag[o] = q[j].done ? 0 : 1;     // keep iff no reference within the band
@@ -569,12 +607,12 @@ __global__ void k_nn_tiles(NNArgs a)
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < a.ntask; t += gridDim.x * blockDim.x) {
         const NNTask T = a.task[t];
         const bool on = T.qn > 0 && (T.rn > 0 || a.band_mode);
-        a.tile_cnt[t] = on ? (int)((T.qn + NN_TILE - 1) / NN_TILE) : 0;
-        a.round_cnt[t] = on ? (int)((T.rn + NN_R - 1) / NN_R) : 0;
+        a.tile_cnt[t] = on ? (int)((T.qn + a.tile_q - 1) / a.tile_q) : 0;
+        a.round_cnt[t] = on ? (int)((T.rn + NN_SR - 1) / NN_SR) : 0;
     }
 }
 
-// one warp per round: the box of each 32-reference block (lane b) and of the round
+// one warp per sub-round: the box of each 32-reference block (lane b < 16) and of the sub-round
 __global__ void k_nn_boxes(NNArgs a)
 {
     const long long nround = min(a.round_off[a.ntask], a.round_cap);
@@ -587,16 +625,18 @@ __global__ void k_nn_boxes(NNArgs a)
             if (a.round_off[mid] <= g) lo = mid; else hi = mid - 1;
         }
         const NNTask T = a.task[lo];
-        const long long k0 = (g - a.round_off[lo]) * NN_R + (long long)lane * NN_BLK;
-        const long long k1 = min(k0 + NN_BLK, T.rn);
+        const long long k0 = (g - a.round_off[lo]) * NN_SR + (long long)lane * NN_BLK;
+        const long long k1 = lane < NN_SRB ? min(k0 + NN_BLK, T.rn) : k0;
         float l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};
         for (long long k = k0; k < k1; ++k) {
             const float4 p = a.r_f4[T.r0 + k];
             l[0] = fminf(l[0], p.x); l[1] = fminf(l[1], p.y); l[2] = fminf(l[2], p.z);
             h[0] = fmaxf(h[0], p.x); h[1] = fmaxf(h[1], p.y); h[2] = fmaxf(h[2], p.z);
         }
-        a.box_blk[2 * (g * NN_RB + lane)] = make_float4(l[0], l[1], l[2], 0.f);
-        a.box_blk[2 * (g * NN_RB + lane) + 1] = make_float4(h[0], h[1], h[2], 0.f);
+        if (lane < NN_SRB) {
+            a.box_blk[2 * (g * NN_SRB + lane)] = make_float4(l[0], l[1], l[2], 0.f);
+            a.box_blk[2 * (g * NN_SRB + lane) + 1] = make_float4(h[0], h[1], h[2], 0.f);
+        }
         for (int k = 0; k < 3; ++k) {
             for (int o = 16; o > 0; o >>= 1) {
                 l[k] = fminf(l[k], __shfl_xor_sync(0xffffffffu, l[k], o));
@@ -610,29 +650,44 @@ __global__ void k_nn_boxes(NNArgs a)
     }
 }
 
-void launch_nn_tiles(NNArgs a, int mode, long long* scan_tmp, cudaStream_t s)
+void launch_nn_tiles(NNArgs a, int mode, int variant, long long* scan_tmp, cudaStream_t s)
 {
     a.band_mode = mode == NN_BAND;
+    a.tile_q = NN_T * nn_var_q(variant);
     k_nn_tiles<<<grid_for(a.ntask, 128), 128, 0, s>>>(a);
     scan_counts(a.tile_cnt, a.tile_off, a.ntask, scan_tmp, s);
     scan_counts(a.round_cnt, a.round_off, a.ntask, scan_tmp, s);
 }
 
-void launch_nn_kernel(NNArgs a, int mode, long long tile_cap, cudaStream_t s)
+template <int MODE>
+static void nn_dispatch(const NNArgs& a, int variant, unsigned grid, cudaStream_t s)
 {
-    a.band_mode = mode == NN_BAND;
-    k_nn_boxes<<<grid_for(a.round_cap * 32, 256), 256, 0, s>>>(a);
-    // one tile per CTA; CTAs past the tile count exit at once
-    const unsigned grid = (unsigned)(tile_cap < 1 ? 1 : (tile_cap > 0x7fffffffLL ? 0x7fffffffLL : tile_cap));
-    if (mode == NN_MIN) k_nn<NN_MIN><<<grid, NN_T, 0, s>>>(a);
-    else if (mode == NN_ARGMIN) k_nn<NN_ARGMIN><<<grid, NN_T, 0, s>>>(a);
-    else k_nn<NN_BAND><<<grid, NN_T, 0, s>>>(a);
+    switch (variant) {
+    case 1: k_nn<MODE, 4, 1><<<grid, NN_T, 0, s>>>(a); break;
+    case 2: k_nn<MODE, 2, 2><<<grid, NN_T, 0, s>>>(a); break;
+    case 3: k_nn<MODE, 2, 1><<<grid, NN_T, 0, s>>>(a); break;
+    default: k_nn<MODE, 4, 2><<<grid, NN_T, 0, s>>>(a); break;
+    }
 }
 
-void launch_nn(NNArgs a, int mode, long long tile_cap, long long* scan_tmp, cudaStream_t s)
+void launch_nn_kernel(NNArgs a, int mode, int variant, long long tile_cap, cudaStream_t s)
 {
-    launch_nn_tiles(a, mode, scan_tmp, s);
-    launch_nn_kernel(a, mode, tile_cap, s);
+    a.band_mode = mode == NN_BAND;
+    a.tile_q = NN_T * nn_var_q(variant);
+    k_nn_boxes<<<grid_for(a.round_cap * 32, 256), 256, 0, s>>>(a);
+    // one tile per CTA (tile_cap bounds the tile count of the largest tiles'
+    // variant times 2); CTAs past the tile count exit at once
+    if (nn_var_q(variant) == 2) tile_cap *= 2;
+    const unsigned grid = (unsigned)(tile_cap < 1 ? 1 : (tile_cap > 0x7fffffffLL ? 0x7fffffffLL : tile_cap));
+    if (mode == NN_MIN) k_nn<NN_MIN, 4, 2><<<grid, NN_T, 0, s>>>(a);      // standalone searches only
+    else if (mode == NN_ARGMIN) nn_dispatch<NN_ARGMIN>(a, variant, grid, s);
+    else nn_dispatch<NN_BAND>(a, variant, grid, s);
+}
+
+void launch_nn(NNArgs a, int mode, int variant, long long tile_cap, long long* scan_tmp, cudaStream_t s)
+{
+    launch_nn_tiles(a, mode, variant, scan_tmp, s);
+    launch_nn_kernel(a, mode, variant, tile_cap, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -686,7 +741,7 @@ __global__ void k_points_task(const double* partials, int nblocks, long long nq,
     tile_cnt[0] = (int)nt;
     tile_off[0] = 0;
     tile_off[1] = nt;
-    const long long nrd = nt > 0 ? (nr + NN_R - 1) / NN_R : 0;
+    const long long nrd = nt > 0 ? (nr + NN_SR - 1) / NN_SR : 0;
     round_cnt[0] = (int)nrd;
     round_off[0] = 0;
     round_off[1] = nrd;

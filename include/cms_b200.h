@@ -187,7 +187,7 @@ cms_status cms_nearest_dots(cms_ctx* ctx, const double* query_xyz, int64_t n_que
  * (NULL: no indices) are device pointers; the work is enqueued on `stream`
  * (NULL: the default stream) and no memory is allocated: the scratch is one
  * fixed 32 MiB device array per GPU, so n_query + n_ref may not exceed
- * 1,966,080 points (CMS_ERR_ARG otherwise, nothing launched).  The first call
+ * 1,964,032 points (CMS_ERR_ARG otherwise, nothing launched).  The first call
  * on a device looks up the scratch address (make it before any stream
  * capture); calls that overlap on the GPU share the scratch and race. */
 cms_status cms_nearest_dots_noalloc(const double* query_xyz, int64_t n_query, const double* ref_xyz,
@@ -206,6 +206,18 @@ cms_status cms_run_graph(cms_ctx* ctx);
  * cms_run_graph, which re-sizes). */
 cms_status cms_graph_launch(cms_ctx* ctx);
 cms_status cms_graph_check(cms_ctx* ctx);
+
+/* Search shapes of the batched pipeline's three nearest-dot searches (CMS, SC
+ * band trim, SC neighbour argmin): variants[3], each 0..3 = (4 queries per
+ * thread, 1024-reference rounds), (4, 512), (2, 1024), (2, 512).  Every shape
+ * gives the same results.  By default an autotuner times all shapes on each
+ * new batch shape before capturing the graph and keeps the fastest per search
+ * (tune_ms[3 x 4]: the times it measured, NULL to skip); cms_set_nn_variants
+ * forces shapes and turns the tuner off, cms_set_autotune(1) turns it back on.
+ * The reference's CuPy kernels have fixed launch shapes (_gpu_kernels.py). */
+cms_status cms_set_nn_variants(cms_ctx* ctx, const int32_t* variants);
+cms_status cms_get_nn_variants(cms_ctx* ctx, int32_t* variants, double* tune_ms);
+cms_status cms_set_autotune(cms_ctx* ctx, int32_t enable);
 
 /* Nearest-dot search work of the last run: pairs[0..5] = (query x reference
  * pairs, queries) of the CMS search, the SC band (trim) search and the SC

@@ -55,3 +55,43 @@ def test_far_offset_coordinates():
     ref = cdist(r, q, metric="sqeuclidean")
     exact("min d2", d2, ref.min(axis=0))
     exact("argmin", idx, ref.argmin(axis=0))
+
+
+@pytest.mark.parametrize("variant", [1, 2, 3])
+def test_search_shapes_give_identical_results(variant):
+    """Every tunable search shape returns the default shape's CMS, SC and gradient bit for bit."""
+    from cms_cuda import _lib
+    from parity import inputs, load_case
+    cases = [load_case(n) for n in ("golden_pkl", "synth_small_s7", "sc_example_pdb")]
+    xyz, rad, off, nb = [], [], [0], []
+    for c in cases:
+        bx, br, tx, tr = inputs(c)
+        xyz += [bx, tx]; rad += [br, tr]; nb.append(len(br)); off.append(off[-1] + len(br) + len(tr))
+    X, R = np.concatenate(xyz), np.concatenate(rad)
+    out = []
+    for v in (0, variant):
+        ctx = _lib.Context(0)
+        ctx.set_nn_variants([v, v, v])
+        ctx.load_batch(np.array(off), np.array(nb), X, R)
+        ctx.generate(all_atoms=False)
+        pa, tot = ctx.contact_ms(per_atom=True)
+        sc, sides = ctx.shape_complementarity()
+        g = ctx.contact_ms_backward(True)
+        out.append((pa, tot, sc, sides, g))
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b, equal_nan=True)
+
+
+def test_autotuner_picks_shapes():
+    from cms_cuda import _lib
+    from parity import inputs, load_case
+    bx, br, tx, tr = inputs(load_case("synth_plain_1200_450"))
+    ctx = _lib.Context(0)
+    ctx.load_batch(np.array([0, len(br) + len(tr)]), np.array([len(br)]), np.concatenate([bx, tx]),
+                   np.concatenate([br, tr]))
+    ctx.run_graph()
+    v, ms = ctx.nn_variants()
+    assert all(0 <= x < 4 for x in v)
+    assert np.isfinite(ms).all() and (ms > 0).all()
+    for k in range(3):
+        assert ms[k, v[k]] == ms[k].min()

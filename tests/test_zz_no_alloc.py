@@ -19,7 +19,7 @@ from parity import exact
 
 pytestmark = pytest.mark.gpu
 
-MAX_POINTS = 1920 * 1024
+MAX_POINTS = 3836 * 512
 
 
 def _lib():
