@@ -23,7 +23,7 @@ PKG = os.path.join(HERE, "cms_cuda")
 ROOT = os.path.dirname(HERE)
 INCLUDE = os.path.join(ROOT, "include")
 
-CUDA_SOURCES = ["k_scan.cu", "k_surface.cu", "k_dots.cu", "k_readout.cu", "k_adjoint.cu", "capi.cu", "k_noalloc.cu"]
+CUDA_SOURCES = ["k_scan.cu", "k_surface.cu", "k_dots.cu", "k_readout.cu", "k_adjoint.cu", "k_refine.cu", "capi.cu", "k_noalloc.cu"]
 HEADERS = ["cms_math.cuh", "cms_internal.cuh", "cms_kernels.cuh", "cms_readout.cuh", "cms_circle.cuh", "cms_dual.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -30,7 +30,8 @@ EXPORTED = (
     "cms_graph_launch", "cms_graph_check", "cms_nn_work", "cms_transfer_bytes", "cms_fp32_peak",
     "cms_nearest_dots", "cms_nearest_dots_noalloc", "cms_contact_ms_backward", "cms_set_backward",
     "cms_set_grad_total", "cms_grad_xyz", "cms_recompute_dots", "cms_export_dot_units",
-    "cms_set_nn_variants", "cms_get_nn_variants", "cms_set_autotune",
+    "cms_set_nn_variants", "cms_get_nn_variants", "cms_set_autotune", "cms_refine_begin",
+    "cms_refine_set_params", "cms_refine_run", "cms_refine_pose", "cms_refine_end",
 )
 
 NN_VARIANT_NAMES = ("q4 r1024", "q4 r512", "q2 r1024", "q2 r512")
@@ -116,6 +117,11 @@ def load():
             "cms_set_nn_variants": [_VP, _VP],
             "cms_get_nn_variants": [_VP, _VP, _VP],
             "cms_set_autotune": [_VP, _I32],
+            "cms_refine_begin": [_VP, _VP, _I32, _I32],
+            "cms_refine_set_params": [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double],
+            "cms_refine_run": [_VP, _I32, _VP, _I32],
+            "cms_refine_pose": [_VP, _VP, _VP, _VP, _I32],
+            "cms_refine_end": [_VP],
         }
         for name, args in sig.items():
             f = getattr(lib, name)
@@ -228,6 +234,29 @@ class Context:
         ms = np.zeros(12)
         self._check(self.lib.cms_get_nn_variants(self.h, _ptr(v), _ptr(ms)))
         return v.tolist(), ms.reshape(3, 4)
+
+    # -- pose refinement ------------------------------------------------------
+    def refine_begin(self, ref_xyz, max_steps):
+        x = np.ascontiguousarray(ref_xyz, dtype=np.float64).reshape(-1, 3)
+        self._check(self.lib.cms_refine_begin(self.h, _ptr(x), int(max_steps), CMS_HOST))
+
+    def refine_set_params(self, eta_t, eta_w, max_t, max_w):
+        self._check(self.lib.cms_refine_set_params(self.h, float(eta_t), float(eta_w), float(max_t), float(max_w)))
+
+    def refine_run(self, steps):
+        """CMS (steps x B) of every evaluated pose."""
+        h = np.empty((int(steps), self.B), dtype=np.float64)
+        self._check(self.lib.cms_refine_run(self.h, int(steps), _ptr(h), CMS_HOST))
+        return h
+
+    def refine_pose(self, xyz=True):
+        rot = np.empty((self.B, 3, 3)); tr = np.empty((self.B, 3))
+        x = np.empty((self.N, 3)) if xyz else None
+        self._check(self.lib.cms_refine_pose(self.h, _ptr(rot), _ptr(tr), _ptr(x), CMS_HOST))
+        return rot, tr, x
+
+    def refine_end(self):
+        self._check(self.lib.cms_refine_end(self.h))
 
     def nn_work(self):
         w = np.zeros(6, dtype=np.int64)

@@ -170,6 +170,14 @@ def config_plain_large(seed=1):
     return make_complex(8000, 1800, seed)
 
 
+def config_refine(B=256, seed=5):
+    """Pose-refinement batch: target uniform 1500-3000, binder uniform 300-800 atoms."""
+    rng = np.random.default_rng(seed)
+    nt = rng.integers(1500, 3001, B).astype(np.int32)
+    nb = rng.integers(300, 801, B).astype(np.int32)
+    return make_batch(nt, nb, seed + 1)
+
+
 def config_batched(B=4096, seed=2):
     """B complexes, target log-uniform 600-4000, binder log-uniform 80-1200, ~5 % ligand binders of 20-60 atoms."""
     rng = np.random.default_rng(seed)

@@ -41,6 +41,15 @@ __global__ void k_fill_i(int* p, long long n, int v)
 
 // totals the host needs after a run: cells, neighbour / buried entries,
 // toroid pairs, probes, dots, buried dots, trimmed dots
+// capacity check of a stage total (two totals summed when b is given)
+__global__ void k_cap_check(const long long* a, const long long* b, long long cap, int* ovf)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        const long long t = *a + (b ? *b : 0);
+        if (t > cap) *ovf = 1;
+    }
+}
+
 __global__ void k_summary(Dev d, Rd r, long long* out)
 {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -206,6 +215,10 @@ struct cms_ctx {
     // nearest-dot search shapes per stage (CMS, SC band, SC argmin), chosen by
     // the autotuner for each batch shape (or forced by cms_set_nn_variants)
     int nn_var[3] = {0, 0, 0};
+    // rigid-body pose refinement (cms_refine_*)
+    bool refine = false;
+    RefineParams rprm{0.002, 0.0002, 0.05, 0.00872664625997};   // max 0.05 A and 0.5 degree per step
+    int hist_cap = 0;
     bool autotune = true;
     long long tune_key[3] = {-1, -1, -1};
     double tune_ms[3][NN_VARIANTS] = {};
@@ -236,7 +249,7 @@ struct cms_ctx {
         S_CMS_IDX, S_ADJ_A, S_ADJ_REFDOT, S_ADJ_REFVEC, S_ADJ_RCNT, S_ADJ_RFILL, S_ADJ_ROFF, S_ADJ_RSLOT,
         S_ADJ_GCONV, S_ADJ_GTOR, S_ADJ_GCONC, S_ADJ_GTOT, S_ADJ_GRAD, S_RECOMP_XYZ, S_RECOMP_AREA,
         S_ADJ_ACT_CONV, S_ADJ_ACT_TOR, S_ADJ_ACT_CONC, S_ADJ_ACT_ATOM, S_ADJ_LIST_CONV, S_ADJ_LIST_TOR,
-        S_ADJ_LIST_CONC, S_ADJ_NACT,
+        S_ADJ_LIST_CONC, S_ADJ_NACT, S_OVF, S_REF_XYZ, S_POSE, S_POSE_CKPT, S_POSE_CEN, S_HIST, S_STEP, S_MAXSUM,
         S_COUNT
     };
 
@@ -309,6 +322,7 @@ void bind_batch(cms_ctx* x)
     d.coin = x->ensure<unsigned long long>(cms_ctx::S_COIN, B);
     d.cell_atom = x->ensure<int>(cms_ctx::S_CELL_ATOM, N);
     d.nnb = x->ensure<int>(cms_ctx::S_NNB, N);
+    d.ovf = x->ensure<int>(cms_ctx::S_OVF, 1);
     d.nb_off = x->ensure<long long>(cms_ctx::S_NB_OFF, N + 1);
     d.nbur = x->ensure<int>(cms_ctx::S_NBUR, N);
     d.bu_off = x->ensure<long long>(cms_ctx::S_BU_OFF, N + 1);
@@ -442,9 +456,13 @@ void mark(cms_ctx* x, int stage)
 // buffers to fit (host syncs between stages); sized = false: enqueue every
 // stage with the current capacities (capturable in a CUDA graph).
 // ---------------------------------------------------------------------------
+// headroom of a grown capacity: need / 8 normally; need / 3 while refining
+// poses (the surfaces change from step to step inside one captured graph)
+static thread_local int t_growth_div = 8;
+
 void grow(long long& cap, long long need)
 {
-    if (need > cap) cap = need + need / 8 + 64;
+    if (need > cap) cap = need + need / t_growth_div + 64;
 }
 
 void enqueue_surface(cms_ctx* x, bool sized)
@@ -454,6 +472,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
     long long* tmp = scan_tmp(x);
     mark(x, -1);
     ck(cudaMemsetAsync(d.status, 0, sizeof(int) * x->B, s), "memset");
+    ck(cudaMemsetAsync(d.ovf, 0, sizeof(int), s), "memset");
     launch_setup(d, s);
     scan_counts(d.ncell, d.ncell_scan, d.B, tmp, s);
     if (sized) {
@@ -462,6 +481,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
         bind_caps(x);
         tmp = scan_tmp(x);
     }
+    k_cap_check<<<1, 32, 0, s>>>(d.ncell_scan + d.B, nullptr, x->cap_cells, d.ovf);
     launch_cells(d, x->cap_cells, tmp, s);
     mark(x, P_CELLS);
     launch_attention(d, s);
@@ -476,6 +496,8 @@ void enqueue_surface(cms_ctx* x, bool sized)
         bind_caps(x);
         tmp = scan_tmp(x);
     }
+    k_cap_check<<<1, 32, 0, s>>>(d.nb_off + d.N, nullptr, x->cap_nb, d.ovf);
+    k_cap_check<<<1, 32, 0, s>>>(d.bu_off + d.N, nullptr, x->cap_bu, d.ovf);
     launch_neighbor_emit(d, s);
     mark(x, P_NB_EMIT);
     launch_pairs(d, false, s);
@@ -485,6 +507,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
         bind_caps(x);
         tmp = scan_tmp(x);
     }
+    k_cap_check<<<1, 32, 0, s>>>(d.tor_off + d.N, nullptr, x->cap_tor, d.ovf);
     launch_pairs(d, true, s);
     mark(x, P_PAIRS);
     launch_triples(d, false, s);
@@ -496,6 +519,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
         bind_caps(x);
         tmp = scan_tmp(x);
     }
+    k_cap_check<<<1, 32, 0, s>>>(d.plus_off + d.N, d.minus_off + d.N, x->cap_probe, d.ovf);
     launch_triples(d, true, s);
     launch_low_probes(d, x->cap_probe, tmp, s);
     mark(x, P_TRIPLES_EMIT);
@@ -519,6 +543,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
         bind_caps(x);
         tmp = scan_tmp(x);
     }
+    k_cap_check<<<1, 32, 0, s>>>(d.dot_off + 2LL * d.B, nullptr, x->cap_dot, d.ovf);
     launch_convex(d, true, s);
     mark(x, P_CONVEX_EMIT);
     launch_toroidal(d, x->cap_tor, true, s);
@@ -546,6 +571,7 @@ NNArgs nn_args(cms_ctx* x, int kind)
     a.box_round = x->get<float4>(cms_ctx::S_BOX_ROUND);
     a.box_blk = x->get<float4>(cms_ctx::S_BOX_BLK);
     a.round_cap = nn_round_cap(x->cap_dot, 2LL * x->B);
+    a.ovf = x->d.ovf;
     return a;
 }
 
@@ -660,6 +686,20 @@ void fill_gtot(cms_ctx* x, const double* g, int where)
     } else {
         k_fill_d<<<grid1(x->B), 256, 0, x->stream>>>(dst, x->B, 1.0);
     }
+}
+
+void enqueue_pose_apply(cms_ctx* x)
+{
+    launch_pose_apply(x->d, x->get<double>(cms_ctx::S_REF_XYZ), x->get<double>(cms_ctx::S_POSE),
+                      x->get<double>(cms_ctx::S_POSE_CEN), x->stream);
+}
+
+void enqueue_pose_update(cms_ctx* x)
+{
+    launch_pose_update(x->d, x->get<double>(cms_ctx::S_ADJ_GRAD), x->get<double>(cms_ctx::S_REF_XYZ),
+                       x->get<double>(cms_ctx::S_POSE), x->get<double>(cms_ctx::S_POSE_CEN),
+                       x->get<double>(cms_ctx::S_TOT_CMS), x->get<double>(cms_ctx::S_HIST),
+                       x->get<int>(cms_ctx::S_STEP), x->hist_cap, x->rprm, x->stream);
 }
 
 void enqueue_summary(cms_ctx* x)
@@ -1214,10 +1254,11 @@ void capture_graph(cms_ctx* x)
     const long long shape[2] = {x->B, x->N};
     const bool new_shape = x->cap_dot == 0 || std::memcmp(shape, x->tune_key, sizeof(shape)) != 0;
     if (new_shape && (x->cap_dot == 0 || x->autotune)) {
+        if (x->refine) enqueue_pose_apply(x);
         run_sized_surface(x, 0);                         // size every buffer for this batch
         autotune_nn(x);                                  // pick the search shapes on it
     }
-    const long long key[4] = {x->B, x->N, x->cap_dot, x->bwd_enabled ? 1 + x->bwd_side : 0};
+    const long long key[4] = {x->B, x->N, x->cap_dot, x->refine ? 100 : (x->bwd_enabled ? 1 + x->bwd_side : 0)};
     const long long vk = (x->nn_var[0] << 8) | (x->nn_var[1] << 4) | x->nn_var[2];
     if (x->gexec && std::memcmp(key, x->graph_key, sizeof(key)) == 0 && vk == x->graph_vk) return;
     if (x->gexec) { cudaGraphExecDestroy(x->gexec); x->gexec = nullptr; }
@@ -1228,12 +1269,24 @@ void capture_graph(cms_ctx* x)
     if (x->bwd_enabled) bind_adj(x);                    // allocate before capture
     ck(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     try {
-        enqueue_surface(x, false);
-        enqueue_split(x);
-        enqueue_cms(x);
-        enqueue_sc(x);
-        if (x->bwd_enabled) enqueue_backward(x);
-        enqueue_summary(x);
+        if (x->refine) {
+            // one refinement step: pose -> surfaces -> CMS -> gradient -> pose step
+            enqueue_pose_apply(x);
+            enqueue_surface(x, false);
+            enqueue_split(x);
+            enqueue_cms(x);
+            enqueue_backward(x);
+            enqueue_pose_update(x);
+            enqueue_summary(x);
+            launch_track_max(x->get<long long>(cms_ctx::S_SUMMARY), x->get<long long>(cms_ctx::S_MAXSUM), x->stream);
+        } else {
+            enqueue_surface(x, false);
+            enqueue_split(x);
+            enqueue_cms(x);
+            enqueue_sc(x);
+            if (x->bwd_enabled) enqueue_backward(x);
+            enqueue_summary(x);
+        }
     } catch (...) {
         cudaGraph_t g = nullptr;
         cudaStreamEndCapture(x->stream, &g);
@@ -1464,6 +1517,168 @@ cms_status cms_profile_stages(cms_ctx* x, double* ms, int32_t cap, int32_t* n_st
     x->bwd_ok = x->bwd_enabled != 0;
     x->max_ok = false;
     API_END
+}
+
+cms_status cms_refine_begin(cms_ctx* x, const double* ref_xyz, int32_t max_steps, int32_t where)
+{
+    if (!x || !ref_xyz || max_steps < 0) return fail(x, CMS_ERR_ARG, "bad argument");
+    API_BEGIN
+    if (!x->have_batch) throw Fail{CMS_ERR_STATE, "no batch loaded"};
+    ck(cudaSetDevice(x->device), "cudaSetDevice");
+    cudaStream_t s = x->stream;
+    double* ref = x->ensure<double>(cms_ctx::S_REF_XYZ, 3 * x->N);
+    if (where == CMS_HOST) x->h2d_bytes += 24LL * x->N;
+    ck(cudaMemcpyAsync(ref, ref_xyz, sizeof(double) * 3 * x->N,
+                       where == CMS_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s), "reference pose");
+    double* cen = x->ensure<double>(cms_ctx::S_POSE_CEN, 3 * x->B);
+    launch_pose_centroid(x->d, ref, cen, s);
+    std::vector<double> id(12 * (size_t)x->B, 0.0);
+    for (int c = 0; c < x->B; ++c) id[12 * c] = id[12 * c + 4] = id[12 * c + 8] = 1.0;
+    double* pose = x->ensure<double>(cms_ctx::S_POSE, 12 * x->B);
+    x->ensure<double>(cms_ctx::S_POSE_CKPT, 12 * x->B);
+    ck(cudaMemcpyAsync(pose, id.data(), sizeof(double) * id.size(), cudaMemcpyHostToDevice, s), "pose");
+    x->hist_cap = max_steps;
+    x->ensure<double>(cms_ctx::S_HIST, std::max(1LL, (long long)max_steps * x->B));
+    ck(cudaMemsetAsync(x->ensure<int>(cms_ctx::S_STEP, 1), 0, sizeof(int), s), "step");
+    x->ensure<long long>(cms_ctx::S_MAXSUM, 8);
+    ck(cudaStreamSynchronize(s), "sync");
+    x->refine = true;
+    x->bwd_enabled = 1;
+    x->bwd_side = 1;
+    fill_gtot(x, nullptr, CMS_DEVICE);
+    x->graph_key[0] = -1;
+    x->tune_key[0] = -1;
+    x->cap_dot = 0;                                      // size again with refinement headroom
+    API_END
+}
+
+cms_status cms_refine_set_params(cms_ctx* x, double eta_t, double eta_w, double max_t, double max_w)
+{
+    if (!x || !(eta_t >= 0) || !(eta_w >= 0) || !(max_t >= 0) || !(max_w >= 0))
+        return fail(x, CMS_ERR_ARG, "step sizes must be non-negative");
+    x->rprm = RefineParams{eta_t, eta_w, max_t, max_w};
+    x->graph_key[0] = -1;                                // parameters are baked into the captured graph
+    return CMS_OK;
+}
+
+cms_status cms_refine_run(cms_ctx* x, int32_t steps, double* cms_hist, int32_t where)
+{
+    if (!x || steps < 0) return fail(x, CMS_ERR_ARG, "bad argument");
+    API_BEGIN
+    if (!x->refine) throw Fail{CMS_ERR_STATE, "cms_refine_begin first"};
+    ck(cudaSetDevice(x->device), "cudaSetDevice");
+    cudaStream_t s = x->stream;
+    const int B = x->B;
+    int* step = x->get<int>(cms_ctx::S_STEP);
+    int step0 = 0;
+    ck(cudaMemcpy(&step0, step, sizeof(int), cudaMemcpyDeviceToHost), "step");
+    if (step0 + steps > x->hist_cap) throw Fail{CMS_ERR_ARG, "more steps than cms_refine_begin's max_steps"};
+    const int chunk = 25;
+    int done = 0, retries = 0;
+    t_growth_div = 3;
+    try {
+        capture_graph(x);                                // size, tune and capture (also for steps = 0)
+        while (done < steps) {
+            const int n = std::min(chunk, steps - done);
+            capture_graph(x);
+            // checkpoint: pose and step counter; the chunk's largest stage totals
+            ck(cudaMemcpyAsync(x->get<double>(cms_ctx::S_POSE_CKPT), x->get<double>(cms_ctx::S_POSE),
+                               sizeof(double) * 12 * B, cudaMemcpyDeviceToDevice, s), "checkpoint");
+            ck(cudaMemsetAsync(x->get<long long>(cms_ctx::S_MAXSUM), 0, 8 * sizeof(long long), s), "max");
+            int ck_step = 0;
+            ck(cudaMemcpyAsync(&ck_step, step, sizeof(int), cudaMemcpyDeviceToHost, s), "step");
+            for (int i = 0; i < n; ++i) ck(cudaGraphLaunch(x->gexec, s), "graph launch");
+            long long mx[8];
+            ck(cudaMemcpyAsync(mx, x->get<long long>(cms_ctx::S_MAXSUM), sizeof(mx), cudaMemcpyDeviceToHost, s), "max");
+            ck(cudaStreamSynchronize(s), "sync");
+            const bool over = mx[0] > x->cap_cells || mx[1] > x->cap_nb || mx[2] > x->cap_bu || mx[3] > x->cap_tor ||
+                              mx[4] > x->cap_probe || mx[5] > x->cap_dot;
+            if (over) {
+                // a step outgrew the workspace: back to the checkpoint, size for it with headroom, redo
+                if (++retries > 8) {
+                    char m[256];
+                    std::snprintf(m, sizeof(m), "refinement keeps outgrowing its workspace (need/capacity: cells "
+                                  "%lld/%lld, neighbours %lld/%lld, buried %lld/%lld, pairs %lld/%lld, probes %lld/%lld, "
+                                  "dots %lld/%lld)", mx[0], x->cap_cells, mx[1], x->cap_nb, mx[2], x->cap_bu, mx[3],
+                                  x->cap_tor, mx[4], x->cap_probe, mx[5], x->cap_dot);
+                    throw Fail{CMS_ERR_CAPACITY, m};
+                }
+                ck(cudaMemcpyAsync(x->get<double>(cms_ctx::S_POSE), x->get<double>(cms_ctx::S_POSE_CKPT),
+                                   sizeof(double) * 12 * B, cudaMemcpyDeviceToDevice, s), "restore");
+                ck(cudaMemcpyAsync(step, &ck_step, sizeof(int), cudaMemcpyHostToDevice, s), "restore step");
+                x->cap_cells = std::max(x->cap_cells, mx[0]); x->cap_nb = std::max(x->cap_nb, mx[1]);
+                x->cap_bu = std::max(x->cap_bu, mx[2]); x->cap_tor = std::max(x->cap_tor, mx[3]);
+                x->cap_probe = std::max(x->cap_probe, mx[4]); x->cap_dot = std::max(x->cap_dot, mx[5]);
+                grow(x->cap_cells, mx[0] + 1); grow(x->cap_nb, mx[1] + 1); grow(x->cap_bu, mx[2] + 1);
+                grow(x->cap_tor, mx[3] + 1); grow(x->cap_probe, mx[4] + 1); grow(x->cap_dot, mx[5] + 1);
+                x->graph_key[0] = -1;
+                continue;
+            }
+            done += n;
+            retries = 0;
+        }
+    } catch (...) {
+        t_growth_div = 8;
+        throw;
+    }
+    t_growth_div = 8;
+    pull_host_state(x);
+    x->surf_ok = true;
+    x->surf_all_atoms = 0;
+    x->cms_ok = x->bwd_ok = true;
+    x->sc_ok = x->max_ok = false;
+    if (cms_hist && steps > 0) {
+        std::vector<double> h((size_t)steps * B);
+        ck(cudaMemcpy(h.data(), x->get<double>(cms_ctx::S_HIST) + (long long)step0 * B, sizeof(double) * h.size(),
+                      cudaMemcpyDeviceToHost), "history");
+        if (where == CMS_HOST) std::memcpy(cms_hist, h.data(), sizeof(double) * h.size());
+        else ck(cudaMemcpy(cms_hist, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice), "history");
+    }
+    API_END
+}
+
+cms_status cms_refine_pose(cms_ctx* x, double* rot, double* trans, double* xyz, int32_t where)
+{
+    if (!x) return CMS_ERR_ARG;
+    API_BEGIN
+    if (!x->refine) throw Fail{CMS_ERR_STATE, "cms_refine_begin first"};
+    ck(cudaSetDevice(x->device), "cudaSetDevice");
+    const int B = x->B;
+    std::vector<double> P(12 * (size_t)B);
+    ck(cudaMemcpy(P.data(), x->get<double>(cms_ctx::S_POSE), sizeof(double) * P.size(), cudaMemcpyDeviceToHost), "pose");
+    std::vector<double> R(9 * (size_t)B), T(3 * (size_t)B);
+    for (int c = 0; c < B; ++c) {
+        for (int k = 0; k < 9; ++k) R[9 * c + k] = P[12 * c + k];
+        for (int k = 0; k < 3; ++k) T[3 * c + k] = P[12 * c + 9 + k];
+    }
+    auto put = [&](double* dst, const std::vector<double>& v) {
+        if (!dst) return;
+        if (where == CMS_HOST) std::memcpy(dst, v.data(), sizeof(double) * v.size());
+        else ck(cudaMemcpy(dst, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice), "copy");
+    };
+    put(rot, R);
+    put(trans, T);
+    if (xyz) {
+        // coordinates of the current poses (the surfaces of the last step are no longer current)
+        enqueue_pose_apply(x);
+        std::vector<double4> a(x->N);
+        ck(cudaMemcpyAsync(a.data(), x->d.xyzr, sizeof(double4) * x->N, cudaMemcpyDeviceToHost, x->stream), "xyz");
+        ck(cudaStreamSynchronize(x->stream), "sync");
+        std::vector<double> v(3 * (size_t)x->N);
+        for (long long g = 0; g < x->N; ++g) { v[3 * g] = a[g].x; v[3 * g + 1] = a[g].y; v[3 * g + 2] = a[g].z; }
+        put(xyz, v);
+        x->surf_ok = x->cms_ok = x->sc_ok = x->bwd_ok = x->max_ok = false;
+    }
+    API_END
+}
+
+cms_status cms_refine_end(cms_ctx* x)
+{
+    if (!x) return CMS_ERR_ARG;
+    x->refine = false;
+    x->bwd_enabled = 0;
+    x->graph_key[0] = -1;
+    return CMS_OK;
 }
 
 cms_status cms_set_nn_variants(cms_ctx* x, const int32_t* variants)

@@ -66,6 +66,7 @@ struct Dev {
     int* ncell;                        // B  cells per complex
     long long* ncell_scan;             // B+1
     int* status;                       // B
+    int* ovf;                          // 1: a capacity of this run was exceeded (set by the check kernels)
     unsigned long long* coin;          // B  first coincident pair (i<<32|j), local
     // cells
     long long cells_cap;
@@ -112,6 +113,14 @@ struct Dev {
 __device__ __forceinline__ V3 atom_xyz(const Dev& d, int g) { double4 a = d.xyzr[g]; return v3(a.x, a.y, a.z); }
 
 // grid helpers
+// Graph-mode runs use fixed capacities; when a stage's total exceeds its
+// capacity the run is flagged (and redone by the host), and every later
+// pipeline kernel returns at entry so nothing indexes past a capacity.
+#define CMS_EXIT_ON_OVERFLOW(d) \
+    do {                        \
+        if (*(d).ovf) return;   \
+    } while (0)
+
 __device__ __forceinline__ int cell_coord(double x, double o, double h, int dim)
 {
     int c = (int)floor((x - o) / h);

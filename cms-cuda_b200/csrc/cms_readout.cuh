@@ -43,6 +43,7 @@ struct NNArgs {
     long long round_cap;    // rounds the box arrays hold
     int band_mode;
     int tile_q;             // queries per tile of the launched variant
+    const int* ovf;         // the batch's overflow flag (null for standalone searches)
 };
 
 // readout workspace, capacity = dot capacity unless noted
@@ -79,6 +80,18 @@ struct AdjBuf {
 void launch_adjoint(const Dev& d, const Rd& r, const AdjBuf& a, const NNTask* cms_task, int side, double* grad,
                     long long* scan_tmp, cudaStream_t s);
 void launch_recompute(const Dev& d, double* xyz, double* area, cudaStream_t s);
+
+// rigid-body pose refinement (k_refine.cu)
+struct RefineParams {
+    double eta_t, eta_w;    // ascent step per unit gradient: A, radians
+    double max_t, max_w;    // step caps: A, radians
+};
+void launch_pose_apply(const Dev& d, const double* ref, const double* pose, const double* cen, cudaStream_t s);
+void launch_pose_update(const Dev& d, const double* grad, const double* ref, double* pose, const double* cen,
+                        const double* totals, double* hist, int* step, int hist_steps, const RefineParams& prm,
+                        cudaStream_t s);
+void launch_track_max(const long long* summary, long long* mx, cudaStream_t s);
+void launch_pose_centroid(const Dev& d, const double* ref, double* cen, cudaStream_t s);
 
 void launch_split_buried(const Dev& d, const Rd& r, long long dot_cap, long long* scan_tmp, cudaStream_t s);
 void launch_tasks(const Dev& d, const Rd& r, int kind, NNTask* task, cudaStream_t s);

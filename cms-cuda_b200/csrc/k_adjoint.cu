@@ -473,6 +473,7 @@ __device__ __forceinline__ void mark_unit(const Dev& d, const AdjBuf& a, int dot
 // pass 1: query dots of `side`; A = (d/dp, d/darea) per dot
 __global__ void k_adj_queries(Dev d, Rd r, AdjBuf a, const NNTask* task, int side)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const long long NB = r.bur_scan[adj_doff(d, 2LL * d.B)];
     const double w = d.st.weight;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < NB; k += (long long)gridDim.x * blockDim.x) {
@@ -505,6 +506,7 @@ __global__ void k_adj_queries(Dev d, Rd r, AdjBuf a, const NNTask* task, int sid
 // pass 2: reference contributions, counting sort by the reference's buried entry
 __global__ void k_adj_ref_count(Dev d, Rd r, AdjBuf a)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const long long NB = r.bur_scan[adj_doff(d, 2LL * d.B)];
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < NB; k += (long long)gridDim.x * blockDim.x) {
         const int re = a.ref_ent[k];
@@ -514,6 +516,7 @@ __global__ void k_adj_ref_count(Dev d, Rd r, AdjBuf a)
 
 __global__ void k_adj_ref_fill(Dev d, Rd r, AdjBuf a)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const long long NB = r.bur_scan[adj_doff(d, 2LL * d.B)];
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < NB; k += (long long)gridDim.x * blockDim.x) {
         const int re = a.ref_ent[k];
@@ -523,6 +526,7 @@ __global__ void k_adj_ref_fill(Dev d, Rd r, AdjBuf a)
 
 __global__ void k_adj_ref_sum(Dev d, Rd r, AdjBuf a)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const long long NB = r.bur_scan[adj_doff(d, 2LL * d.B)];
     for (long long re = blockIdx.x * (long long)blockDim.x + threadIdx.x; re < NB; re += (long long)gridDim.x * blockDim.x) {
         const int n = a.rcnt[re];
@@ -549,6 +553,7 @@ __global__ void k_adj_ref_sum(Dev d, Rd r, AdjBuf a)
 // active units of each kind, in any order (each unit owns its output slots)
 __global__ void k_adj_collect(Dev d, AdjBuf a)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const long long NT = min(d.tor_off[d.N], d.tor_cap);
     const long long NP = min(d.plus_off[d.N] + d.minus_off[d.N], d.probe_cap);
     const long long total = d.N + NT + NP;
@@ -583,6 +588,7 @@ struct AdjLaneF {
 template <int KIND>
 __global__ void k_adj_units(Dev d, AdjBuf a)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     constexpr int K = KIND == 2 ? 9 : 6;       // coordinates of the unit's atoms
     constexpr int G = 32 / K;                  // units per warp
     const int lane = threadIdx.x & 31;
@@ -649,6 +655,7 @@ __device__ __forceinline__ void add_probe_range(const Dev& d, const AdjBuf& a, i
 // its own triples and of its lower-index neighbours' triples
 __global__ void k_adj_gather(Dev d, AdjBuf a, double* grad)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     for (long long aa = blockIdx.x * (long long)blockDim.x + threadIdx.x; aa < d.N; aa += (long long)gridDim.x * blockDim.x) {
         const int at = (int)aa;
         double x = 0.0, y = 0.0, z = 0.0;
@@ -696,6 +703,7 @@ __global__ void k_adj_gather(Dev d, AdjBuf a, double* grad)
 
 __global__ void k_adj_zero(Dev d, AdjBuf a, long long dcap)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const long long nf = (long long)d.N + d.tor_cap + d.probe_cap;
     const long long n = max(dcap, nf);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {

@@ -109,6 +109,7 @@ __device__ __forceinline__ void lat_prefix(LatTable& L, const int* nc, int nl)
 template <bool EMIT>
 __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 5 : 6) k_convex(Dev d)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     __shared__ LatTable tab[CV_WARPS];
     __shared__ int ncs[CV_WARPS][CMS_MAX_SUBDIV];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -476,6 +477,7 @@ __device__ __forceinline__ void tor_emit_spread(const Dev& d, TorArcS* S, int* X
 template <bool EMIT>
 __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     __shared__ TorPair tp[TO_WARPS][TO_PAIRS];
     __shared__ int pool[TO_WARPS][TO_POOL];
     __shared__ int pst[TO_WARPS][TO_PAIRS + 1];             // exclusive scan of torus points per pair
@@ -619,6 +621,7 @@ static constexpr int CC_WARPS = 4;
 template <bool EMIT>
 __global__ void __launch_bounds__(CC_WARPS * 32, EMIT ? 4 : 1) k_concave(Dev d)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     __shared__ LatTable tab[CC_WARPS];
     __shared__ int ncs[CC_WARPS][CMS_MAX_SUBDIV];
     __shared__ int nears[CC_WARPS][CMS_NEAR_CAP];
@@ -802,6 +805,7 @@ __device__ __forceinline__ SegCounts seg_counts(const Dev& d, int c)
 
 __global__ void k_layout_counts(Dev d, int* cm_count)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.B; c += gridDim.x * blockDim.x) {
         SegCounts S = seg_counts(d, c);
         for (int m = 0; m < 2; ++m)
@@ -811,6 +815,7 @@ __global__ void k_layout_counts(Dev d, int* cm_count)
 
 __global__ void k_layout_seg(Dev d)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.B; c += gridDim.x * blockDim.x) {
         SegCounts S = seg_counts(d, c);
         for (int m = 0; m < 2; ++m) {
@@ -841,6 +846,7 @@ void launch_layout(const Dev& d, long long* cm_count_tmp, long long* scan_tmp, c
 // ---------------------------------------------------------------------------
 __global__ void k_tor_last(Dev d)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const long long NT = min(d.tor_off[d.N], d.tor_cap);
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < NT; q += (long long)gridDim.x * blockDim.x)
         atomicMax(&d.tor_last2[d.tor_j[q]], (unsigned long long)(q + 1));
@@ -848,6 +854,7 @@ __global__ void k_tor_last(Dev d)
 
 __global__ void k_tor_access_apply(Dev d)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     for (long long a = blockIdx.x * (long long)blockDim.x + threadIdx.x; a < d.N; a += (long long)gridDim.x * blockDim.x) {
         int8_t v = d.access[a];
         if (d.tor_off[a + 1] > d.tor_off[a]) v |= d.tor_has[d.tor_off[a + 1] - 1];   // rows are grouped by atom1

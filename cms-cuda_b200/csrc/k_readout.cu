@@ -39,6 +39,7 @@ __device__ __forceinline__ long long doff(const Dev& d, long long i) { return mi
 // ---------------------------------------------------------------------------
 __global__ void k_flag_buried(Dev d, Rd r, long long cap)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const long long D = doff(d, 2LL * d.B);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cap; i += (long long)gridDim.x * blockDim.x)
         r.flag[i] = (i < D && d.dbur[i]) ? 1 : 0;
@@ -64,6 +65,7 @@ __device__ __forceinline__ int dot_cm(const Dev& d, long long dot)
 
 __global__ void k_split_buried(Dev d, Rd r, long long cap)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const long long D = doff(d, 2LL * d.B);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cap && i < D; i += (long long)gridDim.x * blockDim.x) {
         const int cm = dot_cm(d, i);
@@ -339,6 +341,7 @@ __device__ __forceinline__ void nn_round_box(const NNArgs& a, long long ro, int 
 template <int MODE, int Q, int SUB>
 __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
 {
+    if (a.ovf && *a.ovf) return;
     constexpr int P = Q / 2;                  // packed query pairs per lane
     constexpr int WQ = 32 * Q;                // queries per warp
     constexpr int TILE = NN_T * Q;            // queries per tile
@@ -604,6 +607,7 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
 
 __global__ void k_nn_tiles(NNArgs a)
 {
+    if (a.ovf && *a.ovf) return;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < a.ntask; t += gridDim.x * blockDim.x) {
         const NNTask T = a.task[t];
         const bool on = T.qn > 0 && (T.rn > 0 || a.band_mode);
@@ -615,6 +619,7 @@ __global__ void k_nn_tiles(NNArgs a)
 // one warp per sub-round: the box of each 32-reference block (lane b < 16) and of the sub-round
 __global__ void k_nn_boxes(NNArgs a)
 {
+    if (a.ovf && *a.ovf) return;
     const long long nround = min(a.round_off[a.ntask], a.round_cap);
     const int lane = threadIdx.x & 31;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -774,6 +779,7 @@ void launch_points_setup(const double* q, long long nq, const double* r, long lo
 // CMS: queries = buried dots of molecule m, references = buried dots of 1-m
 __global__ void k_tasks_cms(Dev d, Rd r, NNTask* task)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 2 * d.B; t += gridDim.x * blockDim.x) {
         const int c = t >> 1, m = t & 1, o = (c * 2) + (1 - m);
         NNTask T;
@@ -790,6 +796,7 @@ __global__ void k_tasks_cms(Dev d, Rd r, NNTask* task)
 // SC trim: queries = buried dots of molecule m, references = accessible dots of m
 __global__ void k_tasks_trim(Dev d, Rd r, NNTask* task)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 2 * d.B; t += gridDim.x * blockDim.x) {
         const long long ds = doff(d, t), de = doff(d, t + 1);
         NNTask T;
@@ -806,6 +813,7 @@ __global__ void k_tasks_trim(Dev d, Rd r, NNTask* task)
 // SC neighbour distance: queries = trimmed dots of m, references = trimmed dots of 1-m
 __global__ void k_tasks_sc(Dev d, Rd r, NNTask* task)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 2 * d.B; t += gridDim.x * blockDim.x) {
         const int c = t >> 1, m = t & 1, o = (c * 2) + (1 - m);
         NNTask T;
@@ -834,6 +842,7 @@ void launch_tasks(const Dev& d, const Rd& r, int kind, NNTask* task, cudaStream_
 // per buried dot: area * exp(-d2 * weight) against the other molecule's buried dots
 __global__ void k_cms_weights(Dev d, Rd r, long long cap)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const long long NB = r.bur_scan[doff(d, 2LL * d.B)];
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cap; k += (long long)gridDim.x * blockDim.x) {
         if (k < NB) {
@@ -849,6 +858,7 @@ __global__ void k_cms_weights(Dev d, Rd r, long long cap)
 // values of every dot of molecule 0 (maximum possible CMS): own = owner or -1
 __global__ void k_area_values(Dev d, Rd r, long long cap)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const long long D = doff(d, 2LL * d.B);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cap; i += (long long)gridDim.x * blockDim.x) {
         if (i < D) {
@@ -929,6 +939,7 @@ __device__ __forceinline__ double block_sum(double v, double* sh)
 
 __global__ void k_atom_totals(Dev d, const double* per_atom, double* tot)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     __shared__ double sh[32];
     const int t = blockIdx.x;                      // complex * 2 + molecule
     const int c = t >> 1, m = t & 1;
@@ -950,6 +961,7 @@ void launch_atom_totals(const Dev& d, const double* per_atom, double* tot, cudaS
 // ---------------------------------------------------------------------------
 __global__ void k_trim_compact_flags(Dev d, Rd r, long long cap)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const long long NB = r.bur_scan[doff(d, 2LL * d.B)];
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cap; k += (long long)gridDim.x * blockDim.x)
         if (k >= NB) r.keep[k] = 0;
@@ -957,6 +969,7 @@ __global__ void k_trim_compact_flags(Dev d, Rd r, long long cap)
 
 __global__ void k_trim_fill(Dev d, Rd r, long long cap)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const long long NB = r.bur_scan[doff(d, 2LL * d.B)];
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cap && k < NB; k += (long long)gridDim.x * blockDim.x) {
         if (r.keep[k]) {
@@ -1028,6 +1041,7 @@ __device__ double binned_median(long long n, double w, G&& get, long long* shl)
 // one block per (complex, molecule): trimmed area, neighbour statistics
 __global__ void k_sc_stats(Dev d, Rd r, const NNTask* task, double* out)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     __shared__ double sh[32];
     __shared__ long long shl[64];
     const int t = blockIdx.x;
@@ -1073,6 +1087,7 @@ __global__ void k_sc_stats(Dev d, Rd r, const NNTask* task, double* out)
 
 __global__ void k_sc_final(Dev d, const double* side, double* out)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < d.B; c += gridDim.x * blockDim.x) {
         const double* s0 = side + (long long)(2 * c) * SC_SIDE_FIELDS;
         const double* s1 = side + (long long)(2 * c + 1) * SC_SIDE_FIELDS;

@@ -121,6 +121,7 @@ __device__ __forceinline__ void atom_cell(const Dev& d, int g, int c, int& cx, i
 
 __global__ void k_cell_count(Dev d)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < d.N; g += (long long)gridDim.x * blockDim.x) {
         int c = d.cplx[g];
         int x, y, z;
@@ -135,6 +136,7 @@ __global__ void k_cell_count(Dev d)
 
 __global__ void k_cell_fill(Dev d)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < d.N; g += (long long)gridDim.x * blockDim.x) {
         int cell = d.cell_of[g];
         if (cell < 0) continue;
@@ -145,6 +147,7 @@ __global__ void k_cell_fill(Dev d)
 
 __global__ void k_cell_sort(Dev d, long long ncells_cap)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const long long ncells = d.ncell_scan[d.B];
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncells && c < ncells_cap;
          c += (long long)gridDim.x * blockDim.x) {
@@ -271,6 +274,7 @@ __device__ __forceinline__ void scan_ball(const Dev& d, int g, int c, double ran
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(NB_WARPS * 32) k_attention(Dev d)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     __shared__ BallScratch sc[NB_WARPS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const long long wid = blockIdx.x * (long long)NB_WARPS + w;
@@ -341,6 +345,7 @@ __device__ __forceinline__ void classify(const Dev& d, int g, V3 xi, double ri, 
 
 __global__ void __launch_bounds__(NB_WARPS * 32) k_nb_count(Dev d)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     __shared__ BallScratch sc[NB_WARPS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const long long wid = blockIdx.x * (long long)NB_WARPS + w;
@@ -380,6 +385,7 @@ void launch_neighbor_count(const Dev& d, cudaStream_t s)
 // (d2, j) rank and buried partners by their atom index
 __global__ void __launch_bounds__(NB_WARPS * 32) k_nb_emit(Dev d, int* __restrict__ tmp_id)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     __shared__ BallScratch sc[NB_WARPS];
     __shared__ double sd2[NB_WARPS][NB_CAP];
     __shared__ int sid[NB_WARPS][NB_CAP];
@@ -496,6 +502,7 @@ __device__ __forceinline__ PairGeo pair_geo(V3 xi, double ri, V3 xj, double rj, 
 template <bool EMIT>
 __global__ void k_pairs(Dev d)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const double rp = d.st.rp;
     for (long long gg = blockIdx.x * (long long)blockDim.x + threadIdx.x; gg < d.N; gg += (long long)gridDim.x * blockDim.x) {
         const int g = (int)gg;
@@ -862,6 +869,7 @@ __device__ __forceinline__ void triples_row_c(const Dev& d, int g, int K, long l
 template <bool EMIT, bool LONG>
 __global__ void __launch_bounds__(TR_WARPS * 32, EMIT ? 8 : 1) k_triples(Dev d)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     __shared__ unsigned queue_s[TR_WARPS][TR_QCAP];
     __shared__ TrRow rows_s[LONG ? 1 : TR_WARPS];
     __shared__ TrPairC pq_s[LONG ? 1 : TR_WARPS][TR_PQ];
@@ -1011,6 +1019,7 @@ void launch_triples(const Dev& d, bool emit, cudaStream_t s)
 // ---------------------------------------------------------------------------
 __global__ void k_low_flag(Dev d, long long cap)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const long long P = d.plus_off[d.N] + d.minus_off[d.N];
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < cap; p += (long long)gridDim.x * blockDim.x)
         d.plow_flag[p] = (p < P && d.ph[p] < d.st.rp) ? 1 : 0;
@@ -1018,6 +1027,7 @@ __global__ void k_low_flag(Dev d, long long cap)
 
 __global__ void k_low_fill(Dev d, long long cap)
 {
+    CMS_EXIT_ON_OVERFLOW(d);
     const long long P = d.plus_off[d.N] + d.minus_off[d.N];
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < cap && p < P; p += (long long)gridDim.x * blockDim.x)
         if (d.plow_flag[p]) d.plow_list[d.plow_off[p]] = (int)p;

@@ -207,6 +207,24 @@ cms_status cms_run_graph(cms_ctx* ctx);
 cms_status cms_graph_launch(cms_ctx* ctx);
 cms_status cms_graph_check(cms_ctx* ctx);
 
+/* Rigid-body pose refinement of every complex's binder by gradient ascent on
+ * the target-side CMS (no reference counterpart; the objective is
+ * calc_contact_molecular_surface, _core.py:946-1004).  cms_refine_begin takes
+ * the reference coordinates (N x 3: binders in their starting poses, targets
+ * fixed) of the loaded batch and up to max_steps of history; each step of
+ * cms_refine_run is one replay of a captured graph -- apply the poses,
+ * regenerate the surfaces, CMS, its adjoint, and a clipped ascent step on
+ * each binder's rotation (about its reference centroid) and translation.
+ * cms_hist (steps x B) receives the CMS of every evaluated pose; the run
+ * checks capacities every 25 steps and redoes a chunk that outgrew them.
+ * cms_refine_pose returns the current rotations (B x 9), translations (B x 3)
+ * and coordinates (N x 3, any may be NULL). */
+cms_status cms_refine_begin(cms_ctx* ctx, const double* ref_xyz, int32_t max_steps, int32_t where);
+cms_status cms_refine_set_params(cms_ctx* ctx, double eta_t, double eta_w, double max_t, double max_w);
+cms_status cms_refine_run(cms_ctx* ctx, int32_t steps, double* cms_hist, int32_t where);
+cms_status cms_refine_pose(cms_ctx* ctx, double* rot, double* trans, double* xyz, int32_t where);
+cms_status cms_refine_end(cms_ctx* ctx);
+
 /* Search shapes of the batched pipeline's three nearest-dot searches (CMS, SC
  * band trim, SC neighbour argmin): variants[3], each 0..3 = (4 queries per
  * thread, 1024-reference rounds), (4, 512), (2, 1024), (2, 512).  Every shape

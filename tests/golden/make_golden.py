@@ -168,6 +168,7 @@ def main():
     tr[5::11] = 0.0
     cases.append(("synth_zero_radii", (bx, br, tx, tr), True, {}))
     cases.append(("synth_plain_1200_450", synth.config_plain_small(0), False, {}))
+    cases.append(("synth_plain_8000_1800", synth.config_plain_large(0), False, {}))
     only = set(sys.argv[1:])
     for name, inputs, full, extra in cases:
         if only and name not in only:

@@ -15,7 +15,7 @@ TOL = 1e-12
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 FULL_CASES = ("golden_pkl", "synth_small_s7", "synth_zero_radii")
-ALL_CASES = FULL_CASES + ("sc_example_pdb", "smallmol_7jkv_pdb", "synth_plain_1200_450")
+ALL_CASES = FULL_CASES + ("sc_example_pdb", "smallmol_7jkv_pdb", "synth_plain_1200_450", "synth_plain_8000_1800")
 
 
 def load_case(name):

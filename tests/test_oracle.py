@@ -33,6 +33,21 @@ def test_scalars(oracle_run):
     exact("max per-atom", mpa, case["per_atom_max"])
 
 
+def test_large_complex():
+    """The plain large complex (1800 + 8000 atoms) against the reference's own run of it."""
+    case = load_case("synth_plain_8000_1800")
+    out = O.run_complex(*inputs(case))
+    exact("cms", out["cms"], case["cms"])
+    exact("cms binder", out["cms_binder"], case["cms_binder"])
+    exact("sc", [out["sc"], out["sc_area"], out["sc_distance"]],
+          [case["sc"], case["sc_area"], case["sc_distance"]])
+    exact("per-atom", out["cms_per_atom"], case["per_atom_target"])
+    exact("per-atom binder", out["cms_binder_per_atom"], case["per_atom_binder"])
+    S = out["surface"]
+    exact("atten", S.atten, case["atten"])
+    exact("access", S.access, case["access"])
+
+
 def test_run_state(oracle_run):
     case, out, _ = oracle_run
     S = out["surface"]
