@@ -190,3 +190,40 @@ def test_public_api(runs):
     close("api max", mx, c["max_cms"])
     with pytest.raises(ValueError):
         calculate_contact_ms(bx, br, tx, tr, device="cpu")
+
+
+def test_graph_capacity_overflow_is_detected_and_recovered():
+    """
+    A graph captured on a batch with a smaller surface (the first complex's
+    binder 100 A away) replayed on the same shape with both complexes in
+    contact exceeds its capacities: the run is
+    flagged (every later kernel stops at entry), graph_check reports it, and
+    run_graph re-sizes and returns the exact results.
+    """
+    from cms_cuda import _lib
+    names = ("golden_pkl", "synth_small_s7")
+    xyz, rad, off, nb = [], [], [0], []
+    for n in names:
+        bx, br, tx, tr = inputs(load_case(n))
+        xyz += [bx, tx]; rad += [br, tr]; nb.append(len(br)); off.append(off[-1] + len(br) + len(tr))
+    X, R = np.concatenate(xyz), np.concatenate(rad)
+    off, nb = np.array(off), np.array(nb)
+    far = X.copy()
+    far[off[0]:off[0] + nb[0], 0] += 100.0
+    ctx = _lib.Context(0)
+    ctx.load_batch(off, nb, far, R)
+    ctx.run_graph()
+    ctx.load_batch(off, nb, X, R)
+    ctx.graph_launch()
+    with pytest.raises(_lib.CmsError):
+        ctx.graph_check()
+    ctx.run_graph()
+    _, tot = ctx.contact_ms(per_atom=False)
+    sc, _ = ctx.shape_complementarity()
+    ref = _lib.Context(0)
+    ref.load_batch(off, nb, X, R)
+    ref.generate(all_atoms=False)
+    _, rtot = ref.contact_ms(per_atom=False)
+    rsc, _ = ref.shape_complementarity()
+    exact("totals after recovery", tot, rtot)
+    exact("sc after recovery", sc, rsc)
