@@ -96,7 +96,8 @@ def ligand_radii(n_atoms, rng):
 class Batch:
     """Concatenated batch: binder atoms then target atoms per complex."""
 
-    def __init__(self, atom_off, n_binder, xyz, radius, gaps=None, ligand=None):
+    def __init__(self, atom_off, n_binder, xyz, radius, gaps=None, ligand=None, names=None):
+        self.names = names          # optional (residue names, atom names, residue numbers) per atom
         self.atom_off = np.asarray(atom_off, dtype=np.int64)
         self.n_binder = np.asarray(n_binder, dtype=np.int64)
         self.xyz = xyz
@@ -119,10 +120,11 @@ class Batch:
         return self.xyz[a0:s1], self.radius[a0:s1], self.xyz[s1:a1], self.radius[s1:a1]
 
 
-def make_batch(n_target, n_binder, seed, ligand=None, threads=None):
+def make_batch(n_target, n_binder, seed, ligand=None, threads=None, names=False):
     """
     Generate a batch of complexes with the given per-complex atom counts.
     ligand: optional bool array marking binders that are ligand clusters.
+    names: also keep each atom's residue name, atom name and residue number.
     """
     n_target = np.asarray(n_target, dtype=np.int32).reshape(-1)
     n_binder = np.asarray(n_binder, dtype=np.int32).reshape(-1)
@@ -144,15 +146,55 @@ def make_batch(n_target, n_binder, seed, ligand=None, threads=None):
     if st != 0:
         raise RuntimeError("synthetic generator failed")
     radius = np.empty(N)
+    res_n = np.empty(N, dtype=object) if names else None
+    atm_n = np.empty(N, dtype=object) if names else None
+    res_i = np.empty(N, dtype=np.int64) if names else None
     for c in range(B):
         crng = np.random.default_rng(int(seeds[c]) ^ 0x5EED)
         a0, a1 = int(atom_off[c]), int(atom_off[c + 1])
         nb = int(n_binder[c])
-        walk_r = residue_radii(a1 - a0, crng)[0]        # radii along the walk
-        radius[a0:a1] = walk_r[perm[a0:a1]]
+        walk_r, wres, watm = residue_radii(a1 - a0, crng)        # radii and names along the walk
+        p = perm[a0:a1]
+        radius[a0:a1] = walk_r[p]
+        if names:
+            starts = np.r_[True, np.array(wres[1:], dtype=object) != np.array(wres[:-1], dtype=object)] \
+                if len(wres) else np.zeros(0, bool)
+            first = [i for i in range(len(watm)) if i == 0 or watm[i] == "N" or starts[i]]
+            rid = np.zeros(len(watm), np.int64)
+            for k, f in enumerate(first):
+                rid[f:] = k + 1
+            res_n[a0:a1] = np.array(wres, dtype=object)[p]
+            atm_n[a0:a1] = np.array(watm, dtype=object)[p]
+            res_i[a0:a1] = rid[p]
         if ligand[c]:
-            radius[a0:a0 + nb] = ligand_radii(nb, crng)[0]
-    return Batch(atom_off, n_binder, xyz, radius, gaps, ligand)
+            lr, lres, latm = ligand_radii(nb, crng)
+            radius[a0:a0 + nb] = lr
+            if names:
+                res_n[a0:a0 + nb] = lres
+                atm_n[a0:a0 + nb] = latm
+                res_i[a0:a0 + nb] = 1
+    return Batch(atom_off, n_binder, xyz, radius, gaps, ligand, (res_n, atm_n, res_i) if names else None)
+
+
+def write_pdb(path, batch, c, binder_chain="B", target_chain="A"):
+    """Write complex c of a batch made with names=True as a PDB file (binder and target chains)."""
+    res_n, atm_n, res_i = batch.names
+    a0, a1 = int(batch.atom_off[c]), int(batch.atom_off[c + 1])
+    s1 = a0 + int(batch.n_binder[c])
+    with open(path, "w") as f:
+        serial = 1
+        for lo, hi, ch in ((a0, s1, binder_chain), (s1, a1, target_chain)):
+            for g in range(lo, hi):
+                nm = str(atm_n[g])
+                name = nm if len(nm) == 4 else " " + nm.ljust(3)
+                rec = "HETATM" if res_n[g] == "LIG" else "ATOM  "
+                x, y, z = batch.xyz[g]
+                el = nm.lstrip("0123456789")[:1]
+                f.write(f"{rec}{serial:5d} {name}{'':1}{res_n[g]:>3s} {ch}{int(res_i[g]):4d}    "
+                        f"{x:8.3f}{y:8.3f}{z:8.3f}{1.0:6.2f}{0.0:6.2f}          {el:>2s}\n")
+                serial += 1
+            f.write("TER\n")
+        f.write("END\n")
 
 
 def make_complex(n_target, n_binder, seed):
