@@ -250,6 +250,7 @@ struct cms_ctx {
         S_ADJ_GCONV, S_ADJ_GTOR, S_ADJ_GCONC, S_ADJ_GTOT, S_ADJ_GRAD, S_RECOMP_XYZ, S_RECOMP_AREA,
         S_ADJ_ACT_CONV, S_ADJ_ACT_TOR, S_ADJ_ACT_CONC, S_ADJ_ACT_ATOM, S_ADJ_LIST_CONV, S_ADJ_LIST_TOR,
         S_ADJ_LIST_CONC, S_ADJ_NACT, S_OVF, S_REF_XYZ, S_POSE, S_POSE_CKPT, S_POSE_CEN, S_HIST, S_STEP, S_MAXSUM,
+        S_TOR_LFLAG, S_TOR_LOFF, S_TOR_LIST,
         S_COUNT
     };
 
@@ -379,6 +380,9 @@ void bind_caps(cms_ctx* x)
     d.tor1_off = x->ensure<long long>(cms_ctx::S_TOR1_OFF, x->cap_tor + 1);
     d.tor2_off = x->ensure<long long>(cms_ctx::S_TOR2_OFF, x->cap_tor + 1);
     d.tor_has = x->ensure<int8_t>(cms_ctx::S_TOR_HAS, x->cap_tor);
+    d.tor_lflag = x->ensure<int>(cms_ctx::S_TOR_LFLAG, x->cap_tor);
+    d.tor_loff = x->ensure<long long>(cms_ctx::S_TOR_LOFF, x->cap_tor + 1);
+    d.tor_list = x->ensure<int>(cms_ctx::S_TOR_LIST, x->cap_tor);
     d.probe_cap = x->cap_probe;
     d.pa0 = x->ensure<int>(cms_ctx::S_PA0, x->cap_probe);
     d.pa1 = x->ensure<int>(cms_ctx::S_PA1, x->cap_probe);
@@ -546,6 +550,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
     k_cap_check<<<1, 32, 0, s>>>(d.dot_off + 2LL * d.B, nullptr, x->cap_dot, d.ovf);
     launch_convex(d, true, s);
     mark(x, P_CONVEX_EMIT);
+    launch_tor_list(d, x->cap_tor, tmp, s);
     launch_toroidal(d, x->cap_tor, true, s);
     mark(x, P_TOROIDAL_EMIT);
     launch_concave(d, x->cap_probe, true, s);

@@ -98,6 +98,8 @@ struct Dev {
     int* tor1_cnt; long long* tor1_off;          // tor_cap, +1
     int* tor2_cnt; long long* tor2_off;          // tor_cap, +1
     int8_t* tor_has;                             // tor_cap (toroidal access)
+    int* tor_lflag; long long* tor_loff;         // tor_cap, +1: pair has dots, its exclusive scan
+    int* tor_list;                               // tor_cap: pairs with dots, in pair order (emit work list)
     int* conc_cnt; long long* conc_off;          // probe_cap, +1
     Seg* seg;                                    // B*8
     long long* dot_off;                          // B*2+1 (per complex & molecule)

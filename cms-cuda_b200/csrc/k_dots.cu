@@ -445,7 +445,7 @@ struct TorArcS {
 // Emit the dots of the warp's arcs (c dots for this lane's arc, e its
 // exclusive scan, tot the warp's total), one dot per lane per step.  Every
 // arc here took the finite path, so its dots are 0 .. c-1 in order.
-__device__ __forceinline__ void tor_emit_spread(const Dev& d, TorArcS* S, int* X, const TorPair* tps, long long q0,
+__device__ __forceinline__ void tor_emit_spread(const Dev& d, TorArcS* S, int* X, const TorPair* tps, const int* tq,
                                                 int c, int e, int tot, V3 pij, const Arc& A, long long pos, int k,
                                                 int s, int8_t bur, int arcbit)
 {
@@ -469,7 +469,7 @@ __device__ __forceinline__ void tor_emit_spread(const Dev& d, TorArcS* S, int* X
         const TorPair& T = tps[a.k];
         const int t = g - X[lo];
         const V3 pt = subdiv_point(a.p, rp, a.x, a.y, T.darc, t);
-        write_dot_b(d, a.pos + t, pt, a.p, tor_area(T, a.ps, pt), arcbit ? T.j : T.i, 2, (int)(q0 + a.k),
+        write_dot_b(d, a.pos + t, pt, a.p, tor_area(T, a.ps, pt), arcbit ? T.j : T.i, 2, tq[a.k],
                     (a.s << 16) | arcbit | t, (int8_t)a.bur);
     }
 }
@@ -479,6 +479,7 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
 {
     CMS_EXIT_ON_OVERFLOW(d);
     __shared__ TorPair tp[TO_WARPS][TO_PAIRS];
+    __shared__ int tq[TO_WARPS][TO_PAIRS];                  // pair index of each batch slot
     __shared__ int pool[TO_WARPS][TO_POOL];
     __shared__ int pst[TO_WARPS][TO_PAIRS + 1];             // exclusive scan of torus points per pair
     __shared__ int l_off[TO_WARPS][3][TO_PAIRS];            // pruned lists: neighbours of i, partners of i, of j
@@ -492,7 +493,8 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int we = EMIT ? w : 0;
     const double rp = d.st.rp;
-    const long long NT = min(d.tor_off[d.N], d.tor_cap);
+    // count: every pair; emit: only the pairs with dots (the work list)
+    const long long NT = EMIT ? d.tor_loff[d.tor_cap] : min(d.tor_off[d.N], d.tor_cap);
     const long long nbatch = (NT + TO_PAIRS - 1) / TO_PAIRS;
     for (long long bt = blockIdx.x * (long long)TO_WARPS + w; bt < nbatch; bt += (long long)gridDim.x * TO_WARPS) {
         const long long q0 = bt * TO_PAIRS;
@@ -500,16 +502,18 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
         __syncwarp();
         int ns = 0;
         if (lane < np) {
-            const TorPair T = tor_pair(d, q0 + lane);
+            const long long q = EMIT ? (long long)d.tor_list[q0 + lane] : q0 + lane;
+            const TorPair T = tor_pair(d, q);
             tp[w][lane] = T;
+            tq[w][lane] = (int)q;
             ns = T.ns;
             run[w][0][lane] = 0; run[w][1][lane] = 0;
             hasf[w][lane] = 0;
             arcf[w][lane] = (unsigned char)((d.atten[T.i] >= 2 ? 1 : 0) | (d.atten[T.j] >= 2 ? 2 : 0));
             if (EMIT) {
                 const int c = d.cplx[T.i], m = d.mol[T.i];
-                base[we][0][lane] = unit_base(d, c, m, 1, d.tor1_off[q0 + lane]);
-                base[we][1][lane] = unit_base(d, c, m, 2, d.tor2_off[q0 + lane]);
+                base[we][0][lane] = unit_base(d, c, m, 1, d.tor1_off[q]);
+                base[we][1][lane] = unit_base(d, c, m, 2, d.tor2_off[q]);
             }
         }
         int tot;
@@ -581,12 +585,13 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
                 if (c1) bur1 = tor_buried(d, T.i, P.pij, pool[w] + l_off[w][1][k], l_cnt[w][1][k]);
                 if (c2) bur2 = tor_buried(d, T.j, P.pij, pool[w] + l_off[w][2][k], l_cnt[w][2][k]);
                 if (__all_sync(0xffffffffu, fast)) {
-                    if (t1) tor_emit_spread(d, arcs[we], arcx[we], tp[w], q0, c1, e1, t1, P.pij, A1, pos1, k, s, bur1, 0);
-                    if (t2) tor_emit_spread(d, arcs[we], arcx[we], tp[w], q0, c2, e2, t2, P.pij, A2, pos2, k, s, bur2,
+                    if (t1) tor_emit_spread(d, arcs[we], arcx[we], tp[w], tq[w], c1, e1, t1, P.pij, A1, pos1, k, s, bur1,
+                                            0);
+                    if (t2) tor_emit_spread(d, arcs[we], arcx[we], tp[w], tq[w], c2, e2, t2, P.pij, A2, pos2, k, s, bur2,
                                             1 << 15);
                 } else {
-                    if (c1) arc_emit(d, T, P, A1, rp, pos1, T.i, q0 + k, s, 0, bur1);
-                    if (c2) arc_emit(d, T, P, A2, rp, pos2, T.j, q0 + k, s, 1 << 15, bur2);
+                    if (c1) arc_emit(d, T, P, A1, rp, pos1, T.i, tq[w][k], s, 0, bur1);
+                    if (c2) arc_emit(d, T, P, A2, rp, pos2, T.j, tq[w][k], s, 1 << 15, bur2);
                 }
             }
             __syncwarp();
@@ -862,6 +867,28 @@ __global__ void k_tor_access_apply(Dev d)
         if (l2 > 0) v |= d.tor_has[l2 - 1];
         d.access[a] = v;
     }
+}
+
+// work list of the emit pass: the toroid pairs with at least one dot, in pair order
+__global__ void k_tor_flag(Dev d)
+{
+    CMS_EXIT_ON_OVERFLOW(d);
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < d.tor_cap; q += (long long)gridDim.x * blockDim.x)
+        d.tor_lflag[q] = (d.tor1_cnt[q] | d.tor2_cnt[q]) != 0 ? 1 : 0;
+}
+
+__global__ void k_tor_list(Dev d)
+{
+    CMS_EXIT_ON_OVERFLOW(d);
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < d.tor_cap; q += (long long)gridDim.x * blockDim.x)
+        if (d.tor_lflag[q]) d.tor_list[d.tor_loff[q]] = (int)q;
+}
+
+void launch_tor_list(const Dev& d, long long tor_grid, long long* scan_tmp, cudaStream_t s)
+{
+    k_tor_flag<<<grid_for(tor_grid, 256), 256, 0, s>>>(d);
+    scan_counts(d.tor_lflag, d.tor_loff, tor_grid, scan_tmp, s);
+    k_tor_list<<<grid_for(tor_grid, 256), 256, 0, s>>>(d);
 }
 
 void launch_tor_access(const Dev& d, long long tor_grid, cudaStream_t s)
