@@ -125,6 +125,7 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 5 : 6) k_convex(Dev d)
             if (!EMIT && lane == 0) d.conv_cnt[g] = 0;
             continue;
         }
+        if (EMIT && d.conv_cnt[g] == 0) continue;                      // no dots: nothing to write
         const double4 ai = d.xyzr[g];
         const V3 xi = v3(ai.x, ai.y, ai.z);
         const double ri = ai.w, eri = ri + rp, dens = d.dens[g];
@@ -638,6 +639,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, EMIT ? 4 : 1) k_concave(Dev d)
     const long long wid = blockIdx.x * (long long)CC_WARPS + w;
     const long long nw = (long long)gridDim.x * CC_WARPS;
     for (long long p = wid; p < NP; p += nw) {
+        if (EMIT && d.conc_cnt[p] == 0) continue;                      // no dots: nothing to write
         const int ia[3] = {d.pa0[p], d.pa1[p], d.pa2[p]};
         V3 xa[3];
         double ra[3];

@@ -883,6 +883,7 @@ __global__ void __launch_bounds__(TR_WARPS * 32, EMIT ? 8 : 1) k_triples(Dev d)
         const int g = (int)gg;
         const int K = d.nnb[g];
         if (LONG != (K > TR_KC)) continue;
+        if (EMIT && d.nplus[g] == 0 && d.nminus[g] == 0) continue;    // no probes: nothing to write
         int nplus = 0, nminus = 0;
         const int8_t ati = d.atten[g];
         const long long off = d.nb_off[g];
