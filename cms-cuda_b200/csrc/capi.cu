@@ -241,7 +241,7 @@ struct cms_ctx {
         S_CONV_CNT, S_CONV_OFF, S_TOR1_CNT, S_TOR1_OFF, S_TOR2_CNT, S_TOR2_OFF, S_TOR_HAS, S_CONC_CNT, S_CONC_OFF,
         S_SEG, S_DOT_OFF, S_DXYZ, S_DNML, S_DAREA, S_DBUR, S_DTYPE, S_DATOM, S_DUNIT, S_DSUB, S_TOR_LAST1, S_TOR_LAST2,
         S_R_FLAG, S_R_BUR_SCAN, S_R_BUR_IDX, S_R_BUR_F4, S_R_BUR_CM, S_R_ACC_IDX, S_R_ACC_F4, S_R_KEEP, S_R_TRIM_SCAN,
-        S_R_TRIM_IDX, S_R_TRIM_F4, S_R_NN_D2, S_R_NN_IDX, S_R_VAL, S_R_OWN, S_R_ACNT, S_R_AFILL, S_R_AOFF, S_R_ASLOT,
+        S_R_TRIM_IDX, S_R_TRIM_F4, S_R_NN_D2, S_R_NN_IDX, S_R_VAL, S_R_OWN,
         S_CM_TMP, S_SCAN_TMP, S_PER_ATOM_CMS, S_TOT_CMS, S_PER_ATOM_MAX, S_TOT_MAX, S_SC_SIDE, S_SC_OUT, S_TASKS,
         S_TILE_CNT, S_TILE_OFF, S_ROUND_CNT, S_ROUND_OFF, S_BOX_ROUND, S_BOX_BLK, S_SUMMARY, S_EXPORT,
         S_NN_Q, S_NN_R, S_NN_QF4, S_NN_RF4, S_NN_PART, S_NN_BBOX, S_NN_TASK, S_NN_TCNT, S_NN_TOFF, S_NN_RCNT, S_NN_ROFF,
@@ -250,7 +250,7 @@ struct cms_ctx {
         S_ADJ_GCONV, S_ADJ_GTOR, S_ADJ_GCONC, S_ADJ_GTOT, S_ADJ_GRAD, S_RECOMP_XYZ, S_RECOMP_AREA,
         S_ADJ_ACT_CONV, S_ADJ_ACT_TOR, S_ADJ_ACT_CONC, S_ADJ_ACT_ATOM, S_ADJ_LIST_CONV, S_ADJ_LIST_TOR,
         S_ADJ_LIST_CONC, S_ADJ_NACT, S_OVF, S_REF_XYZ, S_POSE, S_POSE_CKPT, S_POSE_CEN, S_HIST, S_STEP, S_MAXSUM,
-        S_TOR_LFLAG, S_TOR_LOFF, S_TOR_LIST,
+        S_TOR_LFLAG, S_TOR_LOFF, S_TOR_LIST, S_PTOP, S_SP_A, S_SP_H, S_SP_XYZ, S_SP_ALT, S_SP_G, S_SP_ORD,
         S_COUNT
     };
 
@@ -340,9 +340,6 @@ void bind_batch(cms_ctx* x)
     d.tor_last1 = x->ensure<unsigned long long>(cms_ctx::S_TOR_LAST1, N);
     d.tor_last2 = x->ensure<unsigned long long>(cms_ctx::S_TOR_LAST2, N);
     Rd& r = x->r;
-    r.acnt = x->ensure<int>(cms_ctx::S_R_ACNT, N);
-    r.afill = x->ensure<int>(cms_ctx::S_R_AFILL, N);
-    r.aoff = x->ensure<long long>(cms_ctx::S_R_AOFF, N + 1);
     x->ensure<int>(cms_ctx::S_CM_TMP, 2 * B + 2);
     x->ensure<double>(cms_ctx::S_PER_ATOM_CMS, N);
     x->ensure<double>(cms_ctx::S_TOT_CMS, 2 * B);
@@ -393,6 +390,13 @@ void bind_caps(cms_ctx* x)
     d.plow_flag = x->ensure<int>(cms_ctx::S_PLOW_FLAG, x->cap_probe);
     d.plow_off = x->ensure<long long>(cms_ctx::S_PLOW_OFF, x->cap_probe + 1);
     d.plow_list = x->ensure<int>(cms_ctx::S_PLOW_LIST, x->cap_probe);
+    d.ptop = x->ensure<unsigned long long>(cms_ctx::S_PTOP, 1);
+    d.sp_a = x->ensure<int>(cms_ctx::S_SP_A, 3 * x->cap_probe);
+    d.sp_h = x->ensure<double>(cms_ctx::S_SP_H, x->cap_probe);
+    d.sp_xyz = x->ensure<double>(cms_ctx::S_SP_XYZ, 3 * x->cap_probe);
+    d.sp_alt = x->ensure<double>(cms_ctx::S_SP_ALT, 3 * x->cap_probe);
+    d.sp_g = x->ensure<int>(cms_ctx::S_SP_G, x->cap_probe);
+    d.sp_ord = x->ensure<unsigned>(cms_ctx::S_SP_ORD, x->cap_probe);
     d.conc_cnt = x->ensure<int>(cms_ctx::S_CONC_CNT, x->cap_probe);
     d.conc_off = x->ensure<long long>(cms_ctx::S_CONC_OFF, x->cap_probe + 1);
     d.dot_cap = x->cap_dot;
@@ -421,7 +425,6 @@ void bind_caps(cms_ctx* x)
     x->ensure<int>(cms_ctx::S_CMS_IDX, D);
     r.val = x->ensure<double>(cms_ctx::S_R_VAL, D);
     r.own = x->ensure<int>(cms_ctx::S_R_OWN, D);
-    r.aslot = x->ensure<int>(cms_ctx::S_R_ASLOT, D);
     // search boxes: every search's references are a subset of the dots
     const long long rounds = nn_round_cap(D, 2LL * x->B);
     x->ensure<float4>(cms_ctx::S_BOX_ROUND, 2 * rounds);
@@ -514,17 +517,23 @@ void enqueue_surface(cms_ctx* x, bool sized)
     k_cap_check<<<1, 32, 0, s>>>(d.tor_off + d.N, nullptr, x->cap_tor, d.ovf);
     launch_pairs(d, true, s);
     mark(x, P_PAIRS);
+    ck(cudaMemsetAsync(d.ptop, 0, sizeof(unsigned long long), s), "memset");
     launch_triples(d, false, s);
     scan_counts(d.nplus, d.plus_off, d.N, tmp, s);
     scan_counts(d.nminus, d.minus_off, d.N, tmp, s);
     mark(x, P_TRIPLES_COUNT);
+    // the count pass stashed every probe when they fit the capacity it ran with
+    bool stashed = true;
     if (sized) {
-        grow(x->cap_probe, read_ll(x, d.plus_off + d.N) + read_ll(x, d.minus_off + d.N));
+        const long long need = read_ll(x, d.plus_off + d.N) + read_ll(x, d.minus_off + d.N);
+        stashed = need <= x->cap_probe;
+        grow(x->cap_probe, need);
         bind_caps(x);
         tmp = scan_tmp(x);
     }
     k_cap_check<<<1, 32, 0, s>>>(d.plus_off + d.N, d.minus_off + d.N, x->cap_probe, d.ovf);
-    launch_triples(d, true, s);
+    if (stashed) launch_probe_scatter(d, x->cap_probe, s);
+    else launch_triples(d, true, s);
     launch_low_probes(d, x->cap_probe, tmp, s);
     mark(x, P_TRIPLES_EMIT);
     ck(cudaMemsetAsync(d.tor1_cnt, 0, sizeof(int) * x->cap_tor, s), "memset");
@@ -599,7 +608,7 @@ void enqueue_cms(cms_ctx* x)
     launch_nn(a, NN_ARGMIN, x->nn_var[0], tile_cap(x), tmp, s);
     mark(x, P_CMS_NN);
     launch_cms_weights(d, r, x->cap_dot, s);
-    launch_per_atom_sum(d, r, x->cap_dot, x->get<double>(cms_ctx::S_PER_ATOM_CMS), tmp, s);
+    launch_per_atom_sum(d, r, false, x->get<double>(cms_ctx::S_PER_ATOM_CMS), s);
     launch_atom_totals(d, x->get<double>(cms_ctx::S_PER_ATOM_CMS), x->get<double>(cms_ctx::S_TOT_CMS), s);
     mark(x, P_CMS_SUM);
 }
@@ -639,7 +648,7 @@ void enqueue_max(cms_ctx* x)
     Rd& r = x->r;
     cudaStream_t s = x->stream;
     launch_area_values(d, r, x->cap_dot, s);
-    launch_per_atom_sum(d, r, x->cap_dot, x->get<double>(cms_ctx::S_PER_ATOM_MAX), scan_tmp(x), s);
+    launch_per_atom_sum(d, r, true, x->get<double>(cms_ctx::S_PER_ATOM_MAX), s);
     launch_atom_totals(d, x->get<double>(cms_ctx::S_PER_ATOM_MAX), x->get<double>(cms_ctx::S_TOT_MAX), s);
 }
 

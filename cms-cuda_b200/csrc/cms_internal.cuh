@@ -93,6 +93,11 @@ struct Dev {
     double* ph; double* pxyz; double* palt;   // probe_cap, 3*cap, 3*cap
     int* plow_flag; long long* plow_off;      // probe_cap, probe_cap+1
     int* plow_list;                            // probe_cap
+    // probes stashed by the triple count pass (any order), with their final slot:
+    // generating atom and sign bit (31) | rank among that atom's probes of that sign
+    unsigned long long* ptop;                  // 1: stash entries taken
+    int* sp_a; double* sp_h; double* sp_xyz; double* sp_alt;   // probe_cap (x3, x1, x3, x3)
+    int* sp_g; unsigned* sp_ord;               // probe_cap
     // dots
     int* conv_cnt; long long* conv_off;          // N, N+1
     int* tor1_cnt; long long* tor1_off;          // tor_cap, +1

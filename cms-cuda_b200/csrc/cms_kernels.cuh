@@ -24,6 +24,7 @@ void launch_toroidal(const Dev& d, long long tor_grid, bool emit, cudaStream_t s
 void launch_concave(const Dev& d, long long probe_grid, bool emit, cudaStream_t s);
 void launch_layout(const Dev& d, long long* cm_count_tmp, long long* scan_tmp, cudaStream_t s);
 void launch_tor_access(const Dev& d, long long tor_grid, cudaStream_t s);
+void launch_probe_scatter(const Dev& d, long long probe_grid, cudaStream_t s);
 void launch_tor_list(const Dev& d, long long tor_grid, long long* scan_tmp, cudaStream_t s);
 
 }  // namespace cms

@@ -55,8 +55,6 @@ struct Rd {
     int* trim_idx; float4* trim_f4;             // trimmed dots
     double* nn_d2; int* nn_idx;                 // per query entry
     double* val; int* own;                      // per entry value / owner atom (-1: none)
-    int* acnt; int* afill; long long* aoff;     // N, N, N+1
-    int* aslot;                                 // D
 };
 
 // adjoint of the contact molecular surface (k_adjoint.cu); capacity D = dot
@@ -104,7 +102,7 @@ void launch_points_setup(const double* q, long long nq, const double* r, long lo
                          long long* tile_off, int* round_cnt, long long* round_off, cudaStream_t s);
 void launch_cms_weights(const Dev& d, const Rd& r, long long cap, cudaStream_t s);
 void launch_area_values(const Dev& d, const Rd& r, long long cap, cudaStream_t s);
-void launch_per_atom_sum(const Dev& d, const Rd& r, long long cap, double* out, long long* scan_tmp, cudaStream_t s);
+void launch_per_atom_sum(const Dev& d, const Rd& r, bool dots, double* out, cudaStream_t s);
 void launch_atom_totals(const Dev& d, const double* per_atom, double* tot, cudaStream_t s);
 void launch_trim_compact(const Dev& d, const Rd& r, long long cap, long long* scan_tmp, cudaStream_t s);
 void launch_sc_stats(const Dev& d, const Rd& r, const NNTask* task, double* side, double* out, cudaStream_t s);

@@ -871,46 +871,41 @@ __global__ void k_area_values(Dev d, Rd r, long long cap)
     }
 }
 
-__global__ void k_own_count(Rd r, long long cap, int* cnt)
+// Per-atom sums in entry order, as np.bincount adds them: one warp per
+// complex & molecule segment walks its entries 32 at a time (every atom's
+// entries lie in one segment, so no other warp touches its sum).  Lanes that
+// hold the same owner fold their values in lane order, starting from the
+// atom's running sum; the group's first lane stores it back.
+template <bool DOTS>
+__global__ void k_own_fold(Dev d, Rd r, double* out)
 {
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cap; k += (long long)gridDim.x * blockDim.x) {
-        int a = r.own[k];
-        if (a >= 0) atomicAdd(&cnt[a], 1);
-    }
-}
-
-__global__ void k_own_scatter(Rd r, long long cap, const long long* off, int* fill, int* slot)
-{
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < cap; k += (long long)gridDim.x * blockDim.x) {
-        int a = r.own[k];
-        if (a >= 0) slot[off[a] + atomicAdd(&fill[a], 1)] = (int)k;
-    }
-}
-
-__global__ void k_own_sum(long long N, const long long* off, int* slot, const double* val, double* out)
-{
-    for (long long a = blockIdx.x * (long long)blockDim.x + threadIdx.x; a < N; a += (long long)gridDim.x * blockDim.x) {
-        const long long s = off[a], e = off[a + 1];
-        for (long long i = s + 1; i < e; ++i) {           // entries in increasing dot order
-            int v = slot[i];
-            long long k = i - 1;
-            while (k >= s && slot[k] > v) { slot[k + 1] = slot[k]; --k; }
-            slot[k + 1] = v;
+    CMS_EXIT_ON_OVERFLOW(d);
+    const int lane = threadIdx.x & 31;
+    const long long nw = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long t = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); t < 2LL * d.B; t += nw) {
+        long long s = doff(d, t), e = doff(d, t + 1);
+        if (!DOTS) { s = r.bur_scan[s]; e = r.bur_scan[e]; }
+        for (long long b = s; b < e; b += 32) {
+            const long long k = b + lane;
+            const int a = k < e ? r.own[k] : -1;
+            const double v = k < e ? r.val[k] : 0.0;
+            const unsigned peers = __match_any_sync(0xffffffffu, a);
+            if (a >= 0) {
+                double acc = out[a];
+                for (unsigned m = peers; m; m &= m - 1) acc += __shfl_sync(peers, v, __ffs(m) - 1);
+                if (lane == __ffs(peers) - 1) out[a] = acc;
+            }
+            __syncwarp();
         }
-        double acc = 0.0;
-        for (long long i = s; i < e; ++i) acc += val[slot[i]];
-        out[a] = acc;
     }
 }
 
-void launch_per_atom_sum(const Dev& d, const Rd& r, long long cap, double* out, long long* scan_tmp, cudaStream_t s)
+void launch_per_atom_sum(const Dev& d, const Rd& r, bool dots, double* out, cudaStream_t s)
 {
-    cudaMemsetAsync(r.acnt, 0, sizeof(int) * d.N, s);
-    cudaMemsetAsync(r.afill, 0, sizeof(int) * d.N, s);
-    k_own_count<<<grid_for(cap, 256), 256, 0, s>>>(r, cap, r.acnt);
-    scan_counts(r.acnt, r.aoff, d.N, scan_tmp, s);
-    k_own_scatter<<<grid_for(cap, 256), 256, 0, s>>>(r, cap, r.aoff, r.afill, r.aslot);
-    k_own_sum<<<grid_for(d.N, 128), 128, 0, s>>>(d.N, r.aoff, r.aslot, r.val, out);
+    cudaMemsetAsync(out, 0, sizeof(double) * d.N, s);
+    const unsigned g = grid_for(2LL * d.B, 4);
+    if (dots) k_own_fold<true><<<g, 128, 0, s>>>(d, r, out);
+    else k_own_fold<false><<<g, 128, 0, s>>>(d, r, out);
 }
 
 void launch_cms_weights(const Dev& d, const Rd& r, long long cap, cudaStream_t s)

@@ -595,6 +595,81 @@ __device__ __forceinline__ TripleBase triple_base(const Dev& d, V3 xi, double er
 static constexpr int TR_WARPS = 2;
 static constexpr int TR_QCAP = 256;   // queued (pair slot, k slot) triples per warp
 
+__device__ __forceinline__ void stash_one(const Dev& d, long long e, int a0, int a1, int a2, double h, V3 pt, V3 alt,
+                                          int g, unsigned ord)
+{
+    d.sp_a[3 * e] = a0; d.sp_a[3 * e + 1] = a1; d.sp_a[3 * e + 2] = a2;
+    d.sp_h[e] = h;
+    st3(d.sp_xyz + 3 * e, pt);
+    st3(d.sp_alt + 3 * e, alt);
+    d.sp_g[e] = g;
+    d.sp_ord[e] = ord;
+}
+
+// Count pass: the chunk's probes go to the stash (one reservation per chunk)
+// with their final slot, so the probe arrays are filled by a scatter instead
+// of a second pass over the triples.  The fields are the emit pass's.
+__device__ __forceinline__ void probe_stash(const Dev& d, int g, int j, int k, double h, V3 pp, V3 pm, V3 up,
+                                            bool okp, bool okm, unsigned bp, unsigned bm, int nplus, int nminus)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int np = __popc(bp), nm = __popc(bm);
+    if (np + nm == 0) return;                     // warp-uniform
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(d.ptop, (unsigned long long)(np + nm));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (okp) {
+        const long long e = (long long)base + __popc(bp & lt);
+        if (e < d.probe_cap) stash_one(d, e, g, j, k, h, pp, up * 1.0, g, (unsigned)(nplus + __popc(bp & lt)));
+    }
+    if (okm) {
+        const long long e = (long long)base + np + __popc(bm & lt);
+        if (e < d.probe_cap)
+            stash_one(d, e, j, g, k, h, pm, up * -1.0, g, 0x80000000u | (unsigned)(nminus + __popc(bm & lt)));
+    }
+}
+
+// first "+" and "-" probe slot of atom g: per complex [+mol0 | -mol0 | +mol1 | -mol1]
+__device__ __forceinline__ void probe_bases(const Dev& d, int g, long long& pbase, long long& mbase)
+{
+    const int c = d.cplx[g];
+    const Cplx C = d.cx[c];
+    const int s0 = C.a0, s1 = C.a0 + C.n0, e1 = C.a0 + C.n;
+    const int ms = d.mol[g] == 0 ? s0 : s1, me = d.mol[g] == 0 ? s1 : e1;
+    const long long cbase = d.plus_off[s0] + d.minus_off[s0];
+    const long long m0 = (d.plus_off[s1] - d.plus_off[s0]) + (d.minus_off[s1] - d.minus_off[s0]);
+    const long long mb = cbase + (d.mol[g] == 0 ? 0 : m0);
+    pbase = mb + (d.plus_off[g] - d.plus_off[ms]);
+    mbase = mb + (d.plus_off[me] - d.plus_off[ms]) + (d.minus_off[g] - d.minus_off[ms]);
+}
+
+__global__ void k_probe_scatter(Dev d)
+{
+    CMS_EXIT_ON_OVERFLOW(d);
+    const long long n = min((long long)*d.ptop, d.probe_cap);
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int g = d.sp_g[e];
+        const unsigned o = d.sp_ord[e];
+        long long pbase, mbase;
+        probe_bases(d, g, pbase, mbase);
+        const long long q = ((o >> 31) ? mbase : pbase) + (long long)(o & 0x7fffffffu);
+        const int a0 = d.sp_a[3 * e], a1 = d.sp_a[3 * e + 1], a2 = d.sp_a[3 * e + 2];
+        if (q < d.probe_cap) {
+            d.pa0[q] = a0; d.pa1[q] = a1; d.pa2[q] = a2;
+            d.ph[q] = d.sp_h[e];
+            st3(d.pxyz + 3 * q, ld3(d.sp_xyz + 3 * e));
+            st3(d.palt + 3 * q, ld3(d.sp_alt + 3 * e));
+        }
+        d.access[a0] = 1; d.access[a1] = 1; d.access[a2] = 1;
+    }
+}
+
+void launch_probe_scatter(const Dev& d, long long probe_grid, cudaStream_t s)
+{
+    k_probe_scatter<<<grid_for(probe_grid, 256), 256, 0, s>>>(d);
+}
+
 // probes of the queued triples, in queue order: "+" and "-" probes are
 // ballot-ordered into the atom's two probe ranges
 template <bool EMIT>
@@ -645,6 +720,7 @@ __device__ __forceinline__ void triples_flush(const Dev& d, int g, V3 xi, double
         }
         const unsigned bp = __ballot_sync(0xffffffffu, okp);
         const unsigned bm = __ballot_sync(0xffffffffu, okm);
+        if (!EMIT) probe_stash(d, g, j, k, h, pp, pm, up, okp, okm, bp, bm, nplus, nminus);
         if (EMIT) {
             if (okp) {
                 long long q = pbase + nplus + __popc(bp & lt);
@@ -764,6 +840,7 @@ __device__ __forceinline__ void triples_flush_c(const Dev& d, int g, V3 xi, doub
         }
         const unsigned bp = __ballot_sync(0xffffffffu, okp);
         const unsigned bm = __ballot_sync(0xffffffffu, okm);
+        if (!EMIT) probe_stash(d, g, j, k, h, pp, pm, up, okp, okm, bp, bm, nplus, nminus);
         if (EMIT) {
             if (okp) {
                 long long q = pbase + nplus + __popc(bp & lt);
@@ -867,7 +944,7 @@ __device__ __forceinline__ void triples_row_c(const Dev& d, int g, int K, long l
 
 // LONG = false: atoms whose neighbour row fits the cache; true: the others
 template <bool EMIT, bool LONG>
-__global__ void __launch_bounds__(TR_WARPS * 32, EMIT ? 8 : 1) k_triples(Dev d)
+__global__ void __launch_bounds__(TR_WARPS * 32, EMIT ? 8 : 7) k_triples(Dev d)
 {
     CMS_EXIT_ON_OVERFLOW(d);
     __shared__ unsigned queue_s[TR_WARPS][TR_QCAP];
@@ -902,15 +979,7 @@ __global__ void __launch_bounds__(TR_WARPS * 32, EMIT ? 8 : 1) k_triples(Dev d)
             long long pbase = 0, mbase = 0;
             if (EMIT) {
                 // probe layout per complex: [+mol0 | -mol0 | +mol1 | -mol1]
-                const int c = d.cplx[g];
-                const Cplx C = d.cx[c];
-                const int s0 = C.a0, s1 = C.a0 + C.n0, e1 = C.a0 + C.n;
-                const int ms = d.mol[g] == 0 ? s0 : s1, me = d.mol[g] == 0 ? s1 : e1;
-                const long long cbase = d.plus_off[s0] + d.minus_off[s0];
-                const long long m0 = (d.plus_off[s1] - d.plus_off[s0]) + (d.minus_off[s1] - d.minus_off[s0]);
-                const long long mb = cbase + (d.mol[g] == 0 ? 0 : m0);
-                pbase = mb + (d.plus_off[g] - d.plus_off[ms]);
-                mbase = mb + (d.plus_off[me] - d.plus_off[ms]) + (d.minus_off[g] - d.minus_off[ms]);
+                probe_bases(d, g, pbase, mbase);
             }
             if (!LONG) {
                 triples_row_c<EMIT>(d, g, K, off, xi, ai.w, eri, ati, rows_s[w], queue, pq_s[w], nplus, nminus,

@@ -227,3 +227,44 @@ def test_graph_capacity_overflow_is_detected_and_recovered():
     rsc, _ = ref.shape_complementarity()
     exact("totals after recovery", tot, rtot)
     exact("sc after recovery", sc, rsc)
+
+
+def test_probe_stash_and_recompute_agree():
+    """
+    The triple count pass stashes its probes when they fit the capacity it
+    ran with, and a scatter fills the probe arrays; otherwise (the first run
+    of a fresh context) the emit pass recomputes them.  Both give the same
+    probes, access flags and results.
+    """
+    from cms_cuda import _lib
+    names = ("golden_pkl", "synth_small_s7", "synth_zero_radii")
+    xyz, rad, off, nb = [], [], [0], []
+    for n in names:
+        bx, br, tx, tr = inputs(load_case(n))
+        xyz += [bx, tx]; rad += [br, tr]; nb.append(len(br)); off.append(off[-1] + len(br) + len(tr))
+    X, R = np.concatenate(xyz), np.concatenate(rad)
+    off, nb = np.array(off), np.array(nb)
+    ctx = _lib.Context(0)
+    ctx.load_batch(off, nb, X, R)
+
+    def snapshot():
+        out = []
+        for c in range(len(names)):
+            i = ctx.info(c)
+            n = int(off[c + 1] - off[c])
+            out.append(ctx.export_probes(c, i) + ctx.export_atoms(c, n))
+        return out, ctx.contact_ms(per_atom=True)
+
+    ctx.generate(all_atoms=False)          # capacities sized by this run: recomputed
+    first, cms1 = snapshot()
+    ctx.generate(all_atoms=False)          # capacities fit: stashed and scattered
+    second, cms2 = snapshot()
+    assert sum(len(p[0]) for p in first) > 0
+    for a, b in zip(first, second):
+        for x, y in zip(a, b):
+            exact("probe arrays", x, y)
+    exact("per-atom cms", cms1[0], cms2[0])
+    for c, n in enumerate(names):
+        case = load_case(n)
+        if "probe_point" in case:
+            close("probes vs reference", second[c][4], case["probe_point"])
