@@ -251,6 +251,7 @@ struct cms_ctx {
         S_ADJ_ACT_CONV, S_ADJ_ACT_TOR, S_ADJ_ACT_CONC, S_ADJ_ACT_ATOM, S_ADJ_LIST_CONV, S_ADJ_LIST_TOR,
         S_ADJ_LIST_CONC, S_ADJ_NACT, S_OVF, S_REF_XYZ, S_POSE, S_POSE_CKPT, S_POSE_CEN, S_HIST, S_STEP, S_MAXSUM,
         S_TOR_LFLAG, S_TOR_LOFF, S_TOR_LIST, S_PTOP, S_SP_A, S_SP_H, S_SP_XYZ, S_SP_ALT, S_SP_G, S_SP_ORD,
+        S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1,
         S_COUNT
     };
 
@@ -425,6 +426,10 @@ void bind_caps(cms_ctx* x)
     x->ensure<int>(cms_ctx::S_CMS_IDX, D);
     r.val = x->ensure<double>(cms_ctx::S_R_VAL, D);
     r.own = x->ensure<int>(cms_ctx::S_R_OWN, D);
+    r.so_f4[0] = x->ensure<float4>(cms_ctx::S_SO_F4_0, D);
+    r.so_f4[1] = x->ensure<float4>(cms_ctx::S_SO_F4_1, D);
+    r.so_perm[0] = x->ensure<int>(cms_ctx::S_SO_PERM_0, D);
+    r.so_perm[1] = x->ensure<int>(cms_ctx::S_SO_PERM_1, D);
     // search boxes: every search's references are a subset of the dots
     const long long rounds = nn_round_cap(D, 2LL * x->B);
     x->ensure<float4>(cms_ctx::S_BOX_ROUND, 2 * rounds);
@@ -600,8 +605,10 @@ void enqueue_cms(cms_ctx* x)
     NNTask* task = x->get<NNTask>(cms_ctx::S_TASKS);
     launch_tasks(d, r, 0, task, s);
     k_fill_d<<<grid1(x->cap_dot), 256, 0, s>>>(r.nn_d2, x->cap_dot, INFINITY);
+    launch_spatial_order(d, r, SO_BUR, 0, s);
     NNArgs a = nn_args(x, 0);
-    a.q_f4 = r.bur_f4; a.q_idx = r.bur_idx; a.r_f4 = r.bur_f4; a.r_idx = r.bur_idx;
+    a.q_f4 = r.so_f4[0]; a.q_perm = r.so_perm[0]; a.q_idx = r.bur_idx;
+    a.r_f4 = r.so_f4[0]; a.r_perm = r.so_perm[0]; a.r_idx = r.bur_idx;
     a.q_xyz = a.r_xyz = d.dxyz;
     a.out_d2 = r.nn_d2;
     a.out_idx = x->get<int>(cms_ctx::S_CMS_IDX);       // kept for the adjoint
@@ -621,8 +628,11 @@ void enqueue_sc(cms_ctx* x)
     long long* tmp = scan_tmp(x);
     NNTask* task = x->get<NNTask>(cms_ctx::S_TASKS);
     launch_tasks(d, r, 1, task + 2 * x->B, s);
+    launch_spatial_order(d, r, SO_BUR, 0, s);
+    launch_spatial_order(d, r, SO_ACC, 1, s);
     NNArgs a = nn_args(x, 1);
-    a.q_f4 = r.bur_f4; a.q_idx = r.bur_idx; a.r_f4 = r.acc_f4; a.r_idx = r.acc_idx;
+    a.q_f4 = r.so_f4[0]; a.q_perm = r.so_perm[0]; a.q_idx = r.bur_idx;
+    a.r_f4 = r.so_f4[1]; a.r_perm = r.so_perm[1]; a.r_idx = r.acc_idx;
     a.q_xyz = a.r_xyz = d.dxyz;
     a.out_flag = r.keep;
     a.band_thr64 = x->st.band * x->st.band;
@@ -632,8 +642,10 @@ void enqueue_sc(cms_ctx* x)
     launch_tasks(d, r, 2, task + 4 * x->B, s);
     k_fill_d<<<grid1(x->cap_dot), 256, 0, s>>>(r.nn_d2, x->cap_dot, INFINITY);
     k_fill_i<<<grid1(x->cap_dot), 256, 0, s>>>(r.nn_idx, x->cap_dot, -1);
+    launch_spatial_order(d, r, SO_TRIM, 0, s);
     NNArgs b = nn_args(x, 2);
-    b.q_f4 = r.trim_f4; b.q_idx = r.trim_idx; b.r_f4 = r.trim_f4; b.r_idx = r.trim_idx;
+    b.q_f4 = r.so_f4[0]; b.q_perm = r.so_perm[0]; b.q_idx = r.trim_idx;
+    b.r_f4 = r.so_f4[0]; b.r_perm = r.so_perm[0]; b.r_idx = r.trim_idx;
     b.q_xyz = b.r_xyz = d.dxyz;
     b.out_d2 = r.nn_d2; b.out_idx = r.nn_idx;
     launch_nn(b, NN_ARGMIN, x->nn_var[2], tile_cap(x), tmp, s);

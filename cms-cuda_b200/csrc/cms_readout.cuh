@@ -44,6 +44,9 @@ struct NNArgs {
     int band_mode;
     int tile_q;             // queries per tile of the launched variant
     const int* ovf;         // the batch's overflow flag (null for standalone searches)
+    // spatially ordered lists: the original position of each entry (null: lists in their own order);
+    // outputs go to the queries' original positions, and reference indices are original positions
+    const int* q_perm; const int* r_perm;
 };
 
 // readout workspace, capacity = dot capacity unless noted
@@ -55,7 +58,12 @@ struct Rd {
     int* trim_idx; float4* trim_f4;             // trimmed dots
     double* nn_d2; int* nn_idx;                 // per query entry
     double* val; int* own;                      // per entry value / owner atom (-1: none)
+    // spatially ordered copies (k_readout.cu) of a query list (buried or trimmed dots) and of the
+    // accessible list: points and each entry's original position
+    float4* so_f4[2]; int* so_perm[2];
 };
+
+enum { SO_BUR = 0, SO_ACC = 1, SO_TRIM = 2 };
 
 // adjoint of the contact molecular surface (k_adjoint.cu); capacity D = dot
 // capacity unless noted
@@ -92,6 +100,7 @@ void launch_track_max(const long long* summary, long long* mx, cudaStream_t s);
 void launch_pose_centroid(const Dev& d, const double* ref, double* cen, cudaStream_t s);
 
 void launch_split_buried(const Dev& d, const Rd& r, long long dot_cap, long long* scan_tmp, cudaStream_t s);
+void launch_spatial_order(const Dev& d, const Rd& r, int list, int set, cudaStream_t s);
 void launch_tasks(const Dev& d, const Rd& r, int kind, NNTask* task, cudaStream_t s);
 void launch_nn(NNArgs a, int mode, int variant, long long tile_cap, long long* scan_tmp, cudaStream_t s);
 void launch_nn_tiles(NNArgs a, int mode, int variant, long long* scan_tmp, cudaStream_t s);

@@ -123,6 +123,15 @@ __device__ __forceinline__ double exact_d2(const double* a, const double* b)
     return (dx * dx + dy * dy) + dz * dz;
 }
 
+// original list position of a (possibly spatially ordered) entry, and its point index
+__device__ __forceinline__ long long nn_qpos(const NNArgs& a, long long k) { return a.q_perm ? (long long)a.q_perm[k] : k; }
+__device__ __forceinline__ long long nn_rpos(const NNArgs& a, long long k) { return a.r_perm ? (long long)a.r_perm[k] : k; }
+__device__ __forceinline__ long long nn_rpt(const NNArgs& a, long long k)
+{
+    const long long o = nn_rpos(a, k);
+    return a.r_idx ? (long long)a.r_idx[o] : o;
+}
+
 // Packed FP32 pairs (Blackwell f32x2 arithmetic): one instruction does the
 // same IEEE round-to-nearest operation on two lanes, so packed results equal
 // the scalar ones bit for bit.
@@ -244,8 +253,7 @@ __device__ __forceinline__ void nn_band_warp(const NNArgs& a, const NNTask& T, N
             const int k = k0 + lane;
             const float v = nn_s(qx2, qy2, qz2, sA[k].x, sA[k].z, sB[k].x, sB[k].z);
             if (v <= ts) {
-                const long long rk = T.r0 + rb + k;
-                const double* rp = a.r_xyz + 3LL * (a.r_idx ? a.r_idx[rk] : rk);
+                const double* rp = a.r_xyz + 3LL * nn_rpt(a, T.r0 + rb + k);
                 hit = exact_d2(rp, a.q_xyz + 3LL * qdot) <= a.band_thr64;
             }
         }
@@ -262,8 +270,9 @@ __device__ __forceinline__ void nn_recheck(const NNArgs& a, const NNTask& T, con
     const float v = nn_s(qx2, qy2, qz2, rx, ry, rz, nn_rr(rx, ry, rz));
     if (v <= ts) {
         const long long rk = T.r0 + k;
-        const double e = exact_d2(a.r_xyz + 3LL * (a.r_idx ? a.r_idx[rk] : rk), a.q_xyz + 3LL * qdot);
-        if (e < best || (e == best && (int)k < bidx)) { best = e; bidx = (int)k; }
+        const double e = exact_d2(a.r_xyz + 3LL * nn_rpt(a, rk), a.q_xyz + 3LL * qdot);
+        const int ko = (int)(nn_rpos(a, rk) - T.r0);     // original position: first index on ties
+        if (e < best || (e == best && ko < bidx)) { best = e; bidx = ko; }
     }
 }
 
@@ -381,7 +390,8 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
             if (q[j].live) {
                 const float4 f = a.q_f4[T.q0 + qi];
                 qpx[j] = f.x; qpy[j] = f.y; qpz[j] = f.z;
-                q[j].dot = a.q_idx ? a.q_idx[T.q0 + qi] : (int)(T.q0 + qi);
+                const long long qo = nn_qpos(a, T.q0 + qi);
+                q[j].dot = a.q_idx ? a.q_idx[qo] : (int)qo;
                 wl[0] = fminf(wl[0], f.x); wl[1] = fminf(wl[1], f.y); wl[2] = fminf(wl[2], f.z);
                 wh[0] = fmaxf(wh[0], f.x); wh[1] = fmaxf(wh[1], f.y); wh[2] = fmaxf(wh[2], f.z);
             }
@@ -594,7 +604,7 @@ __global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
 #pragma unroll
         for (int j = 0; j < Q; ++j) {
             if (!q[j].live) continue;
-            const long long o = T.q0 + qw + j * 32 + lane;
+            const long long o = nn_qpos(a, T.q0 + qw + j * 32 + lane);
             if (MODE == NN_BAND) a.out_flag[o] = q[j].done ? 0 : 1;     // keep iff no reference within the band
             else {
                 a.out_d2[o] = q[j].best;
@@ -834,6 +844,115 @@ void launch_tasks(const Dev& d, const Rd& r, int kind, NNTask* task, cudaStream_
     if (kind == 0) k_tasks_cms<<<g, 128, 0, s>>>(d, r, task);
     else if (kind == 1) k_tasks_trim<<<g, 128, 0, s>>>(d, r, task);
     else k_tasks_sc<<<g, 128, 0, s>>>(d, r, task);
+}
+
+// ---------------------------------------------------------------------------
+// Spatial order of the packed lists.  Each complex & molecule range of a list
+// is reordered by the Morton code of a 16^3 grid over its bounding box,
+// stably (list order inside a cell), so 32-entry blocks and 512-entry rounds
+// of the nearest-dot search are compact boxes.  The searches return the same
+// results in any order: ties go to the smallest original position.
+// ---------------------------------------------------------------------------
+static constexpr int SO_GRID = 16;                    // cells per axis
+static constexpr int SO_CELLS = SO_GRID * SO_GRID * SO_GRID;
+
+__device__ __forceinline__ int so_pad(int b) { return b + (b >> 7); }   // 128 buckets per lane, skewed banks
+
+__device__ __forceinline__ unsigned so_spread4(unsigned v)      // 4 bits -> every third bit
+{
+    v &= 0xfu;
+    v = (v | (v << 4)) & 0x0c3u;
+    v = (v | (v << 2)) & 0x249u;
+    return v;
+}
+
+__device__ __forceinline__ void so_range(const Dev& d, const Rd& r, int list, long long t, long long& s, long long& e)
+{
+    const long long ds = doff(d, t), de = doff(d, t + 1);
+    if (list == SO_BUR) { s = r.bur_scan[ds]; e = r.bur_scan[de]; }
+    else if (list == SO_ACC) { s = ds - r.bur_scan[ds]; e = de - r.bur_scan[de]; }
+    else { s = r.trim_scan[r.bur_scan[ds]]; e = r.trim_scan[r.bur_scan[de]]; }
+}
+
+__global__ void __launch_bounds__(32) k_spatial_order(Dev d, Rd r, int list, int set)
+{
+    CMS_EXIT_ON_OVERFLOW(d);
+    __shared__ int cnt[SO_CELLS + SO_CELLS / 128];
+    const int lane = threadIdx.x;
+    const unsigned lt = (1u << lane) - 1u;
+    const float4* f4 = list == SO_BUR ? r.bur_f4 : (list == SO_ACC ? r.acc_f4 : r.trim_f4);
+    float4* of4 = r.so_f4[set];
+    int* operm = r.so_perm[set];
+    for (long long t = blockIdx.x; t < 2LL * d.B; t += gridDim.x) {
+        long long s, e;
+        so_range(d, r, list, t, s, e);
+        const long long n = e - s;
+        if (n <= 0) continue;
+        float l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (long long i = lane; i < n; i += 32) {
+            const float4 p = f4[s + i];
+            l[0] = fminf(l[0], p.x); l[1] = fminf(l[1], p.y); l[2] = fminf(l[2], p.z);
+            h[0] = fmaxf(h[0], p.x); h[1] = fmaxf(h[1], p.y); h[2] = fmaxf(h[2], p.z);
+        }
+        float sc[3];
+        for (int k = 0; k < 3; ++k) {
+            for (int o = 16; o > 0; o >>= 1) {
+                l[k] = fminf(l[k], __shfl_xor_sync(0xffffffffu, l[k], o));
+                h[k] = fmaxf(h[k], __shfl_xor_sync(0xffffffffu, h[k], o));
+            }
+            sc[k] = (float)SO_GRID / fmaxf(h[k] - l[k], 1e-3f);
+        }
+        auto cell = [&](float4 p) -> int {
+            const int ix = min(SO_GRID - 1, max(0, (int)((p.x - l[0]) * sc[0])));
+            const int iy = min(SO_GRID - 1, max(0, (int)((p.y - l[1]) * sc[1])));
+            const int iz = min(SO_GRID - 1, max(0, (int)((p.z - l[2]) * sc[2])));
+            return (int)(so_spread4(ix) | (so_spread4(iy) << 1) | (so_spread4(iz) << 2));
+        };
+        for (int b = lane; b < SO_CELLS; b += 32) cnt[so_pad(b)] = 0;
+        __syncwarp();
+        for (long long i = lane; i < n; i += 32) atomicAdd(&cnt[so_pad(cell(f4[s + i]))], 1);
+        __syncwarp();
+        // exclusive scan: lane L owns cells [128 L, 128 L + 128)
+        int sum = 0;
+        for (int k = 0; k < SO_CELLS / 32; ++k) sum += cnt[so_pad(lane * (SO_CELLS / 32) + k)];
+        int x = sum;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        int run = x - sum;
+        for (int k = 0; k < SO_CELLS / 32; ++k) {
+            const int b = so_pad(lane * (SO_CELLS / 32) + k);
+            const int c = cnt[b];
+            cnt[b] = run;
+            run += c;
+        }
+        __syncwarp();
+        // stable scatter, 32 entries at a time in list order
+        for (long long i0 = 0; i0 < n; i0 += 32) {
+            const long long i = i0 + lane;
+            const bool on = i < n;
+            float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+            int b = SO_CELLS;
+            if (on) { p = f4[s + i]; b = cell(p); }
+            const unsigned peers = __match_any_sync(0xffffffffu, b);
+            const int base = on ? cnt[so_pad(b)] : 0;
+            __syncwarp();
+            if (on && (peers & lt) == 0) cnt[so_pad(b)] = base + __popc(peers);
+            __syncwarp();
+            if (on) {
+                const long long o = s + base + __popc(peers & lt);
+                of4[o] = p;
+                operm[o] = (int)(s + i);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+void launch_spatial_order(const Dev& d, const Rd& r, int list, int set, cudaStream_t s)
+{
+    k_spatial_order<<<grid_for(2LL * d.B, 1, 14), 32, 0, s>>>(d, r, list, set);
 }
 
 // ---------------------------------------------------------------------------
