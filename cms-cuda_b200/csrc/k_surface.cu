@@ -748,7 +748,7 @@ __device__ __forceinline__ void triples_flush(const Dev& d, int g, V3 xi, double
 // unit vector uik = (xk - xi) / dik, which every pair (i, j) of the row
 // reuses.  Queued pairs keep their geometry for the probe pass.
 static constexpr int TR_KC = 128;
-static constexpr int TR_PQ = 32;      // queued pairs per probe pass
+static constexpr int TR_PC = 32;      // neighbour slots (pairs) per chunk of the candidate matrix
 
 struct TrRow {
     double x[TR_KC], y[TR_KC], z[TR_KC], r[TR_KC];
@@ -757,7 +757,14 @@ struct TrRow {
     int8_t at[TR_KC];
 };
 
-struct TrPairC { V3 uij, tij; int ps; };
+struct TrPairC { V3 uij, tij; double rij; int ps; };
+
+// one chunk's pairs (i, j) and their (pair, k) candidate matrix
+struct TrWork {
+    TrPairC pr[TR_PC];
+    unsigned cb[TR_PC][TR_KC / 32];   // candidate k slots of each pair
+    unsigned kill;                    // pairs killed by a degenerate triple
+};
 
 // norm3(v) < T, skipping the square root when the squared comparison settles
 // it: with a 1e-12 relative margin on T^2 the rounded root lies on the same side
@@ -863,10 +870,14 @@ __device__ __forceinline__ void triples_flush_c(const Dev& d, int g, V3 xi, doub
     }
 }
 
-// the triple loop of one atom whose row fits the cache (K <= TR_KC)
+// The triple loop of one atom whose row fits the cache (K <= TR_KC).  The
+// row's pairs (i, j) are taken 32 neighbour slots at a time: their geometry
+// one pair per lane, then the (pair, k) candidate matrix spread over the
+// lanes, then the queue in (pair, k) order -- the order of the reference's
+// loops -- for the probe pass.
 template <bool EMIT>
 __device__ __forceinline__ void triples_row_c(const Dev& d, int g, int K, long long off, V3 xi, double ri, double eri,
-                                              int8_t ati, TrRow& R, unsigned* queue, TrPairC* pq, int& nplus,
+                                              int8_t ati, TrRow& R, unsigned* queue, TrWork& W, int& nplus,
                                               int& nminus, long long pbase, long long mbase)
 {
     const int lane = threadIdx.x & 31;
@@ -884,62 +895,65 @@ __device__ __forceinline__ void triples_row_c(const Dev& d, int g, int K, long l
         R.dk[s] = dk; R.ux[s] = u.x; R.uy[s] = u.y; R.uz[s] = u.z;
     }
     __syncwarp();
-    int qn = 0, npq = 0;
-    for (int ps = 0; ps < K; ++ps) {
-        const int j = R.id[ps];
-        if (j <= g) continue;
-        const V3 xj = v3(R.x[ps], R.y[ps], R.z[ps]);
-        const PairGeo p = pair_geo(xi, ri, xj, R.r[ps], rp);
-        if (!p.ok) continue;
-        const double erj = R.r[ps] + rp;
-        const int8_t atj = R.at[ps];
-        // a degenerate triple (|uij.uik| >= 1) inside the torus kills the whole pair
-        // (_core.py:1524-1543); the others are queued in (pair, k) order
-        bool kill = false;
-        int nq = 0;
-        unsigned cand[TR_KC / 32];
-#pragma unroll
-        for (int r = 0; r < TR_KC / 32; ++r) {
-            const int ks = r * 32 + lane;
-            bool c = false;
-            if (ks < K && triple_ok_c(R, ks, j, xj, erj, eri, ati, atj, rp)) {
-                const double dt = dot_alt(p.uij, v3(R.ux[ks], R.uy[ks], R.uz[ks]));
-                if (dt >= 1.0 || dt <= -1.0) {
-                    const double erk = R.r[ks] + rp;
-                    const double dtijk2 = sq_seq(p.tij - v3(R.x[ks], R.y[ks], R.z[ks]));
-                    const double rkp2 = erk * erk - p.rij * p.rij;
-                    kill |= dtijk2 < rkp2;
-                } else {
-                    c = true;
-                }
+    for (int ps0 = 0; ps0 < K; ps0 += TR_PC) {
+        // pairs (i, j) of the chunk: j after i and the pair geometry ok
+        const int ps = ps0 + lane;
+        bool v = false;
+        PairGeo p;
+        if (ps < K && R.id[ps] > g) {
+            p = pair_geo(xi, ri, v3(R.x[ps], R.y[ps], R.z[ps]), R.r[ps], rp);
+            v = p.ok;
+        }
+        const unsigned vm = __ballot_sync(0xffffffffu, v);
+        const int np = __popc(vm);
+        if (np == 0) continue;
+        if (v) W.pr[__popc(vm & lt)] = TrPairC{p.uij, p.tij, p.rij, ps};
+        for (int t = lane; t < np * (TR_KC / 32); t += 32) W.cb[t / (TR_KC / 32)][t % (TR_KC / 32)] = 0u;
+        if (lane == 0) W.kill = 0u;
+        __syncwarp();
+        // candidate matrix: a degenerate triple (|uij.uik| >= 1) inside the
+        // torus kills its pair (_core.py:1524-1543)
+        for (int c = lane; c < np * K; c += 32) {
+            const int pi = c / K, ks = c - pi * K;
+            const TrPairC& P = W.pr[pi];
+            const int pj = P.ps;
+            if (!triple_ok_c(R, ks, R.id[pj], v3(R.x[pj], R.y[pj], R.z[pj]), R.r[pj] + rp, eri, ati, R.at[pj], rp))
+                continue;
+            const double dt = dot_alt(P.uij, v3(R.ux[ks], R.uy[ks], R.uz[ks]));
+            if (dt >= 1.0 || dt <= -1.0) {
+                const double erk = R.r[ks] + rp;
+                const double dtijk2 = sq_seq(P.tij - v3(R.x[ks], R.y[ks], R.z[ks]));
+                const double rkp2 = erk * erk - P.rij * P.rij;
+                if (dtijk2 < rkp2) atomicOr(&W.kill, 1u << pi);
+            } else {
+                atomicOr(&W.cb[pi][ks >> 5], 1u << (ks & 31));
             }
-            cand[r] = __ballot_sync(0xffffffffu, c);
-            nq += __popc(cand[r]);
-        }
-        if (__any_sync(0xffffffffu, kill)) continue;
-        if (nq == 0) continue;
-        if (qn + nq > TR_QCAP || npq == TR_PQ) {
-            __syncwarp();
-            triples_flush_c<EMIT>(d, g, xi, eri, R, K, queue, pq, qn, nplus, nminus, pbase, mbase);
-            __syncwarp();
-            qn = 0; npq = 0;
-        }
-        if (lane == 0) pq[npq] = TrPairC{p.uij, p.tij, ps};
-        const unsigned slot = (unsigned)npq << 16;
-        ++npq;
-#pragma unroll
-        for (int r = 0; r < TR_KC / 32; ++r) {
-            const unsigned m = cand[r];
-            if ((m >> lane) & 1u) queue[qn + __popc(m & lt)] = slot | (unsigned)(r * 32 + lane);
-            qn += __popc(m);
         }
         __syncwarp();
-    }
-    if (qn > 0) {
+        // queue the live pairs' candidates in (pair, k) order
+        const unsigned kill = W.kill;
+        int qn = 0;
+        for (int pi = 0; pi < np; ++pi) {
+            if ((kill >> pi) & 1u) continue;
+            int nq = 0;
+            for (int r = 0; r * 32 < K; ++r) nq += __popc(W.cb[pi][r]);
+            if (nq == 0) continue;
+            if (qn + nq > TR_QCAP) {
+                __syncwarp();
+                triples_flush_c<EMIT>(d, g, xi, eri, R, K, queue, W.pr, qn, nplus, nminus, pbase, mbase);
+                __syncwarp();
+                qn = 0;
+            }
+            for (int r = 0; r * 32 < K; ++r) {
+                const unsigned m = W.cb[pi][r];
+                if ((m >> lane) & 1u) queue[qn + __popc(m & lt)] = ((unsigned)pi << 16) | (unsigned)(r * 32 + lane);
+                qn += __popc(m);
+            }
+        }
         __syncwarp();
-        triples_flush_c<EMIT>(d, g, xi, eri, R, K, queue, pq, qn, nplus, nminus, pbase, mbase);
+        if (qn > 0) triples_flush_c<EMIT>(d, g, xi, eri, R, K, queue, W.pr, qn, nplus, nminus, pbase, mbase);
+        __syncwarp();
     }
-    __syncwarp();
 }
 
 // LONG = false: atoms whose neighbour row fits the cache; true: the others
@@ -949,7 +963,7 @@ __global__ void __launch_bounds__(TR_WARPS * 32, EMIT ? 8 : 7) k_triples(Dev d)
     CMS_EXIT_ON_OVERFLOW(d);
     __shared__ unsigned queue_s[TR_WARPS][TR_QCAP];
     __shared__ TrRow rows_s[LONG ? 1 : TR_WARPS];
-    __shared__ TrPairC pq_s[LONG ? 1 : TR_WARPS][TR_PQ];
+    __shared__ TrWork work_s[LONG ? 1 : TR_WARPS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     unsigned* queue = queue_s[w];
@@ -982,7 +996,7 @@ __global__ void __launch_bounds__(TR_WARPS * 32, EMIT ? 8 : 7) k_triples(Dev d)
                 probe_bases(d, g, pbase, mbase);
             }
             if (!LONG) {
-                triples_row_c<EMIT>(d, g, K, off, xi, ai.w, eri, ati, rows_s[w], queue, pq_s[w], nplus, nminus,
+                triples_row_c<EMIT>(d, g, K, off, xi, ai.w, eri, ati, rows_s[w], queue, work_s[w], nplus, nminus,
                                     pbase, mbase);
                 if (!EMIT && lane == 0) { d.nplus[g] = nplus; d.nminus[g] = nminus; }
                 continue;
