@@ -755,6 +755,8 @@ struct TrRow {
     double ux[TR_KC], uy[TR_KC], uz[TR_KC], dk[TR_KC];
     int id[TR_KC];
     int8_t at[TR_KC];
+    unsigned char rk[TR_KC];    // rank of the slot's atom id in the row
+    unsigned char ord[TR_KC];   // slot of each id rank
 };
 
 struct TrPairC { V3 uij, tij; double rij; int ps; };
@@ -763,6 +765,7 @@ struct TrPairC { V3 uij, tij; double rij; int ps; };
 struct TrWork {
     TrPairC pr[TR_PC];
     unsigned cb[TR_PC][TR_KC / 32];   // candidate k slots of each pair
+    int cpos[TR_PC];                  // first (pair, k) combination of each pair
     unsigned kill;                    // pairs killed by a degenerate triple
 };
 
@@ -872,9 +875,9 @@ __device__ __forceinline__ void triples_flush_c(const Dev& d, int g, V3 xi, doub
 
 // The triple loop of one atom whose row fits the cache (K <= TR_KC).  The
 // row's pairs (i, j) are taken 32 neighbour slots at a time: their geometry
-// one pair per lane, then the (pair, k) candidate matrix spread over the
-// lanes, then the queue in (pair, k) order -- the order of the reference's
-// loops -- for the probe pass.
+// one pair per lane, then the (pair, k) combinations with k after j (by atom
+// id) spread over the lanes, then the queue in (pair, k slot) order -- the
+// order of the reference's loops -- one pair per lane, for the probe pass.
 template <bool EMIT>
 __device__ __forceinline__ void triples_row_c(const Dev& d, int g, int K, long long off, V3 xi, double ri, double eri,
                                               int8_t ati, TrRow& R, unsigned* queue, TrWork& W, int& nplus,
@@ -895,6 +898,14 @@ __device__ __forceinline__ void triples_row_c(const Dev& d, int g, int K, long l
         R.dk[s] = dk; R.ux[s] = u.x; R.uy[s] = u.y; R.uz[s] = u.z;
     }
     __syncwarp();
+    for (int s = lane; s < K; s += 32) {      // atom ids of a row are distinct
+        const int id = R.id[s];
+        int r = 0;
+        for (int f = 0; f < K; ++f) r += R.id[f] < id ? 1 : 0;
+        R.rk[s] = (unsigned char)r;
+        R.ord[r] = (unsigned char)s;
+    }
+    __syncwarp();
     for (int ps0 = 0; ps0 < K; ps0 += TR_PC) {
         // pairs (i, j) of the chunk: j after i and the pair geometry ok
         const int ps = ps0 + lane;
@@ -907,16 +918,35 @@ __device__ __forceinline__ void triples_row_c(const Dev& d, int g, int K, long l
         const unsigned vm = __ballot_sync(0xffffffffu, v);
         const int np = __popc(vm);
         if (np == 0) continue;
-        if (v) W.pr[__popc(vm & lt)] = TrPairC{p.uij, p.tij, p.rij, ps};
+        // combinations of each pair: the slots whose atom id is above j's
+        int nk = 0;
+        if (v) {
+            const int pi = __popc(vm & lt);
+            W.pr[pi] = TrPairC{p.uij, p.tij, p.rij, ps};
+            nk = K - 1 - (int)R.rk[ps];
+        }
+        int x = nk;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        const int NC = __shfl_sync(0xffffffffu, x, 31);
+        if (v) W.cpos[__popc(vm & lt)] = x - nk;
         for (int t = lane; t < np * (TR_KC / 32); t += 32) W.cb[t / (TR_KC / 32)][t % (TR_KC / 32)] = 0u;
         if (lane == 0) W.kill = 0u;
         __syncwarp();
         // candidate matrix: a degenerate triple (|uij.uik| >= 1) inside the
         // torus kills its pair (_core.py:1524-1543)
-        for (int c = lane; c < np * K; c += 32) {
-            const int pi = c / K, ks = c - pi * K;
+        for (int c = lane; c < NC; c += 32) {
+            int lo = 0, hi = np - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (W.cpos[mid] <= c) lo = mid; else hi = mid - 1;
+            }
+            const int pi = lo;
             const TrPairC& P = W.pr[pi];
             const int pj = P.ps;
+            const int ks = R.ord[(int)R.rk[pj] + 1 + (c - W.cpos[pi])];
             if (!triple_ok_c(R, ks, R.id[pj], v3(R.x[pj], R.y[pj], R.z[pj]), R.r[pj] + rp, eri, ati, R.at[pj], rp))
                 continue;
             const double dt = dot_alt(P.uij, v3(R.ux[ks], R.uy[ks], R.uz[ks]));
@@ -930,29 +960,42 @@ __device__ __forceinline__ void triples_row_c(const Dev& d, int g, int K, long l
             }
         }
         __syncwarp();
-        // queue the live pairs' candidates in (pair, k) order
-        const unsigned kill = W.kill;
-        int qn = 0;
-        for (int pi = 0; pi < np; ++pi) {
-            if ((kill >> pi) & 1u) continue;
-            int nq = 0;
-            for (int r = 0; r * 32 < K; ++r) nq += __popc(W.cb[pi][r]);
-            if (nq == 0) continue;
-            if (qn + nq > TR_QCAP) {
-                __syncwarp();
-                triples_flush_c<EMIT>(d, g, xi, eri, R, K, queue, W.pr, qn, nplus, nminus, pbase, mbase);
-                __syncwarp();
-                qn = 0;
-            }
-            for (int r = 0; r * 32 < K; ++r) {
-                const unsigned m = W.cb[pi][r];
-                if ((m >> lane) & 1u) queue[qn + __popc(m & lt)] = ((unsigned)pi << 16) | (unsigned)(r * 32 + lane);
-                qn += __popc(m);
-            }
+        // queue, one pair per lane: candidates of the live pairs in (pair, k
+        // slot) order, flushed whenever the next pair would overflow the queue
+        int nq = 0;
+        if (lane < np && !((W.kill >> lane) & 1u))
+            for (int r = 0; r * 32 < K; ++r) nq += __popc(W.cb[lane][r]);
+        int qx = nq;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, qx, o);
+            if (lane >= o) qx += y;
         }
-        __syncwarp();
-        if (qn > 0) triples_flush_c<EMIT>(d, g, xi, eri, R, K, queue, W.pr, qn, nplus, nminus, pbase, mbase);
-        __syncwarp();
+        const int qtot = __shfl_sync(0xffffffffu, qx, 31);
+        const int qpos = qx - nq;                 // this pair's first entry in the chunk
+        int base = 0;                             // entries of earlier pairs already flushed
+        while (base < qtot) {
+            // the pairs that fit: every entry in [base, base + TR_QCAP)
+            const bool take = nq > 0 && qpos >= base && qpos + nq <= base + TR_QCAP;
+            const unsigned tm = __ballot_sync(0xffffffffu, take);
+            if (tm == 0u) break;                  // cannot happen: the first pending pair always fits
+            const int last = 31 - __clz(tm);
+            const int end = __shfl_sync(0xffffffffu, qpos + nq, last);
+            if (take) {
+                int t = qpos - base;
+                for (int r = 0; r * 32 < K; ++r) {
+                    unsigned m = W.cb[lane][r];
+                    while (m) {
+                        const int b = __ffs(m) - 1;
+                        m &= m - 1;
+                        queue[t++] = ((unsigned)lane << 16) | (unsigned)(r * 32 + b);
+                    }
+                }
+            }
+            __syncwarp();
+            triples_flush_c<EMIT>(d, g, xi, eri, R, K, queue, W.pr, end - base, nplus, nminus, pbase, mbase);
+            __syncwarp();
+            base = end;
+        }
     }
 }
 
