@@ -35,14 +35,18 @@ __device__ __forceinline__ bool near_circle(V3 x, V3 c, V3 u, double R)
 // Warp-cooperative: compact into out[] (room for cap ids) the atoms ids[s, e)
 // other than `skip` whose sphere of radius r + rp may reach the circle; -1
 // when they do not fit (the caller then scans the full list).  A non-finite
-// distance keeps the atom.  Every lane returns the same count.
+// distance keeps the atom.  Every lane returns the same count.  With `cover`,
+// also reports whether one of the atoms holds the whole circle strictly
+// inside its sphere, CMS_CIRCLE_MARGIN to spare: then every point of the
+// circle collides with it (strict < test).
 __device__ __forceinline__ int circle_prune(const Dev& d, V3 c, V3 u, double R, const int* ids, long long s,
-                                            long long e, int skip, int* out, int cap)
+                                            long long e, int skip, int* out, int cap, bool* cover = nullptr)
 {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     const double rp = d.st.rp;
     int n = 0;
+    bool cov = false;
     for (long long b = s; b < e; b += 32) {
         const long long k = b + lane;
         bool keep = false;
@@ -51,8 +55,16 @@ __device__ __forceinline__ int circle_prune(const Dev& d, V3 c, V3 u, double R, 
             id = ids[k];
             if (id != skip) {
                 const double4 a = d.xyzr[id];
+                const V3 v = v3(a.x, a.y, a.z) - c;
+                const double h = dot_seq(v, u);
+                const double rho = sqrt(fmax(sq_seq(v) - h * h, 0.0));
+                const double dr = rho - R;
                 const double t = a.w + rp + CMS_CIRCLE_MARGIN;
-                keep = !(circle_dist2(v3(a.x, a.y, a.z), c, u, R) > t * t);
+                keep = !(h * h + dr * dr > t * t);
+                if (cover && keep) {
+                    const double far = rho + R, ti = a.w + rp - CMS_CIRCLE_MARGIN;
+                    cov |= ti > 0.0 && h * h + far * far < ti * ti;
+                }
             }
         }
         const unsigned m = __ballot_sync(0xffffffffu, keep);
@@ -60,6 +72,7 @@ __device__ __forceinline__ int circle_prune(const Dev& d, V3 c, V3 u, double R, 
         if (keep && pos < cap) out[pos] = id;
         n += __popc(m);
     }
+    if (cover) *cover = __any_sync(0xffffffffu, cov);
     __syncwarp();
     return n > cap ? -1 : n;
 }

@@ -292,9 +292,9 @@ __device__ __forceinline__ TorPair tor_pair(const Dev& d, long long q)
 
 // atoms of ids[s, e) other than `skip` that may reach the torus circle of T
 __device__ __forceinline__ int tor_prune(const Dev& d, const TorPair& T, const int* ids, long long s, long long e,
-                                         int skip, int* out, int cap)
+                                         int skip, int* out, int cap, bool* cover = nullptr)
 {
-    return circle_prune(d, T.tij, T.uij, T.rij, ids, s, e, skip, out, cap);
+    return circle_prune(d, T.tij, T.uij, T.rij, ids, s, e, skip, out, cap, cover);
 }
 
 struct TorPoint {
@@ -481,6 +481,7 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
     CMS_EXIT_ON_OVERFLOW(d);
     __shared__ TorPair tp[TO_WARPS][TO_PAIRS];
     __shared__ int tq[TO_WARPS][TO_PAIRS];                  // pair index of each batch slot
+    __shared__ int nsv[TO_WARPS][TO_PAIRS];                 // torus points of each pair (0: circle covered)
     __shared__ int pool[TO_WARPS][TO_POOL];
     __shared__ int pst[TO_WARPS][TO_PAIRS + 1];             // exclusive scan of torus points per pair
     __shared__ int l_off[TO_WARPS][3][TO_PAIRS];            // pruned lists: neighbours of i, partners of i, of j
@@ -501,13 +502,12 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
         const long long q0 = bt * TO_PAIRS;
         const int np = (int)min((long long)TO_PAIRS, NT - q0);
         __syncwarp();
-        int ns = 0;
         if (lane < np) {
             const long long q = EMIT ? (long long)d.tor_list[q0 + lane] : q0 + lane;
             const TorPair T = tor_pair(d, q);
             tp[w][lane] = T;
             tq[w][lane] = (int)q;
-            ns = T.ns;
+            nsv[w][lane] = T.ns;
             run[w][0][lane] = 0; run[w][1][lane] = 0;
             hasf[w][lane] = 0;
             arcf[w][lane] = (unsigned char)((d.atten[T.i] >= 2 ? 1 : 0) | (d.atten[T.j] >= 2 ? 2 : 0));
@@ -517,18 +517,16 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
                 base[we][1][lane] = unit_base(d, c, m, 2, d.tor2_off[q]);
             }
         }
-        int tot;
-        const int ex = warp_excl_scan(ns, tot);
-        if (lane < np) pst[w][lane] = ex;
-        if (lane == 0) pst[w][np] = tot;
         __syncwarp();
-        // pruned lists of the batch's pairs
+        // pruned lists of the batch's pairs; a circle inside one neighbour's
+        // sphere has no free point, so its pair takes no torus points
         int used = 0;
         for (int k = 0; k < np; ++k) {
             const TorPair& T = tp[w][k];
+            bool cov;
             int c = tor_prune(d, T, d.nb_id, d.nb_off[T.i], d.nb_off[T.i] + d.nnb[T.i], T.j, pool[w] + used,
-                              TO_POOL - used);
-            if (lane == 0) { l_off[w][0][k] = used; l_cnt[w][0][k] = c; }
+                              TO_POOL - used, &cov);
+            if (lane == 0) { l_off[w][0][k] = used; l_cnt[w][0][k] = c; if (cov) nsv[w][k] = 0; }
             if (c > 0) used += c;
             if (EMIT) {
                 const int af = arcf[w][k];
@@ -542,6 +540,11 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
                 if (c > 0) used += c;
             }
         }
+        __syncwarp();
+        int tot;
+        const int ex = warp_excl_scan(lane < np ? nsv[w][lane] : 0, tot);
+        if (lane < np) pst[w][lane] = ex;
+        if (lane == 0) pst[w][np] = tot;
         __syncwarp();
         // torus points, 32 at a time; lanes of one pair are contiguous
         for (int c0 = 0; c0 < tot; c0 += 32) {
