@@ -197,20 +197,28 @@ def run_reference(args):
 # entry (id 4 + d2 8), 4 B per buried-partner entry, 62 B per emitted dot
 # (coordinates 24, normal 24, area 8, buried 1, type 1, atom 4), 4 B per
 # neighbour entry read by a generating unit, 68 B per probe (3 ids 12,
-# height 8, centre 24, direction 24), 8 B per toroid pair.
-def stage_bytes(name, t):
+# height 8, centre 24, direction 24), 8 B per toroid pair.  The triple count
+# pass also writes each probe to the stash (76 B: the probe and its final
+# slot), which the scatter reads back before writing the probe arrays.  The
+# CMS adjoint reads 4 B per buried entry (its complex & molecule), and per
+# entry of the differentiated side (half the entries) the query and reference
+# points 48 B, the area 8 B and the nearest index 4 B, and writes the dot
+# adjoint 32 B; it writes 24 B of gradient per atom.
+def stage_bytes(name, t, work=None):
     nb4 = 4 * t["nb_entries"]
+    nbur = (work or {}).get("cms_queries")
     table = {
         "neighbor_count": 34 * t["atoms"],
         "neighbor_emit": 34 * t["atoms"] + 12 * t["nb_entries"] + 4 * t["bu_entries"],
-        "triples_count": nb4,
-        "triples_emit": nb4 + 68 * t["probes"],
+        "triples_count": nb4 + 76 * t["probes"],
+        "triples_emit": (76 + 68) * t["probes"],
         "convex_count": nb4,
         "convex_emit": nb4 + 62 * t["convex"],
         "toroidal_count": 8 * t["toroids"] + nb4,
         "toroidal_emit": 8 * t["toroids"] + nb4 + 62 * t["toroidal"],
         "concave_count": 68 * t["probes"],
         "concave_emit": 68 * t["probes"] + 62 * t["concave"],
+        "cms_backward": None if nbur is None else 4 * nbur + (48 + 8 + 4 + 32) * nbur // 2 + 24 * t["atoms"],
     }
     return table.get(name)
 
@@ -249,7 +257,7 @@ def stage_roofline(stages, work, totals, peaks, fp32_peak):
                 "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": stage_traffic(name, totals, work), "ms": ms,
                 "peak_source": "measured FP32 FMA throughput of this GPU (cms_fp32_peak, in this run)"}
     hbm = peaks.get("hbm_gbs")
-    nbytes = stage_bytes(name, totals)
+    nbytes = stage_bytes(name, totals, work)
     achieved = nbytes / (ms * 1e-3) / 1e9 if nbytes is not None else None
     return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm, "unit": "GB/s",
             "frac": (achieved / hbm) if (achieved is not None and hbm) else None,

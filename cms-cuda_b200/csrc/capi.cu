@@ -251,7 +251,7 @@ struct cms_ctx {
         S_ADJ_ACT_CONV, S_ADJ_ACT_TOR, S_ADJ_ACT_CONC, S_ADJ_ACT_ATOM, S_ADJ_LIST_CONV, S_ADJ_LIST_TOR,
         S_ADJ_LIST_CONC, S_ADJ_NACT, S_OVF, S_REF_XYZ, S_POSE, S_POSE_CKPT, S_POSE_CEN, S_HIST, S_STEP, S_MAXSUM,
         S_TOR_LFLAG, S_TOR_LOFF, S_TOR_LIST, S_PTOP, S_SP_A, S_SP_H, S_SP_XYZ, S_SP_ALT, S_SP_G, S_SP_ORD,
-        S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1,
+        S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1, S_KS_TOP, S_KS_BUF, S_CV_SOFF, S_CC_SOFF,
         S_COUNT
     };
 
@@ -336,6 +336,8 @@ void bind_batch(cms_ctx* x)
     d.minus_off = x->ensure<long long>(cms_ctx::S_MINUS_OFF, N + 1);
     d.conv_cnt = x->ensure<int>(cms_ctx::S_CONV_CNT, N);
     d.conv_off = x->ensure<long long>(cms_ctx::S_CONV_OFF, N + 1);
+    d.cv_soff = x->ensure<int>(cms_ctx::S_CV_SOFF, N);
+    d.ks_top = x->ensure<unsigned long long>(cms_ctx::S_KS_TOP, 1);
     d.seg = x->ensure<Seg>(cms_ctx::S_SEG, 8 * B);
     d.dot_off = x->ensure<long long>(cms_ctx::S_DOT_OFF, 2 * B + 1);
     d.tor_last1 = x->ensure<unsigned long long>(cms_ctx::S_TOR_LAST1, N);
@@ -400,9 +402,12 @@ void bind_caps(cms_ctx* x)
     d.sp_ord = x->ensure<unsigned>(cms_ctx::S_SP_ORD, x->cap_probe);
     d.conc_cnt = x->ensure<int>(cms_ctx::S_CONC_CNT, x->cap_probe);
     d.conc_off = x->ensure<long long>(cms_ctx::S_CONC_OFF, x->cap_probe + 1);
+    d.cc_soff = x->ensure<int>(cms_ctx::S_CC_SOFF, x->cap_probe);
     d.dot_cap = x->cap_dot;
     const long long D = x->cap_dot;
     d.dxyz = x->ensure<double>(cms_ctx::S_DXYZ, 3 * D);
+    d.ks_cap = D;
+    d.ks_buf = x->ensure<int>(cms_ctx::S_KS_BUF, D);
     d.dnml = x->ensure<double>(cms_ctx::S_DNML, 3 * D);
     d.darea = x->ensure<double>(cms_ctx::S_DAREA, D);
     d.dbur = x->ensure<int8_t>(cms_ctx::S_DBUR, D);
@@ -544,6 +549,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
     ck(cudaMemsetAsync(d.tor1_cnt, 0, sizeof(int) * x->cap_tor, s), "memset");
     ck(cudaMemsetAsync(d.tor2_cnt, 0, sizeof(int) * x->cap_tor, s), "memset");
     ck(cudaMemsetAsync(d.conc_cnt, 0, sizeof(int) * x->cap_probe, s), "memset");
+    ck(cudaMemsetAsync(d.ks_top, 0, sizeof(unsigned long long), s), "memset");
     launch_convex(d, false, s);
     mark(x, P_CONVEX_COUNT);
     launch_toroidal(d, x->cap_tor, false, s);
@@ -557,9 +563,15 @@ void enqueue_surface(cms_ctx* x, bool sized)
     launch_layout(d, (long long*)x->get<int>(cms_ctx::S_CM_TMP), tmp, s);
     mark(x, P_LAYOUT);
     if (sized) {
+        const long long cap0 = x->cap_dot;
         grow(x->cap_dot, read_ll(x, d.dot_off + 2LL * d.B));
         bind_caps(x);
         tmp = scan_tmp(x);
+        if (x->cap_dot != cap0) {
+            // the kept-candidate buffer may have moved: the emit passes recompute every unit
+            ck(cudaMemsetAsync(d.cv_soff, 0xff, sizeof(int) * d.N, s), "memset");
+            ck(cudaMemsetAsync(d.cc_soff, 0xff, sizeof(int) * x->cap_probe, s), "memset");
+        }
     }
     k_cap_check<<<1, 32, 0, s>>>(d.dot_off + 2LL * d.B, nullptr, x->cap_dot, d.ovf);
     launch_convex(d, true, s);

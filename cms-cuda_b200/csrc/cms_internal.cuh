@@ -106,6 +106,12 @@ struct Dev {
     int* tor_lflag; long long* tor_loff;         // tor_cap, +1: pair has dots, its exclusive scan
     int* tor_list;                               // tor_cap: pairs with dots, in pair order (emit work list)
     int* conc_cnt; long long* conc_off;          // probe_cap, +1
+    // kept candidates of the convex and concave count passes: (latitude << 16 | point) in candidate
+    // order per unit, so the emit passes write those alone; cv_soff / cc_soff: first entry (-1: none)
+    unsigned long long* ks_top;                  // 1: entries taken
+    int* ks_buf; long long ks_cap;               // ks_cap (= dot capacity)
+    int* cv_soff;                                // N
+    int* cc_soff;                                // probe_cap
     Seg* seg;                                    // B*8
     long long* dot_off;                          // B*2+1 (per complex & molecule)
     long long dot_cap;

@@ -74,6 +74,25 @@ __device__ __forceinline__ long long unit_base(const Dev& d, int c, int m, int t
     return s.dot0 + (unit_scan - s.scan0);
 }
 
+// Kept candidates of a unit: the count pass collects them in shared memory
+// (up to KS_CAP) and moves them to the kept-candidate buffer at the unit's
+// end; the emit pass then computes and writes those dots alone.  -1: not
+// stashed (too many, or the buffer is full), the emit pass tests every
+// candidate again.
+static constexpr int KS_CAP = 512;
+
+__device__ __forceinline__ int ks_stash(const Dev& d, const int* list, int kept)
+{
+    const int lane = threadIdx.x & 31;
+    if (kept <= 0 || kept > KS_CAP) return -1;
+    unsigned long long off = 0;
+    if (lane == 0) off = atomicAdd(d.ks_top, (unsigned long long)kept);
+    off = __shfl_sync(0xffffffffu, off, 0);
+    if (off + (unsigned long long)kept > (unsigned long long)d.ks_cap) return -1;
+    for (int e = lane; e < kept; e += 32) d.ks_buf[off + e] = list[e];
+    return (int)off;
+}
+
 // ---------------------------------------------------------------------------
 // convex dots: one warp per atom of the convex queue
 // ---------------------------------------------------------------------------
@@ -112,6 +131,7 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 5 : 6) k_convex(Dev d)
     CMS_EXIT_ON_OVERFLOW(d);
     __shared__ LatTable tab[CV_WARPS];
     __shared__ int ncs[CV_WARPS][CMS_MAX_SUBDIV];
+    __shared__ int ksl[EMIT ? 1 : CV_WARPS][KS_CAP];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     LatTable& L = tab[w];
@@ -189,6 +209,21 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 5 : 6) k_convex(Dev d)
         if (EMIT) base = unit_base(d, d.cplx[g], d.mol[g], 0, d.conv_off[g]);
         int kept = 0;
         const double scale = eri / ri;
+        if (EMIT) {
+            const int so = d.cv_soff[g];
+            if (so >= 0) {
+                // the count pass's kept candidates
+                const int cnt = d.conv_cnt[g];
+                for (int e = lane; e < cnt; e += 32) {
+                    const int sub = d.ks_buf[so + e];
+                    const int l = sub >> 16, i = sub & 0xffff;
+                    const V3 pt = subdiv_point(v3(L.cx[l], L.cy[l], L.cz[l]), L.rad[l], fx, fy, L.delta[l], i);
+                    write_dot(d, base + e, pt, xi + (pt - xi) * scale, L.area[l], g, 1, g, sub);
+                }
+                __syncwarp();
+                continue;
+            }
+        }
         for (int t0 = 0; t0 < total; t0 += 32) {
             const int t = t0 + lane;
             bool keep = false;
@@ -208,9 +243,14 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 5 : 6) k_convex(Dev d)
             }
             const unsigned m = __ballot_sync(0xffffffffu, keep);
             if (EMIT && keep) write_dot(d, base + kept + __popc(m & lt), pt, pcen, L.area[l], g, 1, g, (l << 16) | i);
+            if (!EMIT && keep && kept + __popc(m & lt) < KS_CAP) ksl[EMIT ? 0 : w][kept + __popc(m & lt)] = (l << 16) | i;
             kept += __popc(m);
         }
-        if (!EMIT && lane == 0) d.conv_cnt[g] = kept;
+        if (!EMIT) {
+            __syncwarp();
+            const int so = ks_stash(d, ksl[EMIT ? 0 : w], kept);
+            if (lane == 0) { d.conv_cnt[g] = kept; d.cv_soff[g] = so; }
+        }
         __syncwarp();
     }
 }
@@ -634,6 +674,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, EMIT ? 4 : 1) k_concave(Dev d)
     __shared__ LatTable tab[CC_WARPS];
     __shared__ int ncs[CC_WARPS][CMS_MAX_SUBDIV];
     __shared__ int nears[CC_WARPS][CMS_NEAR_CAP];
+    __shared__ int ksl[EMIT ? 1 : CC_WARPS][KS_CAP];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     LatTable& L = tab[w];
@@ -643,6 +684,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, EMIT ? 4 : 1) k_concave(Dev d)
     const long long nw = (long long)gridDim.x * CC_WARPS;
     for (long long p = wid; p < NP; p += nw) {
         if (EMIT && d.conc_cnt[p] == 0) continue;                      // no dots: nothing to write
+        const int so = EMIT ? d.cc_soff[p] : -1;                         // >= 0: the kept candidates are stashed
         const int ia[3] = {d.pa0[p], d.pa1[p], d.pa2[p]};
         V3 xa[3];
         double ra[3];
@@ -654,7 +696,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, EMIT ? 4 : 1) k_concave(Dev d)
         const int c = d.cplx[ia[0]];
         // nearby low probes of the same complex (d2 <= 4 rp^2), self excluded
         int nnear = 0;
-        if (low) {
+        if (low && so < 0) {
             const Cplx C = d.cx[c];
             const int s0 = C.a0, e1 = C.a0 + C.n;
             const long long pb = min(d.plus_off[s0] + d.minus_off[s0], d.probe_cap);
@@ -736,6 +778,27 @@ __global__ void __launch_bounds__(CC_WARPS * 32, EMIT ? 4 : 1) k_concave(Dev d)
             }
         }
         int kept = 0;
+        if (EMIT && so >= 0) {
+            const int cnt = d.conc_cnt[p];
+            for (int e = lane; e < cnt; e += 32) {
+                const int sub = d.ks_buf[so + e];
+                const int l = sub >> 16, i = sub & 0xffff;
+                const V3 pts = subdiv_point(v3(L.cx[l], L.cy[l], L.cz[l]), L.rad[l], fx, fy, L.delta[l], i) + pijk;
+                double dd[3];
+                for (int k = 0; k < 3; ++k) dd[k] = norm3(pts - xa[k]) - ra[k];
+                int mc = 0;                            // np.argmin: first minimum, NaN wins
+                if (!isnan(dd[0])) {
+                    for (int k = 1; k < 3; ++k) {
+                        if (isnan(dd[k])) { mc = k; break; }
+                        if (dd[k] < dd[mc]) mc = k;
+                    }
+                }
+                write_dot_b(d, base + e, pts, pijk, L.area[l], ia[mc], 3, (int)p, sub,
+                            mc == 0 ? bur3[0] : (mc == 1 ? bur3[1] : bur3[2]));
+            }
+            __syncwarp();
+            continue;
+        }
         for (int t0 = 0; t0 < total; t0 += 32) {
             const int t = t0 + lane;
             bool keep = false;
@@ -770,9 +833,14 @@ __global__ void __launch_bounds__(CC_WARPS * 32, EMIT ? 4 : 1) k_concave(Dev d)
             if (EMIT && keep)
                 write_dot_b(d, base + kept + __popc(m & lt), pts, pijk, L.area[l], ia[mc], 3, (int)p, (l << 16) | i,
                             mc == 0 ? bur3[0] : (mc == 1 ? bur3[1] : bur3[2]));
+            if (!EMIT && keep && kept + __popc(m & lt) < KS_CAP) ksl[EMIT ? 0 : w][kept + __popc(m & lt)] = (l << 16) | i;
             kept += __popc(m);
         }
-        if (!EMIT && lane == 0) d.conc_cnt[p] = kept;
+        if (!EMIT) {
+            __syncwarp();
+            const int sp = ks_stash(d, ksl[EMIT ? 0 : w], kept);
+            if (lane == 0) { d.conc_cnt[p] = kept; d.cc_soff[p] = sp; }
+        }
         __syncwarp();
     }
 }

@@ -233,8 +233,9 @@ def test_probe_stash_and_recompute_agree():
     """
     The triple count pass stashes its probes when they fit the capacity it
     ran with, and a scatter fills the probe arrays; otherwise (the first run
-    of a fresh context) the emit pass recomputes them.  Both give the same
-    probes, access flags and results.
+    of a fresh context) the emit pass recomputes them.  Likewise the convex
+    and concave count passes keep their accepted candidates for the emit
+    passes.  Both ways give the same probes, dots, access flags and results.
     """
     from cms_cuda import _lib
     names = ("golden_pkl", "synth_small_s7", "synth_zero_radii")
@@ -252,7 +253,8 @@ def test_probe_stash_and_recompute_agree():
         for c in range(len(names)):
             i = ctx.info(c)
             n = int(off[c + 1] - off[c])
-            out.append(ctx.export_probes(c, i) + ctx.export_atoms(c, n))
+            out.append(ctx.export_probes(c, i) + ctx.export_atoms(c, n) + ctx.export_dots(c, 0, i)
+                       + ctx.export_dots(c, 1, i))
         return out, ctx.contact_ms(per_atom=True)
 
     ctx.generate(all_atoms=False)          # capacities sized by this run: recomputed
