@@ -251,7 +251,7 @@ struct cms_ctx {
         S_ADJ_ACT_CONV, S_ADJ_ACT_TOR, S_ADJ_ACT_CONC, S_ADJ_ACT_ATOM, S_ADJ_LIST_CONV, S_ADJ_LIST_TOR,
         S_ADJ_LIST_CONC, S_ADJ_NACT, S_OVF, S_REF_XYZ, S_POSE, S_POSE_CKPT, S_POSE_CEN, S_HIST, S_STEP, S_MAXSUM,
         S_TOR_LFLAG, S_TOR_LOFF, S_TOR_LIST, S_PTOP, S_SP_A, S_SP_H, S_SP_XYZ, S_SP_ALT, S_SP_G, S_SP_ORD,
-        S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1, S_KS_TOP, S_KS_BUF, S_CV_SOFF, S_CC_SOFF,
+        S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1, S_KS_TOP, S_KS_BUF, S_CV_SOFF, S_CC_SOFF, S_TOR_SOFF, S_TOR_SN,
         S_COUNT
     };
 
@@ -381,6 +381,8 @@ void bind_caps(cms_ctx* x)
     d.tor2_off = x->ensure<long long>(cms_ctx::S_TOR2_OFF, x->cap_tor + 1);
     d.tor_has = x->ensure<int8_t>(cms_ctx::S_TOR_HAS, x->cap_tor);
     d.tor_lflag = x->ensure<int>(cms_ctx::S_TOR_LFLAG, x->cap_tor);
+    d.tor_soff = x->ensure<int>(cms_ctx::S_TOR_SOFF, x->cap_tor);
+    d.tor_sn = x->ensure<int>(cms_ctx::S_TOR_SN, x->cap_tor);
     d.tor_loff = x->ensure<long long>(cms_ctx::S_TOR_LOFF, x->cap_tor + 1);
     d.tor_list = x->ensure<int>(cms_ctx::S_TOR_LIST, x->cap_tor);
     d.probe_cap = x->cap_probe;
@@ -571,6 +573,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
             // the kept-candidate buffer may have moved: the emit passes recompute every unit
             ck(cudaMemsetAsync(d.cv_soff, 0xff, sizeof(int) * d.N, s), "memset");
             ck(cudaMemsetAsync(d.cc_soff, 0xff, sizeof(int) * x->cap_probe, s), "memset");
+            ck(cudaMemsetAsync(d.tor_soff, 0xff, sizeof(int) * x->cap_tor, s), "memset");
         }
     }
     k_cap_check<<<1, 32, 0, s>>>(d.dot_off + 2LL * d.B, nullptr, x->cap_dot, d.ovf);

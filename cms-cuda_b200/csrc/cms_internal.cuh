@@ -112,6 +112,7 @@ struct Dev {
     int* ks_buf; long long ks_cap;               // ks_cap (= dot capacity)
     int* cv_soff;                                // N
     int* cc_soff;                                // probe_cap
+    int* tor_soff; int* tor_sn;                  // tor_cap: kept torus points (those with arc dots) of a pair
     Seg* seg;                                    // B*8
     long long* dot_off;                          // B*2+1 (per complex & molecule)
     long long dot_cap;

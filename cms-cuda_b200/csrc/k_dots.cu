@@ -45,6 +45,25 @@ __device__ __forceinline__ int8_t buried_test(const Dev& d, int owner, V3 pcen)
     return 0;
 }
 
+// buried_test for one probe centre and up to three owners, the warp's lanes
+// spread over each owner's buried partners (same result: any partner within reach)
+__device__ __forceinline__ int8_t buried_warp(const Dev& d, int owner, V3 pcen)
+{
+    const int lane = threadIdx.x & 31;
+    const long long s = d.bu_off[owner], e = d.bu_off[owner + 1];
+    const double rp = d.st.rp;
+    for (long long b0 = s; b0 < e; b0 += 32) {
+        bool hit = false;
+        if (b0 + lane < e) {
+            const double4 b = d.xyzr[d.bu_id[b0 + lane]];
+            const double t = b.w + rp;
+            hit = sq_seq(v3(b.x, b.y, b.z) - pcen) <= t * t;
+        }
+        if (__any_sync(0xffffffffu, hit)) return 1;
+    }
+    return 0;
+}
+
 __device__ __forceinline__ void write_dot_b(const Dev& d, long long q, V3 pt, V3 pcen, double area, int owner,
                                             int type, int unit, int sub, int8_t bur)
 {
@@ -282,6 +301,7 @@ void launch_convex(const Dev& d, bool emit, cudaStream_t s)
 static constexpr int TO_WARPS = 4;
 static constexpr int TO_PAIRS = 16;   // toroid pairs per warp batch
 static constexpr int TO_POOL = 512;   // pruned atom ids per warp batch (past it: the full lists are scanned)
+static constexpr int TO_KEEP = 512;   // kept torus points per warp batch (past it: the batch is not kept)
 
 struct TorPair {
     int i, j;
@@ -532,7 +552,12 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
     __shared__ long long base[EMIT ? TO_WARPS : 1][2][TO_PAIRS];
     __shared__ TorArcS arcs[EMIT ? TO_WARPS : 1][32];
     __shared__ int arcx[EMIT ? TO_WARPS : 1][33];
+    // count: the batch's torus points with arc dots in (pair, point) order and their number per pair;
+    // emit: each pair's first kept point in the kept-candidate buffer
+    __shared__ int tpl[EMIT ? 1 : TO_WARPS][TO_KEEP];
+    __shared__ int spc[TO_WARPS][TO_PAIRS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int wc = EMIT ? 0 : w;
     const int we = EMIT ? w : 0;
     const double rp = d.st.rp;
     // count: every pair; emit: only the pairs with dots (the work list)
@@ -542,12 +567,19 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
         const long long q0 = bt * TO_PAIRS;
         const int np = (int)min((long long)TO_PAIRS, NT - q0);
         __syncwarp();
+        bool kok = true;                           // emit: the pair's torus points with arc dots were kept
         if (lane < np) {
             const long long q = EMIT ? (long long)d.tor_list[q0 + lane] : q0 + lane;
             const TorPair T = tor_pair(d, q);
             tp[w][lane] = T;
             tq[w][lane] = (int)q;
             nsv[w][lane] = T.ns;
+            spc[w][lane] = 0;
+            if (EMIT) {
+                spc[w][lane] = d.tor_soff[q];
+                kok = spc[w][lane] >= 0;
+                if (kok) nsv[w][lane] = d.tor_sn[q];
+            }
             run[w][0][lane] = 0; run[w][1][lane] = 0;
             hasf[w][lane] = 0;
             arcf[w][lane] = (unsigned char)((d.atten[T.i] >= 2 ? 1 : 0) | (d.atten[T.j] >= 2 ? 2 : 0));
@@ -557,16 +589,23 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
                 base[we][1][lane] = unit_base(d, c, m, 2, d.tor2_off[q]);
             }
         }
+        // emit with every pair's points kept: those points only, all free (no collision list)
+        const bool kept_pts = EMIT && __all_sync(0xffffffffu, kok);
+        if (EMIT && !kept_pts && lane < np) nsv[w][lane] = tp[w][lane].ns;
         __syncwarp();
         // pruned lists of the batch's pairs; a circle inside one neighbour's
         // sphere has no free point, so its pair takes no torus points
         int used = 0;
         for (int k = 0; k < np; ++k) {
             const TorPair& T = tp[w][k];
-            bool cov;
-            int c = tor_prune(d, T, d.nb_id, d.nb_off[T.i], d.nb_off[T.i] + d.nnb[T.i], T.j, pool[w] + used,
+            int c = 0;
+            if (!kept_pts) {
+                bool cov;
+                c = tor_prune(d, T, d.nb_id, d.nb_off[T.i], d.nb_off[T.i] + d.nnb[T.i], T.j, pool[w] + used,
                               TO_POOL - used, &cov);
-            if (lane == 0) { l_off[w][0][k] = used; l_cnt[w][0][k] = c; if (cov) nsv[w][k] = 0; }
+                if (lane == 0 && cov) nsv[w][k] = 0;
+            }
+            if (lane == 0) { l_off[w][0][k] = used; l_cnt[w][0][k] = c; }
             if (c > 0) used += c;
             if (EMIT) {
                 const int af = arcf[w][k];
@@ -587,6 +626,7 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
         if (lane == 0) pst[w][np] = tot;
         __syncwarp();
         // torus points, 32 at a time; lanes of one pair are contiguous
+        int tn = 0;                                // count: kept torus points of the batch
         for (int c0 = 0; c0 < tot; c0 += 32) {
             const int g = c0 + lane;
             const bool on = g < tot;
@@ -600,7 +640,7 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
                 k = lo;
             }
             const TorPair& T = tp[w][k];
-            const int s = on ? g - pst[w][k] : 0;
+            const int s = !on ? 0 : (kept_pts ? d.ks_buf[spc[w][k] + (g - pst[w][k])] : g - pst[w][k]);
             int c1 = 0, c2 = 0;
             bool valid = false, fast = true;
             TorPoint P;
@@ -622,6 +662,12 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
             const int e1 = warp_excl_scan(c1, t1), e2 = warp_excl_scan(c2, t2);
             const int f1 = __shfl_sync(0xffffffffu, e1, first), f2 = __shfl_sync(0xffffffffu, e2, first);
             const unsigned vm = __ballot_sync(0xffffffffu, valid);
+            const unsigned km = __ballot_sync(0xffffffffu, on && c1 + c2 > 0);
+            if (!EMIT) {
+                if (on && c1 + c2 > 0 && tn + __popc(km & ((1u << lane) - 1u)) < TO_KEEP)
+                    tpl[wc][tn + __popc(km & ((1u << lane) - 1u))] = s;
+                tn += __popc(km);
+            }
             if (EMIT) {
                 const long long pos1 = on ? base[we][0][k] + run[w][0][k] + (e1 - f1) : 0;
                 const long long pos2 = on ? base[we][1][k] + run[w][1][k] + (e2 - f2) : 0;
@@ -644,8 +690,28 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
                 run[w][1][k] += (e2 + c2) - f2;
                 const unsigned seg = ((2u << lane) - 1u) & ~((1u << first) - 1u);
                 if (vm & seg) hasf[w][k] = 1;
+                if (!EMIT) spc[w][k] += __popc(km & seg);
             }
             __syncwarp();
+        }
+        if (!EMIT) {
+            // keep the batch's torus points with arc dots for the emit pass
+            long long koff = -1;
+            if (tn > 0 && tn <= TO_KEEP) {
+                unsigned long long o = 0;
+                if (lane == 0) o = atomicAdd(d.ks_top, (unsigned long long)tn);
+                o = __shfl_sync(0xffffffffu, o, 0);
+                if (o + (unsigned long long)tn <= (unsigned long long)d.ks_cap) {
+                    for (int e = lane; e < tn; e += 32) d.ks_buf[o + e] = tpl[wc][e];
+                    koff = (long long)o;
+                }
+            }
+            int kt;
+            const int kx = warp_excl_scan(lane < np ? spc[w][lane] : 0, kt);
+            if (lane < np) {
+                d.tor_sn[q0 + lane] = spc[w][lane];
+                d.tor_soff[q0 + lane] = koff >= 0 ? (int)(koff + kx) : -1;
+            }
         }
         if (!EMIT && lane < np) {
             d.tor1_cnt[q0 + lane] = run[w][0][lane];
@@ -772,9 +838,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, EMIT ? 4 : 1) k_concave(Dev d)
         if (EMIT) {
             base = unit_base(d, c, d.mol[ia[0]], 3, d.conc_off[p]);
             if (d.conc_cnt[p] > 0) {
-                int8_t bk = 0;
-                if (lane < 3) bk = buried_test(d, lane == 0 ? ia[0] : (lane == 1 ? ia[1] : ia[2]), pijk);
-                for (int k = 0; k < 3; ++k) bur3[k] = (int8_t)__shfl_sync(0xffffffffu, (int)bk, k);
+                for (int k = 0; k < 3; ++k) bur3[k] = buried_warp(d, ia[k], pijk);
             }
         }
         int kept = 0;
