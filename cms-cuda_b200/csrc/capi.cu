@@ -251,7 +251,7 @@ struct cms_ctx {
         S_ADJ_ACT_CONV, S_ADJ_ACT_TOR, S_ADJ_ACT_CONC, S_ADJ_ACT_ATOM, S_ADJ_LIST_CONV, S_ADJ_LIST_TOR,
         S_ADJ_LIST_CONC, S_ADJ_NACT, S_OVF, S_REF_XYZ, S_POSE, S_POSE_CKPT, S_POSE_CEN, S_HIST, S_STEP, S_MAXSUM,
         S_TOR_LFLAG, S_TOR_LOFF, S_TOR_LIST, S_PTOP, S_SP_A, S_SP_H, S_SP_XYZ, S_SP_ALT, S_SP_G, S_SP_ORD,
-        S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1, S_KS_TOP, S_KS_BUF, S_CV_SOFF, S_CC_SOFF, S_TOR_SOFF, S_TOR_SN,
+        S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1, S_KS_TOP, S_KS_BUF, S_CV_SOFF, S_CC_SOFF, S_TOR_SOFF, S_TOR_SN, S_NBS_TOP, S_NBS_BUF, S_NB_SOFF,
         S_COUNT
     };
 
@@ -326,6 +326,8 @@ void bind_batch(cms_ctx* x)
     d.nnb = x->ensure<int>(cms_ctx::S_NNB, N);
     d.ovf = x->ensure<int>(cms_ctx::S_OVF, 1);
     d.nb_off = x->ensure<long long>(cms_ctx::S_NB_OFF, N + 1);
+    d.nb_soff = x->ensure<long long>(cms_ctx::S_NB_SOFF, N);
+    d.nbs_top = x->ensure<unsigned long long>(cms_ctx::S_NBS_TOP, 1);
     d.nbur = x->ensure<int>(cms_ctx::S_NBUR, N);
     d.bu_off = x->ensure<long long>(cms_ctx::S_BU_OFF, N + 1);
     d.ntor = x->ensure<int>(cms_ctx::S_NTOR, N);
@@ -372,6 +374,8 @@ void bind_caps(cms_ctx* x)
     d.nb_tmp = x->ensure<int>(cms_ctx::S_NB_TMP, x->cap_nb);
     d.nb_d2 = x->ensure<double>(cms_ctx::S_NB_D2, x->cap_nb);
     d.bu_id = x->ensure<int>(cms_ctx::S_BU_ID, x->cap_bu);
+    d.nbs_cap = x->cap_nb + x->cap_bu;
+    d.nbs_buf = x->ensure<int>(cms_ctx::S_NBS_BUF, d.nbs_cap);
     d.tor_cap = x->cap_tor;
     d.tor_i = x->ensure<int>(cms_ctx::S_TOR_I, x->cap_tor);
     d.tor_j = x->ensure<int>(cms_ctx::S_TOR_J, x->cap_tor);
@@ -505,15 +509,20 @@ void enqueue_surface(cms_ctx* x, bool sized)
     mark(x, P_CELLS);
     launch_attention(d, s);
     mark(x, P_ATTENTION);
+    ck(cudaMemsetAsync(d.nbs_top, 0, sizeof(unsigned long long), s), "memset");
     launch_neighbor_count(d, s);
     scan_counts(d.nnb, d.nb_off, d.N, tmp, s);
     scan_counts(d.nbur, d.bu_off, d.N, tmp, s);
     mark(x, P_NB_COUNT);
     if (sized) {
+        const long long nb0 = x->cap_nb, bu0 = x->cap_bu;
         grow(x->cap_nb, read_ll(x, d.nb_off + d.N));
         grow(x->cap_bu, read_ll(x, d.bu_off + d.N));
         bind_caps(x);
         tmp = scan_tmp(x);
+        // the sorted-row buffer may have moved: the emit pass gathers every row again
+        if (x->cap_nb != nb0 || x->cap_bu != bu0)
+            ck(cudaMemsetAsync(d.nb_soff, 0xff, sizeof(long long) * d.N, s), "memset");
     }
     k_cap_check<<<1, 32, 0, s>>>(d.nb_off + d.N, nullptr, x->cap_nb, d.ovf);
     k_cap_check<<<1, 32, 0, s>>>(d.bu_off + d.N, nullptr, x->cap_bu, d.ovf);

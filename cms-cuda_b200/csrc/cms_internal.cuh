@@ -113,6 +113,11 @@ struct Dev {
     int* cv_soff;                                // N
     int* cc_soff;                                // probe_cap
     int* tor_soff; int* tor_sn;                  // tor_cap: kept torus points (those with arc dots) of a pair
+    // neighbour rows sorted by the count pass: per atom its neighbours then its buried partners, in
+    // the final order; nb_soff: the atom's first entry (-1: not kept, the emit pass gathers them again)
+    unsigned long long* nbs_top;                 // 1: entries taken
+    int* nbs_buf; long long nbs_cap;             // nbs_cap (= neighbour + buried-partner capacity)
+    long long* nb_soff;                          // N
     Seg* seg;                                    // B*8
     long long* dot_off;                          // B*2+1 (per complex & molecule)
     long long dot_cap;
@@ -127,6 +132,29 @@ struct Dev {
 __device__ __forceinline__ V3 atom_xyz(const Dev& d, int g) { double4 a = d.xyzr[g]; return v3(a.x, a.y, a.z); }
 
 // grid helpers
+// Warp-local bump allocation from a buffer shared by all warps: a warp takes
+// STASH_CHUNK entries (or more, for one large request) from the global counter
+// at a time and hands them out to its successive units, so the counter sees
+// one atomic per chunk instead of one per unit.  A chunk's unused tail is left
+// empty.  Returns -1 when the entries would pass the buffer's capacity.
+static constexpr int STASH_CHUNK = 1024;
+struct StashCursor { unsigned long long cur, end; };
+
+__device__ __forceinline__ long long stash_take(unsigned long long* top, long long cap, StashCursor& c, int n)
+{
+    if (c.cur + (unsigned long long)n > c.end) {
+        const unsigned long long want = n > STASH_CHUNK ? (unsigned long long)n : (unsigned long long)STASH_CHUNK;
+        unsigned long long o = 0;
+        if ((threadIdx.x & 31) == 0) o = atomicAdd(top, want);
+        o = __shfl_sync(0xffffffffu, o, 0);
+        c.cur = o;
+        c.end = o + want;
+    }
+    const unsigned long long r = c.cur;
+    c.cur += (unsigned long long)n;
+    return r + (unsigned long long)n <= (unsigned long long)cap ? (long long)r : -1;
+}
+
 // Graph-mode runs use fixed capacities; when a stage's total exceeds its
 // capacity the run is flagged (and redone by the host), and every later
 // pipeline kernel returns at entry so nothing indexes past a capacity.

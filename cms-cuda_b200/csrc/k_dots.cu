@@ -100,14 +100,12 @@ __device__ __forceinline__ long long unit_base(const Dev& d, int c, int m, int t
 // candidate again.
 static constexpr int KS_CAP = 512;
 
-__device__ __forceinline__ int ks_stash(const Dev& d, const int* list, int kept)
+__device__ __forceinline__ int ks_stash(const Dev& d, const int* list, int kept, StashCursor& cur)
 {
     const int lane = threadIdx.x & 31;
     if (kept <= 0 || kept > KS_CAP) return -1;
-    unsigned long long off = 0;
-    if (lane == 0) off = atomicAdd(d.ks_top, (unsigned long long)kept);
-    off = __shfl_sync(0xffffffffu, off, 0);
-    if (off + (unsigned long long)kept > (unsigned long long)d.ks_cap) return -1;
+    const long long off = stash_take(d.ks_top, d.ks_cap, cur, kept);
+    if (off < 0) return -1;
     for (int e = lane; e < kept; e += 32) d.ks_buf[off + e] = list[e];
     return (int)off;
 }
@@ -154,6 +152,7 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 5 : 6) k_convex(Dev d)
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     LatTable& L = tab[w];
+    StashCursor kcur{0, 0};
     const double rp = d.st.rp;
     const long long wid = blockIdx.x * (long long)CV_WARPS + w;
     const long long nw = (long long)gridDim.x * CV_WARPS;
@@ -267,7 +266,7 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 5 : 6) k_convex(Dev d)
         }
         if (!EMIT) {
             __syncwarp();
-            const int so = ks_stash(d, ksl[EMIT ? 0 : w], kept);
+            const int so = ks_stash(d, ksl[EMIT ? 0 : w], kept, kcur);
             if (lane == 0) { d.conv_cnt[g] = kept; d.cv_soff[g] = so; }
         }
         __syncwarp();
@@ -558,6 +557,7 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
     __shared__ int spc[TO_WARPS][TO_PAIRS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int wc = EMIT ? 0 : w;
+    StashCursor kcur{0, 0};
     const int we = EMIT ? w : 0;
     const double rp = d.st.rp;
     // count: every pair; emit: only the pairs with dots (the work list)
@@ -698,12 +698,10 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
             // keep the batch's torus points with arc dots for the emit pass
             long long koff = -1;
             if (tn > 0 && tn <= TO_KEEP) {
-                unsigned long long o = 0;
-                if (lane == 0) o = atomicAdd(d.ks_top, (unsigned long long)tn);
-                o = __shfl_sync(0xffffffffu, o, 0);
-                if (o + (unsigned long long)tn <= (unsigned long long)d.ks_cap) {
+                const long long o = stash_take(d.ks_top, d.ks_cap, kcur, tn);
+                if (o >= 0) {
                     for (int e = lane; e < tn; e += 32) d.ks_buf[o + e] = tpl[wc][e];
-                    koff = (long long)o;
+                    koff = o;
                 }
             }
             int kt;
@@ -744,6 +742,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, EMIT ? 4 : 1) k_concave(Dev d)
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     LatTable& L = tab[w];
+    StashCursor kcur{0, 0};
     const double rp = d.st.rp, rp2 = rp * rp;
     const long long NP = min(d.plus_off[d.N] + d.minus_off[d.N], d.probe_cap);
     const long long wid = blockIdx.x * (long long)CC_WARPS + w;
@@ -902,7 +901,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, EMIT ? 4 : 1) k_concave(Dev d)
         }
         if (!EMIT) {
             __syncwarp();
-            const int sp = ks_stash(d, ksl[EMIT ? 0 : w], kept);
+            const int sp = ks_stash(d, ksl[EMIT ? 0 : w], kept, kcur);
             if (lane == 0) { d.conc_cnt[p] = kept; d.cc_soff[p] = sp; }
         }
         __syncwarp();

@@ -347,9 +347,13 @@ __global__ void __launch_bounds__(NB_WARPS * 32) k_nb_count(Dev d)
 {
     CMS_EXIT_ON_OVERFLOW(d);
     __shared__ BallScratch sc[NB_WARPS];
+    __shared__ int sid[NB_WARPS][NB_CAP];
+    __shared__ int sbid[NB_WARPS][NB_CAP];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
     const long long wid = blockIdx.x * (long long)NB_WARPS + w;
     const long long nw = (long long)gridDim.x * NB_WARPS;
+    StashCursor ncur{0, 0};
     for (long long gg = wid; gg < d.N; gg += nw) {
         const int g = (int)gg;
         const int c = d.cplx[g];
@@ -360,19 +364,35 @@ __global__ void __launch_bounds__(NB_WARPS * 32) k_nb_count(Dev d)
         scan_ball(d, g, c, nb_range(d, c, ai.w), sc[w], [&](int j) {
             bool is_nb, is_bur, coin; double d2;
             classify(d, g, xi, ai.w, mi, j, is_nb, is_bur, coin, d2);
-            nn += __popc(__ballot_sync(0xffffffffu, is_nb));
-            nb += __popc(__ballot_sync(0xffffffffu, is_bur));
+            const unsigned m = __ballot_sync(0xffffffffu, is_nb);
+            if (is_nb && nn + __popc(m & lt) < NB_CAP) sid[w][nn + __popc(m & lt)] = j;
+            nn += __popc(m);
+            const unsigned mb = __ballot_sync(0xffffffffu, is_bur);
+            if (is_bur && nb + __popc(mb & lt) < NB_CAP) sbid[w][nb + __popc(mb & lt)] = j;
+            nb += __popc(mb);
             if (coin) {
                 const int a0 = d.cx[c].a0;
                 unsigned long long key = ((unsigned long long)(g - a0) << 32) | (unsigned)(j - a0);
                 atomicMin(&d.coin[c], key);
             }
         });
+        __syncwarp();
+        // keep the rows (unsorted) for the emit pass
+        long long so = -1;
+        if (nn <= NB_CAP && nb <= NB_CAP && nn + nb > 0) {
+            so = stash_take(d.nbs_top, d.nbs_cap, ncur, nn + nb);
+            if (so >= 0) {
+                for (int e = lane; e < nn; e += 32) d.nbs_buf[so + e] = sid[w][e];
+                for (int e = lane; e < nb; e += 32) d.nbs_buf[so + nn + e] = sbid[w][e];
+            }
+        }
         if (lane == 0) {
             d.nnb[g] = nn;
             d.nbur[g] = nb;
             d.access[g] = nn == 0 ? 1 : 0;
+            d.nb_soff[g] = so;
         }
+        __syncwarp();
     }
 }
 
@@ -409,29 +429,41 @@ __global__ void __launch_bounds__(NB_WARPS * 32) k_nb_emit(Dev d, int* __restric
             continue;
         }
         const bool in_sh = K <= NB_CAP, b_sh = KB <= NB_CAP;
-        int cnt = 0, bcnt = 0;
-        scan_ball(d, g, c, nb_range(d, c, ai.w), sc[w], [&](int j) {
-            bool is_nb, is_bur, coin; double d2;
-            classify(d, g, xi, ai.w, mi, j, is_nb, is_bur, coin, d2);
-            const unsigned m = __ballot_sync(0xffffffffu, is_nb);
-            if (is_nb) {
-                const int pos = cnt + __popc(m & lt);
-                if (pos < K) {
-                    if (in_sh) { sd2[w][pos] = d2; sid[w][pos] = j; }
-                    else { d.nb_d2[off + pos] = d2; tmp_id[off + pos] = j; }
-                }
+        const long long so = d.nb_soff[g];
+        if (so >= 0) {
+            // the count pass's rows (both fit the shared arrays); d2 as classify computes it
+            for (int e = lane; e < K; e += 32) {
+                const int j = d.nbs_buf[so + e];
+                const double4 aj = d.xyzr[j];
+                sd2[w][e] = sq_seq(xi - v3(aj.x, aj.y, aj.z));
+                sid[w][e] = j;
             }
-            cnt += __popc(m);
-            const unsigned mb = __ballot_sync(0xffffffffu, is_bur);
-            if (is_bur) {
-                const int pos = bcnt + __popc(mb & lt);
-                if (pos < KB) {
-                    if (b_sh) sbid[w][pos] = j;
-                    else d.bu_id[boff + pos] = j;
+            for (int e = lane; e < KB; e += 32) sbid[w][e] = d.nbs_buf[so + K + e];
+        } else {
+            int cnt = 0, bcnt = 0;
+            scan_ball(d, g, c, nb_range(d, c, ai.w), sc[w], [&](int j) {
+                bool is_nb, is_bur, coin; double d2;
+                classify(d, g, xi, ai.w, mi, j, is_nb, is_bur, coin, d2);
+                const unsigned m = __ballot_sync(0xffffffffu, is_nb);
+                if (is_nb) {
+                    const int pos = cnt + __popc(m & lt);
+                    if (pos < K) {
+                        if (in_sh) { sd2[w][pos] = d2; sid[w][pos] = j; }
+                        else { d.nb_d2[off + pos] = d2; tmp_id[off + pos] = j; }
+                    }
                 }
-            }
-            bcnt += __popc(mb);
-        });
+                cnt += __popc(m);
+                const unsigned mb = __ballot_sync(0xffffffffu, is_bur);
+                if (is_bur) {
+                    const int pos = bcnt + __popc(mb & lt);
+                    if (pos < KB) {
+                        if (b_sh) sbid[w][pos] = j;
+                        else d.bu_id[boff + pos] = j;
+                    }
+                }
+                bcnt += __popc(mb);
+            });
+        }
         __syncwarp();
         for (int e = lane; e < K; e += 32) {
             const double ke = in_sh ? sd2[w][e] : d.nb_d2[off + e];

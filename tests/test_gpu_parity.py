@@ -234,8 +234,10 @@ def test_probe_stash_and_recompute_agree():
     The triple count pass stashes its probes when they fit the capacity it
     ran with, and a scatter fills the probe arrays; otherwise (the first run
     of a fresh context) the emit pass recomputes them.  Likewise the convex
-    and concave count passes keep their accepted candidates for the emit
-    passes.  Both ways give the same probes, dots, access flags and results.
+    and concave count passes keep their accepted candidates, the toroidal
+    count pass its torus points with arc dots and the neighbour count pass
+    its sorted rows for the emit passes.  Both ways give the same neighbour
+    lists, probes, dots, access flags and results.
     """
     from cms_cuda import _lib
     names = ("golden_pkl", "synth_small_s7", "synth_zero_radii")
@@ -254,7 +256,7 @@ def test_probe_stash_and_recompute_agree():
             i = ctx.info(c)
             n = int(off[c + 1] - off[c])
             out.append(ctx.export_probes(c, i) + ctx.export_atoms(c, n) + ctx.export_dots(c, 0, i)
-                       + ctx.export_dots(c, 1, i))
+                       + ctx.export_dots(c, 1, i) + ctx.export_neighbors(c, n, i))
         return out, ctx.contact_ms(per_atom=True)
 
     ctx.generate(all_atoms=False)          # capacities sized by this run: recomputed
