@@ -244,6 +244,10 @@ def stage_traffic(name, totals, work):
     return None if n is None else per * n
 
 
+# when no measured peaks file is present: an earlier STREAM-style copy on this GPU pool
+FALLBACK_HBM_GBS = 6650.0
+
+
 def stage_roofline(stages, work, totals, peaks, fp32_peak):
     """Roofline of the most expensive stage: the nearest-dot search against the
     measured FP32 throughput (8 FLOP per pair), a surface stage against the
@@ -257,13 +261,16 @@ def stage_roofline(stages, work, totals, peaks, fp32_peak):
                 "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": stage_traffic(name, totals, work), "ms": ms,
                 "peak_source": "measured FP32 FMA throughput of this GPU (cms_fp32_peak, in this run)"}
     hbm = peaks.get("hbm_gbs")
+    source = "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    if not hbm:
+        hbm, source = FALLBACK_HBM_GBS, "fallback copy bandwidth of this GPU pool, 6.65 TB/s (of fallback)"
     nbytes = stage_bytes(name, totals, work)
     achieved = nbytes / (ms * 1e-3) / 1e9 if nbytes is not None else None
     return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": (achieved / hbm) if (achieved is not None and hbm) else None,
+            "frac": (achieved / hbm) if achieved is not None else None,
             "traffic": stage_traffic(name, totals, work), "ms": ms,
             "algorithmic_bytes": nbytes,
-            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if hbm else None,
+            "peak_source": source,
             "note": "FP64 geometry: the stage is bound by FP64 issue latency, not HBM (ncu summaries under profiles/)"}
 
 

@@ -599,6 +599,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
 void enqueue_split(cms_ctx* x)
 {
     launch_split_buried(x->d, x->r, x->cap_dot, scan_tmp(x), x->stream);
+    launch_spatial_order(x->d, x->r, SO_BUR, 0, x->stream);   // the CMS and band searches' lists
     mark(x, P_SPLIT);
 }
 
@@ -629,7 +630,6 @@ void enqueue_cms(cms_ctx* x)
     NNTask* task = x->get<NNTask>(cms_ctx::S_TASKS);
     launch_tasks(d, r, 0, task, s);
     k_fill_d<<<grid1(x->cap_dot), 256, 0, s>>>(r.nn_d2, x->cap_dot, INFINITY);
-    launch_spatial_order(d, r, SO_BUR, 0, s);
     NNArgs a = nn_args(x, 0);
     a.q_f4 = r.so_f4[0]; a.q_perm = r.so_perm[0]; a.q_idx = r.bur_idx;
     a.r_f4 = r.so_f4[0]; a.r_perm = r.so_perm[0]; a.r_idx = r.bur_idx;
@@ -652,7 +652,6 @@ void enqueue_sc(cms_ctx* x)
     long long* tmp = scan_tmp(x);
     NNTask* task = x->get<NNTask>(cms_ctx::S_TASKS);
     launch_tasks(d, r, 1, task + 2 * x->B, s);
-    launch_spatial_order(d, r, SO_BUR, 0, s);
     launch_spatial_order(d, r, SO_ACC, 1, s);
     NNArgs a = nn_args(x, 1);
     a.q_f4 = r.so_f4[0]; a.q_perm = r.so_perm[0]; a.q_idx = r.bur_idx;
@@ -666,10 +665,10 @@ void enqueue_sc(cms_ctx* x)
     launch_tasks(d, r, 2, task + 4 * x->B, s);
     k_fill_d<<<grid1(x->cap_dot), 256, 0, s>>>(r.nn_d2, x->cap_dot, INFINITY);
     k_fill_i<<<grid1(x->cap_dot), 256, 0, s>>>(r.nn_idx, x->cap_dot, -1);
-    launch_spatial_order(d, r, SO_TRIM, 0, s);
+    launch_spatial_order(d, r, SO_TRIM, 1, s);        // the accessible list is no longer needed
     NNArgs b = nn_args(x, 2);
-    b.q_f4 = r.so_f4[0]; b.q_perm = r.so_perm[0]; b.q_idx = r.trim_idx;
-    b.r_f4 = r.so_f4[0]; b.r_perm = r.so_perm[0]; b.r_idx = r.trim_idx;
+    b.q_f4 = r.so_f4[1]; b.q_perm = r.so_perm[1]; b.q_idx = r.trim_idx;
+    b.r_f4 = r.so_f4[1]; b.r_perm = r.so_perm[1]; b.r_idx = r.trim_idx;
     b.q_xyz = b.r_xyz = d.dxyz;
     b.out_d2 = r.nn_d2; b.out_idx = r.nn_idx;
     launch_nn(b, NN_ARGMIN, x->nn_var[2], tile_cap(x), tmp, s);

@@ -58,8 +58,8 @@ struct Rd {
     int* trim_idx; float4* trim_f4;             // trimmed dots
     double* nn_d2; int* nn_idx;                 // per query entry
     double* val; int* own;                      // per entry value / owner atom (-1: none)
-    // spatially ordered copies (k_readout.cu) of a query list (buried or trimmed dots) and of the
-    // accessible list: points and each entry's original position
+    // spatially ordered copies (k_readout.cu) of the buried list (set 0, made with the lists) and of
+    // the accessible, then the trimmed list (set 1): points and each entry's original position
     float4* so_f4[2]; int* so_perm[2];
 };
 

@@ -340,13 +340,16 @@ struct SeedPlain {
     }
 };
 
+// A lane's NT tangents: coordinates [NT k, NT k + NT) of the unit's atoms
+// (x, y, z of atom slot 0, then of slot 1, ...)
+template <int NT>
 struct SeedLane {
     int k;
-    __device__ TV3<Dn<1>> atom(const Dev& d, int a, int slot) const
+    __device__ TV3<Dn<NT>> atom(const Dev& d, int a, int slot) const
     {
         const double4 x = d.xyzr[a];
-        return tv3<Dn<1>>(dn_var<1>(x.x, k == 3 * slot ? 0 : -1), dn_var<1>(x.y, k == 3 * slot + 1 ? 0 : -1),
-                          dn_var<1>(x.z, k == 3 * slot + 2 ? 0 : -1));
+        const int b = 3 * slot - NT * k;         // tangent index of this atom's x coordinate
+        return tv3<Dn<NT>>(dn_var<NT>(x.x, b), dn_var<NT>(x.y, b + 1), dn_var<NT>(x.z, b + 2));
     }
 };
 
@@ -570,29 +573,35 @@ __global__ void k_adj_collect(Dev d, AdjBuf a)
 
 // pass 3: per active unit, one lane per coordinate of its atoms (K lanes);
 // lane k accumulates sum over the unit's dots of A . d(dot)/d(coordinate k)
+template <int NT>
 struct AdjLaneF {
     const double4* A;
-    double g;
+    double g[NT];
     __device__ bool want(long long q) const
     {
         const double4 v = A[q];
         return v.x != 0.0 || v.y != 0.0 || v.z != 0.0 || v.w != 0.0;
     }
-    __device__ void take(long long q, const DotV<Dn<1>>& D)
+    __device__ void take(long long q, const DotV<Dn<NT>>& D)
     {
         const double4 v = A[q];
-        g += ((v.x * D.p.x.d[0] + v.y * D.p.y.d[0]) + v.z * D.p.z.d[0]) + v.w * D.area.d[0];
+#pragma unroll
+        for (int t = 0; t < NT; ++t)
+            g[t] += ((v.x * D.p.x.d[t] + v.y * D.p.y.d[t]) + v.z * D.p.z.d[t]) + v.w * D.area.d[t];
     }
 };
 
-template <int KIND>
+// One active unit per group of K / NT lanes, each lane carrying NT of the
+// unit's K coordinates as dual-number tangents through the unit's geometry.
+template <int KIND, int NT>
 __global__ void k_adj_units(Dev d, AdjBuf a)
 {
     CMS_EXIT_ON_OVERFLOW(d);
     constexpr int K = KIND == 2 ? 9 : 6;       // coordinates of the unit's atoms
-    constexpr int G = 32 / K;                  // units per warp
+    constexpr int L = K / NT;                  // lanes per unit
+    constexpr int G = 32 / L;                  // units per warp
     const int lane = threadIdx.x & 31;
-    const int grp = lane / K, k = lane % K;
+    const int grp = lane / L, k = lane % L;
     const int* list = KIND == 0 ? a.list_conv : (KIND == 1 ? a.list_tor : a.list_conc);
     const long long n = a.nact[KIND];
     const long long wid = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
@@ -601,21 +610,27 @@ __global__ void k_adj_units(Dev d, AdjBuf a)
         const long long e = base + grp;
         if (grp >= G || e >= n) continue;
         const int u = list[e];
-        AdjLaneF f{a.A, 0.0};
-        const SeedLane seed{k};
+        AdjLaneF<NT> f;
+        f.A = a.A;
+#pragma unroll
+        for (int t = 0; t < NT; ++t) f.g[t] = 0.0;
+        const SeedLane<NT> seed{k};
+        double* out;
         if (KIND == 0) {
-            convex_unit_dots<Dn<1>>(d, u, seed, f);
-            a.gconv[6LL * u + k] = f.g;
+            convex_unit_dots<Dn<NT>>(d, u, seed, f);
+            out = a.gconv + 6LL * u;
             if (k == 0) { a.act_atom[u] = 1; a.act_atom[d.nb_id[d.nb_off[u]]] = 1; }
         } else if (KIND == 1) {
-            tor_unit_dots<Dn<1>>(d, u, seed, f);
-            a.gtor[6LL * u + k] = f.g;
+            tor_unit_dots<Dn<NT>>(d, u, seed, f);
+            out = a.gtor + 6LL * u;
             if (k == 0) { a.act_atom[d.tor_i[u]] = 1; a.act_atom[d.tor_j[u]] = 1; }
         } else {
-            conc_unit_dots<Dn<1>>(d, u, seed, f);
-            a.gconc[9LL * u + k] = f.g;
+            conc_unit_dots<Dn<NT>>(d, u, seed, f);
+            out = a.gconc + 9LL * u;
             if (k == 0) { a.act_atom[d.pa0[u]] = 1; a.act_atom[d.pa1[u]] = 1; a.act_atom[d.pa2[u]] = 1; }
         }
+#pragma unroll
+        for (int t = 0; t < NT; ++t) out[NT * k + t] = f.g[t];
     }
 }
 
@@ -730,9 +745,10 @@ void launch_adjoint(const Dev& d, const Rd& r, const AdjBuf& a, const NNTask* cm
     k_adj_ref_fill<<<grid_adj(D, 256), 256, 0, s>>>(d, r, a);
     k_adj_ref_sum<<<grid_adj(D, 256), 256, 0, s>>>(d, r, a);
     k_adj_collect<<<grid_adj((long long)d.N + d.tor_cap + d.probe_cap, 256), 256, 0, s>>>(d, a);
-    k_adj_units<0><<<grid_adj(d.N, 128), 128, 0, s>>>(d, a);
-    k_adj_units<1><<<grid_adj(d.tor_cap, 128), 128, 0, s>>>(d, a);
-    k_adj_units<2><<<grid_adj(d.probe_cap, 128), 128, 0, s>>>(d, a);
+    // convex and concave units: one lane per atom (3 tangents); toroidal units: one lane per coordinate
+    k_adj_units<0, 3><<<grid_adj(d.N, 128), 128, 0, s>>>(d, a);
+    k_adj_units<1, 1><<<grid_adj(d.tor_cap, 128), 128, 0, s>>>(d, a);
+    k_adj_units<2, 3><<<grid_adj(d.probe_cap, 128), 128, 0, s>>>(d, a);
     k_adj_gather<<<grid_adj(d.N, 128), 128, 0, s>>>(d, a, grad);
 }
 

@@ -874,12 +874,21 @@ __device__ __forceinline__ void so_range(const Dev& d, const Rd& r, int list, lo
     else { s = r.trim_scan[r.bur_scan[ds]]; e = r.trim_scan[r.bur_scan[de]]; }
 }
 
-__global__ void __launch_bounds__(32) k_spatial_order(Dev d, Rd r, int list, int set)
+static constexpr int SO_W = 4;                               // warps per range
+static constexpr int SO_STRIDE = SO_CELLS + SO_CELLS / 128;   // padded cell counters of one warp
+
+// One CTA per range: the warps take a quarter of the range each, count its
+// cells, and after a scan over (cell, warp) place its entries in list order,
+// so the order is stable across the whole range.
+__global__ void __launch_bounds__(SO_W * 32) k_spatial_order(Dev d, Rd r, int list, int set)
 {
     CMS_EXIT_ON_OVERFLOW(d);
-    __shared__ int cnt[SO_CELLS + SO_CELLS / 128];
-    const int lane = threadIdx.x;
+    extern __shared__ int so_cnt[];            // SO_W x SO_STRIDE cell counters
+    __shared__ float sbox[SO_W][6];
+    __shared__ int swarp[SO_W];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, tid = threadIdx.x;
     const unsigned lt = (1u << lane) - 1u;
+    int* cnt = so_cnt + w * SO_STRIDE;
     const float4* f4 = list == SO_BUR ? r.bur_f4 : (list == SO_ACC ? r.acc_f4 : r.trim_f4);
     float4* of4 = r.so_f4[set];
     int* operm = r.so_perm[set];
@@ -888,18 +897,25 @@ __global__ void __launch_bounds__(32) k_spatial_order(Dev d, Rd r, int list, int
         so_range(d, r, list, t, s, e);
         const long long n = e - s;
         if (n <= 0) continue;
+        // bounding box of the range
         float l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};
-        for (long long i = lane; i < n; i += 32) {
+        for (long long i = tid; i < n; i += SO_W * 32) {
             const float4 p = f4[s + i];
             l[0] = fminf(l[0], p.x); l[1] = fminf(l[1], p.y); l[2] = fminf(l[2], p.z);
             h[0] = fmaxf(h[0], p.x); h[1] = fmaxf(h[1], p.y); h[2] = fmaxf(h[2], p.z);
         }
-        float sc[3];
         for (int k = 0; k < 3; ++k) {
             for (int o = 16; o > 0; o >>= 1) {
                 l[k] = fminf(l[k], __shfl_xor_sync(0xffffffffu, l[k], o));
                 h[k] = fmaxf(h[k], __shfl_xor_sync(0xffffffffu, h[k], o));
             }
+            if (lane == 0) { sbox[w][k] = l[k]; sbox[w][3 + k] = h[k]; }
+        }
+        __syncthreads();
+        float sc[3];
+        for (int k = 0; k < 3; ++k) {
+            l[k] = sbox[0][k]; h[k] = sbox[0][3 + k];
+            for (int v = 1; v < SO_W; ++v) { l[k] = fminf(l[k], sbox[v][k]); h[k] = fmaxf(h[k], sbox[v][3 + k]); }
             sc[k] = (float)SO_GRID / fmaxf(h[k] - l[k], 1e-3f);
         }
         auto cell = [&](float4 p) -> int {
@@ -908,30 +924,39 @@ __global__ void __launch_bounds__(32) k_spatial_order(Dev d, Rd r, int list, int
             const int iz = min(SO_GRID - 1, max(0, (int)((p.z - l[2]) * sc[2])));
             return (int)(so_spread4(ix) | (so_spread4(iy) << 1) | (so_spread4(iz) << 2));
         };
+        // this warp's quarter of the range and its cell counts
+        const long long c0 = n * w / SO_W, c1 = n * (w + 1) / SO_W;
         for (int b = lane; b < SO_CELLS; b += 32) cnt[so_pad(b)] = 0;
         __syncwarp();
-        for (long long i = lane; i < n; i += 32) atomicAdd(&cnt[so_pad(cell(f4[s + i]))], 1);
-        __syncwarp();
-        // exclusive scan: lane L owns cells [128 L, 128 L + 128)
+        for (long long i = c0 + lane; i < c1; i += 32) atomicAdd(&cnt[so_pad(cell(f4[s + i]))], 1);
+        __syncthreads();
+        // exclusive scan in (cell, warp) order: thread T owns cells [32 T, 32 T + 32)
+        constexpr int PER = SO_CELLS / (SO_W * 32);
         int sum = 0;
-        for (int k = 0; k < SO_CELLS / 32; ++k) sum += cnt[so_pad(lane * (SO_CELLS / 32) + k)];
+        for (int k = 0; k < PER; ++k)
+            for (int v = 0; v < SO_W; ++v) sum += so_cnt[v * SO_STRIDE + so_pad(tid * PER + k)];
         int x = sum;
         for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, x, o);
             if (lane >= o) x += y;
         }
+        if (lane == 31) swarp[w] = x;
+        __syncthreads();
         int run = x - sum;
-        for (int k = 0; k < SO_CELLS / 32; ++k) {
-            const int b = so_pad(lane * (SO_CELLS / 32) + k);
-            const int c = cnt[b];
-            cnt[b] = run;
-            run += c;
+        for (int v = 0; v < w; ++v) run += swarp[v];
+        for (int k = 0; k < PER; ++k) {
+            for (int v = 0; v < SO_W; ++v) {
+                int* c = &so_cnt[v * SO_STRIDE + so_pad(tid * PER + k)];
+                const int cv = *c;
+                *c = run;
+                run += cv;
+            }
         }
-        __syncwarp();
-        // stable scatter, 32 entries at a time in list order
-        for (long long i0 = 0; i0 < n; i0 += 32) {
+        __syncthreads();
+        // stable scatter of this warp's quarter, 32 entries at a time in list order
+        for (long long i0 = c0; i0 < c1; i0 += 32) {
             const long long i = i0 + lane;
-            const bool on = i < n;
+            const bool on = i < c1;
             float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
             int b = SO_CELLS;
             if (on) { p = f4[s + i]; b = cell(p); }
@@ -946,13 +971,15 @@ __global__ void __launch_bounds__(32) k_spatial_order(Dev d, Rd r, int list, int
                 operm[o] = (int)(s + i);
             }
         }
-        __syncwarp();
+        __syncthreads();
     }
 }
 
 void launch_spatial_order(const Dev& d, const Rd& r, int list, int set, cudaStream_t s)
 {
-    k_spatial_order<<<grid_for(2LL * d.B, 1, 14), 32, 0, s>>>(d, r, list, set);
+    const int smem = SO_W * SO_STRIDE * (int)sizeof(int);
+    cudaFuncSetAttribute(k_spatial_order, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_spatial_order<<<grid_for(2LL * d.B, 1, 3), SO_W * 32, smem, s>>>(d, r, list, set);
 }
 
 // ---------------------------------------------------------------------------
