@@ -251,7 +251,7 @@ struct cms_ctx {
         S_ADJ_ACT_CONV, S_ADJ_ACT_TOR, S_ADJ_ACT_CONC, S_ADJ_ACT_ATOM, S_ADJ_LIST_CONV, S_ADJ_LIST_TOR,
         S_ADJ_LIST_CONC, S_ADJ_NACT, S_OVF, S_REF_XYZ, S_POSE, S_POSE_CKPT, S_POSE_CEN, S_HIST, S_STEP, S_MAXSUM,
         S_TOR_LFLAG, S_TOR_LOFF, S_TOR_LIST, S_PTOP, S_SP_A, S_SP_H, S_SP_XYZ, S_SP_ALT, S_SP_G, S_SP_ORD,
-        S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1, S_KS_TOP, S_KS_BUF, S_CV_SOFF, S_CC_SOFF, S_TOR_SOFF, S_TOR_SN, S_NBS_TOP, S_NBS_BUF, S_NB_SOFF,
+        S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1, S_KS_TOP, S_KS_BUF, S_CV_SOFF, S_CC_SOFF, S_TOR_SOFF, S_TOR_SN, S_NBS_TOP, S_NBS_BUF, S_NB_SOFF, S_ADJ_SKEY, S_ADJ_SLIST_CONV, S_ADJ_SLIST_TOR, S_ADJ_SLIST_CONC,
         S_COUNT
     };
 
@@ -713,6 +713,10 @@ AdjBuf bind_adj(cms_ctx* x)
     a.list_tor = x->ensure<int>(cms_ctx::S_ADJ_LIST_TOR, T);
     a.list_conc = x->ensure<int>(cms_ctx::S_ADJ_LIST_CONC, P);
     a.nact = x->ensure<int>(cms_ctx::S_ADJ_NACT, 4);
+    a.skey = x->ensure<int>(cms_ctx::S_ADJ_SKEY, 3 * 256);
+    a.slist_conv = x->ensure<int>(cms_ctx::S_ADJ_SLIST_CONV, x->N);
+    a.slist_tor = x->ensure<int>(cms_ctx::S_ADJ_SLIST_TOR, T);
+    a.slist_conc = x->ensure<int>(cms_ctx::S_ADJ_SLIST_CONC, P);
     x->ensure<double>(cms_ctx::S_ADJ_GRAD, 3 * x->N);
     return a;
 }

@@ -79,6 +79,8 @@ struct AdjBuf {
     int8_t* act_conv; int8_t* act_tor; int8_t* act_conc;   // units holding a dot with a non-zero adjoint
     int8_t* act_atom;      // atoms of active units
     int* list_conv; int* list_tor; int* list_conc;         // active units
+    int* skey;             // 3 x ADJ_KEYS: active units per work key, then each key's next slot
+    int* slist_conv; int* slist_tor; int* slist_conc;      // active units, largest dot counts first
     int* nact;             // 3 counters
     const double* gtot;    // per complex: upstream gradient of the side's CMS
 };

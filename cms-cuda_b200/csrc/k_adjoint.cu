@@ -571,6 +571,85 @@ __global__ void k_adj_collect(Dev d, AdjBuf a)
     }
 }
 
+// Active units ordered by their dot count, largest first, so the units that
+// share a warp run loops of similar length (a counting sort on the clamped
+// count; the order inside a key does not matter: every unit writes its own
+// slots and the gather sums them in a fixed order).
+static constexpr int ADJ_KEYS = 256;
+
+__device__ __forceinline__ int adj_unit_key(const Dev& d, int kind, int u)
+{
+    const int c = kind == 0 ? d.conv_cnt[u] : (kind == 1 ? d.tor1_cnt[u] + d.tor2_cnt[u] : d.conc_cnt[u]);
+    return ADJ_KEYS - 1 - min(max(c, 0), ADJ_KEYS - 1);
+}
+
+__device__ __forceinline__ bool adj_entry(const AdjBuf& a, long long e, int& kind, int& u)
+{
+    const long long n0 = a.nact[0], n1 = a.nact[1], n2 = a.nact[2];
+    if (e < n0) { kind = 0; u = a.list_conv[e]; return true; }
+    if (e < n0 + n1) { kind = 1; u = a.list_tor[e - n0]; return true; }
+    if (e < n0 + n1 + n2) { kind = 2; u = a.list_conc[e - n0 - n1]; return true; }
+    return false;
+}
+
+__global__ void k_adj_key_count(Dev d, AdjBuf a)
+{
+    CMS_EXIT_ON_OVERFLOW(d);
+    __shared__ int h[3 * ADJ_KEYS];
+    for (int i = threadIdx.x; i < 3 * ADJ_KEYS; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const long long total = (long long)a.nact[0] + a.nact[1] + a.nact[2];
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        int kind, u;
+        if (adj_entry(a, e, kind, u)) atomicAdd(&h[kind * ADJ_KEYS + adj_unit_key(d, kind, u)], 1);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 3 * ADJ_KEYS; i += blockDim.x)
+        if (h[i]) atomicAdd(&a.skey[i], h[i]);
+}
+
+// one warp per kind: exclusive scan of its key counts
+__global__ void k_adj_key_scan(Dev d, AdjBuf a)
+{
+    CMS_EXIT_ON_OVERFLOW(d);
+    const int lane = threadIdx.x & 31, kind = threadIdx.x >> 5;
+    if (kind >= 3) return;
+    constexpr int PER = ADJ_KEYS / 32;
+    int* k = a.skey + kind * ADJ_KEYS + lane * PER;
+    int sum = 0;
+    for (int i = 0; i < PER; ++i) sum += k[i];
+    int x = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    int run = x - sum;
+    for (int i = 0; i < PER; ++i) { const int c = k[i]; k[i] = run; run += c; }
+}
+
+__global__ void k_adj_key_scatter(Dev d, AdjBuf a)
+{
+    CMS_EXIT_ON_OVERFLOW(d);
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const long long total = (long long)a.nact[0] + a.nact[1] + a.nact[2];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    // warp-uniform trip count: every lane takes part in the match below
+    for (long long e0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); e0 < total; e0 += stride) {
+        int kind = 0, u = 0, slot = -1;
+        const bool on = adj_entry(a, e0 + lane, kind, u);
+        if (on) slot = kind * ADJ_KEYS + adj_unit_key(d, kind, u);
+        const unsigned peers = __match_any_sync(0xffffffffu, slot);
+        int base = 0;
+        if (on && (peers & lt) == 0) base = atomicAdd(&a.skey[slot], __popc(peers));
+        base = __shfl_sync(0xffffffffu, base, __ffs(peers) - 1);
+        if (on) {
+            int* out = kind == 0 ? a.slist_conv : (kind == 1 ? a.slist_tor : a.slist_conc);
+            out[base + __popc(peers & lt)] = u;
+        }
+    }
+}
+
 // pass 3: per active unit, one lane per coordinate of its atoms (K lanes);
 // lane k accumulates sum over the unit's dots of A . d(dot)/d(coordinate k)
 template <int NT>
@@ -602,7 +681,7 @@ __global__ void k_adj_units(Dev d, AdjBuf a)
     constexpr int G = 32 / L;                  // units per warp
     const int lane = threadIdx.x & 31;
     const int grp = lane / L, k = lane % L;
-    const int* list = KIND == 0 ? a.list_conv : (KIND == 1 ? a.list_tor : a.list_conc);
+    const int* list = KIND == 0 ? a.slist_conv : (KIND == 1 ? a.slist_tor : a.slist_conc);
     const long long n = a.nact[KIND];
     const long long wid = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -745,6 +824,10 @@ void launch_adjoint(const Dev& d, const Rd& r, const AdjBuf& a, const NNTask* cm
     k_adj_ref_fill<<<grid_adj(D, 256), 256, 0, s>>>(d, r, a);
     k_adj_ref_sum<<<grid_adj(D, 256), 256, 0, s>>>(d, r, a);
     k_adj_collect<<<grid_adj((long long)d.N + d.tor_cap + d.probe_cap, 256), 256, 0, s>>>(d, a);
+    cudaMemsetAsync(a.skey, 0, sizeof(int) * 3 * ADJ_KEYS, s);
+    k_adj_key_count<<<grid_adj((long long)d.N + d.tor_cap + d.probe_cap, 256), 256, 0, s>>>(d, a);
+    k_adj_key_scan<<<1, 96, 0, s>>>(d, a);
+    k_adj_key_scatter<<<grid_adj((long long)d.N + d.tor_cap + d.probe_cap, 256), 256, 0, s>>>(d, a);
     // convex and concave units: one lane per atom (3 tangents); toroidal units: one lane per coordinate
     k_adj_units<0, 3><<<grid_adj(d.N, 128), 128, 0, s>>>(d, a);
     k_adj_units<1, 1><<<grid_adj(d.tor_cap, 128), 128, 0, s>>>(d, a);
