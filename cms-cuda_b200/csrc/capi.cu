@@ -191,7 +191,7 @@ struct cms_ctx {
     std::vector<DBuf> bufs;
     Dev d{};
     Rd r{};
-    long long cap_cells = 0, cap_nb = 0, cap_bu = 0, cap_tor = 0, cap_probe = 0, cap_dot = 0;
+    long long cap_cells = 0, cap_nb = 0, cap_bu = 0, cap_tor = 0, cap_probe = 0, cap_dot = 0, cap_conc = 0;
     long long tot[8] = {0};
     bool have_batch = false, surf_ok = false, cms_ok = false, sc_ok = false, max_ok = false;
     int surf_all_atoms = -1;
@@ -251,7 +251,8 @@ struct cms_ctx {
         S_ADJ_ACT_CONV, S_ADJ_ACT_TOR, S_ADJ_ACT_CONC, S_ADJ_ACT_ATOM, S_ADJ_LIST_CONV, S_ADJ_LIST_TOR,
         S_ADJ_LIST_CONC, S_ADJ_NACT, S_OVF, S_REF_XYZ, S_POSE, S_POSE_CKPT, S_POSE_CEN, S_HIST, S_STEP, S_MAXSUM,
         S_TOR_LFLAG, S_TOR_LOFF, S_TOR_LIST, S_PTOP, S_SP_A, S_SP_H, S_SP_XYZ, S_SP_ALT, S_SP_G, S_SP_ORD,
-        S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1, S_KS_TOP, S_KS_BUF, S_CV_SOFF, S_CC_SOFF, S_TOR_SOFF, S_TOR_SN, S_NBS_TOP, S_NBS_BUF, S_NB_SOFF, S_ADJ_SKEY, S_ADJ_SLIST_CONV, S_ADJ_SLIST_TOR, S_ADJ_SLIST_CONC,
+        S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1, S_KS_TOP, S_KS_BUF, S_CV_SOFF, S_CC_SOFF, S_TOR_SOFF, S_TOR_SN, S_NBS_TOP, S_NBS_BUF, S_NB_SOFF, S_ADJ_SKEY, S_ADJ_SLIST_CONV, S_ADJ_SLIST_TOR, S_ADJ_SLIST_CONC, S_CS_TOP, S_CS_XYZ, S_CS_AREA, S_CS_OWN,
+        S_CS_SUB, S_CS_BUR,
         S_COUNT
     };
 
@@ -409,6 +410,13 @@ void bind_caps(cms_ctx* x)
     d.conc_cnt = x->ensure<int>(cms_ctx::S_CONC_CNT, x->cap_probe);
     d.conc_off = x->ensure<long long>(cms_ctx::S_CONC_OFF, x->cap_probe + 1);
     d.cc_soff = x->ensure<int>(cms_ctx::S_CC_SOFF, x->cap_probe);
+    d.cs_cap = x->cap_conc;
+    d.cs_top = x->ensure<unsigned long long>(cms_ctx::S_CS_TOP, 1);
+    d.cs_xyz = x->ensure<double>(cms_ctx::S_CS_XYZ, 3 * x->cap_conc);
+    d.cs_area = x->ensure<double>(cms_ctx::S_CS_AREA, x->cap_conc);
+    d.cs_own = x->ensure<int>(cms_ctx::S_CS_OWN, x->cap_conc);
+    d.cs_sub = x->ensure<int>(cms_ctx::S_CS_SUB, x->cap_conc);
+    d.cs_bur = x->ensure<int8_t>(cms_ctx::S_CS_BUR, x->cap_conc);
     d.dot_cap = x->cap_dot;
     const long long D = x->cap_dot;
     d.dxyz = x->ensure<double>(cms_ctx::S_DXYZ, 3 * D);
@@ -561,6 +569,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
     ck(cudaMemsetAsync(d.tor2_cnt, 0, sizeof(int) * x->cap_tor, s), "memset");
     ck(cudaMemsetAsync(d.conc_cnt, 0, sizeof(int) * x->cap_probe, s), "memset");
     ck(cudaMemsetAsync(d.ks_top, 0, sizeof(unsigned long long), s), "memset");
+    ck(cudaMemsetAsync(d.cs_top, 0, sizeof(unsigned long long), s), "memset");
     launch_convex(d, false, s);
     mark(x, P_CONVEX_COUNT);
     launch_toroidal(d, x->cap_tor, false, s);
@@ -574,12 +583,13 @@ void enqueue_surface(cms_ctx* x, bool sized)
     launch_layout(d, (long long*)x->get<int>(cms_ctx::S_CM_TMP), tmp, s);
     mark(x, P_LAYOUT);
     if (sized) {
-        const long long cap0 = x->cap_dot;
+        const long long cap0 = x->cap_dot, conc0 = x->cap_conc;
         grow(x->cap_dot, read_ll(x, d.dot_off + 2LL * d.B));
+        grow(x->cap_conc, read_ll(x, d.conc_off + x->cap_probe));
         bind_caps(x);
         tmp = scan_tmp(x);
-        if (x->cap_dot != cap0) {
-            // the kept-candidate buffer may have moved: the emit passes recompute every unit
+        if (x->cap_dot != cap0 || x->cap_conc != conc0) {
+            // the kept-candidate buffers may have moved: the emit passes recompute every unit
             ck(cudaMemsetAsync(d.cv_soff, 0xff, sizeof(int) * d.N, s), "memset");
             ck(cudaMemsetAsync(d.cc_soff, 0xff, sizeof(int) * x->cap_probe, s), "memset");
             ck(cudaMemsetAsync(d.tor_soff, 0xff, sizeof(int) * x->cap_tor, s), "memset");

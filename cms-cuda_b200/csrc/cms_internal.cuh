@@ -111,8 +111,11 @@ struct Dev {
     unsigned long long* ks_top;                  // 1: entries taken
     int* ks_buf; long long ks_cap;               // ks_cap (= dot capacity)
     int* cv_soff;                                // N
-    int* cc_soff;                                // probe_cap
+    int* cc_soff;                                // probe_cap: first of the probe's dots in cs_* (-1: none)
     int* tor_soff; int* tor_sn;                  // tor_cap: kept torus points (those with arc dots) of a pair
+    // concave dots made by the count pass (cc_soff indexes these): point, area, owner, sub-index, burial
+    unsigned long long* cs_top;                  // 1: entries taken
+    double* cs_xyz; double* cs_area; int* cs_own; int* cs_sub; int8_t* cs_bur; long long cs_cap;
     // neighbour rows sorted by the count pass: per atom its neighbours then its buried partners, in
     // the final order; nb_soff: the atom's first entry (-1: not kept, the emit pass gathers them again)
     unsigned long long* nbs_top;                 // 1: entries taken

@@ -732,7 +732,7 @@ void launch_toroidal(const Dev& d, long long tor_grid, bool emit, cudaStream_t s
 static constexpr int CC_WARPS = 4;
 
 template <bool EMIT>
-__global__ void __launch_bounds__(CC_WARPS * 32, EMIT ? 4 : 1) k_concave(Dev d)
+__global__ void __launch_bounds__(CC_WARPS * 32, 4) k_concave(Dev d)
 {
     CMS_EXIT_ON_OVERFLOW(d);
     __shared__ LatTable tab[CC_WARPS];
@@ -749,7 +749,18 @@ __global__ void __launch_bounds__(CC_WARPS * 32, EMIT ? 4 : 1) k_concave(Dev d)
     const long long nw = (long long)gridDim.x * CC_WARPS;
     for (long long p = wid; p < NP; p += nw) {
         if (EMIT && d.conc_cnt[p] == 0) continue;                      // no dots: nothing to write
-        const int so = EMIT ? d.cc_soff[p] : -1;                         // >= 0: the kept candidates are stashed
+        const int so = EMIT ? d.cc_soff[p] : -1;                         // >= 0: the count pass made the dots
+        if (EMIT && so >= 0) {
+            const long long base = unit_base(d, d.cplx[d.pa0[p]], d.mol[d.pa0[p]], 3, d.conc_off[p]);
+            const V3 pijk = ld3(d.pxyz + 3 * p);
+            const int cnt = d.conc_cnt[p];
+            for (int e = lane; e < cnt; e += 32) {
+                const long long k = (long long)so + e;
+                write_dot_b(d, base + e, ld3(d.cs_xyz + 3 * k), pijk, d.cs_area[k], d.cs_own[k], 3, (int)p,
+                            d.cs_sub[k], d.cs_bur[k]);
+            }
+            continue;
+        }
         const int ia[3] = {d.pa0[p], d.pa1[p], d.pa2[p]};
         V3 xa[3];
         double ra[3];
@@ -761,7 +772,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, EMIT ? 4 : 1) k_concave(Dev d)
         const int c = d.cplx[ia[0]];
         // nearby low probes of the same complex (d2 <= 4 rp^2), self excluded
         int nnear = 0;
-        if (low && so < 0) {
+        if (low) {
             const Cplx C = d.cx[c];
             const int s0 = C.a0, e1 = C.a0 + C.n;
             const long long pb = min(d.plus_off[s0] + d.minus_off[s0], d.probe_cap);
@@ -841,27 +852,6 @@ __global__ void __launch_bounds__(CC_WARPS * 32, EMIT ? 4 : 1) k_concave(Dev d)
             }
         }
         int kept = 0;
-        if (EMIT && so >= 0) {
-            const int cnt = d.conc_cnt[p];
-            for (int e = lane; e < cnt; e += 32) {
-                const int sub = d.ks_buf[so + e];
-                const int l = sub >> 16, i = sub & 0xffff;
-                const V3 pts = subdiv_point(v3(L.cx[l], L.cy[l], L.cz[l]), L.rad[l], fx, fy, L.delta[l], i) + pijk;
-                double dd[3];
-                for (int k = 0; k < 3; ++k) dd[k] = norm3(pts - xa[k]) - ra[k];
-                int mc = 0;                            // np.argmin: first minimum, NaN wins
-                if (!isnan(dd[0])) {
-                    for (int k = 1; k < 3; ++k) {
-                        if (isnan(dd[k])) { mc = k; break; }
-                        if (dd[k] < dd[mc]) mc = k;
-                    }
-                }
-                write_dot_b(d, base + e, pts, pijk, L.area[l], ia[mc], 3, (int)p, sub,
-                            mc == 0 ? bur3[0] : (mc == 1 ? bur3[1] : bur3[2]));
-            }
-            __syncwarp();
-            continue;
-        }
         for (int t0 = 0; t0 < total; t0 += 32) {
             const int t = t0 + lane;
             bool keep = false;
@@ -900,9 +890,35 @@ __global__ void __launch_bounds__(CC_WARPS * 32, EMIT ? 4 : 1) k_concave(Dev d)
             kept += __popc(m);
         }
         if (!EMIT) {
+            // make the probe's dots now (point, owner, burial) for the emit pass to copy
             __syncwarp();
-            const int sp = ks_stash(d, ksl[EMIT ? 0 : w], kept, kcur);
-            if (lane == 0) { d.conc_cnt[p] = kept; d.cc_soff[p] = sp; }
+            long long sp = -1;
+            if (kept > 0 && kept <= KS_CAP) sp = stash_take(d.cs_top, d.cs_cap, kcur, kept);
+            if (sp >= 0) {
+                int8_t b3[3];
+                for (int k = 0; k < 3; ++k) b3[k] = buried_warp(d, ia[k], pijk);
+                for (int e = lane; e < kept; e += 32) {
+                    const int sub = ksl[EMIT ? 0 : w][e];
+                    const int l = sub >> 16, i = sub & 0xffff;
+                    const V3 pts = subdiv_point(v3(L.cx[l], L.cy[l], L.cz[l]), L.rad[l], fx, fy, L.delta[l], i) + pijk;
+                    double dd[3];
+                    for (int k = 0; k < 3; ++k) dd[k] = norm3(pts - xa[k]) - ra[k];
+                    int mc = 0;                        // np.argmin: first minimum, NaN wins
+                    if (!isnan(dd[0])) {
+                        for (int k = 1; k < 3; ++k) {
+                            if (isnan(dd[k])) { mc = k; break; }
+                            if (dd[k] < dd[mc]) mc = k;
+                        }
+                    }
+                    const long long q = sp + e;
+                    st3(d.cs_xyz + 3 * q, pts);
+                    d.cs_area[q] = L.area[l];
+                    d.cs_own[q] = ia[mc];
+                    d.cs_sub[q] = sub;
+                    d.cs_bur[q] = mc == 0 ? b3[0] : (mc == 1 ? b3[1] : b3[2]);
+                }
+            }
+            if (lane == 0) { d.conc_cnt[p] = kept; d.cc_soff[p] = (int)sp; }
         }
         __syncwarp();
     }
