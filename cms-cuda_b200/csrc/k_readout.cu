@@ -52,15 +52,11 @@ __device__ __forceinline__ float4 pack_f4(const Dev& d, long long dot, int c)
     return make_float4((float)(p[0] - C.ctr[0]), (float)(p[1] - C.ctr[1]), (float)(p[2] - C.ctr[2]), 0.f);
 }
 
-// dot -> complex via binary search of dot_off (per complex & molecule)
+// dot -> complex * 2 + molecule, from its owner atom (every dot lies in its owner's segment)
 __device__ __forceinline__ int dot_cm(const Dev& d, long long dot)
 {
-    int lo = 0, hi = 2 * d.B - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (doff(d, mid) <= dot) lo = mid; else hi = mid - 1;
-    }
-    return lo;
+    const int a = d.datom[dot];
+    return 2 * d.cplx[a] + d.mol[a];
 }
 
 __global__ void k_split_buried(Dev d, Rd r, long long cap)
