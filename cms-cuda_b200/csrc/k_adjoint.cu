@@ -655,9 +655,11 @@ __global__ void k_adj_key_scatter(Dev d, AdjBuf a)
 template <int NT>
 struct AdjLaneF {
     const double4* A;
+    const int8_t* bur;      // only buried dots carry an adjoint (the others' slots are not cleared)
     double g[NT];
     __device__ bool want(long long q) const
     {
+        if (!bur[q]) return false;
         const double4 v = A[q];
         return v.x != 0.0 || v.y != 0.0 || v.z != 0.0 || v.w != 0.0;
     }
@@ -691,6 +693,7 @@ __global__ void k_adj_units(Dev d, AdjBuf a)
         const int u = list[e];
         AdjLaneF<NT> f;
         f.A = a.A;
+        f.bur = d.dbur;
 #pragma unroll
         for (int t = 0; t < NT; ++t) f.g[t] = 0.0;
         const SeedLane<NT> seed{k};
@@ -795,14 +798,17 @@ __global__ void k_adj_gather(Dev d, AdjBuf a, double* grad)
     }
 }
 
-__global__ void k_adj_zero(Dev d, AdjBuf a, long long dcap)
+// clears the per-dot adjoint of the buried dots (the only ones that get one)
+// and the per-entry and per-unit counters
+__global__ void k_adj_zero(Dev d, Rd r, AdjBuf a, long long dcap)
 {
     CMS_EXIT_ON_OVERFLOW(d);
     const long long nf = (long long)d.N + d.tor_cap + d.probe_cap;
     const long long n = max(dcap, nf);
+    const long long NB = r.bur_scan[adj_doff(d, 2LL * d.B)];
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        if (i < NB) a.A[r.bur_idx[i]] = make_double4(0.0, 0.0, 0.0, 0.0);
         if (i < dcap) {
-            a.A[i] = make_double4(0.0, 0.0, 0.0, 0.0);
             a.rcnt[i] = 0;
             a.rfill[i] = 0;
         }
@@ -817,7 +823,7 @@ void launch_adjoint(const Dev& d, const Rd& r, const AdjBuf& a, const NNTask* cm
                     long long* scan_tmp, cudaStream_t s)
 {
     const long long D = d.dot_cap;
-    k_adj_zero<<<grid_adj(std::max(D, (long long)d.N + d.tor_cap + d.probe_cap), 256), 256, 0, s>>>(d, a, D);
+    k_adj_zero<<<grid_adj(std::max(D, (long long)d.N + d.tor_cap + d.probe_cap), 256), 256, 0, s>>>(d, r, a, D);
     k_adj_queries<<<grid_adj(D, 256), 256, 0, s>>>(d, r, a, cms_task, side);
     k_adj_ref_count<<<grid_adj(D, 256), 256, 0, s>>>(d, r, a);
     scan_counts(a.rcnt, a.roff, D, scan_tmp, s);
