@@ -227,11 +227,12 @@ def stage_bytes(name, t, work=None):
 # one launch, ncu on the 256-complex batch of this generator, divided by that
 # batch's units); scaled by the units of the measured batch
 TRAFFIC_PER_UNIT = {
-    "toroidal_emit": (369.3e6 / 5021616, "toroidal"),      # per toroidal dot
-    "triples_count": (96.95e6 / 558670, "atoms"),          # per atom
-    "triples_emit": (106.8e6 / 558670, "atoms"),
-    "cms_nn": (174.2e6 / 2750610, "cms_queries"),          # per query dot
-    "sc_band_nn": (380.9e6 / 2750610, "band_queries"),
+    "toroidal_emit": (365.19e6 / 5021616, "toroidal"),     # per toroidal dot
+    "toroidal_count": (45.53e6 / 558670, "atoms"),         # per atom
+    "triples_count": (98.78e6 / 558670, "atoms"),          # per atom
+    "triples_emit": (19.46e6 / 558670, "atoms"),           # the probe scatter
+    "cms_nn": (104.73e6 / 2750610, "cms_queries"),         # per query dot
+    "sc_band_nn": (405.62e6 / 2750610, "band_queries"),
 }
 
 

@@ -234,10 +234,10 @@ def test_probe_stash_and_recompute_agree():
     The triple count pass stashes its probes when they fit the capacity it
     ran with, and a scatter fills the probe arrays; otherwise (the first run
     of a fresh context) the emit pass recomputes them.  Likewise the convex
-    and concave count passes keep their accepted candidates, the toroidal
-    count pass its torus points with arc dots and the neighbour count pass
-    its sorted rows for the emit passes.  Both ways give the same neighbour
-    lists, probes, dots, access flags and results.
+    count pass keeps its accepted candidates, the concave count pass makes
+    its dots, the toroidal count pass keeps its torus points with arc dots
+    and the neighbour count pass its rows for the emit passes.  Both ways
+    give the same neighbour lists, probes, dots, access flags and results.
     """
     from cms_cuda import _lib
     names = ("golden_pkl", "synth_small_s7", "synth_zero_radii")
