@@ -51,6 +51,26 @@ __device__ __forceinline__ int subdiv_count(double delta, double angle)
     return n;
 }
 
+// subdiv_count for long circles (latitudes of a sphere: tens of points).  For
+// delta > 0 the rounded products delta*(n + 0.5) do not decrease with n
+// (n + 0.5 is exact and rounding is monotone), so the points that exist are a
+// prefix: start from an FP32 estimate of the quotient and settle the exact
+// boundary with the same FP64 comparisons the loop makes.  Inputs outside the
+// FP32 range take the loop.
+__device__ __forceinline__ int subdiv_count_long(double delta, double angle)
+{
+    int n = 0;
+    if (delta > 1e-30 && delta < 1e30 && fabs(angle) < 1e30) {
+        const float e = __fdividef((float)angle, (float)delta) + 0.5f;
+        n = !(e > 0.f) ? 0 : (e >= (float)CMS_MAX_SUBDIV ? CMS_MAX_SUBDIV : (int)e);
+        while (n > 0 && !(delta * ((double)(n - 1) + 0.5) <= angle)) --n;
+        while (n < CMS_MAX_SUBDIV && delta * ((double)n + 0.5) <= angle) ++n;
+        return n;
+    }
+    while (n < CMS_MAX_SUBDIV && delta * ((double)n + 0.5) <= angle) ++n;
+    return n;
+}
+
 __device__ __forceinline__ double subdiv_delta(double density, double rad)
 {
     return 1.0 / (sqrt(density) * rad);
