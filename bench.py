@@ -393,17 +393,18 @@ def run_ours(args):
     # ---- end to end through the public batch API ---------------------------
     from cms_cuda.batch import BatchCalculator
     bc = BatchCalculator(local)
+    grad_h = torch.empty((xyz_np.shape[0], 3), dtype=torch.float64).pin_memory().numpy()
     bc.load(batch.atom_off, batch.n_binder, xyz_np, rad_np)
-    r = bc.run(graph=True, grad=True)
+    r = bc.run(graph=True, grad=True, grad_out=grad_h)
     for _ in range(args.warmup):
         bc.load(batch.atom_off, batch.n_binder, xyz_np, rad_np)
-        r = bc.run(graph=True, grad=True)
+        r = bc.run(graph=True, grad=True, grad_out=grad_h)
     h0, d0 = bc.ctx.transfer_bytes()
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         bc.load(batch.atom_off, batch.n_binder, xyz_np, rad_np)
-        r = bc.run(graph=True, grad=True)
+        r = bc.run(graph=True, grad=True, grad_out=grad_h)
     e2e_s = (time.perf_counter() - t0) / args.steps
     h1, d1 = bc.ctx.transfer_bytes()
     same = bool(np.array_equal(r.cms, totals[:, 1]) and np.array_equal(r.sc, sc[:, 0]) and

@@ -321,8 +321,13 @@ class Context:
         g = np.ascontiguousarray(grad_total, dtype=np.float64)
         self._check(self.lib.cms_set_grad_total(self.h, _ptr(g), CMS_HOST))
 
-    def grad_xyz(self):
-        out = np.empty((self.N, 3), dtype=np.float64)
+    def grad_xyz(self, out=None):
+        """The last run's gradient (N x 3); `out` (float64, C-contiguous, N x 3), e.g. a pinned
+        buffer reused across steps, receives it instead of a new array."""
+        if out is None:
+            out = np.empty((self.N, 3), dtype=np.float64)
+        elif out.dtype != np.float64 or out.shape != (self.N, 3) or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous float64 array of shape ({self.N}, 3)")
         self._check(self.lib.cms_grad_xyz(self.h, _ptr(out), CMS_HOST))
         return out
 

@@ -49,11 +49,12 @@ class BatchCalculator:
     def load(self, atom_off, n_binder, xyz, radius, density=None):
         self.ctx.load_batch(atom_off, n_binder, xyz, radius, density)
 
-    def run(self, graph=True, per_atom=False, grad=False):
+    def run(self, graph=True, per_atom=False, grad=False, grad_out=None):
         """
         Surfaces + CMS (both sides) + SC of every loaded complex; with
         grad=True also d(target-side CMS)/d(xyz) of every atom (in the
-        captured graph when graph=True).
+        captured graph when graph=True), written to `grad_out` when given
+        (N x 3 float64; a pinned buffer makes the read-back a direct copy).
         """
         if graph:
             if grad != self._grad:
@@ -66,7 +67,13 @@ class BatchCalculator:
         sc, sides = self.ctx.shape_complementarity()
         g = None
         if grad:
-            g = self.ctx.grad_xyz() if graph else self.ctx.contact_ms_backward(target_side=True)
+            if graph:
+                g = self.ctx.grad_xyz(grad_out)
+            else:
+                g = self.ctx.contact_ms_backward(target_side=True)
+                if grad_out is not None:
+                    grad_out[...] = g
+                    g = grad_out
         return BatchResult(totals, sc, sides, pa if per_atom else None, g)
 
     def statuses(self):
