@@ -674,8 +674,10 @@ struct AdjLaneF {
 
 // One active unit per group of K / NT lanes, each lane carrying NT of the
 // unit's K coordinates as dual-number tangents through the unit's geometry.
+// four CTAs per SM: twice the warps of the unbounded register count, which
+// outweighs the spills it costs (measured)
 template <int KIND, int NT>
-__global__ void k_adj_units(Dev d, AdjBuf a)
+__global__ void __launch_bounds__(128, 4) k_adj_units(Dev d, AdjBuf a)
 {
     CMS_EXIT_ON_OVERFLOW(d);
     constexpr int K = KIND == 2 ? 9 : 6;       // coordinates of the unit's atoms
