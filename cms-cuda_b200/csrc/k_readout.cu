@@ -344,7 +344,7 @@ __device__ __forceinline__ void nn_round_box(const NNArgs& a, long long ro, int 
 // otherwise.  The band search stops a query at its first FP64 hit and a tile
 // once every query has one or no round is left within reach.
 template <int MODE, int Q, int SUB>
-__global__ void __launch_bounds__(NN_T) k_nn(NNArgs a)
+__global__ void __launch_bounds__(NN_T, MODE == NN_BAND ? 10 : 8) k_nn(NNArgs a)
 {
     if (a.ovf && *a.ovf) return;
     constexpr int P = Q / 2;                  // packed query pairs per lane
