@@ -343,7 +343,7 @@ __device__ __forceinline__ void classify(const Dev& d, int g, V3 xi, double ri, 
     }
 }
 
-__global__ void __launch_bounds__(NB_WARPS * 32) k_nb_count(Dev d)
+__global__ void __launch_bounds__(NB_WARPS * 32, 8) k_nb_count(Dev d)
 {
     CMS_EXIT_ON_OVERFLOW(d);
     __shared__ BallScratch sc[NB_WARPS];
