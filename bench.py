@@ -229,7 +229,7 @@ def stage_bytes(name, t, work=None):
 TRAFFIC_PER_UNIT = {
     "toroidal_emit": (365.19e6 / 5021616, "toroidal"),     # per toroidal dot
     "toroidal_count": (45.53e6 / 558670, "atoms"),         # per atom
-    "triples_count": (98.78e6 / 558670, "atoms"),          # per atom
+    "triples_count": (105.68e6 / 558670, "atoms"),         # per atom
     "triples_emit": (19.46e6 / 558670, "atoms"),           # the probe scatter
     "cms_nn": (104.73e6 / 2750610, "cms_queries"),         # per query dot
     "sc_band_nn": (405.62e6 / 2750610, "band_queries"),
