@@ -54,19 +54,23 @@ __global__ void k_scan_tiles(const int* __restrict__ in, long long n, long long*
     if (threadIdx.x == 0) tile_sum[blockIdx.x] = total;
 }
 
+// one block: thread t owns a contiguous run of tile sums, so a single block
+// scan covers any tile count
 __global__ void k_scan_top(long long* __restrict__ tile_sum, long long ntiles, long long* __restrict__ out_total)
 {
     __shared__ long long sh[32];
-    long long carry = 0;
-    for (long long b = 0; b < ntiles; b += SCAN_T) {
-        long long i = b + threadIdx.x;
-        long long v = i < ntiles ? tile_sum[i] : 0;
-        long long total;
-        long long ex = block_excl_scan(v, sh, total);
-        if (i < ntiles) tile_sum[i] = carry + ex;
-        carry += total;
+    const long long per = (ntiles + SCAN_T - 1) / SCAN_T;
+    const long long b = (long long)threadIdx.x * per, e = min(b + per, ntiles);
+    long long s = 0;
+    for (long long i = b; i < e; ++i) s += tile_sum[i];
+    long long total;
+    long long run = block_excl_scan(s, sh, total);
+    for (long long i = b; i < e; ++i) {
+        const long long v = tile_sum[i];
+        tile_sum[i] = run;
+        run += v;
     }
-    if (threadIdx.x == 0) *out_total = carry;
+    if (threadIdx.x == 0) *out_total = total;
 }
 
 __global__ void k_scan_apply(const int* __restrict__ in, long long n, const long long* __restrict__ tile_off,
