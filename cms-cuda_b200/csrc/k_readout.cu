@@ -169,6 +169,7 @@ struct NNQ {
     float ms, ms2;        // smallest block minimum of s; smallest among the other blocks
     int mb;               // block holding ms
     float ts;             // s threshold: candidates have s <= ts
+    float tslo;           // band: s at or below this is a hit for certain (d32 + eps <= band^2)
     float cth;            // cull threshold on the squared box distance
     double best;
     int bidx;
@@ -415,6 +416,7 @@ __global__ void __launch_bounds__(NN_T, MODE == NN_BAND ? 10 : 8) k_nn(NNArgs a)
             tl = nn_tile(cx, cy, cz, 0.5 * sqrt(ex * ex + ey * ey + ez * ez), T.E);
         }
         const double band_th = MODE == NN_BAND ? a.band_thr64 + nn_eps(a.band_thr64, tl.rho, tl.E0) * 1.01 : 0.0;
+        const double band_lo = MODE == NN_BAND ? a.band_thr64 - nn_eps(a.band_thr64, tl.rho, tl.E0) * 1.01 : 0.0;
         const float band_cth = MODE == NN_BAND ? nn_cull_th(band_th, tl) : 0.f;
         float cthw = -INFINITY;        // warp cull threshold: max over its open queries
 #pragma unroll
@@ -427,6 +429,7 @@ __global__ void __launch_bounds__(NN_T, MODE == NN_BAND ? 10 : 8) k_nn(NNArgs a)
             q[j].done = !q[j].live;
             if (MODE == NN_BAND) {
                 q[j].ts = __double2float_ru(band_th - q[j].qq);
+                q[j].tslo = __double2float_rd(band_lo - q[j].qq);
                 q[j].cth = band_cth;
             } else {
                 q[j].ts = INFINITY;
@@ -526,6 +529,9 @@ __global__ void __launch_bounds__(NN_T, MODE == NN_BAND ? 10 : 8) k_nn(NNArgs a)
                     if (MODE == NN_BAND) {
 #pragma unroll
                         for (int j = 0; j < Q; ++j) {
+                            // a block minimum within band^2 - eps is a hit without the FP64 recheck;
+                            // only minima in the uncertain strip go to it
+                            if (!q[j].done && mv[j] <= q[j].tslo) q[j].done = true;
                             const unsigned nj = __ballot_sync(0xffffffffu, !q[j].done && mv[j] <= q[j].ts);
                             if (nj) nn_band_warp(a, T, q[j], nj, sA, sB, sb, n, rb);
                         }
