@@ -1168,13 +1168,15 @@ __device__ double binned_median(long long n, double w, G&& get, long long* shl)
         return s;
     };
     // smallest bin t with cumulative percentage >= 50 (np.searchsorted 'left')
+    // (bins of non-finite values can span the whole int64 range: the midpoint is
+    // taken on the unsigned difference, so every step narrows [a, b])
     long long a = lo, b = hi;
     while (a < b) {
-        long long mid = a + ((b - a) >> 1);
+        const long long mid = a + (long long)(((unsigned long long)b - (unsigned long long)a) >> 1);
         if ((double)count_le(mid) * pct >= 50.0) b = mid; else a = mid + 1;
     }
     const long long cum = count_le(a);
-    const long long cnt = cum - count_le(a - 1);
+    const long long cnt = cum - (a == LLONG_MIN ? 0 : count_le(a - 1));
     const double cumperc = (double)cum * pct;
     const double before = cumperc - (double)cnt * pct;
     const double bin_perc = (double)cnt * pct;
