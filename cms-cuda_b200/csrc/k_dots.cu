@@ -1,6 +1,9 @@
 // Surface pipeline, back half: convex, toroidal and concave dot generation
 // with the burial test, in two passes (count, then emit) that share one code
-// path so the two passes agree by construction.
+// path so the two passes agree by construction.  The count passes keep what
+// the emit passes need (convex: the accepted candidates; toroidal: the torus
+// points with arc dots; concave: the finished dots) in buffers sized by the
+// capacities; a unit that does not fit is recomputed by the emit pass.
 //
 // Reference behaviour (cms-cuda/_core.py):
 //   generate_convex_surface        _core.py:1646-1840
