@@ -273,6 +273,33 @@ __device__ __forceinline__ void nn_recheck(const NNArgs& a, const NNTask& T, con
     }
 }
 
+// nn_recheck over one block [k0, k1) (at most NN_BLK references): the FP32
+// filter first for all of them (independent loads), then the FP64 test for
+// the few under the threshold; ties resolve by original index in any order
+__device__ __forceinline__ void nn_recheck_block(const NNArgs& a, const NNTask& T, const NNTile& tl, float qx2,
+                                                 float qy2, float qz2, float ts, int qdot, long long k0, long long k1,
+                                                 double& best, int& bidx)
+{
+    unsigned cand = 0u;
+#pragma unroll 8
+    for (int t = 0; t < NN_BLK; ++t) {
+        const long long k = k0 + t;
+        if (k < k1) {
+            const float4 r = a.r_f4[T.r0 + k];
+            const float rx = r.x - tl.cx, ry = r.y - tl.cy, rz = r.z - tl.cz;
+            if (nn_s(qx2, qy2, qz2, rx, ry, rz, nn_rr(rx, ry, rz)) <= ts) cand |= 1u << t;
+        }
+    }
+    while (cand) {
+        const int t = __ffs(cand) - 1;
+        cand &= cand - 1;
+        const long long rk = T.r0 + k0 + t;
+        const double e = exact_d2(a.r_xyz + 3LL * nn_rpt(a, rk), a.q_xyz + 3LL * qdot);
+        const int ko = (int)(nn_rpos(a, rk) - T.r0);     // original position: first index on ties
+        if (e < best || (e == best && ko < bidx)) { best = e; bidx = ko; }
+    }
+}
+
 // Minimum searches, rare case: candidates may sit in more than one block.
 // The warp rechecks every reference of the task for each flagged lane,
 // skipping blocks whose box is beyond the lane's cull threshold, and keeps
@@ -590,8 +617,7 @@ __global__ void __launch_bounds__(NN_T, MODE == NN_BAND ? 10 : 8) k_nn(NNArgs a)
                     const long long k1 = min(k0 + NN_BLK, T.rn);
                     double best = INFINITY;
                     int bidx = 0x7fffffff;
-                    for (long long k = k0; k < k1; ++k)
-                        nn_recheck(a, T, tl, q[j].qx2, q[j].qy2, q[j].qz2, q[j].ts, q[j].dot, k, best, bidx);
+                    nn_recheck_block(a, T, tl, q[j].qx2, q[j].qy2, q[j].qz2, q[j].ts, q[j].dot, k0, k1, best, bidx);
                     q[j].best = best; q[j].bidx = bidx;
                 } else {
                     full[j] = true;
