@@ -31,7 +31,8 @@ EXPORTED = (
     "cms_nearest_dots", "cms_nearest_dots_noalloc", "cms_contact_ms_backward", "cms_set_backward",
     "cms_set_grad_total", "cms_grad_xyz", "cms_recompute_dots", "cms_export_dot_units",
     "cms_set_nn_variants", "cms_get_nn_variants", "cms_set_autotune", "cms_refine_begin",
-    "cms_refine_set_params", "cms_refine_run", "cms_refine_pose", "cms_refine_end",
+    "cms_refine_set_params", "cms_refine_run", "cms_refine_pose", "cms_refine_end", "cms_residue_sums",
+    "cms_nn_evaluated",
 )
 
 NN_VARIANT_NAMES = ("q4 r1024", "q4 r512", "q2 r1024", "q2 r512")
@@ -122,6 +123,8 @@ def load():
             "cms_refine_run": [_VP, _I32, _VP, _I32],
             "cms_refine_pose": [_VP, _VP, _VP, _VP, _I32],
             "cms_refine_end": [_VP],
+            "cms_residue_sums": [_VP, _I32, ctypes.c_int64, _PI64, ctypes.c_int64, _VP, _VP, _I32],
+            "cms_nn_evaluated": [_VP, _PI64],
         }
         for name, args in sig.items():
             f = getattr(lib, name)
@@ -264,6 +267,14 @@ class Context:
         return dict(cms_pairs=int(w[0]), cms_queries=int(w[1]), band_pairs=int(w[2]), band_queries=int(w[3]),
                     sc_pairs=int(w[4]), sc_queries=int(w[5]))
 
+    def nn_evaluated(self):
+        """Pairs the FP32 filter evaluated after culling and FP64 rechecks, per search (one counted run)."""
+        w = np.zeros(6, dtype=np.int64)
+        self._check(self.lib.cms_nn_evaluated(self.h, w.ctypes.data_as(_PI64)))
+        names = ("cms", "band", "sc")
+        return {**{f"{n}_evaluated": int(w[k]) for k, n in enumerate(names)},
+                **{f"{n}_rechecks": int(w[3 + k]) for k, n in enumerate(names)}}
+
     def kernel_launches(self):
         return int(self.lib.cms_kernel_launches(self.h))
 
@@ -344,6 +355,20 @@ class Context:
         totals = np.empty(self.B, dtype=np.float64)
         self._check(self.lib.cms_max_contact_ms(self.h, _ptr(per_atom), _ptr(totals), CMS_HOST))
         return per_atom, totals
+
+    def residue_sums(self, res_off, res_atoms, values="cms"):
+        """
+        Per-residue sums of the per-atom CMS ("cms") or maximum CMS ("max") on
+        the device: residue r adds atoms res_atoms[res_off[r]:res_off[r+1]]
+        (batch atom indices) in that order.
+        """
+        off = np.ascontiguousarray(res_off, dtype=np.int64)
+        atoms = np.ascontiguousarray(res_atoms, dtype=np.int32)
+        n = len(off) - 1
+        out = np.empty(max(n, 0), dtype=np.float64)
+        self._check(self.lib.cms_residue_sums(self.h, {"cms": 0, "max": 1}[values], n, off.ctypes.data_as(_PI64),
+                                              len(atoms), _ptr(atoms), _ptr(out), CMS_HOST))
+        return out
 
     def shape_complementarity(self):
         sc = np.empty(self.B * SC_FIELDS, dtype=np.float64)

@@ -169,7 +169,7 @@ class _Run:
         self.radmax = 0.0
         self.results = RESULTS()
         self._host = {}
-        self._state = None          # (lease, inputs, n, n0, sc_done) once a surface exists
+        self._state = None          # (lease, inputs, n, n0, sc_done, order) once a surface exists
         self.surfaces_generated = False
         self.surfaces_generated_all_atoms = None
 
@@ -189,14 +189,31 @@ class _Run:
 
 
 def _export(run, st, name):
-    """Host copy of one calc.run container from the device state of the run's surface."""
-    lease, (xyz, rad, dens, mol), n, n0, sc_done = st
+    """
+    Host copy of one calc.run container from the device state of the run's
+    surface.  The device holds the atoms binder first; `order` (None when the
+    atoms were added binder first) maps each device position to the atom's
+    position in AddMolecule order, the reference's natom numbering
+    (_core.py:372-399), and every container is returned in that numbering.
+    """
+    lease, (xyz, rad, dens, mol), n, n0, sc_done, order = st
     ctx = lease.ctx
+
+    def user(idx):
+        return idx if order is None else order[idx].astype(np.int32)
+
+    def rows_by_atom(atom_of_row):
+        # rows are grouped by generating atom in device order; the reference groups them in natom order
+        return slice(None) if order is None else np.argsort(order[atom_of_row], kind="stable")
+
     if name == "atoms":
         a = AtomArray(n)
-        a.xyz, a.radius, a.density, a.molecule = xyz, rad, dens, mol
         atten, access, _, _ = ctx.export_atoms(0, n)
-        a.atten, a.access = atten, access
+        if order is not None:          # device order -> AddMolecule order (the inputs are kept in that order)
+            atten_d, access_d = atten, access
+            atten, access = np.empty_like(atten_d), np.empty_like(access_d)
+            atten[order], access[order] = atten_d, access_d
+        a.xyz, a.radius, a.density, a.molecule, a.atten, a.access = xyz, rad, dens, mol, atten, access
         return a
     info = ctx.info(0)
     if name in ("neighbor_array", "buried_array"):
@@ -207,16 +224,26 @@ def _export(run, st, name):
         arr = SimpleNeighborArray(n, K)
         rows = np.repeat(np.arange(n), cnt)
         cols = np.arange(len(ids)) - np.repeat(off[:-1], cnt)
+        ids = user(ids)
+        if order is not None:
+            rows = order[rows]
         arr.natom[rows, cols] = ids
         arr.radius[rows, cols] = rad[ids]
         arr.xyz[rows, cols] = xyz[ids]
-        arr.nneighbors[:] = cnt
+        arr.nneighbors[np.arange(n) if order is None else order] = cnt
         return arr
     if name == "toroid_queue":
         a1, a2, uij, tij, rij, bet = ctx.export_toroid(0, info)
+        k = rows_by_atom(a1)
+        a1, a2, uij, tij, rij, bet = user(a1)[k], user(a2)[k], uij[k], tij[k], rij[k], bet[k]
         return [(int(a1[k]), int(a2[k]), uij[k], tij[k], float(rij[k]), bool(bet[k])) for k in range(len(a1))]
     if name == "probes":
         a0, a1, a2, h, pt, alt = ctx.export_probes(0, info)
+        if order is not None:
+            # all '+' probes (atoms i, j, k), then all '-' probes (atoms j, i, k), each in natom order of i
+            npl = int(info.n_probes_plus[0] + info.n_probes_plus[1])
+            k = np.concatenate([rows_by_atom(a0[:npl]), npl + rows_by_atom(a1[npl:])])
+            a0, a1, a2, h, pt, alt = user(a0)[k], user(a1)[k], user(a2)[k], h[k], pt[k], alt[k]
         p = ProbeArray()
         p.atom_idx_0, p.atom_idx_1, p.atom_idx_2, p.height, p.point_xyz, p.alt_xyz = a0, a1, a2, h, pt, alt
         return p
@@ -225,6 +252,7 @@ def _export(run, st, name):
         for m in (0, 1):
             d = DotArray()
             d.coor_xyz, d.outnml_xyz, d.area, d.buried, d.type_, d.atom_idx = ctx.export_dots(0, m, info)
+            d.atom_idx = user(d.atom_idx)
             out.append(d)
         return out
     if name == "trimmed_dots":
@@ -277,10 +305,11 @@ class MolecularSurfaceCalculator:
 
     def AddMolecule(self, molecule, xyz, radii):
         """
-        Load atoms of one molecule (0 = binder, anything else = target).
-        Atoms with radius <= 0 are kept so per-atom outputs stay aligned.
-        Molecule-0 atoms must be added before molecule-1 atoms (the order of
-        add_binder_and_target).
+        Load atoms of one molecule (0 = binder, anything else = target), in
+        any order and any number of calls (_core.py:923-943).  Atoms with
+        radius <= 0 are kept so per-atom outputs stay aligned.  Atoms are
+        numbered in call order (calc.run uses that numbering); per-atom
+        readouts list one molecule's atoms in the order they were added.
         """
         if hasattr(xyz, "detach"):
             xyz = xyz.detach().cpu().numpy()
@@ -292,8 +321,6 @@ class MolecularSurfaceCalculator:
         xyz = np.asarray(xyz, dtype=np.float64).reshape(n, 3) if n else np.zeros((0, 3))
         if n == 0:
             return
-        if mol == 0 and any(m == 1 for m in self._mol):
-            raise NotImplementedError("molecule 0 (binder) atoms must be added before molecule 1 (target) atoms")
         self._xyz.append(xyz.copy())
         self._rad.append(radii.copy())
         self._dens.append(np.full(n, float(self.settings.density)))
@@ -302,12 +329,16 @@ class MolecularSurfaceCalculator:
         self.run.results.nAtoms += n
 
     def _arrays(self):
+        """Atoms in AddMolecule order, and the device order: binder atoms first, each molecule in call order."""
         xyz = np.concatenate(self._xyz) if self._xyz else np.zeros((0, 3))
         rad = np.concatenate(self._rad) if self._rad else np.zeros(0)
         dens = np.concatenate(self._dens) if self._dens else np.zeros(0)
         mol = np.concatenate([np.full(len(r), m, np.int8) for r, m in zip(self._rad, self._mol)]) \
             if self._rad else np.zeros(0, np.int8)
-        return xyz, rad, dens, mol
+        order = np.argsort(mol, kind="stable")
+        if np.all(mol[:-1] <= mol[1:]):
+            order = None
+        return xyz, rad, dens, mol, order
 
     # -- generation --------------------------------------------------------------
     def _context(self):
@@ -328,23 +359,29 @@ class MolecularSurfaceCalculator:
                     "and re-add your atoms, or use a fresh MolecularSurfaceCalculator()."
                 )
             return
-        xyz, rad, dens, mol = self._arrays()
+        xyz, rad, dens, mol, order = self._arrays()
         assert len(rad) > 0
         ctx = self._context()
         ctx.set_settings(self.settings)
         n0 = int((mol == 0).sum())
-        ctx.load_batch(np.array([0, len(rad)]), np.array([n0]), xyz, rad, dens)
+        if order is None:
+            ctx.load_batch(np.array([0, len(rad)]), np.array([n0]), xyz, rad, dens)
+        else:
+            ctx.load_batch(np.array([0, len(rad)]), np.array([n0]), xyz[order], rad[order], dens[order])
         ctx.generate(all_atoms=all_atoms)
         info = ctx.info(0)
         if info.status & _lib.ST_COINCIDENT:
             i, j = info.coincident_i, info.coincident_j
+            if order is not None:
+                i, j = sorted((int(order[i]), int(order[j])))
             raise RuntimeError(f"Coincident atoms: {i}:: == {j}::")
         if info.status & _lib.ST_NEAR_OVERFLOW:
             raise RuntimeError("too many nearby low probes for one probe (limit 512)")
         self._n = len(rad)
         self._n0 = n0
+        self._order = order
         self._sc_done = [False]
-        self.run._state = (self._lease, (xyz, rad, dens, mol), len(rad), n0, self._sc_done)
+        self.run._state = (self._lease, (xyz, rad, dens, mol), len(rad), n0, self._sc_done, order)
         self.run.radmax = np.float64(rad.max())
         r = self.run.results
         r.dots.convex += int(info.convex)
@@ -384,15 +421,20 @@ class MolecularSurfaceCalculator:
 
     def calc_contact_molecular_surface_gradient(self, target_side=True):
         """
-        d(CMS)/d(xyz) of every loaded atom (N x 3, in AddMolecule order:
-        binder rows, then target rows) for the target-side (or binder-side)
+        d(CMS)/d(xyz) of every loaded atom (N x 3, rows in AddMolecule order)
+        for the target-side (or binder-side)
         CMS, with the generated dot topology held fixed.  The reference has
         no gradient; this is the FP64 adjoint of calc_contact_molecular_surface.
         """
         self._ensure_surfaces_generated(all_atoms=False)
         if self._cms is None:
             self.calc_contact_molecular_surface(target_side)
-        return self._context().contact_ms_backward(target_side=target_side)
+        g = self._context().contact_ms_backward(target_side=target_side)
+        if self._order is None:
+            return g
+        out = np.empty_like(g)
+        out[self._order] = g
+        return out
 
     def calc_max_possible_contact_molecular_surface(self, target_side=True):
         if self._max is None:

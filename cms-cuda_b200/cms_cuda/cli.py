@@ -3,12 +3,18 @@ Batch command line: contact molecular surface (CMS) and shape
 complementarity (SC) of many complex structures (PDB or mmCIF) in one GPU
 batch.
 
-Same arguments, printed rows, CSV columns and per-residue tables as the
-reference's example CLI (examples/calculate_cms_sc.py), but every structure
-of the command line is evaluated in one batched pass of the CUDA pipeline
-instead of one calculator per file; a structure that cannot be loaded gets an
-error row and the others proceed.  "seconds" is the batch's wall time shared
-equally between its structures.
+The command-line contract is the reference example CLI's
+(examples/calculate_cms_sc.py:130-211): the same options, the same
+``key=value`` rows (structure, device, atom counts, cms, cms_binder, sc,
+sc_area, sc_median_dist, max_cms_*, cms_fraction_*, seconds; or structure and
+error), the same CSV columns and per-residue tables
+``<structure>_<side>_cms.csv`` (chain, resnum, resname, cms).  The work is
+organised differently: every loadable structure of the command line goes into
+one batched pass of the CUDA pipeline (plus one all-atoms batch for
+``--max-cms``), and the per-residue tables are summed on the device for the
+whole batch at once.  A structure that cannot be loaded gets an error row and
+the others proceed; ``seconds`` is the batch's wall time divided evenly
+between its structures.
 
   python -m cms_cuda.cli designs/*.pdb --binder-chains B --target-chains A \\
       --csv cms_sc.csv --per-residue per_residue/ --max-cms
@@ -22,135 +28,226 @@ import time
 
 import numpy as np
 
-from .loader import load_atoms, per_residue
+from .loader import load_atoms, residue_groups
+
+SIDES = ("binder", "target")
+ROUND = 4          # decimals of every printed / written value
 
 
-def _split(s):
-    return [x for x in s.split(",") if x] if s else None
+def _names(text):
+    """'A,B,,C' -> ['A', 'B', 'C']; None / '' -> None."""
+    items = [t for t in (text or "").split(",") if t]
+    return items or None
 
 
-def _unmatched(info, radii):
-    return sorted({(i[2], i[3]) for i, r in zip(info, radii) if r == 0.0})
+class Selection:
+    """Which atoms of a structure form one side (the loader's keyword arguments)."""
+
+    def __init__(self, chains=None, resnames=None, exclude=None, keep_water=False, keep_ions=False):
+        self.kwargs = dict(chains=chains, resnames=set(resnames) if resnames else None,
+                           exclude_resnames=set(exclude or ()), keep_water=keep_water, keep_ions=keep_ions)
+        self.defined = bool(chains or resnames)
+
+    @classmethod
+    def from_args(cls, args, side):
+        return cls(_names(getattr(args, f"{side}_chains")), _names(getattr(args, f"{side}_resnames")),
+                   _names(getattr(args, f"{side}_exclude")), args.keep_water, args.keep_ions)
+
+    def load(self, path):
+        return load_atoms(path, **self.kwargs)
+
+
+class Loaded:
+    """One structure's two sides as loaded: coordinates, radii and per-atom records."""
+
+    def __init__(self, slot, name, sides):
+        self.slot, self.name = slot, name
+        (self.bx, self.br, self.binfo), (self.tx, self.tr, self.tinfo) = sides
+
+    def invisible_atoms(self):
+        """Per side: (count, sample of (residue, atom) names) of atoms with no radius-table entry."""
+        out = {}
+        for side, radii, info in (("binder", self.br, self.binfo), ("target", self.tr, self.tinfo)):
+            zero = np.nonzero(radii == 0.0)[0]
+            if len(zero):
+                out[side] = (len(zero), sorted({(info[a][2], info[a][3]) for a in zero}))
+        return out
 
 
 def parser():
     ap = argparse.ArgumentParser(prog="python -m cms_cuda.cli", description=__doc__,
                                  formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("structures", nargs="+", help="PDB / mmCIF files of the complexes")
-    for side in ("binder", "target"):
-        ap.add_argument(f"--{side}-chains", help=f"comma-separated chain IDs of the {side} (default: all)")
-        ap.add_argument(f"--{side}-resnames", help=f"only these residue names in the {side}, e.g. BTN")
-        ap.add_argument(f"--{side}-exclude", help=f"residue names to drop from the {side}, e.g. BTN")
-    ap.add_argument("--keep-water", action="store_true", help="keep water molecules")
-    ap.add_argument("--keep-ions", action="store_true", help="keep single-atom ions (most get radius 0)")
-    ap.add_argument("--device", default="auto", help="auto, cuda, gpu or cuda:N (no CPU path)")
-    ap.add_argument("--no-sc", action="store_true", help="skip shape complementarity")
+    ap.add_argument("structures", nargs="+", help="structure files (.pdb / .ent / .cif / .mmcif), one complex each")
+    for side in SIDES:
+        ap.add_argument(f"--{side}-chains", metavar="IDS",
+                        help=f"chains forming the {side}, comma-separated (all chains if not given)")
+        ap.add_argument(f"--{side}-resnames", metavar="NAMES",
+                        help=f"restrict the {side} to residues with these names, comma-separated")
+        ap.add_argument(f"--{side}-exclude", metavar="NAMES",
+                        help=f"leave residues with these names out of the {side}, comma-separated")
+    ap.add_argument("--keep-water", action="store_true", help="do not drop water residues")
+    ap.add_argument("--keep-ions", action="store_true",
+                    help="do not drop one-atom hetero residues (ions; most have no radius and stay invisible)")
+    ap.add_argument("--device", default="auto", help="auto, cuda, gpu or cuda:N (there is no CPU path)")
+    ap.add_argument("--no-sc", action="store_true", help="report CMS only, no shape complementarity")
     ap.add_argument("--max-cms", action="store_true",
-                    help="also compute the maximum possible CMS (total molecular surface) of each side")
-    ap.add_argument("--csv", help="write one row per structure to this CSV file")
-    ap.add_argument("--per-residue", metavar="DIR", help="write per-residue CMS tables to this directory")
+                    help="add each side's maximum possible CMS (its whole molecular surface area)")
+    ap.add_argument("--csv", metavar="FILE", help="also write the rows, one per structure, as CSV")
+    ap.add_argument("--per-residue", metavar="DIR", help="write a per-residue CMS table per structure and side")
     return ap
+
+
+def _pack(loaded):
+    """Batch arrays: per complex its binder atoms, then its target atoms."""
+    n_binder = np.array([len(L.br) for L in loaded], np.int64)
+    atom_off = np.zeros(len(loaded) + 1, np.int64)
+    atom_off[1:] = np.cumsum([len(L.br) + len(L.tr) for L in loaded])
+    xyz = np.concatenate([a for L in loaded for a in (L.bx, L.tx)])
+    rad = np.concatenate([a for L in loaded for a in (L.br, L.tr)])
+    return atom_off, n_binder, xyz, rad
+
+
+def _residue_tables(ctx, loaded, atom_off):
+    """Per structure and side: [(chain, resnum, resname, summed per-atom CMS)], summed on the device."""
+    parts, offs, atoms, base = [], [np.zeros(1, np.int64)], [], 0
+    for c, L in enumerate(loaded):
+        for side, info, first in (("target", L.tinfo, atom_off[c] + len(L.br)), ("binder", L.binfo, atom_off[c])):
+            keys, off, members = residue_groups(info, first)
+            parts.append((c, side, keys))
+            offs.append(off[1:] + base)
+            atoms.append(members)
+            base += len(members)
+    sums = ctx.residue_sums(np.concatenate(offs), np.concatenate(atoms))
+    tables, r = {}, 0
+    for c, side, keys in parts:
+        tables[(c, side)] = [(*k, float(v)) for k, v in zip(keys, sums[r:r + len(keys)])]
+        r += len(keys)
+    return tables
+
+
+def _max_cms(dev, loaded):
+    """Maximum possible CMS of every target and binder (each alone as molecule 0, all atoms attended)."""
+    from . import _lib
+    alone = [(L.tx, L.tr) for L in loaded] + [(L.bx, L.br) for L in loaded]
+    off = np.zeros(len(alone) + 1, np.int64)
+    off[1:] = np.cumsum([len(r) for _, r in alone])
+    ctx = _lib.Context(dev)
+    ctx.load_batch(off, np.diff(off), np.concatenate([x for x, _ in alone]), np.concatenate([r for _, r in alone]))
+    ctx.generate(all_atoms=True)
+    totals = ctx.max_contact_ms()[1]
+    return totals[:len(loaded)], totals[len(loaded):]
+
+
+def evaluate(loaded, dev, sc=True, max_cms=False, per_residue=False):
+    """
+    One batched pass over the loaded structures: a result dict per structure
+    (its row values, or an error), plus per-residue tables when asked.
+    """
+    from . import _lib
+    atom_off, n_binder, xyz, rad = _pack(loaded)
+    ctx = _lib.Context(dev)
+    ctx.load_batch(atom_off, n_binder, xyz, rad)
+    ctx.generate(all_atoms=False)
+    infos = [ctx.info(c) for c in range(len(loaded))]
+    _, totals = ctx.contact_ms(per_atom=False)
+    sc_out = ctx.shape_complementarity()[0] if sc else None
+    max_t, max_b = _max_cms(dev, loaded) if max_cms else (None, None)
+    tables = _residue_tables(ctx, loaded, atom_off) if per_residue else {}
+    results = []
+    for c, L in enumerate(loaded):
+        i = infos[c]
+        if i.status & _lib.ST_COINCIDENT:
+            results.append(dict(error=f"Coincident atoms: {i.coincident_i}:: == {i.coincident_j}::"))
+            continue
+        res = dict(cms=float(totals[c, 1]), cms_binder=float(totals[c, 0]))
+        if sc_out is not None:
+            res.update(sc=float(sc_out[c, 0]), sc_area=float(sc_out[c, 1]), sc_median_dist=float(sc_out[c, 2]))
+        if max_t is not None:
+            res.update(max_cms_target=float(max_t[c]), max_cms_binder=float(max_b[c]))
+        res["residues"] = {side: tables.get((c, side)) for side in ("target", "binder")}
+        results.append(res)
+    return results
+
+
+def _row(L, dev, res, seconds):
+    """The printed / CSV row of one evaluated structure (the reference CLI's keys, values rounded)."""
+    if "error" in res:
+        return dict(structure=L.name, error=res["error"])
+    row = dict(structure=L.name, device=f"cuda:{dev}", binder_atoms=len(L.br), target_atoms=len(L.tr),
+               cms=round(res["cms"], ROUND), cms_binder=round(res["cms_binder"], ROUND))
+    if "sc" in res:
+        row.update({k: round(res[k], ROUND) for k in ("sc", "sc_area", "sc_median_dist")})
+    if "max_cms_target" in res:
+        mt, mb = res["max_cms_target"], res["max_cms_binder"]
+        row.update(max_cms_target=round(mt, ROUND), max_cms_binder=round(mb, ROUND),
+                   cms_fraction_target=round(res["cms"] / mt, ROUND) if mt else 0.0,
+                   cms_fraction_binder=round(res["cms_binder"] / mb, ROUND) if mb else 0.0)
+    row["seconds"] = round(seconds, 3)
+    return row
+
+
+def write_residue_table(path, table):
+    with open(path, "w", newline="") as f:
+        out = csv.writer(f)
+        out.writerow(("chain", "resnum", "resname", "cms"))
+        for chain, resnum, resname, value in table:
+            out.writerow((chain, resnum, resname, round(value, ROUND)))
+
+
+def write_rows_csv(path, rows):
+    columns = list(dict.fromkeys(k for row in rows for k in row))
+    with open(path, "w", newline="") as f:
+        out = csv.DictWriter(f, fieldnames=columns)
+        out.writeheader()
+        out.writerows(rows)
 
 
 def main(argv=None, out=sys.stdout):
     ap = parser()
     args = ap.parse_args(argv)
-    if not (args.binder_chains or args.binder_resnames) or not (args.target_chains or args.target_resnames):
-        ap.error("select both sides, e.g. --binder-chains B --target-chains A")
-    from . import _lib
+    selections = [Selection.from_args(args, side) for side in SIDES]
+    if not all(s.defined for s in selections):
+        ap.error("both sides need a selection, e.g. --binder-chains B --target-chains A")
     from ._api import _device_index
     dev = _device_index(args.device)
-
-    def sel(side):
-        return dict(chains=_split(getattr(args, f"{side}_chains")),
-                    resnames=set(_split(getattr(args, f"{side}_resnames")) or []) or None,
-                    exclude_resnames=set(_split(getattr(args, f"{side}_exclude")) or []),
-                    keep_water=args.keep_water, keep_ions=args.keep_ions)
-
     if args.per_residue:
         os.makedirs(args.per_residue, exist_ok=True)
-    t0 = time.perf_counter()
-    loaded, rows = [], [None] * len(args.structures)
-    for k, path in enumerate(args.structures):
+
+    start = time.perf_counter()
+    rows = [None] * len(args.structures)
+    loaded = []
+    for slot, path in enumerate(args.structures):
         name = os.path.basename(path)
         try:
-            bx, br, binfo = load_atoms(path, **sel("binder"))
-            tx, tr, tinfo = load_atoms(path, **sel("target"))
-            if len(bx) == 0 or len(tx) == 0:
-                raise ValueError(f"empty selection (binder {len(bx)} atoms, target {len(tx)} atoms)")
-            for side, info, radii in (("binder", binfo, br), ("target", tinfo, tr)):
-                bad = _unmatched(info, radii)
-                if bad:
-                    print(f"  warning: {name} {side}: {int((radii == 0).sum())} atoms have radius 0 "
-                          f"(no entry in the radius table, they are invisible): {bad[:8]}", file=sys.stderr)
-            loaded.append((k, name, bx, br, binfo, tx, tr, tinfo))
-        except Exception as exc:
-            rows[k] = dict(structure=name, error=str(exc))
+            sides = [sel.load(path) for sel in selections]
+            if any(len(radii) == 0 for _, radii, _ in sides):
+                raise ValueError("empty selection (binder %d atoms, target %d atoms)"
+                                 % (len(sides[0][1]), len(sides[1][1])))
+        except Exception as exc:           # one bad file does not stop the batch
+            rows[slot] = dict(structure=name, error=str(exc))
             print(f"  error: {name}: {exc}", file=sys.stderr)
+            continue
+        L = Loaded(slot, name, sides)
+        for side, (count, names) in L.invisible_atoms().items():
+            print(f"  warning: {name} {side}: {count} atom(s) without a radius-table entry get radius 0 and add "
+                  f"no surface: {names[:8]}", file=sys.stderr)
+        loaded.append(L)
 
     if loaded:
-        # one batch: per complex the binder atoms, then the target atoms
-        off = np.zeros(len(loaded) + 1, np.int64)
-        nb = np.array([len(L[2]) for L in loaded], np.int64)
-        off[1:] = np.cumsum([len(L[2]) + len(L[5]) for L in loaded])
-        xyz = np.concatenate([np.concatenate([L[2], L[5]]) for L in loaded])
-        rad = np.concatenate([np.concatenate([L[3], L[6]]) for L in loaded])
-        ctx = _lib.Context(dev)
-        ctx.load_batch(off, nb, xyz, rad)
-        ctx.generate(all_atoms=False)
-        statuses = [ctx.info(c).status for c in range(len(loaded))]
-        per_atom, tot = ctx.contact_ms(per_atom=True)
-        sc = ctx.shape_complementarity()[0] if not args.no_sc else None
-        mx = None
-        if args.max_cms:
-            # maximum possible CMS: each side alone as molecule 0, all atoms attended
-            sides = [(L[5], L[6]) for L in loaded] + [(L[2], L[3]) for L in loaded]
-            moff = np.zeros(len(sides) + 1, np.int64)
-            moff[1:] = np.cumsum([len(s[1]) for s in sides])
-            m = _lib.Context(dev)
-            m.load_batch(moff, np.diff(moff), np.concatenate([s[0] for s in sides]),
-                         np.concatenate([s[1] for s in sides]))
-            m.generate(all_atoms=True)
-            mx = m.max_contact_ms()[1]
-        share = (time.perf_counter() - t0) / len(loaded)
-        for c, (k, name, bx, br, binfo, tx, tr, tinfo) in enumerate(loaded):
-            if statuses[c] & _lib.ST_COINCIDENT:
-                i = ctx.info(c)
-                rows[k] = dict(structure=name, error=f"Coincident atoms: {i.coincident_i}:: == {i.coincident_j}::")
-                continue
-            a0, n = int(off[c]), len(bx)
-            cms, cms_b = float(tot[c, 1]), float(tot[c, 0])
-            row = dict(structure=name, device=f"cuda:{dev}", binder_atoms=len(bx), target_atoms=len(tx),
-                       cms=round(cms, 4), cms_binder=round(cms_b, 4))
-            if sc is not None:
-                row.update(sc=round(float(sc[c, 0]), 4), sc_area=round(float(sc[c, 1]), 4),
-                           sc_median_dist=round(float(sc[c, 2]), 4))
-            if mx is not None:
-                max_t, max_b = float(mx[c]), float(mx[len(loaded) + c])
-                row.update(max_cms_target=round(max_t, 4), max_cms_binder=round(max_b, 4),
-                           cms_fraction_target=round(cms / max_t, 4) if max_t else 0.0,
-                           cms_fraction_binder=round(cms_b / max_b, 4) if max_b else 0.0)
-            row["seconds"] = round(share, 3)
-            if args.per_residue:
-                base = os.path.splitext(name)[0]
-                pa_t = per_atom[a0 + n:int(off[c + 1])]
-                pa_b = per_atom[a0:a0 + n]
-                for side, info, values in (("target", tinfo, pa_t), ("binder", binfo, pa_b)):
-                    with open(os.path.join(args.per_residue, f"{base}_{side}_cms.csv"), "w", newline="") as f:
-                        w = csv.writer(f)
-                        w.writerow(["chain", "resnum", "resname", "cms"])
-                        w.writerows((ch, nr, rn, round(v, 4)) for ch, nr, rn, v in per_residue(info, values))
-            rows[k] = row
+        results = evaluate(loaded, dev, sc=not args.no_sc, max_cms=args.max_cms,
+                           per_residue=bool(args.per_residue))
+        seconds = (time.perf_counter() - start) / len(loaded)
+        for L, res in zip(loaded, results):
+            rows[L.slot] = _row(L, dev, res, seconds)
+            if args.per_residue and "error" not in res:
+                stem = os.path.splitext(L.name)[0]
+                for side in ("target", "binder"):
+                    write_residue_table(os.path.join(args.per_residue, f"{stem}_{side}_cms.csv"),
+                                        res["residues"][side])
     for row in rows:
         print("  ".join(f"{k}={v}" for k, v in row.items()), file=out)
     if args.csv:
-        keys = []
-        for r in rows:
-            keys += [k for k in r if k not in keys]
-        with open(args.csv, "w", newline="") as f:
-            w = csv.DictWriter(f, fieldnames=keys)
-            w.writeheader()
-            w.writerows(rows)
+        write_rows_csv(args.csv, rows)
         print(f"wrote {args.csv}", file=out)
     return rows
 

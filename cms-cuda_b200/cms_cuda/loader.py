@@ -177,14 +177,21 @@ def load_atoms(path, chains=None, resnames=None, exclude_resnames=(), keep_water
     return xyz, get_radii_from_names(res_names, atom_names), info
 
 
-def per_residue(info, per_atom):
-    """Sum a per-atom array over residues, in order of first appearance:
-    list of (chain, residue number, residue name, value)."""
-    sums, order = {}, []
-    for (chain, resnum, resname, _, _), v in zip(info, per_atom):
-        key = (chain, resnum, resname)
-        if key not in sums:
-            sums[key] = 0.0
-            order.append(key)
-        sums[key] += float(v)
-    return [(*k, sums[k]) for k in order]
+def residue_groups(info, first_atom=0):
+    """
+    Residues of one side as a CSR map for the device's per-residue sums
+    (``Context.residue_sums``): the residue keys (chain, residue number, residue
+    name) in order of first appearance, offsets (len(keys) + 1, int64) and the
+    member atoms of each residue in atom order (int32), shifted by
+    ``first_atom`` -- the side's first atom in a batch.  The reference CLI keys
+    its per-residue table the same way (examples/calculate_cms_sc.py:105-114).
+    """
+    slot = {}
+    member = np.empty(len(info), dtype=np.int64)
+    for a, rec in enumerate(info):
+        member[a] = slot.setdefault(rec[:3], len(slot))
+    keys = list(slot)
+    atoms = np.argsort(member, kind="stable").astype(np.int32) + np.int32(first_atom)
+    off = np.zeros(len(keys) + 1, dtype=np.int64)
+    np.cumsum(np.bincount(member, minlength=len(keys)), out=off[1:])
+    return keys, off, atoms

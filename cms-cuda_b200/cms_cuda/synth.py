@@ -120,11 +120,13 @@ class Batch:
         return self.xyz[a0:s1], self.radius[a0:s1], self.xyz[s1:a1], self.radius[s1:a1]
 
 
-def make_batch(n_target, n_binder, seed, ligand=None, threads=None, names=False):
+def make_batch(n_target, n_binder, seed, ligand=None, threads=None, names=False, select=None):
     """
     Generate a batch of complexes with the given per-complex atom counts.
     ligand: optional bool array marking binders that are ligand clusters.
     names: also keep each atom's residue name, atom name and residue number.
+    select: optional complex indices; only those complexes are generated (in
+    that order), each identical to its copy in the full batch.
     """
     n_target = np.asarray(n_target, dtype=np.int32).reshape(-1)
     n_binder = np.asarray(n_binder, dtype=np.int32).reshape(-1)
@@ -132,6 +134,10 @@ def make_batch(n_target, n_binder, seed, ligand=None, threads=None, names=False)
     ligand = np.zeros(B, bool) if ligand is None else np.asarray(ligand, bool)
     rng = np.random.default_rng(seed)
     seeds = rng.integers(0, 2**63 - 1, size=B, dtype=np.int64).astype(np.uint64)
+    if select is not None:
+        select = np.asarray(select, dtype=np.int64)
+        n_target, n_binder, ligand, seeds = n_target[select], n_binder[select], ligand[select], seeds[select]
+        B = len(select)
     atom_off = np.zeros(B + 1, dtype=np.int64)
     atom_off[1:] = np.cumsum(n_target.astype(np.int64) + n_binder)
     N = int(atom_off[-1])
@@ -220,11 +226,21 @@ def config_refine(B=256, seed=5):
     return make_batch(nt, nb, seed + 1)
 
 
-def config_batched(B=4096, seed=2):
-    """B complexes, target log-uniform 600-4000, binder log-uniform 80-1200, ~5 % ligand binders of 20-60 atoms."""
+def batched_sizes(B=4096, seed=2):
+    """(target atoms, binder atoms, ligand flag) per complex of config_batched(B, seed), without the coordinates."""
     rng = np.random.default_rng(seed)
     nt = np.exp(rng.uniform(np.log(600), np.log(4000), B)).astype(np.int32)
     nb = np.exp(rng.uniform(np.log(80), np.log(1200), B)).astype(np.int32)
     lig = rng.random(B) < 0.05
     nb[lig] = rng.integers(20, 61, int(lig.sum()))
-    return make_batch(nt, nb, seed + 1, ligand=lig)
+    return nt, nb, lig
+
+
+def config_batched(B=4096, seed=2, select=None):
+    """
+    B complexes, target log-uniform 600-4000, binder log-uniform 80-1200, ~5 %
+    ligand binders of 20-60 atoms; `select` generates only those complexes
+    (a shard of the batch).
+    """
+    nt, nb, lig = batched_sizes(B, seed)
+    return make_batch(nt, nb, seed + 1, ligand=lig, select=select)

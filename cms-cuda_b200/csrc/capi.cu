@@ -39,6 +39,31 @@ __global__ void k_fill_i(int* p, long long n, int v)
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) p[i] = v;
 }
 
+// Per-residue sums of a per-atom array: residue r adds the values of atoms
+// res_atoms[res_off[r] .. res_off[r+1]) in that order, starting from 0.0 --
+// the running dictionary sum of the reference CLI's per_residue
+// (examples/calculate_cms_sc.py:105-114), one residue per thread.  Offsets
+// outside [0, n_entries] or decreasing, and atom indices outside [0, N), set
+// *bad and are skipped.
+__global__ void k_residue_sums(const double* per_atom, long long N, const long long* res_off, long long n_res,
+                               const int* res_atoms, long long n_entries, double* out, int* bad)
+{
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n_res; r += (long long)gridDim.x * blockDim.x) {
+        long long k0 = res_off[r], k1 = res_off[r + 1];
+        if (k0 < 0 || k1 > n_entries || k1 < k0) {
+            *bad = 1;
+            k0 = k1 = 0;
+        }
+        double acc = 0.0;
+        for (long long k = k0; k < k1; ++k) {
+            const int a = res_atoms[k];
+            if (a < 0 || a >= N) { *bad = 1; continue; }
+            acc += per_atom[a];
+        }
+        out[r] = acc;
+    }
+}
+
 // totals the host needs after a run: cells, neighbour / buried entries,
 // toroid pairs, probes, dots, buried dots, trimmed dots
 // capacity check of a stage total (two totals summed when b is given)
@@ -226,6 +251,7 @@ struct cms_ctx {
     std::string err;
     // stage timing: an event after each pipeline stage when profiling
     bool profiling = false;
+    bool counting = false;   // readouts run with the nearest-dot work counters (cms_nn_evaluated)
     long long h2d_bytes = 0, d2h_bytes = 0;   // host<->device bytes moved by the hot path
     std::vector<cudaEvent_t> marks;
     std::vector<int> mark_ids;
@@ -252,7 +278,7 @@ struct cms_ctx {
         S_ADJ_LIST_CONC, S_ADJ_NACT, S_OVF, S_REF_XYZ, S_POSE, S_POSE_CKPT, S_POSE_CEN, S_HIST, S_STEP, S_MAXSUM,
         S_TOR_LFLAG, S_TOR_LOFF, S_TOR_LIST, S_PTOP, S_SP_A, S_SP_H, S_SP_XYZ, S_SP_ALT, S_SP_G, S_SP_ORD,
         S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1, S_KS_TOP, S_KS_BUF, S_CV_SOFF, S_CC_SOFF, S_TOR_SOFF, S_TOR_SN, S_NBS_TOP, S_NBS_BUF, S_NB_SOFF, S_ADJ_SKEY, S_ADJ_SLIST_CONV, S_ADJ_SLIST_TOR, S_ADJ_SLIST_CONC, S_CS_TOP, S_CS_XYZ, S_CS_AREA, S_CS_OWN,
-        S_CS_SUB, S_CS_BUR,
+        S_CS_SUB, S_CS_BUR, S_RES_OFF, S_RES_ATOMS, S_RES_SUM, S_RES_FLAG, S_NN_COUNT,
         S_COUNT
     };
 
@@ -626,6 +652,11 @@ NNArgs nn_args(cms_ctx* x, int kind)
     a.box_blk = x->get<float4>(cms_ctx::S_BOX_BLK);
     a.round_cap = nn_round_cap(x->cap_dot, 2LL * x->B);
     a.ovf = x->d.ovf;
+    if (x->counting) {
+        unsigned long long* c = x->get<unsigned long long>(cms_ctx::S_NN_COUNT);
+        a.pair_count = c + kind;
+        a.recheck_count = c + 3 + kind;
+    }
     return a;
 }
 
@@ -1011,6 +1042,56 @@ cms_status cms_contact_ms(cms_ctx* x, double* per_atom, double* totals, int32_t 
     }
     if (per_atom) copy_out(x, per_atom, x->get<double>(cms_ctx::S_PER_ATOM_CMS), sizeof(double) * x->N, where);
     if (totals) copy_out(x, totals, x->get<double>(cms_ctx::S_TOT_CMS), sizeof(double) * 2 * x->B, where);
+    API_END
+}
+
+cms_status cms_residue_sums(cms_ctx* x, int32_t values, int64_t n_residues, const int64_t* res_off,
+                            int64_t n_entries, const int32_t* res_atoms, double* sums, int32_t where)
+{
+    if (!x) return CMS_ERR_ARG;
+    if (n_residues < 0 || n_entries < 0 || (values != 0 && values != 1) || (n_residues > 0 && (!res_off || !sums)) ||
+        (n_entries > 0 && !res_atoms))
+        return fail(x, CMS_ERR_ARG, "cms_residue_sums: bad arguments");
+    API_BEGIN
+    need_surface(x);
+    if (values == 0 && !x->cms_ok) {
+        enqueue_cms(x);
+        ck(cudaGetLastError(), "cms kernels");
+        x->cms_ok = true;
+    }
+    if (values == 1 && !x->max_ok) {
+        enqueue_max(x);
+        ck(cudaGetLastError(), "max cms kernels");
+        x->max_ok = true;
+    }
+    if (n_residues == 0) return CMS_OK;
+    cudaStream_t s = x->stream;
+    const long long* doff = (const long long*)res_off;
+    const int* datoms = res_atoms;
+    double* dsum = sums;
+    if (where == CMS_HOST) {
+        if (res_off[0] != 0 || res_off[n_residues] != n_entries)
+            throw Fail{CMS_ERR_ARG, "cms_residue_sums: offsets must run from 0 to n_entries"};
+        long long* o = x->ensure<long long>(cms_ctx::S_RES_OFF, n_residues + 1);
+        int* a = x->ensure<int>(cms_ctx::S_RES_ATOMS, n_entries);
+        x->h2d_bytes += (long long)(sizeof(long long) * (n_residues + 1) + sizeof(int) * n_entries);
+        ck(cudaMemcpyAsync(o, res_off, sizeof(long long) * (n_residues + 1), cudaMemcpyHostToDevice, s), "upload");
+        if (n_entries > 0)
+            ck(cudaMemcpyAsync(a, res_atoms, sizeof(int) * n_entries, cudaMemcpyHostToDevice, s), "upload");
+        doff = o;
+        datoms = a;
+        dsum = x->ensure<double>(cms_ctx::S_RES_SUM, n_residues);
+    }
+    int* flag = (int*)(x->pinned + 32);
+    int* dflag = x->ensure<int>(cms_ctx::S_RES_FLAG, 1);
+    ck(cudaMemsetAsync(dflag, 0, sizeof(int), s), "clear flag");
+    const double* vals = x->get<double>(values == 0 ? cms_ctx::S_PER_ATOM_CMS : cms_ctx::S_PER_ATOM_MAX);
+    k_residue_sums<<<grid1(n_residues), 256, 0, s>>>(vals, x->N, doff, n_residues, datoms, n_entries, dsum, dflag);
+    ck(cudaGetLastError(), "residue sums");
+    ck(cudaMemcpyAsync(flag, dflag, sizeof(int), cudaMemcpyDeviceToHost, s), "readback");
+    ck(cudaStreamSynchronize(s), "sync");
+    if (*flag) throw Fail{CMS_ERR_ARG, "cms_residue_sums: residue offsets or atom indices out of range"};
+    if (where == CMS_HOST) copy_out(x, sums, dsum, sizeof(double) * n_residues, CMS_HOST);
     API_END
 }
 
@@ -1449,6 +1530,30 @@ cms_status cms_nn_work(cms_ctx* x, int64_t* pairs)
     API_END
 }
 
+cms_status cms_nn_evaluated(cms_ctx* x, int64_t* counts)
+{
+    if (!x || !counts) return fail(x, CMS_ERR_ARG, "null argument");
+    struct Off {
+        cms_ctx* x;
+        ~Off() { x->counting = false; }
+    } off{x};
+    API_BEGIN
+    need_surface(x);
+    unsigned long long* c = x->ensure<unsigned long long>(cms_ctx::S_NN_COUNT, 6);
+    ck(cudaMemsetAsync(c, 0, 6 * sizeof(unsigned long long), x->stream), "memset");
+    x->counting = true;
+    enqueue_cms(x);
+    enqueue_sc(x);
+    x->counting = false;
+    ck(cudaGetLastError(), "counted readouts");
+    unsigned long long h[6];
+    ck(cudaMemcpyAsync(h, c, sizeof(h), cudaMemcpyDeviceToHost, x->stream), "copy");
+    ck(cudaStreamSynchronize(x->stream), "sync");
+    for (int k = 0; k < 6; ++k) counts[k] = (int64_t)h[k];
+    x->cms_ok = x->sc_ok = true;
+    API_END
+}
+
 int64_t cms_kernel_launches(cms_ctx* x) { return x ? x->launches : -1; }
 
 cms_status cms_nearest_dots(cms_ctx* x, const double* query_xyz, int64_t n_query, const double* ref_xyz,
@@ -1495,7 +1600,7 @@ cms_status cms_nearest_dots(cms_ctx* x, const double* query_xyz, int64_t n_query
     a.q_f4 = qf; a.q_idx = nullptr; a.r_f4 = rf; a.r_idx = nullptr;
     a.q_xyz = q; a.r_xyz = r;
     a.out_d2 = d2; a.out_idx = idx;
-    launch_nn_kernel(a, NN_ARGMIN, 0, n_query / 512 + 2, s);
+    launch_nn_kernel(a, NN_ARGMIN, 0, nn_standalone_tile_cap(n_query), s);
     ck(cudaGetLastError(), "nearest-dot kernels");
     if (where == CMS_HOST) {
         ck(cudaMemcpyAsync(out_d2, d2, sizeof(double) * n_query, cudaMemcpyDeviceToHost, s), "copy out");

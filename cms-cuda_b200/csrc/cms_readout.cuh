@@ -47,6 +47,9 @@ struct NNArgs {
     // spatially ordered lists: the original position of each entry (null: lists in their own order);
     // outputs go to the queries' original positions, and reference indices are original positions
     const int* q_perm; const int* r_perm;
+    // instrumented runs only (null otherwise): (query, reference) pairs the FP32 filter evaluated in the
+    // scan, and references rechecked in FP64
+    unsigned long long* pair_count; unsigned long long* recheck_count;
 };
 
 // readout workspace, capacity = dot capacity unless noted
@@ -107,6 +110,8 @@ void launch_tasks(const Dev& d, const Rd& r, int kind, NNTask* task, cudaStream_
 void launch_nn(NNArgs a, int mode, int variant, long long tile_cap, long long* scan_tmp, cudaStream_t s);
 void launch_nn_tiles(NNArgs a, int mode, int variant, long long* scan_tmp, cudaStream_t s);
 void launch_nn_kernel(NNArgs a, int mode, int variant, long long tile_cap, cudaStream_t s);
+// tile_cap for launch_nn_kernel (variant 0) of a standalone search of n_query points
+long long nn_standalone_tile_cap(long long n_query);
 // standalone search helpers: bounding box of two point sets, FP32 packing, one task
 void launch_points_setup(const double* q, long long nq, const double* r, long long nr, double* partials,
                          int partial_blocks, double* bbox, float4* q_f4, float4* r_f4, NNTask* task, int* tile_cnt,

@@ -1,15 +1,15 @@
 // cms_nearest_dots_noalloc: the brute-force nearest-dot search for callers
 // that cannot allocate GPU memory.
 //
-// Some callers cannot call cudaMalloc: code running inside a CUDA graph
-// capture or a memory-pool-controlled framework (where an allocation would
-// break the capture or bypass the framework's allocator), real-time loops
-// that must never hit the allocator's synchronisation, and plugins hosted by
-// applications that own every device allocation.  This entry point gives
-// them the same search as cms_nearest_dots without any allocation: the caller
-// passes device pointers for inputs and outputs, and the search's scratch
-// (the bounding-box partials, the search task, the FP32-packed copies of
-// both point sets and the boxes of the reference blocks) lives in one fixed
+// Some callers cannot call cudaMalloc: a framework or application that owns
+// every device allocation through its own pool (an allocation behind its back
+// would bypass its accounting and limits), plugins hosted by such an
+// application, and real-time loops that must never meet the allocator's
+// implicit device synchronisation.  This entry point gives them the same
+// search as cms_nearest_dots without any allocation: the caller passes device
+// pointers for inputs and outputs, and the search's scratch (the
+// bounding-box partials, the search task, the FP32-packed copies of both
+// point sets and the boxes of the reference blocks) lives in one fixed
 // file-scope device array.
 //
 // Contract:
@@ -17,14 +17,23 @@
 //    the library is loaded and held until the process exits; it fits at most
 //    CMS_NOALLOC_MAX_POINTS query + reference points per call -- larger
 //    inputs are rejected with CMS_ERR_ARG before anything is launched;
+//  - the four pointers must be memory a kernel on the current device can
+//    read or write: device memory of that device, managed memory, or mapped
+//    pinned host memory; anything else (plain pageable host memory, another
+//    device's memory) is rejected with CMS_ERR_ARG before anything is
+//    launched;
 //  - the first call on a device (with that device current) looks up the
 //    array's device address once and caches it; make that first call before
-//    any stream capture;
+//    any stream capture.  The cached address belongs to the device's primary
+//    context: calls after a cudaDeviceReset of that device are not supported;
 //  - every call on a device shares the one array, and the array keeps the
 //    previous call's contents (everything a call reads is written earlier in
 //    the same call); calls that overlap on the GPU -- on different streams
 //    without ordering between them -- race on it and must be serialised by
 //    the caller;
+//  - a CUDA error already pending on the calling thread when the call starts
+//    is left in place for its owner and the call returns CMS_ERR_CUDA without
+//    launching; otherwise CMS_ERR_CUDA reports this call's own launches;
 //  - no cudaMalloc, cudaFree or allocating library routine is called.
 #include <mutex>
 
@@ -70,6 +79,24 @@ cms_status noalloc_scratch(unsigned char** out)
     return CMS_OK;
 }
 
+// a kernel on the current device can access p (device memory of this device, managed or mapped pinned memory)
+bool noalloc_device_accessible(const void* p)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();          // the query's own error (an unknown pointer), not a launch error
+        return false;
+    }
+    switch (at.type) {
+    case cudaMemoryTypeDevice: return at.device == dev;
+    case cudaMemoryTypeManaged: return true;
+    case cudaMemoryTypeHost: return at.devicePointer == p;
+    default: return false;
+    }
+}
+
 }  // namespace
 
 extern "C" cms_status cms_nearest_dots_noalloc(const double* query_xyz, int64_t n_query, const double* ref_xyz,
@@ -78,6 +105,10 @@ extern "C" cms_status cms_nearest_dots_noalloc(const double* query_xyz, int64_t 
     if (n_query < 0 || n_ref <= 0 || !ref_xyz || (n_query > 0 && (!query_xyz || !out_d2))) return CMS_ERR_ARG;
     if ((unsigned long long)n_query + (unsigned long long)n_ref > CMS_NOALLOC_MAX_POINTS) return CMS_ERR_ARG;
     if (n_query == 0) return CMS_OK;
+    if (cudaPeekAtLastError() != cudaSuccess) return CMS_ERR_CUDA;
+    if (!noalloc_device_accessible(query_xyz) || !noalloc_device_accessible(ref_xyz) ||
+        !noalloc_device_accessible(out_d2) || (out_index && !noalloc_device_accessible(out_index)))
+        return CMS_ERR_ARG;
     unsigned char* base = nullptr;
     cms_status st = noalloc_scratch(&base);
     if (st != CMS_OK) return st;
@@ -104,6 +135,6 @@ extern "C" cms_status cms_nearest_dots_noalloc(const double* query_xyz, int64_t 
     a.q_f4 = q_f4; a.q_idx = nullptr; a.r_f4 = r_f4; a.r_idx = nullptr;
     a.q_xyz = query_xyz; a.r_xyz = ref_xyz;
     a.out_d2 = out_d2; a.out_idx = out_index;
-    launch_nn_kernel(a, out_index ? NN_ARGMIN : NN_MIN, 0, n_query / 512 + 2, s);
+    launch_nn_kernel(a, out_index ? NN_ARGMIN : NN_MIN, 0, nn_standalone_tile_cap(n_query), s);
     return cudaGetLastError() == cudaSuccess ? CMS_OK : CMS_ERR_CUDA;
 }

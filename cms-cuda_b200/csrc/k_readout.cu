@@ -245,14 +245,19 @@ __device__ __forceinline__ void nn_band_warp(const NNArgs& a, const NNTask& T, N
         const float qz2 = __shfl_sync(0xffffffffu, q.qz2, L);
         const float ts = __shfl_sync(0xffffffffu, q.ts, L);
         const int qdot = __shfl_sync(0xffffffffu, q.dot, L);
-        bool hit = false;
+        bool hit = false, tested = false;
         if (lane < n) {
             const int k = k0 + lane;
             const float v = nn_s(qx2, qy2, qz2, sA[k].x, sA[k].z, sB[k].x, sB[k].z);
             if (v <= ts) {
                 const double* rp = a.r_xyz + 3LL * nn_rpt(a, T.r0 + rb + k);
                 hit = exact_d2(rp, a.q_xyz + 3LL * qdot) <= a.band_thr64;
+                tested = true;
             }
+        }
+        if (a.recheck_count) {
+            const unsigned t = __ballot_sync(0xffffffffu, tested);
+            if (lane == 0 && t) atomicAdd(a.recheck_count, (unsigned long long)__popc(t));
         }
         if (__any_sync(0xffffffffu, hit) && lane == L) q.done = true;
     }
@@ -267,6 +272,7 @@ __device__ __forceinline__ void nn_recheck(const NNArgs& a, const NNTask& T, con
     const float v = nn_s(qx2, qy2, qz2, rx, ry, rz, nn_rr(rx, ry, rz));
     if (v <= ts) {
         const long long rk = T.r0 + k;
+        if (a.recheck_count) atomicAdd(a.recheck_count, 1ull);
         const double e = exact_d2(a.r_xyz + 3LL * nn_rpt(a, rk), a.q_xyz + 3LL * qdot);
         const int ko = (int)(nn_rpos(a, rk) - T.r0);     // original position: first index on ties
         if (e < best || (e == best && ko < bidx)) { best = e; bidx = ko; }
@@ -290,6 +296,7 @@ __device__ __forceinline__ void nn_recheck_block(const NNArgs& a, const NNTask& 
             if (nn_s(qx2, qy2, qz2, rx, ry, rz, nn_rr(rx, ry, rz)) <= ts) cand |= 1u << t;
         }
     }
+    if (a.recheck_count && cand) atomicAdd(a.recheck_count, (unsigned long long)__popc(cand));
     while (cand) {
         const int t = __ffs(cand) - 1;
         cand &= cand - 1;
@@ -535,6 +542,7 @@ __global__ void __launch_bounds__(NN_T, MODE == NN_BAND ? 10 : 8) k_nn(NNArgs a)
                                      !box_far(box_gap2(qpx[j], qpy[j], qpz[j], qpx[j], qpy[j], qpz[j], blo, bhi), q[j].cth);
                     if (!__any_sync(0xffffffffu, lane_need)) continue;
                     const int n = min(NN_BLK, nr - sb);
+                    if (a.pair_count && lane == 0) atomicAdd(a.pair_count, (unsigned long long)n * WQ);
                     float mv[Q];
 #pragma unroll
                     for (int j = 0; j < Q; ++j) mv[j] = INFINITY;
@@ -726,6 +734,9 @@ void launch_nn_kernel(NNArgs a, int mode, int variant, long long tile_cap, cudaS
     else if (mode == NN_ARGMIN) nn_dispatch<NN_ARGMIN>(a, variant, grid, s);
     else nn_dispatch<NN_BAND>(a, variant, grid, s);
 }
+
+// CTAs a standalone search launches: one per tile of the default shape (k_points_task makes the tiles), plus one
+long long nn_standalone_tile_cap(long long n_query) { return (n_query + NN_TILE - 1) / NN_TILE + 1; }
 
 void launch_nn(NNArgs a, int mode, int variant, long long tile_cap, long long* scan_tmp, cudaStream_t s)
 {

@@ -135,6 +135,17 @@ cms_status cms_recompute_dots(cms_ctx* ctx, int32_t c, int32_t molecule, double*
  * Replaces calc_max_possible_contact_molecular_surface (_core.py:1007-1034). */
 cms_status cms_max_contact_ms(cms_ctx* ctx, double* per_atom, double* totals, int32_t where);
 
+/* Per-residue sums of a per-atom readout, for the whole batch in one launch:
+ * values 0 = the per-atom CMS of cms_contact_ms, 1 = the per-atom maximum
+ * CMS of cms_max_contact_ms (either is computed first when needed).  Residue
+ * r adds the values of atoms res_atoms[res_off[r] .. res_off[r+1]) (batch
+ * atom indices; res_off has n_residues + 1 entries from 0 to n_entries) in
+ * that order, starting from 0.0, into sums[r].  Replaces the reference CLI's
+ * per_residue loop (examples/calculate_cms_sc.py:105-114).  Offsets or atom
+ * indices out of range give CMS_ERR_ARG. */
+cms_status cms_residue_sums(cms_ctx* ctx, int32_t values, int64_t n_residues, const int64_t* res_off,
+                            int64_t n_entries, const int32_t* res_atoms, double* sums, int32_t where);
+
 /* Shape complementarity.  sc (B x 5): sc, interface area, median distance,
  * mean distance, mean normal score (surface 2).  sides (B x 2 x 7):
  * d_mean, d_median, s_mean, s_median, trimmedArea, nTrimmedDots, nAllDots of
@@ -181,15 +192,20 @@ cms_status cms_nearest_dots(cms_ctx* ctx, const double* query_xyz, int64_t n_que
                             int64_t n_ref, double* out_d2, int32_t* out_index, int32_t where);
 
 /* Allocation-free variant of cms_nearest_dots, for callers that cannot
- * allocate GPU memory (inside a stream capture or a framework that owns the
- * allocator, real-time loops, hosted plugins).  This entry point has no
- * counterpart in the reference.  query_xyz, ref_xyz, out_d2 and out_index
- * (NULL: no indices) are device pointers; the work is enqueued on `stream`
- * (NULL: the default stream) and no memory is allocated: the scratch is one
- * fixed 32 MiB device array per GPU, so n_query + n_ref may not exceed
- * 1,964,032 points (CMS_ERR_ARG otherwise, nothing launched).  The first call
- * on a device looks up the scratch address (make it before any stream
- * capture); calls that overlap on the GPU share the scratch and race. */
+ * allocate GPU memory: a framework or application that owns every device
+ * allocation through its own pool, plugins it hosts, and real-time loops that
+ * must not meet cudaMalloc's implicit synchronisation.  This entry point has
+ * no counterpart in the reference.  query_xyz, ref_xyz, out_d2 and out_index
+ * (NULL: no indices) must be memory a kernel on the current device can use
+ * (its device memory, managed or mapped pinned memory; anything else is
+ * CMS_ERR_ARG, nothing launched); the work is enqueued on `stream` (NULL: the
+ * default stream) and no memory is allocated: the scratch is one fixed
+ * 32 MiB device array per GPU, so n_query + n_ref may not exceed 1,964,032
+ * points (CMS_ERR_ARG otherwise, nothing launched).  The first call on a
+ * device looks up the scratch address (make it before any stream capture;
+ * calls after a cudaDeviceReset are not supported); calls that overlap on the
+ * GPU share the scratch and race.  A CUDA error already pending on the
+ * calling thread is left in place and the call returns CMS_ERR_CUDA. */
 cms_status cms_nearest_dots_noalloc(const double* query_xyz, int64_t n_query, const double* ref_xyz,
                                     int64_t n_ref, double* out_d2, int32_t* out_index, void* stream);
 
@@ -241,6 +257,15 @@ cms_status cms_set_autotune(cms_ctx* ctx, int32_t enable);
  * pairs, queries) of the CMS search, the SC band (trim) search and the SC
  * neighbour search -- the algorithmic work behind the FP32 roofline. */
 cms_status cms_nn_work(cms_ctx* ctx, int64_t* pairs);
+
+/* Nearest-dot search work the kernels actually did, counted by the kernels
+ * themselves in one extra (eager) run of the CMS and SC readouts on the
+ * current surfaces: counts[0..2] = (query, reference) pairs the FP32 filter
+ * evaluated in the CMS, SC band and SC argmin searches after the box culling,
+ * counts[3..5] = references rechecked in FP64 by each.  The readout results
+ * are unchanged.  No reference counterpart (its searches are plain brute
+ * force, _gpu_kernels.py:78-117). */
+cms_status cms_nn_evaluated(cms_ctx* ctx, int64_t* counts);
 
 /* Measured FP32 FMA throughput of the context's device (TFLOP/s, FMA = 2
  * FLOP): the denominator of the nearest-dot search's roofline. */

@@ -54,3 +54,38 @@ def test_roofline_peak_sources(bench):
     # a search stage on top is reported against the FP32 throughput
     n = bench.stage_roofline({"cms_nn": 5.0}, WORK, TOTALS, {}, 80.0)
     assert n["bound"] == "fp32" and n["unit"] == "TFLOP/s"
+
+
+def test_search_roofline_uses_evaluated_pairs(bench):
+    ev = {"cms_evaluated": 10 ** 8, "cms_rechecks": 5}
+    r = bench.stage_roofline({"cms_nn": 5.0}, WORK, TOTALS, {}, 80.0, ev)
+    assert r["evaluated_pairs"] == 10 ** 8 and r["fp64_rechecks"] == 5
+    assert r["achieved"] == pytest.approx(8.0 * 10 ** 8 / 5e-3 / 1e12)
+    assert r["brute_force_equivalent_tflops"] == pytest.approx(8.0 * WORK["cms_pairs"] / 5e-3 / 1e12)
+    assert r["frac"] == pytest.approx(r["achieved"] / 80.0)
+    rows = bench.stage_rooflines({"cms_nn": 5.0, "triples_count": 10.0, "attention": 5.0}, WORK, TOTALS, {}, 80.0,
+                                 ev)
+    assert rows["attention"]["bound"] == "latency" and rows["triples_count"]["bound"] == "hbm"
+    assert "fp64_pipe_active_pct" in rows["triples_count"]
+    assert sum(v["share"] for v in rows.values()) == pytest.approx(1.0)
+
+
+def test_stratified_sample_spans_sizes_and_ligands(bench):
+    import numpy as np
+    rng = np.random.default_rng(0)
+    sizes = rng.integers(600, 5000, 500)
+    ligand = rng.random(500) < 0.05
+    pick = bench.stratified_sample(sizes, ligand, 16)
+    assert int(np.argmin(sizes)) in pick and int(np.argmax(sizes)) in pick
+    assert int(ligand[pick].sum()) >= 2
+    assert 14 <= len(pick) <= 16
+    assert list(sizes[pick]) == sorted(sizes[pick])
+
+
+def test_extrapolation_fit(bench):
+    import numpy as np
+    sizes = np.array([1000, 2000, 4000])
+    secs = 1e-6 * sizes ** 1.5
+    total, expo = bench._fit_extrapolation(sizes, secs, [1000, 1000, 4000])
+    assert expo == pytest.approx(1.5)
+    assert total == pytest.approx(2 * 1e-6 * 1000 ** 1.5 + 1e-6 * 4000 ** 1.5)

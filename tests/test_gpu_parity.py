@@ -94,6 +94,11 @@ def test_counts_and_flags(runs, name):
         for t in (1, 2, 3):
             exact(f"dots[{m}] type {t}", int((d.type_ == t).sum()), int(c[f"n_type{t}_{m}"]))
         exact(f"trimmed[{m}] count", len(r.trimmed_dots[m]), int(c[f"n_trimmed{m}"]))
+        if f"dots{m}_atom" in c:
+            # every dot's owner, burial flag and type (all fixtures keep them; the large plain complex too)
+            exact(f"dots[{m}].atom_idx", d.atom_idx, c[f"dots{m}_atom"])
+            exact(f"dots[{m}].buried", d.buried, c[f"dots{m}_buried"])
+            exact(f"dots[{m}].type_", d.type_, c[f"dots{m}_type"])
     mr = R["mcalc"].run
     exact("max-cms dot counts", [mr.results.dots.convex, mr.results.dots.toroidal, mr.results.dots.concave],
           c["max_counts"])

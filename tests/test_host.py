@@ -62,9 +62,10 @@ def test_radii_of_golden_inputs():
     from cms_cuda.structure import read_pdb_chains
     from cms_cuda import get_radii_from_names
     case = load_case("sc_example_pdb")
-    pdb = "/root/reference/test/sc_example.pdb"
+    ref = os.environ.get("CMS_REFERENCE_DIR")
+    pdb = os.path.join(ref, "test", "sc_example.pdb") if ref else ""
     if not os.path.exists(pdb):
-        pytest.skip("reference checkout not present")
+        pytest.skip("no reference checkout named by CMS_REFERENCE_DIR")
     ch = read_pdb_chains(pdb)
     np.testing.assert_array_equal(get_radii_from_names(ch["B"][1], ch["B"][2]), case["br"])
     np.testing.assert_array_equal(ch["A"][0], case["tx"])

@@ -114,12 +114,15 @@ def test_mmcif_matches_pdb(tmp_path):
         assert [(a[0], a[2], a[3]) for a in i1] == [(a[0], a[2], a[3]) for a in i2]
 
 
-def test_per_residue_sums_in_first_appearance_order():
-    from cms_cuda.loader import per_residue
+def test_residue_groups_in_first_appearance_order():
+    from cms_cuda.loader import residue_groups
     info = [("A", "1", "ALA", "N", "N"), ("A", "1", "ALA", "CA", "C"), ("A", "2", "GLY", "N", "N"),
             ("A", "1", "ALA", "CB", "C")]
-    out = per_residue(info, [1.0, 2.0, 4.0, 8.0])
-    assert out == [("A", "1", "ALA", 11.0), ("A", "2", "GLY", 4.0)]
+    keys, off, atoms = residue_groups(info, first_atom=10)
+    assert keys == [("A", "1", "ALA"), ("A", "2", "GLY")]
+    assert off.tolist() == [0, 3, 4] and atoms.tolist() == [10, 11, 13, 12]
+    keys, off, atoms = residue_groups([])
+    assert keys == [] and off.tolist() == [0] and len(atoms) == 0
 
 
 def test_discontinuous_chain_is_joined_to_its_first_block(tmp_path):

@@ -95,3 +95,22 @@ def test_binned_median_known_answers():
     v = np.array([0.01, 0.03, 0.05, 0.07])
     # bins 0,1,2,3 with 25 % each; 50 % reached at bin 1 -> 0.02 + (50-25)*0.02/25
     assert abs(O.binned_median(v, 0.02) - 0.04) < 1e-15
+
+
+@pytest.mark.parametrize("slot", [0, 6])
+def test_ligand_binders_of_the_batched_workload(slot):
+    """Two ligand-binder complexes of the batched workload (HETATM C*/N*/O* radii) against the reference's run."""
+    z = load_case("batched_4096_sample")
+    assert bool(z["ligand"][slot])
+    case = {k[len(f"k{slot}_"):]: v for k, v in z.items() if k.startswith(f"k{slot}_")}
+    out = O.run_complex(*inputs(case))
+    exact("cms", out["cms"], case["cms"])
+    exact("cms binder", out["cms_binder"], case["cms_binder"])
+    exact("sc", [out["sc"], out["sc_area"], out["sc_distance"]], [case["sc"], case["sc_area"], case["sc_distance"]])
+    exact("per-atom", out["cms_per_atom"], case["per_atom_target"])
+    S = out["surface"]
+    for m in (0, 1):
+        d = S.dot_arrays[m]
+        exact(f"dots{m}.atom", d["atom"], case[f"dots{m}_atom"])
+        exact(f"dots{m}.buried", d["buried"], case[f"dots{m}_buried"])
+        exact(f"dots{m}.type", d["type"], case[f"dots{m}_type"])

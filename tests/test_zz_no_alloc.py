@@ -1,13 +1,15 @@
 """
 cms_nearest_dots_noalloc -- the nearest-dot search for callers that cannot
-allocate GPU memory (a stream capture in progress, a framework that owns the
-allocator, a hosted plugin): inputs and outputs are the caller's device
-buffers and the scratch is a fixed device array inside the library.
+allocate GPU memory (a framework or application that owns every device
+allocation through its own pool, plugins it hosts, real-time loops that must
+not meet cudaMalloc's synchronisation): inputs and outputs are the caller's
+device buffers and the scratch is a fixed device array inside the library.
 
 Checked through the C ABI against the allocating entry point cms_nearest_dots
 on two calls in a row (the shared scratch keeps the previous call's contents,
-so the second call must not depend on it), plus the size limit.  Collected
-last so that a run stopping at the first failure has run everything else.
+so the second call must not depend on it), that a warm call leaves the
+device's free memory unchanged, plus the size limit.  Collected last so that a run stopping at the first
+failure has run everything else.
 """
 
 import ctypes
@@ -33,16 +35,20 @@ def _lib():
 
 
 def _call(f, q, r, with_index=True):
+    """One call through the C ABI; also returns the device's free memory right after it."""
     import torch
     qd = torch.from_numpy(q).cuda()
     rd = torch.from_numpy(r).cuda()
     d2 = torch.empty(len(q), dtype=torch.float64, device="cuda")
     idx = torch.empty(len(q), dtype=torch.int32, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
     st = f(qd.data_ptr(), len(q), rd.data_ptr(), len(r), d2.data_ptr(), idx.data_ptr() if with_index else None,
            stream)
     torch.cuda.synchronize()
-    return st, d2.cpu().numpy(), idx.cpu().numpy()
+    free1 = torch.cuda.mem_get_info()[0]
+    return st, d2.cpu().numpy(), idx.cpu().numpy(), (free0, free1)
 
 
 def test_matches_allocating_entry_point_twice():
@@ -54,8 +60,11 @@ def test_matches_allocating_entry_point_twice():
         r = rng.uniform(-25, 25, (nr, 3))
         r[nr - 1] = r[3]                      # exact tie: the first index wins
         q[0] = r[3]
-        st, d2, idx = _call(f, q, r)
+        st, d2, idx, (free0, free1) = _call(f, q, r)
         assert st == 0, f"call {call}: status {st}"
+        if call > 0:
+            # the scratch is static: a warm call leaves the device's free memory as it was
+            assert free1 == free0, (free0, free1)
         ref_d2, ref_idx = ctx.nearest_dots(q, r)
         exact(f"call {call} min d2", d2, ref_d2)
         exact(f"call {call} argmin", idx, ref_idx)
@@ -68,7 +77,7 @@ def test_without_indices_and_size_limit():
     rng = np.random.default_rng(8)
     q = rng.uniform(-10, 10, (300, 3))
     r = rng.uniform(-10, 10, (400, 3))
-    st, d2, _ = _call(f, q, r, with_index=False)
+    st, d2, _, _ = _call(f, q, r, with_index=False)
     assert st == 0
     exact("min d2 (no index)", d2, ctx.nearest_dots(q, r)[0])
     # past the fixed scratch: rejected before any launch, outputs untouched

@@ -288,8 +288,12 @@ def contact_ms(X, R, rp, weight, topo, side=1):
     return (aq[torch.as_tensor(q)] * torch.exp(-d2 * weight)).sum()
 
 
-def topology(ctx, c, density=15.0):
-    """Export the topology of complex c of a generated context."""
+def topology(ctx, c, density=15.0, nearest=None):
+    """
+    Export the topology of complex c of a generated context.  nearest(q, r)
+    -> (min d2, first argmin) picks each query dot's nearest dot (default:
+    scipy cdist; the library's exact search gives the same indices).
+    """
     from scipy.spatial.distance import cdist
     info = ctx.info(c)
     n = int(info.n_atoms)
@@ -311,7 +315,12 @@ def topology(ctx, c, density=15.0):
     for m in (0, 1):
         q = dots_[m]["coor"][dots_[m]["bur"]]
         r = dots_[1 - m]["coor"][dots_[1 - m]["bur"]]
-        nn.append(np.argmin(cdist(r, q, "sqeuclidean"), axis=0) if len(q) and len(r) else np.zeros(0, np.int64))
+        if not (len(q) and len(r)):
+            nn.append(np.zeros(0, np.int64))
+        elif nearest is not None:
+            nn.append(np.asarray(nearest(q, r)[1], np.int64))
+        else:
+            nn.append(np.argmin(cdist(r, q, "sqeuclidean"), axis=0))
     return dict(frame=frame, a1=a1.astype(np.int64), a2=a2.astype(np.int64),
                 pa=(p0.astype(np.int64), p1.astype(np.int64), p2.astype(np.int64)), plus=plus,
                 dots=dots_, nn=nn, dens=np.full(n, float(density)))
