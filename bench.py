@@ -647,25 +647,36 @@ def pose_refinement(args, device):
 # ---------------------------------------------------------------------------
 # our implementation
 # ---------------------------------------------------------------------------
+def rank_batch(per_gpu, seed, rank, world):
+    """
+    This rank's share of one global batch of per_gpu * world complexes, split
+    by cost (atoms) over the ranks: (global size, global indices, the batch of
+    those complexes, each identical to its copy in the whole batch).
+    """
+    from cms_cuda import synth
+    from cms_cuda.shard import balanced_shards
+    B_global = per_gpu * world
+    if world == 1:
+        batch = synth.config_batched(B_global, seed)
+        return B_global, np.arange(batch.B), batch
+    nt, nb, _ = synth.batched_sizes(B_global, seed)
+    mine = balanced_shards(nt.astype(np.int64) + nb, world)[rank]
+    return B_global, mine, synth.config_batched(B_global, seed, select=mine)
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
     rank, world, local = dist_env()
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    from cms_cuda import _lib, synth
-    from cms_cuda.shard import balanced_shards, gather_per_complex, max_over_ranks
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    from cms_cuda import _lib
+    from cms_cuda.shard import gather_per_complex, max_over_ranks
 
-    # one global batch of `batch` complexes per GPU, split by cost (atoms) over the ranks
-    B_global = args.batch * world
-    nt, nb, _ = synth.batched_sizes(B_global, args.seed)
-    mine = balanced_shards(nt.astype(np.int64) + nb, world)[rank] if world > 1 else None
-    batch = synth.config_batched(B_global, args.seed, select=mine)
-    if mine is None:
-        mine = np.arange(batch.B)
+    B_global, mine, batch = rank_batch(args.batch, args.seed, rank, world)
     B, N = batch.B, batch.N
     # pinned host inputs for the end-to-end path
     xyz_h = torch.from_numpy(batch.xyz).pin_memory()

@@ -89,3 +89,42 @@ def test_extrapolation_fit(bench):
     total, expo = bench._fit_extrapolation(sizes, secs, [1000, 1000, 4000])
     assert expo == pytest.approx(1.5)
     assert total == pytest.approx(2 * 1e-6 * 1000 ** 1.5 + 1e-6 * 4000 ** 1.5)
+
+
+def test_multi_gpu_self_launch_command(bench, monkeypatch):
+    """--gpus N without a launcher re-runs the script under torch.distributed.run with N ranks on 127.0.0.1."""
+    import subprocess
+    import sys
+    seen = {}
+
+    class Done:
+        returncode = 0
+
+    def fake_run(cmd, *a, **k):
+        seen["cmd"] = cmd
+        return Done()
+
+    monkeypatch.setattr(subprocess, "run", fake_run)
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--gpus", "4", "--steps", "2"])
+    assert bench.self_launch(bench.parse(["--gpus", "4", "--steps", "2"])) == 0
+    cmd = seen["cmd"]
+    assert cmd[:4] == ["timeout", "-k", "60", "3600"]
+    assert "torch.distributed.run" in cmd and "--nproc-per-node=4" in cmd and "127.0.0.1" in cmd
+    assert cmd[-4:] == ["--gpus", "4", "--steps", "2"]
+
+
+def test_global_batch_shards_cover_the_batch(bench):
+    """The ranks' shards of one global batch cover every complex once and balance the atoms."""
+    import numpy as np
+    from cms_cuda import synth
+    from cms_cuda.shard import balanced_shards
+    nt, nb, lig = synth.batched_sizes(4096 * 4, 2)
+    shards = balanced_shards(nt.astype(np.int64) + nb, 4)
+    allidx = np.sort(np.concatenate(shards))
+    assert np.array_equal(allidx, np.arange(4096 * 4))
+    loads = [int((nt[s] + nb[s]).sum()) for s in shards]
+    assert max(loads) - min(loads) <= int((nt + nb).max())
+    # a shard is generated alone, identical to its complexes in the whole batch
+    b = synth.config_batched(64, 2, select=[3, 40])
+    full_sizes = synth.batched_sizes(64, 2)
+    assert list(np.diff(b.atom_off)) == [int(full_sizes[0][c] + full_sizes[1][c]) for c in (3, 40)]
