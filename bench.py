@@ -700,6 +700,10 @@ def run_ours(args):
     autotune = {stage: {"shape": _lib.NN_VARIANT_NAMES[tv[k]],
                         "ms": {_lib.NN_VARIANT_NAMES[v]: round(float(tms[k, v]), 3) for v in range(4)}}
                 for k, stage in enumerate(("cms_nn", "sc_band_nn", "sc_argmin_nn"))}
+    sv, sms = ctx.surface_variants()
+    for k, stage in enumerate(_lib.SURFACE_STAGES):
+        names = _lib.SURFACE_VARIANT_NAMES[stage.split("_")[0]]
+        autotune[stage] = {"shape": names[sv[k]], "ms": {names[v]: round(float(sms[k, v]), 3) for v in range(2)}}
     free_b, total_b = torch.cuda.mem_get_info(dev)
     device_gb = (total_b - free_b) / 1e9             # whole GPU in use while the context holds its workspace
 

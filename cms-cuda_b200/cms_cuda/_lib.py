@@ -32,10 +32,13 @@ EXPORTED = (
     "cms_set_grad_total", "cms_grad_xyz", "cms_recompute_dots", "cms_export_dot_units",
     "cms_set_nn_variants", "cms_get_nn_variants", "cms_set_autotune", "cms_refine_begin",
     "cms_refine_set_params", "cms_refine_run", "cms_refine_pose", "cms_refine_end", "cms_residue_sums",
-    "cms_nn_evaluated",
+    "cms_nn_evaluated", "cms_set_surface_variants", "cms_get_surface_variants",
 )
 
 NN_VARIANT_NAMES = ("q4 r1024", "q4 r512", "q2 r1024", "q2 r512")
+SURFACE_STAGES = ("toroidal_count", "toroidal_emit", "concave_count", "concave_emit")
+SURFACE_VARIANT_NAMES = {"toroidal": ("16 pairs x 4 warps", "32 pairs x 2 warps"),
+                         "concave": ("4 CTAs/SM", "5 CTAs/SM")}
 
 
 class Settings(ctypes.Structure):
@@ -125,6 +128,8 @@ def load():
             "cms_refine_end": [_VP],
             "cms_residue_sums": [_VP, _I32, ctypes.c_int64, _PI64, ctypes.c_int64, _VP, _VP, _I32],
             "cms_nn_evaluated": [_VP, _PI64],
+            "cms_set_surface_variants": [_VP, _VP],
+            "cms_get_surface_variants": [_VP, _VP, _VP],
         }
         for name, args in sig.items():
             f = getattr(lib, name)
@@ -227,6 +232,18 @@ class Context:
         """Force the three search shapes (CMS, SC band, SC argmin); turns the autotuner off."""
         v = np.ascontiguousarray(variants, dtype=np.int32)
         self._check(self.lib.cms_set_nn_variants(self.h, _ptr(v)))
+
+    def set_surface_variants(self, variants):
+        """Force the surface kernels' shapes (toroidal count / emit, concave count / emit); turns the tuner off."""
+        v = np.ascontiguousarray(variants, dtype=np.int32)
+        self._check(self.lib.cms_set_surface_variants(self.h, _ptr(v)))
+
+    def surface_variants(self):
+        """(shape per tuned surface stage, measured ms per stage and shape) of the autotuner."""
+        v = np.zeros(4, np.int32)
+        ms = np.zeros(4 * 2)
+        self._check(self.lib.cms_get_surface_variants(self.h, _ptr(v), _ptr(ms)))
+        return v.tolist(), ms.reshape(4, 2)
 
     def set_autotune(self, enable=True):
         self._check(self.lib.cms_set_autotune(self.h, 1 if enable else 0))

@@ -247,6 +247,10 @@ struct cms_ctx {
     bool autotune = true;
     long long tune_key[3] = {-1, -1, -1};
     double tune_ms[3][NN_VARIANTS] = {};
+    // surface kernel shapes (toroidal count, toroidal emit, concave count, concave emit), tuned with the
+    // search shapes (or forced by cms_set_surface_variants)
+    int sv[4] = {0, 0, 0, 0};
+    double sv_ms[4][SURF_VARIANTS] = {};
     long long launches = -1;
     std::string err;
     // stage timing: an event after each pipeline stage when profiling
@@ -598,9 +602,9 @@ void enqueue_surface(cms_ctx* x, bool sized)
     ck(cudaMemsetAsync(d.cs_top, 0, sizeof(unsigned long long), s), "memset");
     launch_convex(d, false, s);
     mark(x, P_CONVEX_COUNT);
-    launch_toroidal(d, x->cap_tor, false, s);
+    launch_toroidal(d, x->cap_tor, false, x->sv[0], s);
     mark(x, P_TOROIDAL_COUNT);
-    launch_concave(d, x->cap_probe, false, s);
+    launch_concave(d, x->cap_probe, false, x->sv[2], s);
     mark(x, P_CONCAVE_COUNT);
     scan_counts(d.conv_cnt, d.conv_off, d.N, tmp, s);
     scan_counts(d.tor1_cnt, d.tor1_off, x->cap_tor, tmp, s);
@@ -625,9 +629,9 @@ void enqueue_surface(cms_ctx* x, bool sized)
     launch_convex(d, true, s);
     mark(x, P_CONVEX_EMIT);
     launch_tor_list(d, x->cap_tor, tmp, s);
-    launch_toroidal(d, x->cap_tor, true, s);
+    launch_toroidal(d, x->cap_tor, true, x->sv[1], s);
     mark(x, P_TOROIDAL_EMIT);
-    launch_concave(d, x->cap_probe, true, s);
+    launch_concave(d, x->cap_probe, true, x->sv[3], s);
     mark(x, P_CONCAVE_EMIT);
     launch_tor_access(d, x->cap_tor, s);
 }
@@ -1392,6 +1396,42 @@ void autotune_nn(cms_ctx* x)
     x->cms_ok = x->sc_ok = true;
 }
 
+// Autotuner of the surface kernels' shapes: with the buffers sized for the
+// loaded batch, generate the surfaces once per shape (every tunable stage
+// timed with events), twice over, and keep the fastest shape per stage.
+// Every shape generates the same surfaces.
+void autotune_surface(cms_ctx* x)
+{
+    const long long key[3] = {x->B, x->N, x->cap_dot};
+    if (!x->autotune || std::memcmp(key, x->tune_key, sizeof(key)) == 0) return;
+    static const int stage[4] = {P_TOROIDAL_COUNT, P_TOROIDAL_EMIT, P_CONCAVE_COUNT, P_CONCAVE_EMIT};
+    for (int k = 0; k < 4; ++k)
+        for (int v = 0; v < SURF_VARIANTS; ++v) x->sv_ms[k][v] = INFINITY;
+    double ms[P_NSTAGES];
+    for (int rep = 0; rep < 2; ++rep) {
+        for (int v = 0; v < SURF_VARIANTS; ++v) {
+            for (int k = 0; k < 4; ++k) x->sv[k] = v;
+            x->profiling = true;
+            try {
+                mark(x, -1);
+                enqueue_surface(x, false);
+            } catch (...) {
+                x->profiling = false;
+                throw;
+            }
+            x->profiling = false;
+            take_stage_times(x, ms, P_NSTAGES);
+            for (int k = 0; k < 4; ++k) x->sv_ms[k][v] = std::min(x->sv_ms[k][v], ms[stage[k]]);
+        }
+    }
+    for (int k = 0; k < 4; ++k) {
+        int best = 0;
+        for (int v = 1; v < SURF_VARIANTS; ++v)
+            if (x->sv_ms[k][v] < x->sv_ms[k][best]) best = v;
+        x->sv[k] = best;
+    }
+}
+
 // capture the whole batched pipeline into a CUDA graph for the current shape
 void capture_graph(cms_ctx* x)
 {
@@ -1400,10 +1440,12 @@ void capture_graph(cms_ctx* x)
     if (new_shape && (x->cap_dot == 0 || x->autotune)) {
         if (x->refine) enqueue_pose_apply(x);
         run_sized_surface(x, 0);                         // size every buffer for this batch
-        autotune_nn(x);                                  // pick the search shapes on it
+        autotune_surface(x);                             // pick the surface kernels' shapes on it
+        autotune_nn(x);                                  // and the search shapes
     }
     const long long key[4] = {x->B, x->N, x->cap_dot, x->refine ? 100 : (x->bwd_enabled ? 1 + x->bwd_side : 0)};
-    const long long vk = (x->nn_var[0] << 8) | (x->nn_var[1] << 4) | x->nn_var[2];
+    const long long vk = (x->nn_var[0] << 8) | (x->nn_var[1] << 4) | x->nn_var[2] |
+                         ((long long)(x->sv[0] | (x->sv[1] << 1) | (x->sv[2] << 2) | (x->sv[3] << 3)) << 12);
     if (x->gexec && std::memcmp(key, x->graph_key, sizeof(key)) == 0 && vk == x->graph_vk) return;
     if (x->gexec) { cudaGraphExecDestroy(x->gexec); x->gexec = nullptr; }
     if (x->graph) { cudaGraphDestroy(x->graph); x->graph = nullptr; }
@@ -1857,6 +1899,26 @@ cms_status cms_set_nn_variants(cms_ctx* x, const int32_t* variants)
     for (int k = 0; k < 3; ++k) x->nn_var[k] = variants[k];
     x->autotune = false;
     x->cms_ok = x->sc_ok = false;
+    return CMS_OK;
+}
+
+cms_status cms_set_surface_variants(cms_ctx* x, const int32_t* variants)
+{
+    if (!x || !variants) return fail(x, CMS_ERR_ARG, "null argument");
+    for (int k = 0; k < 4; ++k)
+        if (variants[k] < 0 || variants[k] >= SURF_VARIANTS) return fail(x, CMS_ERR_ARG, "surface shape out of range");
+    for (int k = 0; k < 4; ++k) x->sv[k] = variants[k];
+    x->autotune = false;
+    return CMS_OK;
+}
+
+cms_status cms_get_surface_variants(cms_ctx* x, int32_t* variants, double* tune_ms)
+{
+    if (!x || !variants) return fail(x, CMS_ERR_ARG, "null argument");
+    for (int k = 0; k < 4; ++k) variants[k] = x->sv[k];
+    if (tune_ms)
+        for (int k = 0; k < 4; ++k)
+            for (int v = 0; v < SURF_VARIANTS; ++v) tune_ms[k * SURF_VARIANTS + v] = x->sv_ms[k][v];
     return CMS_OK;
 }
 

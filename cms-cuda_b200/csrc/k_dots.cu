@@ -458,10 +458,11 @@ void launch_convex(const Dev& d, bool emit, cudaStream_t s)
 // TO_PAIRS pairs at a time and spreads their points over its lanes; when
 // emitting, the dots of the 32 points of a chunk are spread over the lanes
 // again, so consecutive lanes write consecutive dots.
-static constexpr int TO_WARPS = 4;
-static constexpr int TO_PAIRS = 16;   // toroid pairs per warp batch
-static constexpr int TO_POOL = 512;   // pruned atom ids per warp batch (past it: the full lists are scanned)
-static constexpr int TO_KEEP = 512;   // kept torus points per warp batch (past it: the batch is not kept)
+//
+// Two batch shapes, picked per batch shape by the autotuner: NPB pairs per
+// warp batch and NW warps per CTA -- (16, 4) or (32, 2).  Per batch up to
+// NPB * 32 pruned atom ids (past it: the full lists are scanned) and as many
+// kept torus points (past it: the batch is not kept).
 
 struct TorPair {
     int i, j;
@@ -695,9 +696,10 @@ __device__ __forceinline__ void tor_emit_spread(const Dev& d, TorArcS* S, int* X
     }
 }
 
-template <bool EMIT>
-__global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
+template <bool EMIT, int NPB, int NW>
+__global__ void __launch_bounds__(NW * 32) k_toroidal(Dev d)
 {
+    constexpr int TO_WARPS = NW, TO_PAIRS = NPB, TO_POOL = NPB * 32, TO_KEEP = NPB * 32;
     CMS_EXIT_ON_OVERFLOW(d);
     __shared__ TorPair tp[TO_WARPS][TO_PAIRS];
     __shared__ int tq[TO_WARPS][TO_PAIRS];                  // pair index of each batch slot
@@ -880,11 +882,17 @@ __global__ void __launch_bounds__(TO_WARPS * 32) k_toroidal(Dev d)
     }
 }
 
-void launch_toroidal(const Dev& d, long long tor_grid, bool emit, cudaStream_t s)
+void launch_toroidal(const Dev& d, long long tor_grid, bool emit, int variant, cudaStream_t s)
 {
-    const long long batches = (tor_grid + TO_PAIRS - 1) / TO_PAIRS;
-    if (emit) k_toroidal<true><<<grid_for(batches, TO_WARPS), TO_WARPS * 32, 0, s>>>(d);
-    else k_toroidal<false><<<grid_for(batches, TO_WARPS), TO_WARPS * 32, 0, s>>>(d);
+    if (variant == 0) {
+        const long long batches = (tor_grid + 15) / 16;
+        if (emit) k_toroidal<true, 16, 4><<<grid_for(batches, 4), 4 * 32, 0, s>>>(d);
+        else k_toroidal<false, 16, 4><<<grid_for(batches, 4), 4 * 32, 0, s>>>(d);
+    } else {
+        const long long batches = (tor_grid + 31) / 32;
+        if (emit) k_toroidal<true, 32, 2><<<grid_for(batches, 2), 2 * 32, 0, s>>>(d);
+        else k_toroidal<false, 32, 2><<<grid_for(batches, 2), 2 * 32, 0, s>>>(d);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -892,8 +900,11 @@ void launch_toroidal(const Dev& d, long long tor_grid, bool emit, cudaStream_t s
 // ---------------------------------------------------------------------------
 static constexpr int CC_WARPS = 4;
 
-template <bool EMIT>
-__global__ void __launch_bounds__(CC_WARPS * 32, 4) k_concave(Dev d)
+// MINB: CTAs per SM the register allocation must allow -- 4 (128 registers)
+// or 5 (102 registers, more warps to hide the FP64 latency, some spills);
+// the autotuner picks per batch shape
+template <bool EMIT, int MINB>
+__global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
 {
     CMS_EXIT_ON_OVERFLOW(d);
     __shared__ LatTable tab[CC_WARPS];
@@ -1095,10 +1106,15 @@ __global__ void __launch_bounds__(CC_WARPS * 32, 4) k_concave(Dev d)
     }
 }
 
-void launch_concave(const Dev& d, long long probe_grid, bool emit, cudaStream_t s)
+void launch_concave(const Dev& d, long long probe_grid, bool emit, int variant, cudaStream_t s)
 {
-    if (emit) k_concave<true><<<grid_for(probe_grid, CC_WARPS), CC_WARPS * 32, 0, s>>>(d);
-    else k_concave<false><<<grid_for(probe_grid, CC_WARPS), CC_WARPS * 32, 0, s>>>(d);
+    if (variant == 0) {
+        if (emit) k_concave<true, 4><<<grid_for(probe_grid, CC_WARPS), CC_WARPS * 32, 0, s>>>(d);
+        else k_concave<false, 4><<<grid_for(probe_grid, CC_WARPS), CC_WARPS * 32, 0, s>>>(d);
+    } else {
+        if (emit) k_concave<true, 5><<<grid_for(probe_grid, CC_WARPS), CC_WARPS * 32, 0, s>>>(d);
+        else k_concave<false, 5><<<grid_for(probe_grid, CC_WARPS), CC_WARPS * 32, 0, s>>>(d);
+    }
 }
 
 // ---------------------------------------------------------------------------

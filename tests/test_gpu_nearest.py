@@ -95,3 +95,53 @@ def test_autotuner_picks_shapes():
     assert np.isfinite(ms).all() and (ms > 0).all()
     for k in range(3):
         assert ms[k, v[k]] == ms[k].min()
+
+
+@pytest.mark.parametrize("graph", [False, True], ids=["staged", "graph"])
+def test_surface_shapes_give_identical_surfaces(graph):
+    """Every toroidal / concave kernel shape the autotuner may pick generates the same dots, bit for bit."""
+    from cms_cuda import _lib
+    from parity import inputs, load_case
+    names = ("golden_pkl", "synth_small_s7", "synth_zero_radii", "smallmol_7jkv_pdb")
+    xyz, rad, off, nb = [], [], [0], []
+    for n in names:
+        bx, br, tx, tr = inputs(load_case(n))
+        xyz += [bx, tx]; rad += [br, tr]; nb.append(len(br)); off.append(off[-1] + len(br) + len(tr))
+    X, R = np.concatenate(xyz), np.concatenate(rad)
+    out = []
+    for v in ([0, 0, 0, 0], [1, 1, 1, 1], [1, 0, 0, 1]):
+        ctx = _lib.Context(0)
+        ctx.set_surface_variants(v)
+        ctx.load_batch(np.array(off), np.array(nb), X, R)
+        if graph:
+            ctx.run_graph()
+            ctx.graph_launch()             # a replay with the stashes of the captured run
+        else:
+            ctx.generate(all_atoms=False)
+        dots = []
+        for c in range(len(names)):
+            i = ctx.info(c)
+            dots += [ctx.export_dots(c, m, i) for m in (0, 1)]
+        pa, tot = ctx.contact_ms(per_atom=True)
+        assert ctx.surface_variants()[0] == v
+        out.append((dots, pa, tot))
+    for other in out[1:]:
+        for a, b in zip(out[0][0], other[0]):
+            for x, y in zip(a, b):
+                assert np.array_equal(x, y, equal_nan=True)
+        assert np.array_equal(out[0][1], other[1]) and np.array_equal(out[0][2], other[2])
+
+
+def test_autotuner_picks_surface_shapes():
+    from cms_cuda import _lib
+    from parity import inputs, load_case
+    bx, br, tx, tr = inputs(load_case("synth_plain_1200_450"))
+    ctx = _lib.Context(0)
+    ctx.load_batch(np.array([0, len(br) + len(tr)]), np.array([len(br)]), np.concatenate([bx, tx]),
+                   np.concatenate([br, tr]))
+    ctx.run_graph()
+    v, ms = ctx.surface_variants()
+    assert all(x in (0, 1) for x in v)
+    assert np.isfinite(ms).all() and (ms >= 0).all()
+    for k in range(4):
+        assert ms[k, v[k]] == ms[k].min()
