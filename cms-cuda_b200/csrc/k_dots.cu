@@ -118,129 +118,11 @@ __device__ __forceinline__ int ks_stash(const Dev& d, const int* list, int kept,
 // ---------------------------------------------------------------------------
 static constexpr int CV_WARPS = 4;
 
-// candidate index ranges of a concave latitude circle (tri_ranges)
-static constexpr int TRI_MAXR = 4;
-
 struct LatTable {
     double cx[CMS_MAX_SUBDIV], cy[CMS_MAX_SUBDIV], cz[CMS_MAX_SUBDIV];
     double rad[CMS_MAX_SUBDIV], delta[CMS_MAX_SUBDIV], area[CMS_MAX_SUBDIV];
     int start[CMS_MAX_SUBDIV + 1];
 };
-
-// concave only: each latitude's candidate points as index ranges [rlo, rhi)
-struct LatRanges {
-    unsigned char rlo[CMS_MAX_SUBDIV][TRI_MAXR], rhi[CMS_MAX_SUBDIV][TRI_MAXR];
-    unsigned char nr[CMS_MAX_SUBDIV];
-};
-
-// convex only: per latitude, the neighbour slots whose sphere may reach the
-// circle of its probe centres (rows of up to CV_MASK_SLOTS neighbours)
-static constexpr int CV_MASK_SLOTS = 128;
-struct LatMasks {
-    unsigned m[CMS_MAX_SUBDIV][CV_MASK_SLOTS / 32];
-};
-
-// point index of the o-th candidate of latitude l
-__device__ __forceinline__ int lat_range_index(const LatRanges& L, int l, int o)
-{
-    for (int r = 0; r < L.nr[l]; ++r) {
-        const int len = (int)L.rhi[l][r] - (int)L.rlo[l][r];
-        if (o < len) return (int)L.rlo[l][r] + o;
-        o -= len;
-    }
-    return o;           // not reached: o < the latitude's candidate count
-}
-
-// Candidate points of one latitude circle of a concave probe.  A point of the
-// circle, pt = c + rad (cos a fx + sin a fy) with a = delta (i + 0.5), is kept
-// only when pt . v_k < 0 for the three plane normals v_k of the probe's
-// spherical triangle (_core.py:2218-2230).  Along the circle
-// pt . v_k = C_k + rad (P_k cos a + Q_k sin a) = C_k + rad M_k cos(a - phi_k),
-// so each plane allows one arc, where this is below TRI_TAU; outside it the
-// exactly computed pt . v_k is at least TRI_TAU minus its rounding error
-// (~1e-15), so the point is not kept.  The allowed arcs, widened by TRI_MU
-// radians and by one point on each side (far above the rounding of acos and
-// atan2 near the arcs' ends), are intersected into index ranges; every
-// candidate still takes the exact test, so the kept points are those of the
-// full enumeration.  Writes up to TRI_MAXR ranges [lo, hi) (ascending,
-// disjoint) and returns their number, or -1 when the circle is enumerated in
-// full (a non-finite quantity, no constraining plane, or too many ranges).
-#define TRI_TAU 1e-9
-#define TRI_MU 1e-6
-
-__device__ __noinline__ int tri_ranges(V3 cen, double rad, V3 fx, V3 fy, double delta, int nc, V3 v0, V3 v1,
-                                          V3 v2, unsigned char* lo, unsigned char* hi)
-{
-    if (nc <= 0) return 0;
-    if (!(isfinite(rad) && rad > 0.0 && isfinite(delta) && delta > 0.0)) return -1;
-    const V3 vec[3] = {v0, v1, v2};
-    double plo[8], phi_[8];            // pieces of the intersection on the unrolled line [0, 4 pi)
-    int np = 0;
-    bool first = true;
-    for (int k = 0; k < 3; ++k) {
-        const double C = dot_seq(cen, vec[k]), P = dot_seq(fx, vec[k]), Q = dot_seq(fy, vec[k]);
-        if (!(isfinite(C) && isfinite(P) && isfinite(Q))) return -1;
-        const double M = sqrt(P * P + Q * Q);
-        const double b = (TRI_TAU - C) / rad;
-        if (b >= M) continue;                      // this plane allows the whole circle
-        if (b <= -M) return 0;                     // pt . v_k >= TRI_TAU everywhere: no point is kept
-        const double al = acos(b / M);             // allowed: cos(a - phi) < b / M, a - phi in (al, 2 pi - al)
-        const double len = (CMS_TWO_PI - 2.0 * al) + 2.0 * TRI_MU;
-        if (!(len < CMS_TWO_PI)) continue;
-        double s = atan2(Q, P) + al - TRI_MU;
-        s -= CMS_TWO_PI * floor(s / CMS_TWO_PI);
-        if (!(s >= 0.0 && s < CMS_TWO_PI)) return -1;
-        if (first) {
-            plo[0] = s; phi_[0] = s + len; np = 1; first = false;
-            continue;
-        }
-        double nlo[8], nhi[8];
-        int nn = 0;
-        for (int q = 0; q < np; ++q) {
-            for (int sh = -1; sh <= 1; ++sh) {
-                const double a0 = fmax(plo[q], s + sh * CMS_TWO_PI);
-                const double a1 = fmin(phi_[q], s + sh * CMS_TWO_PI + len);
-                if (a0 < a1) {
-                    if (nn == 8) return -1;
-                    nlo[nn] = a0; nhi[nn] = a1; ++nn;
-                }
-            }
-        }
-        if (nn == 0) return 0;
-        for (int q = 0; q < nn; ++q) { plo[q] = nlo[q]; phi_[q] = nhi[q]; }
-        np = nn;
-    }
-    if (first) return -1;
-    // pieces -> index ranges, the part past 2 pi wrapped to the start of the circle
-    int rl[16], rh[16];
-    int nr = 0;
-    for (int q = 0; q < np; ++q) {
-        for (int wrap = 0; wrap < 2; ++wrap) {
-            const double x = fmax(plo[q] - wrap * CMS_TWO_PI, 0.0), y = fmin(phi_[q] - wrap * CMS_TWO_PI, CMS_TWO_PI);
-            if (!(x < y)) continue;
-            const double f0 = fmin(fmax(ceil(x / delta - 0.5) - 1.0, 0.0), (double)nc);
-            const double f1 = fmin(fmax(floor(y / delta - 0.5) + 1.0, -1.0), (double)(nc - 1));
-            if (f0 <= f1) { rl[nr] = (int)f0; rh[nr] = (int)f1 + 1; ++nr; }
-        }
-    }
-    for (int a = 1; a < nr; ++a) {                 // insertion sort by start
-        const int x = rl[a], y = rh[a];
-        int b = a - 1;
-        while (b >= 0 && rl[b] > x) { rl[b + 1] = rl[b]; rh[b + 1] = rh[b]; --b; }
-        rl[b + 1] = x; rh[b + 1] = y;
-    }
-    int m = 0;
-    for (int a = 0; a < nr; ++a) {                 // merge overlapping or touching ranges
-        if (m > 0 && rl[a] <= rh[m - 1]) {
-            rh[m - 1] = max(rh[m - 1], rh[a]);
-        } else {
-            rl[m] = rl[a]; rh[m] = rh[a]; ++m;
-        }
-    }
-    if (m > TRI_MAXR) return -1;
-    for (int a = 0; a < m; ++a) { lo[a] = (unsigned char)rl[a]; hi[a] = (unsigned char)rh[a]; }
-    return m;
-}
 
 __device__ __forceinline__ int find_lat(const LatTable& L, int nl, int t)
 {
@@ -268,13 +150,11 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 5 : 6) k_convex(Dev d)
 {
     CMS_EXIT_ON_OVERFLOW(d);
     __shared__ LatTable tab[CV_WARPS];
-    __shared__ LatMasks masks[CV_WARPS];
     __shared__ int ncs[CV_WARPS][CMS_MAX_SUBDIV];
     __shared__ int ksl[EMIT ? 1 : CV_WARPS][KS_CAP];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     LatTable& L = tab[w];
-    LatMasks& LM = masks[w];
     StashCursor kcur{0, 0};
     const double rp = d.st.rp;
     const long long wid = blockIdx.x * (long long)CV_WARPS + w;
@@ -365,30 +245,6 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 5 : 6) k_convex(Dev d)
                 continue;
             }
         }
-        // The probe centres of latitude l lie on one circle (axis north, centre xi + (c_l - xi) scale, radius
-        // rad_l scale): only the neighbours whose sphere r + rp can reach it can collide with them
-        // (cms_circle.cuh), so each latitude gets the mask of those slots (slot 0, the frame atom, is skipped
-        // as the reference skips it); rows longer than CV_MASK_SLOTS take the full scan.
-        const bool masked = K <= CV_MASK_SLOTS;
-        if (masked) {
-            for (int l = 0; l < nl; ++l) {
-                if (ncs[w][l] == 0) continue;            // no points on this latitude
-                const V3 cc = xi + (v3(L.cx[l], L.cy[l], L.cz[l]) - xi) * scale;
-                const double R = L.rad[l] * scale;
-                for (int r = 0; r * 32 < K; ++r) {
-                    const int sl = r * 32 + lane;
-                    bool reach = false;
-                    if (sl >= 1 && sl < K) {
-                        const double4 b = d.xyzr[d.nb_id[off + sl]];
-                        const double tt = b.w + rp + CMS_CIRCLE_MARGIN;
-                        reach = !(circle_dist2(v3(b.x, b.y, b.z), cc, north, R) > tt * tt);
-                    }
-                    const unsigned m = __ballot_sync(0xffffffffu, reach);
-                    if (lane == 0) LM.m[l][r] = m;
-                }
-            }
-            __syncwarp();
-        }
         for (int t0 = 0; t0 < total; t0 += 32) {
             const int t = t0 + lane;
             bool keep = false;
@@ -400,24 +256,10 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 5 : 6) k_convex(Dev d)
                 pt = subdiv_point(v3(L.cx[l], L.cy[l], L.cz[l]), L.rad[l], fx, fy, L.delta[l], i);
                 pcen = xi + (pt - xi) * scale;
                 keep = true;
-                if (masked && near_circle(pcen, xi + (v3(L.cx[l], L.cy[l], L.cz[l]) - xi) * scale, north,
-                                          L.rad[l] * scale)) {
-                    for (int r = 0; r * 32 < K && keep; ++r) {
-                        unsigned m = LM.m[l][r];
-                        while (m) {
-                            const int sl = r * 32 + __ffs(m) - 1;
-                            m &= m - 1;
-                            const double4 b = d.xyzr[d.nb_id[off + sl]];
-                            const double tt = b.w + rp;
-                            if (sq_seq(v3(b.x, b.y, b.z) - pcen) <= tt * tt) { keep = false; break; }
-                        }
-                    }
-                } else {
-                    for (int s = 1; s < K; ++s) {        // slot 0 (the frame atom) is skipped
-                        double4 b = d.xyzr[d.nb_id[off + s]];
-                        double tt = b.w + rp;
-                        if (sq_seq(v3(b.x, b.y, b.z) - pcen) <= tt * tt) { keep = false; break; }
-                    }
+                for (int s = 1; s < K; ++s) {        // slot 0 (the frame atom) is skipped
+                    double4 b = d.xyzr[d.nb_id[off + s]];
+                    double tt = b.w + rp;
+                    if (sq_seq(v3(b.x, b.y, b.z) - pcen) <= tt * tt) { keep = false; break; }
                 }
             }
             const unsigned m = __ballot_sync(0xffffffffu, keep);
@@ -908,14 +750,12 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
 {
     CMS_EXIT_ON_OVERFLOW(d);
     __shared__ LatTable tab[CC_WARPS];
-    __shared__ LatRanges rng[CC_WARPS];
     __shared__ int ncs[CC_WARPS][CMS_MAX_SUBDIV];
     __shared__ int nears[CC_WARPS][CMS_NEAR_CAP];
     __shared__ int ksl[EMIT ? 1 : CC_WARPS][KS_CAP];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     LatTable& L = tab[w];
-    LatRanges& LR = rng[w];
     StashCursor kcur{0, 0};
     const double rp = d.st.rp, rp2 = rp * rp;
     const long long NP = min(d.plus_off[d.N] + d.minus_off[d.N], d.probe_cap);
@@ -1011,15 +851,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
             }
             L.cx[l] = cen.x; L.cy[l] = cen.y; L.cz[l] = cen.z;
             L.rad[l] = rad; L.delta[l] = delta; L.area[l] = ps * cs;
-            // candidate ranges of the latitude (every other point fails the triangle test)
-            int nr = tri_ranges(cen, rad, fx, fy, delta, nc, vec0, vec1, vec2, LR.rlo[l], LR.rhi[l]);
-            int ncand = 0;
-            if (nr < 0) {
-                nr = 1; LR.rlo[l][0] = 0; LR.rhi[l][0] = (unsigned char)nc;
-            }
-            for (int r = 0; r < nr; ++r) ncand += (int)LR.rhi[l][r] - (int)LR.rlo[l][r];
-            LR.nr[l] = (unsigned char)nr;
-            ncs[w][l] = ncand;
+            ncs[w][l] = nc;
         }
         __syncwarp();
         lat_prefix(L, ncs[w], nl);
@@ -1041,7 +873,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
             int l = 0, i = 0, mc = 0;
             if (t < total) {
                 l = find_lat(L, nl, t);
-                i = lat_range_index(LR, l, t - L.start[l]);
+                i = t - L.start[l];
                 V3 pt = subdiv_point(v3(L.cx[l], L.cy[l], L.cz[l]), L.rad[l], fx, fy, L.delta[l], i);
                 keep = !(dot_seq(pt, vec0) >= 0 || dot_seq(pt, vec1) >= 0 || dot_seq(pt, vec2) >= 0);
                 if (keep) {

@@ -10,7 +10,6 @@
 // Every distance test keeps the reference's summation order (dot_seq for
 // cdist / np.sum / norm, dot_alt for einsum) and strictness.
 #include "cms_kernels.cuh"
-#include "cms_circle.cuh"
 
 namespace cms {
 
@@ -798,7 +797,6 @@ struct TrPairC { V3 uij, tij; double rij; int ps; };
 struct TrWork {
     TrPairC pr[TR_PC];
     unsigned cb[TR_PC][TR_KC / 32];   // candidate k slots of each pair
-    unsigned pm[TR_PC][TR_KC / 32];   // slots whose sphere may reach the pair's circle (collision candidates)
     int cpos[TR_PC];                  // first (pair, k) combination of each pair
     unsigned kill;                    // pairs killed by a degenerate triple
 };
@@ -836,32 +834,11 @@ __device__ __forceinline__ bool probe_collides_c(const TrRow& R, int K, V3 pt, i
     return false;
 }
 
-// probe_collides_c over the pair's circle-pruned slots: every probe of pair (i, j) lies on its circle, so
-// only the slots of `pm` can hold a colliding neighbour (j is not among them); the full row is scanned for a
-// point that is not within CMS_CIRCLE_TOL of the circle
-__device__ __forceinline__ bool probe_collides_pm(const TrRow& R, int K, const unsigned* pm, const TrPairC& P,
-                                                  V3 pt, int j, int k, double rp)
-{
-    if (!near_circle(pt, P.tij, P.uij, P.rij)) return probe_collides_c(R, K, pt, j, k, rp);
-    for (int r = 0; r * 32 < K; ++r) {
-        unsigned m = pm[r];
-        while (m) {
-            const int s = r * 32 + __ffs(m) - 1;
-            m &= m - 1;
-            if (R.id[s] == k) continue;
-            const double t = R.r[s] + rp;
-            if (sq_alt(pt - v3(R.x[s], R.y[s], R.z[s])) <= t * t) return true;
-        }
-    }
-    return false;
-}
-
 template <bool EMIT>
 __device__ __forceinline__ void triples_flush_c(const Dev& d, int g, V3 xi, double eri, const TrRow& R, int K,
-                                                const unsigned* queue, const TrWork& W, int qn, int& nplus,
+                                                const unsigned* queue, const TrPairC* pq, int qn, int& nplus,
                                                 int& nminus, long long pbase, long long mbase)
 {
-    const TrPairC* pq = W.pr;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     const double rp = d.st.rp;
@@ -898,9 +875,8 @@ __device__ __forceinline__ void triples_flush_c(const Dev& d, int g, V3 xi, doub
                     up = uijk;
                     pp = bijk + uijk * (h * 1.0);
                     pm = bijk + uijk * (h * -1.0);
-                    const unsigned* cm = W.pm[ent >> 16];
-                    okp = !probe_collides_pm(R, K, cm, P, pp, j, k, rp);
-                    okm = !probe_collides_pm(R, K, cm, P, pm, j, k, rp);
+                    okp = !probe_collides_c(R, K, pp, j, k, rp);
+                    okm = !probe_collides_c(R, K, pm, j, k, rp);
                 }
             }
         }
@@ -1016,30 +992,6 @@ __device__ __forceinline__ void triples_row_c(const Dev& d, int g, int K, long l
             }
         }
         __syncwarp();
-        // collision candidates of each live pair with candidates: the row slots
-        // (other than j's) whose sphere r + rp may reach the pair's circle
-        for (int pi = 0; pi < np; ++pi) {
-            if ((W.kill >> pi) & 1u) continue;
-            unsigned any = 0u;
-            for (int r = 0; r * 32 < K; ++r) any |= W.cb[pi][r];
-            if (!any) continue;
-            const TrPairC& P = W.pr[pi];
-            for (int r = 0; r * 32 < K; ++r) {
-                const int s = r * 32 + lane;
-                bool keep = false;
-                if (s < K && s != P.ps) {
-                    const V3 v = v3(R.x[s], R.y[s], R.z[s]) - P.tij;
-                    const double hh = dot_seq(v, P.uij);
-                    const double rho = sqrt(fmax(sq_seq(v) - hh * hh, 0.0));
-                    const double dr = rho - P.rij;
-                    const double t = R.r[s] + rp + CMS_CIRCLE_MARGIN;
-                    keep = !(hh * hh + dr * dr > t * t);       // a NaN distance keeps the slot
-                }
-                const unsigned m = __ballot_sync(0xffffffffu, keep);
-                if (lane == 0) W.pm[pi][r] = m;
-            }
-        }
-        __syncwarp();
         // queue, one pair per lane: candidates of the live pairs in (pair, k
         // slot) order, flushed whenever the next pair would overflow the queue
         int nq = 0;
@@ -1072,7 +1024,7 @@ __device__ __forceinline__ void triples_row_c(const Dev& d, int g, int K, long l
                 }
             }
             __syncwarp();
-            triples_flush_c<EMIT>(d, g, xi, eri, R, K, queue, W, end - base, nplus, nminus, pbase, mbase);
+            triples_flush_c<EMIT>(d, g, xi, eri, R, K, queue, W.pr, end - base, nplus, nminus, pbase, mbase);
             __syncwarp();
             base = end;
         }
