@@ -282,7 +282,8 @@ struct cms_ctx {
         S_ADJ_LIST_CONC, S_ADJ_NACT, S_OVF, S_REF_XYZ, S_POSE, S_POSE_CKPT, S_POSE_CEN, S_HIST, S_STEP, S_MAXSUM,
         S_TOR_LFLAG, S_TOR_LOFF, S_TOR_LIST, S_PTOP, S_SP_A, S_SP_H, S_SP_XYZ, S_SP_ALT, S_SP_G, S_SP_ORD,
         S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1, S_KS_TOP, S_KS_BUF, S_CV_SOFF, S_CC_SOFF, S_TOR_SOFF, S_TOR_SN, S_NBS_TOP, S_NBS_BUF, S_NB_SOFF, S_ADJ_SKEY, S_ADJ_SLIST_CONV, S_ADJ_SLIST_TOR, S_ADJ_SLIST_CONC, S_CS_TOP, S_CS_XYZ, S_CS_AREA, S_CS_OWN,
-        S_CS_SUB, S_CS_BUR, S_RES_OFF, S_RES_ATOMS, S_RES_SUM, S_RES_FLAG, S_NN_COUNT,
+        S_CS_SUB, S_CS_BUR, S_RES_OFF, S_RES_ATOMS, S_RES_SUM, S_RES_FLAG, S_NN_COUNT, S_PLC_CNT, S_PLC_FILL, S_PLC_START,
+        S_PLC_ITEM, S_PLC_CELL,
         S_COUNT
     };
 
@@ -430,6 +431,11 @@ void bind_caps(cms_ctx* x)
     d.plow_flag = x->ensure<int>(cms_ctx::S_PLOW_FLAG, x->cap_probe);
     d.plow_off = x->ensure<long long>(cms_ctx::S_PLOW_OFF, x->cap_probe + 1);
     d.plow_list = x->ensure<int>(cms_ctx::S_PLOW_LIST, x->cap_probe);
+    d.plc_cnt = x->ensure<int>(cms_ctx::S_PLC_CNT, x->cap_cells);
+    d.plc_fill = x->ensure<int>(cms_ctx::S_PLC_FILL, x->cap_cells);
+    d.plc_start = x->ensure<long long>(cms_ctx::S_PLC_START, x->cap_cells + 1);
+    d.plc_item = x->ensure<int>(cms_ctx::S_PLC_ITEM, x->cap_probe);
+    d.plc_cell = x->ensure<int>(cms_ctx::S_PLC_CELL, x->cap_probe);
     d.ptop = x->ensure<unsigned long long>(cms_ctx::S_PTOP, 1);
     d.sp_a = x->ensure<int>(cms_ctx::S_SP_A, 3 * x->cap_probe);
     d.sp_h = x->ensure<double>(cms_ctx::S_SP_H, x->cap_probe);

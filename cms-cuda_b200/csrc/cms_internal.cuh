@@ -93,6 +93,10 @@ struct Dev {
     double* ph; double* pxyz; double* palt;   // probe_cap, 3*cap, 3*cap
     int* plow_flag; long long* plow_off;      // probe_cap, probe_cap+1
     int* plow_list;                            // probe_cap
+    // low probes by cell of their complex's atom grid (clamped to it): counts, scan, probe ids, cell of each
+    int* plc_cnt; int* plc_fill;               // cells
+    long long* plc_start;                      // cells+1
+    int* plc_item; int* plc_cell;              // probe_cap
     // probes stashed by the triple count pass (any order), with their final slot:
     // generating atom and sign bit (31) | rank among that atom's probes of that sign
     unsigned long long* ptop;                  // 1: stash entries taken

@@ -752,6 +752,8 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
     __shared__ LatTable tab[CC_WARPS];
     __shared__ int ncs[CC_WARPS][CMS_MAX_SUBDIV];
     __shared__ int nears[CC_WARPS][CMS_NEAR_CAP];
+    __shared__ int cpre[CC_WARPS][33];                 // low-probe cell columns: exclusive scan of lengths
+    __shared__ long long cbeg[CC_WARPS][32];           // and each column's first entry
     __shared__ int ksl[EMIT ? 1 : CC_WARPS][KS_CAP];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
@@ -784,26 +786,59 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
         const V3 uijk = ld3(d.palt + 3 * p);
         const bool low = d.ph[p] < rp;
         const int c = d.cplx[ia[0]];
-        // nearby low probes of the same complex (d2 <= 4 rp^2), self excluded
+        // nearby low probes of the same complex (d2 <= 4 rp^2), self excluded: the low probes of the cells
+        // (clamped to the complex's grid) that meet the box of the 2 rp ball, one (x, y) column per lane,
+        // each column's cells contiguous, then one probe per lane
         int nnear = 0;
         if (low) {
             const Cplx C = d.cx[c];
-            const int s0 = C.a0, e1 = C.a0 + C.n;
-            const long long pb = min(d.plus_off[s0] + d.minus_off[s0], d.probe_cap);
-            const long long pe = min(d.plus_off[e1] + d.minus_off[e1], d.probe_cap);
-            const long long ls = d.plow_off[pb], le = d.plow_off[pe];
-            for (long long b = ls; b < le; b += 32) {
-                long long li = b + lane;
-                bool near = false;
-                int qi = -1;
-                if (li < le) {
-                    qi = d.plow_list[li];
-                    if (qi != p) near = sq_seq(pijk - ld3(d.pxyz + 3 * (long long)qi)) <= 4 * rp2;
+            const double re = (2.0 * rp) * (1.0 + 1e-9) + 1e-9;
+            const int x0 = cell_coord(pijk.x - re, C.org[0], C.h, C.dims[0]);
+            const int x1 = cell_coord(pijk.x + re, C.org[0], C.h, C.dims[0]);
+            const int y0 = cell_coord(pijk.y - re, C.org[1], C.h, C.dims[1]);
+            const int y1 = cell_coord(pijk.y + re, C.org[1], C.h, C.dims[1]);
+            const int z0 = cell_coord(pijk.z - re, C.org[2], C.h, C.dims[2]);
+            const int z1 = cell_coord(pijk.z + re, C.org[2], C.h, C.dims[2]);
+            const int ny = y1 - y0 + 1;
+            const int ncol = (x1 - x0 + 1) * ny;
+            const long long c0 = d.ncell_scan[c];
+            for (int cb = 0; cb < ncol; cb += 32) {
+                const int col = cb + lane;
+                long long s0 = 0;
+                int len = 0;
+                if (col < ncol) {
+                    const long long base = c0 + ((long long)(x0 + col / ny) * C.dims[1] + (y0 + col % ny)) * C.dims[2];
+                    if (base + z1 < d.cells_cap) {
+                        s0 = d.plc_start[base + z0];
+                        len = (int)(d.plc_start[base + z1 + 1] - s0);
+                    }
                 }
-                unsigned m = __ballot_sync(0xffffffffu, near);
-                int pos = nnear + __popc(m & lt);
-                if (near && pos < CMS_NEAR_CAP) nears[w][pos] = qi;
-                nnear += __popc(m);
+                int tot;
+                const int ex = warp_excl_scan(len, tot);
+                __syncwarp();
+                cpre[w][lane] = ex;
+                cbeg[w][lane] = s0;
+                if (lane == 31) cpre[w][32] = tot;
+                __syncwarp();
+                for (int b = 0; b < tot; b += 32) {
+                    const int i = b + lane;
+                    bool near = false;
+                    int qi = -1;
+                    if (i < tot) {
+                        int lo = 0, hi = 31;          // column holding i: largest k with cpre[k] <= i
+                        while (lo < hi) {
+                            const int mid = (lo + hi + 1) >> 1;
+                            if (cpre[w][mid] <= i) lo = mid; else hi = mid - 1;
+                        }
+                        qi = d.plc_item[cbeg[w][lo] + (i - cpre[w][lo])];
+                        if (qi != p) near = sq_seq(pijk - ld3(d.pxyz + 3 * (long long)qi)) <= 4 * rp2;
+                    }
+                    unsigned m = __ballot_sync(0xffffffffu, near);
+                    int pos = nnear + __popc(m & lt);
+                    if (near && pos < CMS_NEAR_CAP) nears[w][pos] = qi;
+                    nnear += __popc(m);
+                }
+                __syncwarp();
             }
             if (nnear > CMS_NEAR_CAP) {
                 if (lane == 0) atomicOr(&d.status[c], ST_NEAR_OVERFLOW);

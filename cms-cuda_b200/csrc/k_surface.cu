@@ -1192,11 +1192,52 @@ __global__ void k_low_fill(Dev d, long long cap)
         if (d.plow_flag[p]) d.plow_list[d.plow_off[p]] = (int)p;
 }
 
+// Low probes sorted by cell of their complex's atom grid, coordinates clamped
+// to the grid (probes can lie just outside the atoms' box; clamping is
+// monotone, so a search over the clamped cell range of a ball still meets
+// every low probe inside the ball).  The concave kernels look up a probe's
+// nearby low probes there instead of scanning all of the complex's low probes.
+__global__ void k_low_cell_count(Dev d, long long cap)
+{
+    CMS_EXIT_ON_OVERFLOW(d);
+    const long long NL = d.plow_off[cap];
+    for (long long li = blockIdx.x * (long long)blockDim.x + threadIdx.x; li < NL; li += (long long)gridDim.x * blockDim.x) {
+        const int p = d.plow_list[li];
+        const int c = d.cplx[d.pa0[p]];
+        const Cplx& C = d.cx[c];
+        const double* x = d.pxyz + 3LL * p;
+        const int cx = cell_coord(x[0], C.org[0], C.h, C.dims[0]);
+        const int cy = cell_coord(x[1], C.org[1], C.h, C.dims[1]);
+        const int cz = cell_coord(x[2], C.org[2], C.h, C.dims[2]);
+        long long cell = d.ncell_scan[c] + ((long long)cx * C.dims[1] + cy) * C.dims[2] + cz;
+        if (cell >= d.cells_cap) { atomicOr(&d.status[c], ST_OVERFLOW); cell = -1; }
+        d.plc_cell[li] = (int)cell;
+        if (cell >= 0) atomicAdd(&d.plc_cnt[cell], 1);
+    }
+}
+
+__global__ void k_low_cell_fill(Dev d, long long cap)
+{
+    CMS_EXIT_ON_OVERFLOW(d);
+    const long long NL = d.plow_off[cap];
+    for (long long li = blockIdx.x * (long long)blockDim.x + threadIdx.x; li < NL; li += (long long)gridDim.x * blockDim.x) {
+        const int cell = d.plc_cell[li];
+        if (cell < 0) continue;
+        const int pos = atomicAdd(&d.plc_fill[cell], 1);
+        d.plc_item[d.plc_start[cell] + pos] = d.plow_list[li];
+    }
+}
+
 void launch_low_probes(const Dev& d, long long probe_cap, long long* scan_tmp, cudaStream_t s)
 {
     k_low_flag<<<grid_for(probe_cap, 256), 256, 0, s>>>(d, probe_cap);
     scan_counts(d.plow_flag, d.plow_off, probe_cap, scan_tmp, s);
     k_low_fill<<<grid_for(probe_cap, 256), 256, 0, s>>>(d, probe_cap);
+    k_zero_int<<<grid_for(d.cells_cap, 256), 256, 0, s>>>(d.plc_cnt, d.cells_cap);
+    k_zero_int<<<grid_for(d.cells_cap, 256), 256, 0, s>>>(d.plc_fill, d.cells_cap);
+    k_low_cell_count<<<grid_for(probe_cap, 256), 256, 0, s>>>(d, probe_cap);
+    scan_counts(d.plc_cnt, d.plc_start, d.cells_cap, scan_tmp, s);
+    k_low_cell_fill<<<grid_for(probe_cap, 256), 256, 0, s>>>(d, probe_cap);
 }
 
 }  // namespace cms
