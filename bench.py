@@ -246,7 +246,7 @@ def cpu_baseline_single(cores, large_max=False):
         out[name][f"{what}_value"] = vals.get("max_cms" if what == "max_cms" else "cms")
     if not large_max:
         out["1800+8000"]["max_cms_s"] = None
-        out["1800+8000"]["note"] = "max-CMS of the 8000-atom target not timed on the CPU (about 40 GB of RAM)"
+        out["1800+8000"]["note"] = "max-CMS of the 8000-atom target not timed on the CPU (needs about 40 GB of RAM)"
     return out
 
 
@@ -794,7 +794,8 @@ def run_ours(args):
             extras["pose_refinement"], poses = pose_refinement(args, local)
         # CPU legs (the oracle, on the host cores)
         extras["cpu_baseline"] = cpu_baseline_batched(batch, args.cpu_sample, cores)
-        cpu_single = cpu_baseline_single(cores)
+        ram_gb = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES") / 1e9
+        cpu_single = cpu_baseline_single(cores, large_max=ram_gb >= 96)
         for name, row in cpu_single.items():
             extras["single_complex"][name]["oracle_cpu"] = row
         if poses is not None:

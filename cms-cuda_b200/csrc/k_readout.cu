@@ -892,18 +892,19 @@ void launch_tasks(const Dev& d, const Rd& r, int kind, NNTask* task, cudaStream_
 // of the nearest-dot search are compact boxes.  The searches return the same
 // results in any order: ties go to the smallest original position.
 // ---------------------------------------------------------------------------
-static constexpr int SO_GRID = 16;                    // cells per axis
+static constexpr int SO_GRID = 8;                     // cells per axis (a range holds a few thousand entries)
 static constexpr int SO_CELLS = SO_GRID * SO_GRID * SO_GRID;
 
 __device__ __forceinline__ int so_pad(int b) { return b + (b >> 7); }   // 128 buckets per lane, skewed banks
 
-__device__ __forceinline__ unsigned so_spread4(unsigned v)      // 4 bits -> every third bit
+__device__ __forceinline__ unsigned so_spread4(unsigned v)      // up to 4 bits -> every third bit
 {
     v &= 0xfu;
     v = (v | (v << 4)) & 0x0c3u;
     v = (v | (v << 2)) & 0x249u;
     return v;
 }
+static_assert(SO_GRID <= 16 && (SO_GRID & (SO_GRID - 1)) == 0, "Morton cells of up to 4 bits per axis");
 
 __device__ __forceinline__ void so_range(const Dev& d, const Rd& r, int list, long long t, long long& s, long long& e)
 {
@@ -1018,7 +1019,7 @@ void launch_spatial_order(const Dev& d, const Rd& r, int list, int set, cudaStre
 {
     const int smem = SO_W * SO_STRIDE * (int)sizeof(int);
     cudaFuncSetAttribute(k_spatial_order, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    k_spatial_order<<<grid_for(2LL * d.B, 1, 3), SO_W * 32, smem, s>>>(d, r, list, set);
+    k_spatial_order<<<grid_for(2LL * d.B, 1, 12), SO_W * 32, smem, s>>>(d, r, list, set);
 }
 
 // ---------------------------------------------------------------------------

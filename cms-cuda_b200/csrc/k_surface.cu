@@ -9,6 +9,8 @@
 //   vec_third_loop             _core.py:1445-1643
 // Every distance test keeps the reference's summation order (dot_seq for
 // cdist / np.sum / norm, dot_alt for einsum) and strictness.
+#include <type_traits>
+
 #include "cms_kernels.cuh"
 
 namespace cms {
@@ -182,8 +184,10 @@ void launch_cells(const Dev& d, long long n_cells, long long* scan_tmp, cudaStre
 // radius `range` around atom g (a superset of the atoms within range).  The
 // cells of one (x, y) column that meet the ball are contiguous in cell_atom,
 // so the warp lays the columns end to end and hands one atom to each lane;
-// f(j) is called by all 32 lanes together, j = -1 past the end.  Cell
-// bounds get a 1e-9 A margin over the rounding of the cell assignment.
+// f(j) is called by all 32 lanes together, j = -1 past the end; when f
+// returns bool, the scan stops after the first call where any lane returned
+// true.  Cell bounds get a 1e-9 A margin over the rounding of the cell
+// assignment.
 // ---------------------------------------------------------------------------
 static constexpr int NB_WARPS = 4;
 
@@ -262,7 +266,14 @@ __device__ __forceinline__ void scan_ball(const Dev& d, int g, int c, double ran
                 }
                 j = d.cell_atom[S.beg[lo] + (i - S.pre[lo])];
             }
-            f(j);
+            if constexpr (std::is_same<decltype(f(j)), bool>::value) {
+                if (__any_sync(0xffffffffu, f(j))) {
+                    __syncwarp();
+                    return;
+                }
+            } else {
+                f(j);
+            }
         }
     }
     __syncwarp();
@@ -295,12 +306,16 @@ __global__ void __launch_bounds__(NB_WARPS * 32) k_attention(Dev d)
             const double se = d.st.sep * (1.0 + 1e-9) + 1e-9;
             if (gx * gx + gy * gy + gz * gz > se * se) { if (lane == 0) d.atten[g] = 1; continue; }
         }
-        double best = INFINITY;
-        scan_ball(d, g, c, d.st.sep, sc[w], [&](int j) {
-            if (j >= 0 && d.mol[j] != mi) best = fmin(best, sq_seq(xi - atom_xyz(d, j)));
+        // the reference's min over the other molecule of cdist >= sep fails as soon as one distance is
+        // below sep (sqrt is monotone): stop the scan at the first such atom
+        bool near = false;
+        scan_ball(d, g, c, d.st.sep, sc[w], [&](int j) -> bool {
+            const bool hit = j >= 0 && d.mol[j] != mi && !(sqrt(sq_seq(xi - atom_xyz(d, j))) >= d.st.sep);
+            near |= hit;
+            return hit;
         });
-        for (int o = 16; o > 0; o >>= 1) best = fmin(best, __shfl_xor_sync(0xffffffffu, best, o));
-        if (lane == 0) d.atten[g] = (sqrt(best) >= d.st.sep) ? 1 : 5;
+        near = __any_sync(0xffffffffu, near);
+        if (lane == 0) d.atten[g] = near ? 5 : 1;
     }
 }
 
