@@ -116,11 +116,15 @@ __device__ __forceinline__ int ks_stash(const Dev& d, const int* list, int kept,
 // ---------------------------------------------------------------------------
 // convex dots: one warp per atom of the convex queue
 // ---------------------------------------------------------------------------
-static constexpr int CV_WARPS = 4;
+static constexpr int CV_WARPS = 2;
+static constexpr int CV_ROW = 128;    // neighbour rows up to this long are cached in shared memory
 
+// Latitude table of one sphere: each latitude's offset dt along the polar
+// axis (its circle's centre is recomputed as the table was made: xi + north dt
+// for convex, south dt for concave), radius, subdivision step, dot area and
+// first point in the sphere's enumeration.
 struct LatTable {
-    double cx[CMS_MAX_SUBDIV], cy[CMS_MAX_SUBDIV], cz[CMS_MAX_SUBDIV];
-    double rad[CMS_MAX_SUBDIV], delta[CMS_MAX_SUBDIV], area[CMS_MAX_SUBDIV];
+    double dt[CMS_MAX_SUBDIV], rad[CMS_MAX_SUBDIV], delta[CMS_MAX_SUBDIV], area[CMS_MAX_SUBDIV];
     int start[CMS_MAX_SUBDIV + 1];
 };
 
@@ -146,12 +150,13 @@ __device__ __forceinline__ void lat_prefix(LatTable& L, const int* nc, int nl)
 }
 
 template <bool EMIT>
-__global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 5 : 6) k_convex(Dev d)
+__global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 10 : 12) k_convex(Dev d)
 {
     CMS_EXIT_ON_OVERFLOW(d);
     __shared__ LatTable tab[CV_WARPS];
     __shared__ int ncs[CV_WARPS][CMS_MAX_SUBDIV];
     __shared__ int ksl[EMIT ? 1 : CV_WARPS][KS_CAP];
+    __shared__ double4 nrow[CV_WARPS][CV_ROW];   // the atom's neighbours: x, y, z, r + rp
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     LatTable& L = tab[w];
@@ -209,7 +214,6 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 5 : 6) k_convex(Dev d)
         for (int l = lane; l < nl; l += 32) {
             V3 lat = subdiv_point(v3(0.0, 0.0, 0.0), ri, north, ylat, dl, l);
             double dt = dot_seq(lat, north);
-            V3 cen = xi + north * dt;
             double rsq = ri * ri - dt * dt;
             double rad = rsq > 0.0 ? sqrt(rsq) : 0.0;
             int nc = 0;
@@ -219,7 +223,7 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 5 : 6) k_convex(Dev d)
                 nc = subdiv_count_long(delta, CMS_TWO_PI);
                 ps = subdiv_ps(rad, CMS_TWO_PI, nc);
             }
-            L.cx[l] = cen.x; L.cy[l] = cen.y; L.cz[l] = cen.z;
+            L.dt[l] = dt;
             L.rad[l] = rad; L.delta[l] = delta; L.area[l] = ps * cs;
             ncs[w][l] = nc;
         }
@@ -238,12 +242,21 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 5 : 6) k_convex(Dev d)
                 for (int e = lane; e < cnt; e += 32) {
                     const int sub = d.ks_buf[so + e];
                     const int l = sub >> 16, i = sub & 0xffff;
-                    const V3 pt = subdiv_point(v3(L.cx[l], L.cy[l], L.cz[l]), L.rad[l], fx, fy, L.delta[l], i);
+                    const V3 pt = subdiv_point(xi + north * L.dt[l], L.rad[l], fx, fy, L.delta[l], i);
                     write_dot(d, base + e, pt, xi + (pt - xi) * scale, L.area[l], g, 1, g, sub);
                 }
                 __syncwarp();
                 continue;
             }
+        }
+        // the neighbour row in shared memory (the collision test reads it for every point)
+        const bool cached = K <= CV_ROW;
+        if (cached) {
+            for (int s = lane; s < K; s += 32) {
+                const double4 b = d.xyzr[d.nb_id[off + s]];
+                nrow[w][s] = make_double4(b.x, b.y, b.z, b.w + rp);
+            }
+            __syncwarp();
         }
         for (int t0 = 0; t0 < total; t0 += 32) {
             const int t = t0 + lane;
@@ -253,13 +266,20 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 5 : 6) k_convex(Dev d)
             if (t < total) {
                 l = find_lat(L, nl, t);
                 i = t - L.start[l];
-                pt = subdiv_point(v3(L.cx[l], L.cy[l], L.cz[l]), L.rad[l], fx, fy, L.delta[l], i);
+                pt = subdiv_point(xi + north * L.dt[l], L.rad[l], fx, fy, L.delta[l], i);
                 pcen = xi + (pt - xi) * scale;
                 keep = true;
-                for (int s = 1; s < K; ++s) {        // slot 0 (the frame atom) is skipped
-                    double4 b = d.xyzr[d.nb_id[off + s]];
-                    double tt = b.w + rp;
-                    if (sq_seq(v3(b.x, b.y, b.z) - pcen) <= tt * tt) { keep = false; break; }
+                if (cached) {
+                    for (int s = 1; s < K; ++s) {    // slot 0 (the frame atom) is skipped
+                        const double4 b = nrow[w][s];
+                        if (sq_seq(v3(b.x, b.y, b.z) - pcen) <= b.w * b.w) { keep = false; break; }
+                    }
+                } else {
+                    for (int s = 1; s < K; ++s) {
+                        double4 b = d.xyzr[d.nb_id[off + s]];
+                        double tt = b.w + rp;
+                        if (sq_seq(v3(b.x, b.y, b.z) - pcen) <= tt * tt) { keep = false; break; }
+                    }
                 }
             }
             const unsigned m = __ballot_sync(0xffffffffu, keep);
@@ -371,7 +391,21 @@ __device__ __forceinline__ bool tor_collides(const Dev& d, const TorPair& T, V3 
 {
     const double rp = d.st.rp;
     if (nnear >= 0) {
-        for (int k = 0; k < nnear; ++k) {
+        // four independent loads at a time, then the tests
+        int k = 0;
+        for (; k + 4 <= nnear; k += 4) {
+            double4 b[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) b[u] = d.xyzr[near[k + u]];
+            bool hit = false;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const double t = b[u].w + rp;
+                hit |= sq_alt(pij - v3(b[u].x, b[u].y, b[u].z)) < t * t;
+            }
+            if (hit) return true;
+        }
+        for (; k < nnear; ++k) {
             const double4 b = d.xyzr[near[k]];
             const double t = b.w + rp;
             if (sq_alt(pij - v3(b.x, b.y, b.z)) < t * t) return true;
@@ -874,7 +908,6 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
         for (int l = lane; l < nl; l += 32) {
             V3 lat = subdiv_point(v3(0.0, 0.0, 0.0), rp, vtop, ylat, dl, l);
             double dt = dot_seq(lat, south);
-            V3 cen = south * dt;
             double rsq = rp2 - dt * dt;
             double rad = sqrt(rsq < 0.0 ? 0.0 : rsq);
             int nc = 0;
@@ -884,7 +917,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
                 nc = subdiv_count_long(delta, CMS_TWO_PI);
                 ps = subdiv_ps(rad, CMS_TWO_PI, nc);
             }
-            L.cx[l] = cen.x; L.cy[l] = cen.y; L.cz[l] = cen.z;
+            L.dt[l] = dt;
             L.rad[l] = rad; L.delta[l] = delta; L.area[l] = ps * cs;
             ncs[w][l] = nc;
         }
@@ -909,7 +942,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
             if (t < total) {
                 l = find_lat(L, nl, t);
                 i = t - L.start[l];
-                V3 pt = subdiv_point(v3(L.cx[l], L.cy[l], L.cz[l]), L.rad[l], fx, fy, L.delta[l], i);
+                V3 pt = subdiv_point(south * L.dt[l], L.rad[l], fx, fy, L.delta[l], i);
                 keep = !(dot_seq(pt, vec0) >= 0 || dot_seq(pt, vec1) >= 0 || dot_seq(pt, vec2) >= 0);
                 if (keep) {
                     pts = pt + pijk;
@@ -949,7 +982,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
                 for (int e = lane; e < kept; e += 32) {
                     const int sub = ksl[EMIT ? 0 : w][e];
                     const int l = sub >> 16, i = sub & 0xffff;
-                    const V3 pts = subdiv_point(v3(L.cx[l], L.cy[l], L.cz[l]), L.rad[l], fx, fy, L.delta[l], i) + pijk;
+                    const V3 pts = subdiv_point(south * L.dt[l], L.rad[l], fx, fy, L.delta[l], i) + pijk;
                     double dd[3];
                     for (int k = 0; k < 3; ++k) dd[k] = norm3(pts - xa[k]) - ra[k];
                     int mc = 0;                        // np.argmin: first minimum, NaN wins

@@ -849,6 +849,24 @@ __device__ __forceinline__ bool probe_collides_c(const TrRow& R, int K, V3 pt, i
     return false;
 }
 
+// probe_collides_c for the triple's two probes in one pass over the row (each neighbour read once); the
+// loop ends when both have collided
+__device__ __forceinline__ void probe_pair_collides_c(const TrRow& R, int K, V3 pp, V3 pm, int j, int k, double rp,
+                                                      bool& cp, bool& cm)
+{
+    cp = cm = false;
+    for (int s = 0; s < K; ++s) {
+        const int n = R.id[s];
+        if (n == j || n == k) continue;
+        const double t = R.r[s] + rp;
+        const double t2 = t * t;
+        const V3 x = v3(R.x[s], R.y[s], R.z[s]);
+        cp = cp || sq_alt(pp - x) <= t2;
+        cm = cm || sq_alt(pm - x) <= t2;
+        if (cp && cm) return;
+    }
+}
+
 template <bool EMIT>
 __device__ __forceinline__ void triples_flush_c(const Dev& d, int g, V3 xi, double eri, const TrRow& R, int K,
                                                 const unsigned* queue, const TrPairC* pq, int qn, int& nplus,
@@ -890,8 +908,10 @@ __device__ __forceinline__ void triples_flush_c(const Dev& d, int g, V3 xi, doub
                     up = uijk;
                     pp = bijk + uijk * (h * 1.0);
                     pm = bijk + uijk * (h * -1.0);
-                    okp = !probe_collides_c(R, K, pp, j, k, rp);
-                    okm = !probe_collides_c(R, K, pm, j, k, rp);
+                    bool cp, cm;
+                    probe_pair_collides_c(R, K, pp, pm, j, k, rp, cp, cm);
+                    okp = !cp;
+                    okm = !cm;
                 }
             }
         }
