@@ -703,7 +703,8 @@ def run_ours(args):
     sv, sms = ctx.surface_variants()
     for k, stage in enumerate(_lib.SURFACE_STAGES):
         names = _lib.SURFACE_VARIANT_NAMES[stage.split("_")[0]]
-        autotune[stage] = {"shape": names[sv[k]], "ms": {names[v]: round(float(sms[k, v]), 3) for v in range(2)}}
+        autotune[stage] = {"shape": names[sv[k]],
+                           "ms": {names[v]: round(float(sms[k, v]), 3) for v in range(_lib.SURFACE_VARIANTS)}}
     free_b, total_b = torch.cuda.mem_get_info(dev)
     device_gb = (total_b - free_b) / 1e9             # whole GPU in use while the context holds its workspace
 

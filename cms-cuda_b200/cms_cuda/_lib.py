@@ -37,8 +37,9 @@ EXPORTED = (
 
 NN_VARIANT_NAMES = ("q4 r1024", "q4 r512", "q2 r1024", "q2 r512")
 SURFACE_STAGES = ("toroidal_count", "toroidal_emit", "concave_count", "concave_emit")
-SURFACE_VARIANT_NAMES = {"toroidal": ("16 pairs x 4 warps", "32 pairs x 2 warps"),
-                         "concave": ("4 CTAs/SM", "5 CTAs/SM")}
+SURFACE_VARIANTS = 3
+SURFACE_VARIANT_NAMES = {"toroidal": ("16 pairs x 4 warps", "32 pairs x 2 warps", "16 pairs x 4 warps, 6 CTAs/SM"),
+                         "concave": ("4 CTAs/SM", "5 CTAs/SM", "6 CTAs/SM")}
 
 
 class Settings(ctypes.Structure):
@@ -241,9 +242,9 @@ class Context:
     def surface_variants(self):
         """(shape per tuned surface stage, measured ms per stage and shape) of the autotuner."""
         v = np.zeros(4, np.int32)
-        ms = np.zeros(4 * 2)
+        ms = np.zeros(4 * SURFACE_VARIANTS)
         self._check(self.lib.cms_get_surface_variants(self.h, _ptr(v), _ptr(ms)))
-        return v.tolist(), ms.reshape(4, 2)
+        return v.tolist(), ms.reshape(4, SURFACE_VARIANTS)
 
     def set_autotune(self, enable=True):
         self._check(self.lib.cms_set_autotune(self.h, 1 if enable else 0))

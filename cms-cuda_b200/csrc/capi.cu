@@ -1451,7 +1451,7 @@ void capture_graph(cms_ctx* x)
     }
     const long long key[4] = {x->B, x->N, x->cap_dot, x->refine ? 100 : (x->bwd_enabled ? 1 + x->bwd_side : 0)};
     const long long vk = (x->nn_var[0] << 8) | (x->nn_var[1] << 4) | x->nn_var[2] |
-                         ((long long)(x->sv[0] | (x->sv[1] << 1) | (x->sv[2] << 2) | (x->sv[3] << 3)) << 12);
+                         ((long long)(x->sv[0] | (x->sv[1] << 2) | (x->sv[2] << 4) | (x->sv[3] << 6)) << 12);
     if (x->gexec && std::memcmp(key, x->graph_key, sizeof(key)) == 0 && vk == x->graph_vk) return;
     if (x->gexec) { cudaGraphExecDestroy(x->gexec); x->gexec = nullptr; }
     if (x->graph) { cudaGraphDestroy(x->graph); x->graph = nullptr; }

@@ -20,9 +20,9 @@ void launch_low_probes(const Dev& d, long long probe_cap, long long* scan_tmp, c
 
 // dots (k_dots.cu)
 void launch_convex(const Dev& d, bool emit, cudaStream_t s);
-// variant: the autotuned shape (toroidal: 0 = 16 pairs x 4 warps, 1 = 32 pairs x 2 warps per batch / CTA;
-// concave: 0 = 4 CTAs per SM of registers, 1 = 5)
-static constexpr int SURF_VARIANTS = 2;
+// variant: the autotuned shape (toroidal: 0 = 16 pairs x 4 warps, 1 = 32 pairs x 2 warps per batch / CTA,
+// 2 = 16 x 4 with registers for 6 CTAs per SM; concave: registers for 4, 5 or 6 CTAs per SM)
+static constexpr int SURF_VARIANTS = 3;
 void launch_toroidal(const Dev& d, long long tor_grid, bool emit, int variant, cudaStream_t s);
 void launch_concave(const Dev& d, long long probe_grid, bool emit, int variant, cudaStream_t s);
 void launch_layout(const Dev& d, long long* cm_count_tmp, long long* scan_tmp, cudaStream_t s);

@@ -321,8 +321,9 @@ void launch_convex(const Dev& d, bool emit, cudaStream_t s)
 // emitting, the dots of the 32 points of a chunk are spread over the lanes
 // again, so consecutive lanes write consecutive dots.
 //
-// Two batch shapes, picked per batch shape by the autotuner: NPB pairs per
-// warp batch and NW warps per CTA -- (16, 4) or (32, 2).  Per batch up to
+// Three shapes, picked per batch shape by the autotuner: NPB pairs per warp
+// batch, NW warps per CTA and registers for MINB CTAs per SM -- (16, 4, 4),
+// (32, 2, any), (16, 4, 6).  Per batch up to
 // NPB * 32 pruned atom ids (past it: the full lists are scanned) and as many
 // kept torus points (past it: the batch is not kept).
 
@@ -572,8 +573,8 @@ __device__ __forceinline__ void tor_emit_spread(const Dev& d, TorArcS* S, int* X
     }
 }
 
-template <bool EMIT, int NPB, int NW>
-__global__ void __launch_bounds__(NW * 32) k_toroidal(Dev d)
+template <bool EMIT, int NPB, int NW, int MINB>
+__global__ void __launch_bounds__(NW * 32, MINB) k_toroidal(Dev d)
 {
     constexpr int TO_WARPS = NW, TO_PAIRS = NPB, TO_POOL = NPB * 32, TO_KEEP = NPB * 32;
     CMS_EXIT_ON_OVERFLOW(d);
@@ -760,14 +761,19 @@ __global__ void __launch_bounds__(NW * 32) k_toroidal(Dev d)
 
 void launch_toroidal(const Dev& d, long long tor_grid, bool emit, int variant, cudaStream_t s)
 {
-    if (variant == 0) {
-        const long long batches = (tor_grid + 15) / 16;
-        if (emit) k_toroidal<true, 16, 4><<<grid_for(batches, 4), 4 * 32, 0, s>>>(d);
-        else k_toroidal<false, 16, 4><<<grid_for(batches, 4), 4 * 32, 0, s>>>(d);
-    } else {
+    if (variant == 1) {
         const long long batches = (tor_grid + 31) / 32;
-        if (emit) k_toroidal<true, 32, 2><<<grid_for(batches, 2), 2 * 32, 0, s>>>(d);
-        else k_toroidal<false, 32, 2><<<grid_for(batches, 2), 2 * 32, 0, s>>>(d);
+        if (emit) k_toroidal<true, 32, 2, 1><<<grid_for(batches, 2), 2 * 32, 0, s>>>(d);
+        else k_toroidal<false, 32, 2, 1><<<grid_for(batches, 2), 2 * 32, 0, s>>>(d);
+        return;
+    }
+    const long long batches = (tor_grid + 15) / 16;
+    if (variant == 0) {
+        if (emit) k_toroidal<true, 16, 4, 4><<<grid_for(batches, 4), 4 * 32, 0, s>>>(d);
+        else k_toroidal<false, 16, 4, 4><<<grid_for(batches, 4), 4 * 32, 0, s>>>(d);
+    } else {      // registers capped for 6 CTAs per SM (24 warps)
+        if (emit) k_toroidal<true, 16, 4, 6><<<grid_for(batches, 4), 4 * 32, 0, s>>>(d);
+        else k_toroidal<false, 16, 4, 6><<<grid_for(batches, 4), 4 * 32, 0, s>>>(d);
     }
 }
 
@@ -776,9 +782,9 @@ void launch_toroidal(const Dev& d, long long tor_grid, bool emit, int variant, c
 // ---------------------------------------------------------------------------
 static constexpr int CC_WARPS = 4;
 
-// MINB: CTAs per SM the register allocation must allow -- 4 (128 registers)
-// or 5 (102 registers, more warps to hide the FP64 latency, some spills);
-// the autotuner picks per batch shape
+// MINB: CTAs per SM the register allocation must allow -- 4 (128 registers),
+// 5 (102) or 6 (85: more warps to hide the FP64 latency, more spills); the
+// autotuner picks per batch shape
 template <bool EMIT, int MINB>
 __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
 {
@@ -1011,9 +1017,12 @@ void launch_concave(const Dev& d, long long probe_grid, bool emit, int variant, 
     if (variant == 0) {
         if (emit) k_concave<true, 4><<<grid_for(probe_grid, CC_WARPS), CC_WARPS * 32, 0, s>>>(d);
         else k_concave<false, 4><<<grid_for(probe_grid, CC_WARPS), CC_WARPS * 32, 0, s>>>(d);
-    } else {
+    } else if (variant == 1) {
         if (emit) k_concave<true, 5><<<grid_for(probe_grid, CC_WARPS), CC_WARPS * 32, 0, s>>>(d);
         else k_concave<false, 5><<<grid_for(probe_grid, CC_WARPS), CC_WARPS * 32, 0, s>>>(d);
+    } else {
+        if (emit) k_concave<true, 6><<<grid_for(probe_grid, CC_WARPS), CC_WARPS * 32, 0, s>>>(d);
+        else k_concave<false, 6><<<grid_for(probe_grid, CC_WARPS), CC_WARPS * 32, 0, s>>>(d);
     }
 }
 
