@@ -32,7 +32,7 @@ EXPORTED = (
     "cms_set_grad_total", "cms_grad_xyz", "cms_recompute_dots", "cms_export_dot_units",
     "cms_set_nn_variants", "cms_get_nn_variants", "cms_set_autotune", "cms_refine_begin",
     "cms_refine_set_params", "cms_refine_run", "cms_refine_pose", "cms_refine_end", "cms_residue_sums",
-    "cms_nn_evaluated", "cms_set_surface_variants", "cms_get_surface_variants",
+    "cms_nn_evaluated", "cms_set_surface_variants", "cms_get_surface_variants", "cms_set_concurrency",
 )
 
 NN_VARIANT_NAMES = ("q4 r1024", "q4 r512", "q2 r1024", "q2 r512")
@@ -131,6 +131,7 @@ def load():
             "cms_nn_evaluated": [_VP, _PI64],
             "cms_set_surface_variants": [_VP, _VP],
             "cms_get_surface_variants": [_VP, _VP, _VP],
+            "cms_set_concurrency": [_VP, _I32],
         }
         for name, args in sig.items():
             f = getattr(lib, name)
@@ -245,6 +246,10 @@ class Context:
         ms = np.zeros(4 * SURFACE_VARIANTS)
         self._check(self.lib.cms_get_surface_variants(self.h, _ptr(v), _ptr(ms)))
         return v.tolist(), ms.reshape(4, SURFACE_VARIANTS)
+
+    def set_concurrency(self, enable=True):
+        """Run the convex, toroidal and concave passes concurrently (default) or one after the other."""
+        self._check(self.lib.cms_set_concurrency(self.h, 1 if enable else 0))
 
     def set_autotune(self, enable=True):
         self._check(self.lib.cms_set_autotune(self.h, 1 if enable else 0))

@@ -255,6 +255,10 @@ struct cms_ctx {
     std::string err;
     // stage timing: an event after each pipeline stage when profiling
     bool profiling = false;
+    // side streams of the concurrent surface passes (graph and eager runs with the current capacities)
+    bool concurrent = true;
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
     bool counting = false;   // readouts run with the nearest-dot work counters (cms_nn_evaluated)
     long long h2d_bytes = 0, d2h_bytes = 0;   // host<->device bytes moved by the hot path
     std::vector<cudaEvent_t> marks;
@@ -532,8 +536,42 @@ void grow(long long& cap, long long need)
     if (need > cap) cap = need + need / t_growth_div + 64;
 }
 
+// The convex, toroidal and concave passes are independent of each other (each
+// reads the neighbour lists, the toroid queue or the probes and writes its own
+// counts, stash entries and dot segments; the shared kept-candidate buffer is
+// handed out by an atomic cursor, and a unit that does not get room is
+// recomputed by its emit pass).  Outside the sizing run and stage profiling
+// they run concurrently on the context's stream and two side streams (a
+// fork / join by events, which a stream capture records as graph branches),
+// so the SMs hold the warps of two or three latency-bound kernels at once.
+void ensure_side_streams(cms_ctx* x)
+{
+    if (x->side[0]) return;
+    for (int k = 0; k < 2; ++k) {
+        ck(cudaStreamCreateWithFlags(&x->side[k], cudaStreamNonBlocking), "side stream");
+        ck(cudaEventCreateWithFlags(&x->ev_join[k], cudaEventDisableTiming), "event");
+    }
+    ck(cudaEventCreateWithFlags(&x->ev_fork, cudaEventDisableTiming), "event");
+}
+
+void fork_side(cms_ctx* x)
+{
+    ck(cudaEventRecord(x->ev_fork, x->stream), "fork");
+    for (int k = 0; k < 2; ++k) ck(cudaStreamWaitEvent(x->side[k], x->ev_fork, 0), "fork");
+}
+
+void join_side(cms_ctx* x)
+{
+    for (int k = 0; k < 2; ++k) {
+        ck(cudaEventRecord(x->ev_join[k], x->side[k]), "join");
+        ck(cudaStreamWaitEvent(x->stream, x->ev_join[k], 0), "join");
+    }
+}
+
 void enqueue_surface(cms_ctx* x, bool sized)
 {
+    const bool par = !sized && !x->profiling && x->concurrent;
+    if (par) ensure_side_streams(x);
     Dev& d = x->d;
     cudaStream_t s = x->stream;
     long long* tmp = scan_tmp(x);
@@ -606,12 +644,20 @@ void enqueue_surface(cms_ctx* x, bool sized)
     ck(cudaMemsetAsync(d.conc_cnt, 0, sizeof(int) * x->cap_probe, s), "memset");
     ck(cudaMemsetAsync(d.ks_top, 0, sizeof(unsigned long long), s), "memset");
     ck(cudaMemsetAsync(d.cs_top, 0, sizeof(unsigned long long), s), "memset");
-    launch_convex(d, false, s);
-    mark(x, P_CONVEX_COUNT);
-    launch_toroidal(d, x->cap_tor, false, x->sv[0], s);
-    mark(x, P_TOROIDAL_COUNT);
-    launch_concave(d, x->cap_probe, false, x->sv[2], s);
-    mark(x, P_CONCAVE_COUNT);
+    if (par) {
+        fork_side(x);
+        launch_convex(d, false, s);
+        launch_toroidal(d, x->cap_tor, false, x->sv[0], x->side[0]);
+        launch_concave(d, x->cap_probe, false, x->sv[2], x->side[1]);
+        join_side(x);
+    } else {
+        launch_convex(d, false, s);
+        mark(x, P_CONVEX_COUNT);
+        launch_toroidal(d, x->cap_tor, false, x->sv[0], s);
+        mark(x, P_TOROIDAL_COUNT);
+        launch_concave(d, x->cap_probe, false, x->sv[2], s);
+        mark(x, P_CONCAVE_COUNT);
+    }
     scan_counts(d.conv_cnt, d.conv_off, d.N, tmp, s);
     scan_counts(d.tor1_cnt, d.tor1_off, x->cap_tor, tmp, s);
     scan_counts(d.tor2_cnt, d.tor2_off, x->cap_tor, tmp, s);
@@ -632,13 +678,23 @@ void enqueue_surface(cms_ctx* x, bool sized)
         }
     }
     k_cap_check<<<1, 32, 0, s>>>(d.dot_off + 2LL * d.B, nullptr, x->cap_dot, d.ovf);
-    launch_convex(d, true, s);
-    mark(x, P_CONVEX_EMIT);
-    launch_tor_list(d, x->cap_tor, tmp, s);
-    launch_toroidal(d, x->cap_tor, true, x->sv[1], s);
-    mark(x, P_TOROIDAL_EMIT);
-    launch_concave(d, x->cap_probe, true, x->sv[3], s);
-    mark(x, P_CONCAVE_EMIT);
+    if (par) {
+        // the toroidal work list's scan is the only user of the scan scratch in this phase
+        fork_side(x);
+        launch_convex(d, true, s);
+        launch_tor_list(d, x->cap_tor, tmp, x->side[0]);
+        launch_toroidal(d, x->cap_tor, true, x->sv[1], x->side[0]);
+        launch_concave(d, x->cap_probe, true, x->sv[3], x->side[1]);
+        join_side(x);
+    } else {
+        launch_convex(d, true, s);
+        mark(x, P_CONVEX_EMIT);
+        launch_tor_list(d, x->cap_tor, tmp, s);
+        launch_toroidal(d, x->cap_tor, true, x->sv[1], s);
+        mark(x, P_TOROIDAL_EMIT);
+        launch_concave(d, x->cap_probe, true, x->sv[3], s);
+        mark(x, P_CONCAVE_EMIT);
+    }
     launch_tor_access(d, x->cap_tor, s);
 }
 
@@ -951,6 +1007,11 @@ cms_status cms_ctx_destroy(cms_ctx* x)
     for (auto& b : x->bufs) if (b.p) cudaFree(b.p);
     if (x->pinned) cudaFreeHost(x->pinned);
     if (x->own_stream && x->stream) cudaStreamDestroy(x->stream);
+    for (int k = 0; k < 2; ++k) {
+        if (x->side[k]) cudaStreamDestroy(x->side[k]);
+        if (x->ev_join[k]) cudaEventDestroy(x->ev_join[k]);
+    }
+    if (x->ev_fork) cudaEventDestroy(x->ev_fork);
     delete x;
     return CMS_OK;
 }
@@ -1925,6 +1986,14 @@ cms_status cms_get_surface_variants(cms_ctx* x, int32_t* variants, double* tune_
     if (tune_ms)
         for (int k = 0; k < 4; ++k)
             for (int v = 0; v < SURF_VARIANTS; ++v) tune_ms[k * SURF_VARIANTS + v] = x->sv_ms[k][v];
+    return CMS_OK;
+}
+
+cms_status cms_set_concurrency(cms_ctx* x, int32_t enable)
+{
+    if (!x) return CMS_ERR_ARG;
+    x->concurrent = enable != 0;
+    x->graph_key[0] = -1;            // recapture with the new stream layout
     return CMS_OK;
 }
 

@@ -145,3 +145,38 @@ def test_autotuner_picks_surface_shapes():
     assert np.isfinite(ms).all() and (ms >= 0).all()
     for k in range(4):
         assert ms[k, v[k]] == ms[k].min()
+
+
+def test_concurrent_dot_passes_give_identical_surfaces():
+    """
+    The convex / toroidal / concave passes on side streams (graph branches of
+    the captured pipeline) generate the same dots as one after the other.
+    """
+    from cms_cuda import _lib
+    from parity import inputs, load_case
+    names = ("golden_pkl", "synth_small_s7", "synth_zero_radii", "smallmol_7jkv_pdb", "sc_example_pdb")
+    xyz, rad, off, nb = [], [], [0], []
+    for n in names:
+        bx, br, tx, tr = inputs(load_case(n))
+        xyz += [bx, tx]; rad += [br, tr]; nb.append(len(br)); off.append(off[-1] + len(br) + len(tr))
+    X, R = np.concatenate(xyz), np.concatenate(rad)
+    out = []
+    for conc in (False, True):
+        ctx = _lib.Context(0)
+        ctx.set_concurrency(conc)
+        ctx.load_batch(np.array(off), np.array(nb), X, R)
+        ctx.run_graph()
+        ctx.graph_launch()                 # a replay: every pass keeps and reuses its stash
+        dots = []
+        for c in range(len(names)):
+            i = ctx.info(c)
+            dots += [ctx.export_dots(c, m, i) for m in (0, 1)]
+            dots.append(ctx.export_atoms(c, int(off[c + 1] - off[c])))
+        pa, tot = ctx.contact_ms(per_atom=True)
+        sc, _ = ctx.shape_complementarity()
+        out.append((dots, pa, tot, sc))
+    for a, b in zip(out[0][0], out[1][0]):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y, equal_nan=True)
+    for k in (1, 2, 3):
+        assert np.array_equal(out[0][k], out[1][k])
