@@ -287,7 +287,8 @@ struct cms_ctx {
         S_TOR_LFLAG, S_TOR_LOFF, S_TOR_LIST, S_PTOP, S_SP_A, S_SP_H, S_SP_XYZ, S_SP_ALT, S_SP_G, S_SP_ORD,
         S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1, S_KS_TOP, S_KS_BUF, S_CV_SOFF, S_CC_SOFF, S_TOR_SOFF, S_TOR_SN, S_NBS_TOP, S_NBS_BUF, S_NB_SOFF, S_ADJ_SKEY, S_ADJ_SLIST_CONV, S_ADJ_SLIST_TOR, S_ADJ_SLIST_CONC, S_CS_TOP, S_CS_XYZ, S_CS_AREA, S_CS_OWN,
         S_CS_SUB, S_CS_BUR, S_RES_OFF, S_RES_ATOMS, S_RES_SUM, S_RES_FLAG, S_NN_COUNT, S_PLC_CNT, S_PLC_FILL, S_PLC_START,
-        S_PLC_ITEM, S_PLC_CELL,
+        S_PLC_ITEM, S_PLC_CELL, S_TILE_CNT2, S_TILE_OFF2, S_ROUND_CNT2, S_ROUND_OFF2, S_BOX_ROUND2,
+        S_BOX_BLK2, S_SCAN_TMP2, S_R_SC_D2,
         S_COUNT
     };
 
@@ -393,6 +394,11 @@ void bind_batch(cms_ctx* x)
     x->ensure<long long>(cms_ctx::S_TILE_OFF, 2 * B + 1);
     x->ensure<int>(cms_ctx::S_ROUND_CNT, 2 * B);
     x->ensure<long long>(cms_ctx::S_ROUND_OFF, 2 * B + 1);
+    // the second set of search scratch, for the SC searches when they run beside the CMS search
+    x->ensure<int>(cms_ctx::S_TILE_CNT2, 2 * B);
+    x->ensure<long long>(cms_ctx::S_TILE_OFF2, 2 * B + 1);
+    x->ensure<int>(cms_ctx::S_ROUND_CNT2, 2 * B);
+    x->ensure<long long>(cms_ctx::S_ROUND_OFF2, 2 * B + 1);
     x->ensure<long long>(cms_ctx::S_SUMMARY, 8);
 }
 
@@ -495,6 +501,18 @@ void bind_caps(cms_ctx* x)
     x->ensure<float4>(cms_ctx::S_BOX_BLK, 2 * rounds * (NN_ROUND / 32));
     long long mx = std::max({x->N + 1, x->cap_cells + 1, x->cap_tor + 1, x->cap_probe + 1, D + 1, 2LL * x->B + 2});
     x->ensure<long long>(cms_ctx::S_SCAN_TMP, scan_tmp_elems(mx) + 8);
+}
+
+// Buffers of the SC searches when they run beside the CMS search (graph path):
+// their own tile / round / box scratch, scan scratch and neighbour distances.
+void bind_sc_side(cms_ctx* x)
+{
+    const long long D = x->cap_dot;
+    const long long rounds = nn_round_cap(D, 2LL * x->B);
+    x->ensure<float4>(cms_ctx::S_BOX_ROUND2, 2 * rounds);
+    x->ensure<float4>(cms_ctx::S_BOX_BLK2, 2 * rounds * (NN_ROUND / 32));
+    x->ensure<long long>(cms_ctx::S_SCAN_TMP2, scan_tmp_elems(D + 1) + 8);
+    x->ensure<double>(cms_ctx::S_R_SC_D2, D);
 }
 
 void set_settings_dev(cms_ctx* x)
@@ -705,17 +723,17 @@ void enqueue_split(cms_ctx* x)
     mark(x, P_SPLIT);
 }
 
-NNArgs nn_args(cms_ctx* x, int kind)
+NNArgs nn_args(cms_ctx* x, int kind, int set = 0)
 {
     NNArgs a{};
     a.task = x->get<NNTask>(cms_ctx::S_TASKS) + kind * 2 * x->B;
     a.ntask = 2 * x->B;
-    a.tile_cnt = x->get<int>(cms_ctx::S_TILE_CNT);
-    a.tile_off = x->get<long long>(cms_ctx::S_TILE_OFF);
-    a.round_cnt = x->get<int>(cms_ctx::S_ROUND_CNT);
-    a.round_off = x->get<long long>(cms_ctx::S_ROUND_OFF);
-    a.box_round = x->get<float4>(cms_ctx::S_BOX_ROUND);
-    a.box_blk = x->get<float4>(cms_ctx::S_BOX_BLK);
+    a.tile_cnt = x->get<int>(set ? cms_ctx::S_TILE_CNT2 : cms_ctx::S_TILE_CNT);
+    a.tile_off = x->get<long long>(set ? cms_ctx::S_TILE_OFF2 : cms_ctx::S_TILE_OFF);
+    a.round_cnt = x->get<int>(set ? cms_ctx::S_ROUND_CNT2 : cms_ctx::S_ROUND_CNT);
+    a.round_off = x->get<long long>(set ? cms_ctx::S_ROUND_OFF2 : cms_ctx::S_ROUND_OFF);
+    a.box_round = x->get<float4>(set ? cms_ctx::S_BOX_ROUND2 : cms_ctx::S_BOX_ROUND);
+    a.box_blk = x->get<float4>(set ? cms_ctx::S_BOX_BLK2 : cms_ctx::S_BOX_BLK);
     a.round_cap = nn_round_cap(x->cap_dot, 2LL * x->B);
     a.ovf = x->d.ovf;
     if (x->counting) {
@@ -751,16 +769,21 @@ void enqueue_cms(cms_ctx* x)
     mark(x, P_CMS_SUM);
 }
 
-void enqueue_sc(cms_ctx* x)
+// SC readout; side = true: on the first side stream with the second set of
+// search scratch and its own neighbour distances (beside the CMS search, which
+// writes r.nn_d2)
+void enqueue_sc(cms_ctx* x, bool side = false)
 {
     Dev& d = x->d;
-    Rd& r = x->r;
-    cudaStream_t s = x->stream;
-    long long* tmp = scan_tmp(x);
+    Rd r = x->r;
+    const cudaStream_t s = side ? x->side[0] : x->stream;
+    long long* tmp = side ? x->get<long long>(cms_ctx::S_SCAN_TMP2) : scan_tmp(x);
+    if (side) r.nn_d2 = x->get<double>(cms_ctx::S_R_SC_D2);
+    const int set = side ? 1 : 0;
     NNTask* task = x->get<NNTask>(cms_ctx::S_TASKS);
     launch_tasks(d, r, 1, task + 2 * x->B, s);
     launch_spatial_order(d, r, SO_ACC, 1, s);
-    NNArgs a = nn_args(x, 1);
+    NNArgs a = nn_args(x, 1, set);
     a.q_f4 = r.so_f4[0]; a.q_perm = r.so_perm[0]; a.q_idx = r.bur_idx;
     a.r_f4 = r.so_f4[1]; a.r_perm = r.so_perm[1]; a.r_idx = r.acc_idx;
     a.q_xyz = a.r_xyz = d.dxyz;
@@ -773,7 +796,7 @@ void enqueue_sc(cms_ctx* x)
     k_fill_d<<<grid1(x->cap_dot), 256, 0, s>>>(r.nn_d2, x->cap_dot, INFINITY);
     k_fill_i<<<grid1(x->cap_dot), 256, 0, s>>>(r.nn_idx, x->cap_dot, -1);
     launch_spatial_order(d, r, SO_TRIM, 1, s);        // the accessible list is no longer needed
-    NNArgs b = nn_args(x, 2);
+    NNArgs b = nn_args(x, 2, set);
     b.q_f4 = r.so_f4[1]; b.q_perm = r.so_perm[1]; b.q_idx = r.trim_idx;
     b.r_f4 = r.so_f4[1]; b.r_perm = r.so_perm[1]; b.r_idx = r.trim_idx;
     b.q_xyz = b.r_xyz = d.dxyz;
@@ -1520,6 +1543,10 @@ void capture_graph(cms_ctx* x)
     set_settings_dev(x);
     bind_caps(x);
     if (x->bwd_enabled) bind_adj(x);                    // allocate before capture
+    if (x->concurrent) {
+        ensure_side_streams(x);
+        bind_sc_side(x);
+    }
     ck(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     try {
         if (x->refine) {
@@ -1535,9 +1562,18 @@ void capture_graph(cms_ctx* x)
         } else {
             enqueue_surface(x, false);
             enqueue_split(x);
-            enqueue_cms(x);
-            enqueue_sc(x);
-            if (x->bwd_enabled) enqueue_backward(x);
+            if (x->concurrent) {
+                // the SC searches beside the CMS search and its adjoint
+                fork_side(x);
+                enqueue_sc(x, true);
+                enqueue_cms(x);
+                if (x->bwd_enabled) enqueue_backward(x);
+                join_side(x);
+            } else {
+                enqueue_cms(x);
+                enqueue_sc(x);
+                if (x->bwd_enabled) enqueue_backward(x);
+            }
             enqueue_summary(x);
         }
     } catch (...) {

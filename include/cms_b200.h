@@ -271,12 +271,13 @@ cms_status cms_get_surface_variants(cms_ctx* ctx, int32_t* variants, double* tun
  * neighbour search -- the algorithmic work behind the FP32 roofline. */
 cms_status cms_nn_work(cms_ctx* ctx, int64_t* pairs);
 
-/* Run the independent convex, toroidal and concave dot passes concurrently
- * on the context's stream and two side streams (enable = 1, the default; a
- * captured graph gets them as parallel branches) or one after the other
- * (0).  The surfaces are the same either way; the sizing run and
- * cms_profile_stages always run the passes in order.  No reference
- * counterpart. */
+/* Run independent stages of the captured pipeline concurrently (enable = 1,
+ * the default): the convex, toroidal and concave dot passes on the context's
+ * stream and two side streams, and the SC searches beside the CMS search and
+ * its adjoint -- parallel branches of the graph -- or one after the other
+ * (0).  The results are the same either way; the sizing run, the stage-
+ * synchronised path and cms_profile_stages always run the stages in order.
+ * No reference counterpart. */
 cms_status cms_set_concurrency(cms_ctx* ctx, int32_t enable);
 
 /* Nearest-dot search work the kernels actually did, counted by the kernels

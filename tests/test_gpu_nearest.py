@@ -149,8 +149,10 @@ def test_autotuner_picks_surface_shapes():
 
 def test_concurrent_dot_passes_give_identical_surfaces():
     """
-    The convex / toroidal / concave passes on side streams (graph branches of
-    the captured pipeline) generate the same dots as one after the other.
+    The convex / toroidal / concave passes on side streams, and the SC
+    searches beside the CMS search and its adjoint (graph branches of the
+    captured pipeline), give the same dots, CMS, SC and gradient as the
+    passes one after the other.
     """
     from cms_cuda import _lib
     from parity import inputs, load_case
@@ -164,19 +166,24 @@ def test_concurrent_dot_passes_give_identical_surfaces():
     for conc in (False, True):
         ctx = _lib.Context(0)
         ctx.set_concurrency(conc)
+        ctx.set_backward(True, target_side=True)
         ctx.load_batch(np.array(off), np.array(nb), X, R)
         ctx.run_graph()
         ctx.graph_launch()                 # a replay: every pass keeps and reuses its stash
+        grad = ctx.grad_xyz()
         dots = []
         for c in range(len(names)):
             i = ctx.info(c)
             dots += [ctx.export_dots(c, m, i) for m in (0, 1)]
             dots.append(ctx.export_atoms(c, int(off[c + 1] - off[c])))
         pa, tot = ctx.contact_ms(per_atom=True)
-        sc, _ = ctx.shape_complementarity()
-        out.append((dots, pa, tot, sc))
+        sc, sides = ctx.shape_complementarity()
+        trimmed = [ctx.export_trimmed(c, m, ctx.info(c)) for c in range(len(names)) for m in (0, 1)]
+        out.append((dots, pa, tot, sc, sides, grad, trimmed))
     for a, b in zip(out[0][0], out[1][0]):
         for x, y in zip(a, b):
             assert np.array_equal(x, y, equal_nan=True)
-    for k in (1, 2, 3):
+    for k in (1, 2, 3, 4, 5):
         assert np.array_equal(out[0][k], out[1][k])
+    for x, y in zip(out[0][6], out[1][6]):
+        assert np.array_equal(x, y)
