@@ -44,6 +44,8 @@ enum : int {
 };
 
 #define CMS_NEAR_CAP 512
+// complexes with more low probes than this find a probe's nearby low probes through cell lists (k_surface.cu)
+#define CMS_LOW_CELL_MIN 4096
 
 // Device pointers of one batch (workspace owned by the context).
 struct Dev {

@@ -392,21 +392,7 @@ __device__ __forceinline__ bool tor_collides(const Dev& d, const TorPair& T, V3 
 {
     const double rp = d.st.rp;
     if (nnear >= 0) {
-        // four independent loads at a time, then the tests
-        int k = 0;
-        for (; k + 4 <= nnear; k += 4) {
-            double4 b[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) b[u] = d.xyzr[near[k + u]];
-            bool hit = false;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const double t = b[u].w + rp;
-                hit |= sq_alt(pij - v3(b[u].x, b[u].y, b[u].z)) < t * t;
-            }
-            if (hit) return true;
-        }
-        for (; k < nnear; ++k) {
+        for (int k = 0; k < nnear; ++k) {
             const double4 b = d.xyzr[near[k]];
             const double t = b.w + rp;
             if (sq_alt(pij - v3(b.x, b.y, b.z)) < t * t) return true;
@@ -826,12 +812,34 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
         const V3 uijk = ld3(d.palt + 3 * p);
         const bool low = d.ph[p] < rp;
         const int c = d.cplx[ia[0]];
-        // nearby low probes of the same complex (d2 <= 4 rp^2), self excluded: the low probes of the cells
-        // (clamped to the complex's grid) that meet the box of the 2 rp ball, one (x, y) column per lane,
-        // each column's cells contiguous, then one probe per lane
+        // nearby low probes of the same complex (d2 <= 4 rp^2), self excluded.  A complex with few low
+        // probes has them scanned in list order; one with many (a whole molecule's surface) has them looked
+        // up through its cells (clamped to the complex's grid) that meet the box of the 2 rp ball, one
+        // (x, y) column per lane, each column's cells contiguous, then one probe per lane.
         int nnear = 0;
+        const Cplx C = d.cx[c];
+        long long ls = 0, le = 0;
         if (low) {
-            const Cplx C = d.cx[c];
+            const int s0 = C.a0, e1 = C.a0 + C.n;
+            const long long pb = min(d.plus_off[s0] + d.minus_off[s0], d.probe_cap);
+            const long long pe = min(d.plus_off[e1] + d.minus_off[e1], d.probe_cap);
+            ls = d.plow_off[pb]; le = d.plow_off[pe];
+        }
+        if (low && le - ls <= CMS_LOW_CELL_MIN) {
+            for (long long b = ls; b < le; b += 32) {
+                long long li = b + lane;
+                bool near = false;
+                int qi = -1;
+                if (li < le) {
+                    qi = d.plow_list[li];
+                    if (qi != p) near = sq_seq(pijk - ld3(d.pxyz + 3 * (long long)qi)) <= 4 * rp2;
+                }
+                unsigned m = __ballot_sync(0xffffffffu, near);
+                int pos = nnear + __popc(m & lt);
+                if (near && pos < CMS_NEAR_CAP) nears[w][pos] = qi;
+                nnear += __popc(m);
+            }
+        } else if (low) {
             const double re = (2.0 * rp) * (1.0 + 1e-9) + 1e-9;
             const int x0 = cell_coord(pijk.x - re, C.org[0], C.h, C.dims[0]);
             const int x1 = cell_coord(pijk.x + re, C.org[0], C.h, C.dims[0]);
@@ -880,6 +888,8 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
                 }
                 __syncwarp();
             }
+        }
+        if (low) {
             if (nnear > CMS_NEAR_CAP) {
                 if (lane == 0) atomicOr(&d.status[c], ST_NEAR_OVERFLOW);
                 nnear = CMS_NEAR_CAP;

@@ -1227,11 +1227,22 @@ __global__ void k_low_fill(Dev d, long long cap)
         if (d.plow_flag[p]) d.plow_list[d.plow_off[p]] = (int)p;
 }
 
-// Low probes sorted by cell of their complex's atom grid, coordinates clamped
-// to the grid (probes can lie just outside the atoms' box; clamping is
-// monotone, so a search over the clamped cell range of a ball still meets
-// every low probe inside the ball).  The concave kernels look up a probe's
-// nearby low probes there instead of scanning all of the complex's low probes.
+// Low probes of the complexes with more than CMS_LOW_CELL_MIN of them, sorted
+// by cell of the complex's atom grid, coordinates clamped to the grid (probes
+// can lie just outside the atoms' box; clamping is monotone, so a search over
+// the clamped cell range of a ball still meets every low probe inside the
+// ball).  The concave kernels look up such a complex's nearby low probes there
+// instead of scanning all of its low probes (a cost quadratic in their number:
+// whole-molecule surfaces); the others keep the plain scan.
+__device__ __forceinline__ long long complex_low_count(const Dev& d, int c)
+{
+    const Cplx& C = d.cx[c];
+    const int s0 = C.a0, e1 = C.a0 + C.n;
+    const long long pb = min(d.plus_off[s0] + d.minus_off[s0], d.probe_cap);
+    const long long pe = min(d.plus_off[e1] + d.minus_off[e1], d.probe_cap);
+    return d.plow_off[pe] - d.plow_off[pb];
+}
+
 __global__ void k_low_cell_count(Dev d, long long cap)
 {
     CMS_EXIT_ON_OVERFLOW(d);
@@ -1239,6 +1250,7 @@ __global__ void k_low_cell_count(Dev d, long long cap)
     for (long long li = blockIdx.x * (long long)blockDim.x + threadIdx.x; li < NL; li += (long long)gridDim.x * blockDim.x) {
         const int p = d.plow_list[li];
         const int c = d.cplx[d.pa0[p]];
+        if (complex_low_count(d, c) <= CMS_LOW_CELL_MIN) { d.plc_cell[li] = -1; continue; }
         const Cplx& C = d.cx[c];
         const double* x = d.pxyz + 3LL * p;
         const int cx = cell_coord(x[0], C.org[0], C.h, C.dims[0]);
