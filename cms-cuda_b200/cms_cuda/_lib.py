@@ -36,10 +36,12 @@ EXPORTED = (
 )
 
 NN_VARIANT_NAMES = ("q4 r1024", "q4 r512", "q2 r1024", "q2 r512")
-SURFACE_STAGES = ("toroidal_count", "toroidal_emit", "concave_count", "concave_emit")
+SURFACE_STAGES = ("toroidal_count", "toroidal_emit", "concave_count", "concave_emit", "triples_count")
 SURFACE_VARIANTS = 3
 SURFACE_VARIANT_NAMES = {"toroidal": ("16 pairs x 4 warps", "32 pairs x 2 warps", "16 pairs x 4 warps, 6 CTAs/SM"),
-                         "concave": ("4 CTAs/SM", "5 CTAs/SM", "6 CTAs/SM")}
+                         "concave": ("4 CTAs/SM", "5 CTAs/SM", "6 CTAs/SM"),
+                         "triples": ("rows <= 128 cached", "rows <= 64 cached, 10 CTAs/SM",
+                                     "rows <= 64 cached, 12 CTAs/SM")}
 
 
 class Settings(ctypes.Structure):
@@ -236,16 +238,17 @@ class Context:
         self._check(self.lib.cms_set_nn_variants(self.h, _ptr(v)))
 
     def set_surface_variants(self, variants):
-        """Force the surface kernels' shapes (toroidal count / emit, concave count / emit); turns the tuner off."""
+        """Force the surface kernels' shapes (toroidal count / emit, concave count / emit, triple count); turns
+        the tuner off."""
         v = np.ascontiguousarray(variants, dtype=np.int32)
         self._check(self.lib.cms_set_surface_variants(self.h, _ptr(v)))
 
     def surface_variants(self):
         """(shape per tuned surface stage, measured ms per stage and shape) of the autotuner."""
-        v = np.zeros(4, np.int32)
-        ms = np.zeros(4 * SURFACE_VARIANTS)
+        v = np.zeros(len(SURFACE_STAGES), np.int32)
+        ms = np.zeros(len(SURFACE_STAGES) * SURFACE_VARIANTS)
         self._check(self.lib.cms_get_surface_variants(self.h, _ptr(v), _ptr(ms)))
-        return v.tolist(), ms.reshape(4, SURFACE_VARIANTS)
+        return v.tolist(), ms.reshape(len(SURFACE_STAGES), SURFACE_VARIANTS)
 
     def set_concurrency(self, enable=True):
         """Run the convex, toroidal and concave passes concurrently (default) or one after the other."""

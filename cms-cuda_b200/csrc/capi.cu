@@ -249,8 +249,8 @@ struct cms_ctx {
     double tune_ms[3][NN_VARIANTS] = {};
     // surface kernel shapes (toroidal count, toroidal emit, concave count, concave emit), tuned with the
     // search shapes (or forced by cms_set_surface_variants)
-    int sv[4] = {0, 0, 0, 0};
-    double sv_ms[4][SURF_VARIANTS] = {};
+    int sv[SURF_TUNED] = {0, 0, 0, 0, 0};
+    double sv_ms[SURF_TUNED][SURF_VARIANTS] = {};
     long long launches = -1;
     std::string err;
     // stage timing: an event after each pipeline stage when profiling
@@ -639,7 +639,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
     launch_pairs(d, true, s);
     mark(x, P_PAIRS);
     ck(cudaMemsetAsync(d.ptop, 0, sizeof(unsigned long long), s), "memset");
-    launch_triples(d, false, s);
+    launch_triples(d, false, x->sv[4], s);
     scan_counts(d.nplus, d.plus_off, d.N, tmp, s);
     scan_counts(d.nminus, d.minus_off, d.N, tmp, s);
     mark(x, P_TRIPLES_COUNT);
@@ -654,7 +654,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
     }
     k_cap_check<<<1, 32, 0, s>>>(d.plus_off + d.N, d.minus_off + d.N, x->cap_probe, d.ovf);
     if (stashed) launch_probe_scatter(d, x->cap_probe, s);
-    else launch_triples(d, true, s);
+    else launch_triples(d, true, x->sv[4], s);
     launch_low_probes(d, x->cap_probe, tmp, s);
     mark(x, P_TRIPLES_EMIT);
     ck(cudaMemsetAsync(d.tor1_cnt, 0, sizeof(int) * x->cap_tor, s), "memset");
@@ -1494,13 +1494,14 @@ void autotune_surface(cms_ctx* x)
 {
     const long long key[3] = {x->B, x->N, x->cap_dot};
     if (!x->autotune || std::memcmp(key, x->tune_key, sizeof(key)) == 0) return;
-    static const int stage[4] = {P_TOROIDAL_COUNT, P_TOROIDAL_EMIT, P_CONCAVE_COUNT, P_CONCAVE_EMIT};
-    for (int k = 0; k < 4; ++k)
+    static const int stage[SURF_TUNED] = {P_TOROIDAL_COUNT, P_TOROIDAL_EMIT, P_CONCAVE_COUNT, P_CONCAVE_EMIT,
+                                          P_TRIPLES_COUNT};
+    for (int k = 0; k < SURF_TUNED; ++k)
         for (int v = 0; v < SURF_VARIANTS; ++v) x->sv_ms[k][v] = INFINITY;
     double ms[P_NSTAGES];
     for (int rep = 0; rep < 2; ++rep) {
         for (int v = 0; v < SURF_VARIANTS; ++v) {
-            for (int k = 0; k < 4; ++k) x->sv[k] = v;
+            for (int k = 0; k < SURF_TUNED; ++k) x->sv[k] = v;
             x->profiling = true;
             try {
                 mark(x, -1);
@@ -1511,10 +1512,10 @@ void autotune_surface(cms_ctx* x)
             }
             x->profiling = false;
             take_stage_times(x, ms, P_NSTAGES);
-            for (int k = 0; k < 4; ++k) x->sv_ms[k][v] = std::min(x->sv_ms[k][v], ms[stage[k]]);
+            for (int k = 0; k < SURF_TUNED; ++k) x->sv_ms[k][v] = std::min(x->sv_ms[k][v], ms[stage[k]]);
         }
     }
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < SURF_TUNED; ++k) {
         int best = 0;
         for (int v = 1; v < SURF_VARIANTS; ++v)
             if (x->sv_ms[k][v] < x->sv_ms[k][best]) best = v;
@@ -1535,7 +1536,7 @@ void capture_graph(cms_ctx* x)
     }
     const long long key[4] = {x->B, x->N, x->cap_dot, x->refine ? 100 : (x->bwd_enabled ? 1 + x->bwd_side : 0)};
     const long long vk = (x->nn_var[0] << 8) | (x->nn_var[1] << 4) | x->nn_var[2] |
-                         ((long long)(x->sv[0] | (x->sv[1] << 2) | (x->sv[2] << 4) | (x->sv[3] << 6)) << 12);
+                         ((long long)(x->sv[0] | (x->sv[1] << 2) | (x->sv[2] << 4) | (x->sv[3] << 6) | (x->sv[4] << 8)) << 12);
     if (x->gexec && std::memcmp(key, x->graph_key, sizeof(key)) == 0 && vk == x->graph_vk) return;
     if (x->gexec) { cudaGraphExecDestroy(x->gexec); x->gexec = nullptr; }
     if (x->graph) { cudaGraphDestroy(x->graph); x->graph = nullptr; }
@@ -2008,9 +2009,9 @@ cms_status cms_set_nn_variants(cms_ctx* x, const int32_t* variants)
 cms_status cms_set_surface_variants(cms_ctx* x, const int32_t* variants)
 {
     if (!x || !variants) return fail(x, CMS_ERR_ARG, "null argument");
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < SURF_TUNED; ++k)
         if (variants[k] < 0 || variants[k] >= SURF_VARIANTS) return fail(x, CMS_ERR_ARG, "surface shape out of range");
-    for (int k = 0; k < 4; ++k) x->sv[k] = variants[k];
+    for (int k = 0; k < SURF_TUNED; ++k) x->sv[k] = variants[k];
     x->autotune = false;
     return CMS_OK;
 }
@@ -2018,9 +2019,9 @@ cms_status cms_set_surface_variants(cms_ctx* x, const int32_t* variants)
 cms_status cms_get_surface_variants(cms_ctx* x, int32_t* variants, double* tune_ms)
 {
     if (!x || !variants) return fail(x, CMS_ERR_ARG, "null argument");
-    for (int k = 0; k < 4; ++k) variants[k] = x->sv[k];
+    for (int k = 0; k < SURF_TUNED; ++k) variants[k] = x->sv[k];
     if (tune_ms)
-        for (int k = 0; k < 4; ++k)
+        for (int k = 0; k < SURF_TUNED; ++k)
             for (int v = 0; v < SURF_VARIANTS; ++v) tune_ms[k * SURF_VARIANTS + v] = x->sv_ms[k][v];
     return CMS_OK;
 }

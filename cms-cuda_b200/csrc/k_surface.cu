@@ -790,28 +790,32 @@ __device__ __forceinline__ void triples_flush(const Dev& d, int g, V3 xi, double
     }
 }
 
-// Rows of up to TR_KC neighbours run from shared memory: the row's
+// Rows of up to KC neighbours run from shared memory: the row's
 // coordinates and radii, and per neighbour k the distance dik = |xk - xi| and
 // unit vector uik = (xk - xi) / dik, which every pair (i, j) of the row
 // reuses.  Queued pairs keep their geometry for the probe pass.
-static constexpr int TR_KC = 128;
+// The row cache holds KC = 128 or 64 neighbours: the smaller cache halves the
+// shared memory of a warp, so more warps fit an SM (registers capped to match;
+// longer rows take the LONG kernel), picked per batch shape by the autotuner.
 static constexpr int TR_PC = 32;      // neighbour slots (pairs) per chunk of the candidate matrix
 
+template <int KC>
 struct TrRow {
-    double x[TR_KC], y[TR_KC], z[TR_KC], r[TR_KC];
-    double ux[TR_KC], uy[TR_KC], uz[TR_KC], dk[TR_KC];
-    int id[TR_KC];
-    int8_t at[TR_KC];
-    unsigned char rk[TR_KC];    // rank of the slot's atom id in the row
-    unsigned char ord[TR_KC];   // slot of each id rank
+    double x[KC], y[KC], z[KC], r[KC];
+    double ux[KC], uy[KC], uz[KC], dk[KC];
+    int id[KC];
+    int8_t at[KC];
+    unsigned char rk[KC];    // rank of the slot's atom id in the row
+    unsigned char ord[KC];   // slot of each id rank
 };
 
 struct TrPairC { V3 uij, tij; double rij; int ps; };
 
 // one chunk's pairs (i, j) and their (pair, k) candidate matrix
+template <int KC>
 struct TrWork {
     TrPairC pr[TR_PC];
-    unsigned cb[TR_PC][TR_KC / 32];   // candidate k slots of each pair
+    unsigned cb[TR_PC][KC / 32];      // candidate k slots of each pair
     int cpos[TR_PC];                  // first (pair, k) combination of each pair
     unsigned kill;                    // pairs killed by a degenerate triple
 };
@@ -828,7 +832,8 @@ __device__ __forceinline__ bool norm_lt(V3 v, double T)
 }
 
 // triple_base on the cached row: k after j, not all three blockers, the two distance tests
-__device__ __forceinline__ bool triple_ok_c(const TrRow& R, int ks, int j, V3 xj, double erj, double eri,
+template <int KC>
+__device__ __forceinline__ bool triple_ok_c(const TrRow<KC>& R, int ks, int j, V3 xj, double erj, double eri,
                                             int8_t ati, int8_t atj, double rp)
 {
     if (R.id[ks] <= j) return false;
@@ -838,7 +843,8 @@ __device__ __forceinline__ bool triple_ok_c(const TrRow& R, int ks, int j, V3 xj
     return R.dk[ks] < eri + erk;
 }
 
-__device__ __forceinline__ bool probe_collides_c(const TrRow& R, int K, V3 pt, int j, int k, double rp)
+template <int KC>
+__device__ __forceinline__ bool probe_collides_c(const TrRow<KC>& R, int K, V3 pt, int j, int k, double rp)
 {
     for (int s = 0; s < K; ++s) {
         const int n = R.id[s];
@@ -851,7 +857,8 @@ __device__ __forceinline__ bool probe_collides_c(const TrRow& R, int K, V3 pt, i
 
 // probe_collides_c for the triple's two probes in one pass over the row (each neighbour read once); the
 // loop ends when both have collided
-__device__ __forceinline__ void probe_pair_collides_c(const TrRow& R, int K, V3 pp, V3 pm, int j, int k, double rp,
+template <int KC>
+__device__ __forceinline__ void probe_pair_collides_c(const TrRow<KC>& R, int K, V3 pp, V3 pm, int j, int k, double rp,
                                                       bool& cp, bool& cm)
 {
     cp = cm = false;
@@ -867,8 +874,8 @@ __device__ __forceinline__ void probe_pair_collides_c(const TrRow& R, int K, V3 
     }
 }
 
-template <bool EMIT>
-__device__ __forceinline__ void triples_flush_c(const Dev& d, int g, V3 xi, double eri, const TrRow& R, int K,
+template <bool EMIT, int KC>
+__device__ __forceinline__ void triples_flush_c(const Dev& d, int g, V3 xi, double eri, const TrRow<KC>& R, int K,
                                                 const unsigned* queue, const TrPairC* pq, int qn, int& nplus,
                                                 int& nminus, long long pbase, long long mbase)
 {
@@ -940,14 +947,14 @@ __device__ __forceinline__ void triples_flush_c(const Dev& d, int g, V3 xi, doub
     }
 }
 
-// The triple loop of one atom whose row fits the cache (K <= TR_KC).  The
+// The triple loop of one atom whose row fits the cache (K <= KC).  The
 // row's pairs (i, j) are taken 32 neighbour slots at a time: their geometry
 // one pair per lane, then the (pair, k) combinations with k after j (by atom
 // id) spread over the lanes, then the queue in (pair, k slot) order -- the
 // order of the reference's loops -- one pair per lane, for the probe pass.
-template <bool EMIT>
+template <bool EMIT, int KC>
 __device__ __forceinline__ void triples_row_c(const Dev& d, int g, int K, long long off, V3 xi, double ri, double eri,
-                                              int8_t ati, TrRow& R, unsigned* queue, TrWork& W, int& nplus,
+                                              int8_t ati, TrRow<KC>& R, unsigned* queue, TrWork<KC>& W, int& nplus,
                                               int& nminus, long long pbase, long long mbase)
 {
     const int lane = threadIdx.x & 31;
@@ -999,7 +1006,7 @@ __device__ __forceinline__ void triples_row_c(const Dev& d, int g, int K, long l
         }
         const int NC = __shfl_sync(0xffffffffu, x, 31);
         if (v) W.cpos[__popc(vm & lt)] = x - nk;
-        for (int t = lane; t < np * (TR_KC / 32); t += 32) W.cb[t / (TR_KC / 32)][t % (TR_KC / 32)] = 0u;
+        for (int t = lane; t < np * (KC / 32); t += 32) W.cb[t / (KC / 32)][t % (KC / 32)] = 0u;
         if (lane == 0) W.kill = 0u;
         __syncwarp();
         // candidate matrix: a degenerate triple (|uij.uik| >= 1) inside the
@@ -1059,21 +1066,21 @@ __device__ __forceinline__ void triples_row_c(const Dev& d, int g, int K, long l
                 }
             }
             __syncwarp();
-            triples_flush_c<EMIT>(d, g, xi, eri, R, K, queue, W.pr, end - base, nplus, nminus, pbase, mbase);
+            triples_flush_c<EMIT, KC>(d, g, xi, eri, R, K, queue, W.pr, end - base, nplus, nminus, pbase, mbase);
             __syncwarp();
             base = end;
         }
     }
 }
 
-// LONG = false: atoms whose neighbour row fits the cache; true: the others
-template <bool EMIT, bool LONG>
-__global__ void __launch_bounds__(TR_WARPS * 32, EMIT ? 8 : 7) k_triples(Dev d)
+// LONG = false: atoms whose neighbour row fits the cache (KC); true: the others
+template <bool EMIT, bool LONG, int KC, int MINB>
+__global__ void __launch_bounds__(TR_WARPS * 32, MINB) k_triples(Dev d)
 {
     CMS_EXIT_ON_OVERFLOW(d);
     __shared__ unsigned queue_s[TR_WARPS][TR_QCAP];
-    __shared__ TrRow rows_s[LONG ? 1 : TR_WARPS];
-    __shared__ TrWork work_s[LONG ? 1 : TR_WARPS];
+    __shared__ TrRow<KC> rows_s[LONG ? 1 : TR_WARPS];
+    __shared__ TrWork<KC> work_s[LONG ? 1 : TR_WARPS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     unsigned* queue = queue_s[w];
@@ -1083,7 +1090,7 @@ __global__ void __launch_bounds__(TR_WARPS * 32, EMIT ? 8 : 7) k_triples(Dev d)
     for (long long gg = wid; gg < d.N; gg += nw) {
         const int g = (int)gg;
         const int K = d.nnb[g];
-        if (LONG != (K > TR_KC)) continue;
+        if (LONG != (K > KC)) continue;
         if (EMIT && d.nplus[g] == 0 && d.nminus[g] == 0) continue;    // no probes: nothing to write
         int nplus = 0, nminus = 0;
         const int8_t ati = d.atten[g];
@@ -1106,8 +1113,8 @@ __global__ void __launch_bounds__(TR_WARPS * 32, EMIT ? 8 : 7) k_triples(Dev d)
                 probe_bases(d, g, pbase, mbase);
             }
             if (!LONG) {
-                triples_row_c<EMIT>(d, g, K, off, xi, ai.w, eri, ati, rows_s[w], queue, work_s[w], nplus, nminus,
-                                    pbase, mbase);
+                triples_row_c<EMIT, KC>(d, g, K, off, xi, ai.w, eri, ati, rows_s[w], queue, work_s[w], nplus, nminus,
+                                        pbase, mbase);
                 if (!EMIT && lane == 0) { d.nplus[g] = nplus; d.nminus[g] = nminus; }
                 continue;
             }
@@ -1196,15 +1203,33 @@ __global__ void __launch_bounds__(TR_WARPS * 32, EMIT ? 8 : 7) k_triples(Dev d)
     }
 }
 
-void launch_triples(const Dev& d, bool emit, cudaStream_t s)
+void launch_triples(const Dev& d, bool emit, int variant, cudaStream_t s)
 {
     const unsigned g = grid_for(d.N, TR_WARPS, 32);
-    if (emit) {
-        k_triples<true, false><<<g, TR_WARPS * 32, 0, s>>>(d);
-        k_triples<true, true><<<g, TR_WARPS * 32, 0, s>>>(d);
+    if (variant == 0) {
+        if (emit) {
+            k_triples<true, false, 128, 8><<<g, TR_WARPS * 32, 0, s>>>(d);
+            k_triples<true, true, 128, 8><<<g, TR_WARPS * 32, 0, s>>>(d);
+        } else {
+            k_triples<false, false, 128, 7><<<g, TR_WARPS * 32, 0, s>>>(d);
+            k_triples<false, true, 128, 7><<<g, TR_WARPS * 32, 0, s>>>(d);
+        }
+    } else if (variant == 1) {
+        if (emit) {
+            k_triples<true, false, 64, 10><<<g, TR_WARPS * 32, 0, s>>>(d);
+            k_triples<true, true, 64, 10><<<g, TR_WARPS * 32, 0, s>>>(d);
+        } else {
+            k_triples<false, false, 64, 10><<<g, TR_WARPS * 32, 0, s>>>(d);
+            k_triples<false, true, 64, 10><<<g, TR_WARPS * 32, 0, s>>>(d);
+        }
     } else {
-        k_triples<false, false><<<g, TR_WARPS * 32, 0, s>>>(d);
-        k_triples<false, true><<<g, TR_WARPS * 32, 0, s>>>(d);
+        if (emit) {
+            k_triples<true, false, 64, 12><<<g, TR_WARPS * 32, 0, s>>>(d);
+            k_triples<true, true, 64, 12><<<g, TR_WARPS * 32, 0, s>>>(d);
+        } else {
+            k_triples<false, false, 64, 12><<<g, TR_WARPS * 32, 0, s>>>(d);
+            k_triples<false, true, 64, 12><<<g, TR_WARPS * 32, 0, s>>>(d);
+        }
     }
 }
 

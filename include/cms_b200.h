@@ -254,13 +254,15 @@ cms_status cms_get_nn_variants(cms_ctx* ctx, int32_t* variants, double* tune_ms)
 cms_status cms_set_autotune(cms_ctx* ctx, int32_t enable);
 
 /* Shapes of the surface kernels that the autotuner also picks per batch
- * shape, variants[4] for the toroidal count, toroidal emit, concave count and
- * concave emit passes: toroidal 0 = 16 toroid pairs per warp batch, 4 warps
- * per CTA, 1 = 32 pairs, 2 warps, 2 = 16 pairs, 4 warps, registers for 6
- * CTAs per SM; concave 0, 1, 2 = registers for 4, 5, 6 CTAs per SM.  Every
- * shape generates the same surfaces.  cms_get_surface_variants returns the
- * shapes in use and the tuner's measured stage times (tune_ms[4 x 3], NULL
- * to skip); cms_set_surface_variants
+ * shape, variants[5] for the toroidal count, toroidal emit, concave count,
+ * concave emit and triple count passes: toroidal 0 = 16 toroid pairs per warp
+ * batch, 4 warps per CTA, 1 = 32 pairs, 2 warps, 2 = 16 pairs, 4 warps,
+ * registers for 6 CTAs per SM; concave 0, 1, 2 = registers for 4, 5, 6 CTAs
+ * per SM; triples 0 = neighbour rows of up to 128 cached per warp, 1 / 2 =
+ * up to 64, registers for 10 / 12 CTAs of 2 warps.  Every shape generates the
+ * same surfaces.  cms_get_surface_variants returns the shapes in use and the
+ * tuner's measured stage times (tune_ms[5 x 3], NULL to skip);
+ * cms_set_surface_variants
  * forces shapes and turns the tuner off (cms_set_autotune(1) turns it back
  * on).  The reference's kernels have fixed launch shapes. */
 cms_status cms_set_surface_variants(cms_ctx* ctx, const int32_t* variants);

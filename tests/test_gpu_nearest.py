@@ -109,7 +109,7 @@ def test_surface_shapes_give_identical_surfaces(graph):
         xyz += [bx, tx]; rad += [br, tr]; nb.append(len(br)); off.append(off[-1] + len(br) + len(tr))
     X, R = np.concatenate(xyz), np.concatenate(rad)
     out = []
-    for v in ([0, 0, 0, 0], [1, 1, 1, 1], [2, 2, 2, 2], [1, 0, 2, 1]):
+    for v in ([0, 0, 0, 0, 0], [1, 1, 1, 1, 1], [2, 2, 2, 2, 2], [1, 0, 2, 1, 1]):
         ctx = _lib.Context(0)
         ctx.set_surface_variants(v)
         ctx.load_batch(np.array(off), np.array(nb), X, R)
@@ -143,7 +143,7 @@ def test_autotuner_picks_surface_shapes():
     v, ms = ctx.surface_variants()
     assert all(x in (0, 1, 2) for x in v)
     assert np.isfinite(ms).all() and (ms >= 0).all()
-    for k in range(4):
+    for k in range(5):
         assert ms[k, v[k]] == ms[k].min()
 
 
