@@ -38,6 +38,8 @@ EXPORTED = (
 NN_VARIANT_NAMES = ("q4 r1024", "q4 r512", "q2 r1024", "q2 r512")
 SURFACE_STAGES = ("toroidal_count", "toroidal_emit", "concave_count", "concave_emit", "triples_count")
 SURFACE_VARIANTS = 3
+# cms_set_concurrency bits (CMS_CONC_* of the C header)
+CONC_COUNT, CONC_EMIT, CONC_READOUT = 1, 2, 4
 SURFACE_VARIANT_NAMES = {"toroidal": ("16 pairs x 4 warps", "32 pairs x 2 warps", "16 pairs x 4 warps, 6 CTAs/SM"),
                          "concave": ("4 CTAs/SM", "5 CTAs/SM", "6 CTAs/SM"),
                          "triples": ("rows <= 128 cached", "rows <= 64 cached, 10 CTAs/SM",
@@ -250,9 +252,12 @@ class Context:
         self._check(self.lib.cms_get_surface_variants(self.h, _ptr(v), _ptr(ms)))
         return v.tolist(), ms.reshape(len(SURFACE_STAGES), SURFACE_VARIANTS)
 
-    def set_concurrency(self, enable=True):
-        """Run the convex, toroidal and concave passes concurrently (default) or one after the other."""
-        self._check(self.lib.cms_set_concurrency(self.h, 1 if enable else 0))
+    def set_concurrency(self, mode=True):
+        """Stages run as parallel graph branches: an OR of CONC_COUNT, CONC_EMIT and CONC_READOUT
+        (True: all three, False: every stage in order)."""
+        if isinstance(mode, bool):
+            mode = CONC_COUNT | CONC_EMIT | CONC_READOUT if mode else 0
+        self._check(self.lib.cms_set_concurrency(self.h, int(mode)))
 
     def set_autotune(self, enable=True):
         self._check(self.lib.cms_set_autotune(self.h, 1 if enable else 0))

@@ -13,6 +13,9 @@
 
 using namespace cms;
 
+// stage groups run as parallel graph branches unless cms_set_concurrency says otherwise
+#define CMS_CONC_DEFAULT (CMS_CONC_COUNT | CMS_CONC_EMIT | CMS_CONC_READOUT)
+
 namespace {
 
 struct DBuf {
@@ -255,8 +258,8 @@ struct cms_ctx {
     std::string err;
     // stage timing: an event after each pipeline stage when profiling
     bool profiling = false;
-    // side streams of the concurrent surface passes (graph and eager runs with the current capacities)
-    bool concurrent = true;
+    // stages run concurrently (CMS_CONC_* bits; graph and eager runs with the current capacities)
+    int conc = CMS_CONC_DEFAULT;
     cudaStream_t side[2] = {nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
     bool counting = false;   // readouts run with the nearest-dot work counters (cms_nn_evaluated)
@@ -588,8 +591,9 @@ void join_side(cms_ctx* x)
 
 void enqueue_surface(cms_ctx* x, bool sized)
 {
-    const bool par = !sized && !x->profiling && x->concurrent;
-    if (par) ensure_side_streams(x);
+    const bool par_count = !sized && !x->profiling && (x->conc & CMS_CONC_COUNT);
+    const bool par_emit = !sized && !x->profiling && (x->conc & CMS_CONC_EMIT);
+    if (par_count || par_emit) ensure_side_streams(x);
     Dev& d = x->d;
     cudaStream_t s = x->stream;
     long long* tmp = scan_tmp(x);
@@ -662,7 +666,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
     ck(cudaMemsetAsync(d.conc_cnt, 0, sizeof(int) * x->cap_probe, s), "memset");
     ck(cudaMemsetAsync(d.ks_top, 0, sizeof(unsigned long long), s), "memset");
     ck(cudaMemsetAsync(d.cs_top, 0, sizeof(unsigned long long), s), "memset");
-    if (par) {
+    if (par_count) {
         fork_side(x);
         launch_convex(d, false, s);
         launch_toroidal(d, x->cap_tor, false, x->sv[0], x->side[0]);
@@ -696,7 +700,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
         }
     }
     k_cap_check<<<1, 32, 0, s>>>(d.dot_off + 2LL * d.B, nullptr, x->cap_dot, d.ovf);
-    if (par) {
+    if (par_emit) {
         // the toroidal work list's scan is the only user of the scan scratch in this phase
         fork_side(x);
         launch_convex(d, true, s);
@@ -1544,10 +1548,8 @@ void capture_graph(cms_ctx* x)
     set_settings_dev(x);
     bind_caps(x);
     if (x->bwd_enabled) bind_adj(x);                    // allocate before capture
-    if (x->concurrent) {
-        ensure_side_streams(x);
-        bind_sc_side(x);
-    }
+    if (x->conc) ensure_side_streams(x);
+    if (x->conc & CMS_CONC_READOUT) bind_sc_side(x);
     ck(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     try {
         if (x->refine) {
@@ -1563,7 +1565,7 @@ void capture_graph(cms_ctx* x)
         } else {
             enqueue_surface(x, false);
             enqueue_split(x);
-            if (x->concurrent) {
+            if (x->conc & CMS_CONC_READOUT) {
                 // the SC searches beside the CMS search and its adjoint
                 fork_side(x);
                 enqueue_sc(x, true);
@@ -2026,10 +2028,12 @@ cms_status cms_get_surface_variants(cms_ctx* x, int32_t* variants, double* tune_
     return CMS_OK;
 }
 
-cms_status cms_set_concurrency(cms_ctx* x, int32_t enable)
+cms_status cms_set_concurrency(cms_ctx* x, int32_t mode)
 {
     if (!x) return CMS_ERR_ARG;
-    x->concurrent = enable != 0;
+    if (mode < 0 || mode > (CMS_CONC_COUNT | CMS_CONC_EMIT | CMS_CONC_READOUT))
+        return fail(x, CMS_ERR_ARG, "concurrency mode outside 0..7");
+    x->conc = mode;
     x->graph_key[0] = -1;            // recapture with the new stream layout
     return CMS_OK;
 }

@@ -46,6 +46,13 @@ enum {
 
 enum { CMS_HOST = 0, CMS_DEVICE = 1 };
 
+/* Stages that cms_set_concurrency may run as parallel branches. */
+enum {
+    CMS_CONC_COUNT = 1,        /* the convex, toroidal and concave count passes */
+    CMS_CONC_EMIT = 2,         /* the convex, toroidal and concave emit passes */
+    CMS_CONC_READOUT = 4       /* the SC searches beside the CMS search and its adjoint */
+};
+
 /* Settings of the calculator; defaults of _core.py:766-773. */
 typedef struct {
     double rp;             /* probe radius, 1.7 */
@@ -273,14 +280,13 @@ cms_status cms_get_surface_variants(cms_ctx* ctx, int32_t* variants, double* tun
  * neighbour search -- the algorithmic work behind the FP32 roofline. */
 cms_status cms_nn_work(cms_ctx* ctx, int64_t* pairs);
 
-/* Run independent stages of the captured pipeline concurrently (enable = 1,
- * the default): the convex, toroidal and concave dot passes on the context's
- * stream and two side streams, and the SC searches beside the CMS search and
- * its adjoint -- parallel branches of the graph -- or one after the other
- * (0).  The results are the same either way; the sizing run, the stage-
- * synchronised path and cms_profile_stages always run the stages in order.
- * No reference counterpart. */
-cms_status cms_set_concurrency(cms_ctx* ctx, int32_t enable);
+/* Run independent stages of the captured pipeline concurrently: mode is an
+ * OR of CMS_CONC_* bits (0 = every stage in order).  A set bit runs that
+ * group on the context's stream and two side streams -- parallel branches of
+ * the graph.  The results are the same for every mode; the sizing run, the
+ * stage-synchronised path and cms_profile_stages always run the stages in
+ * order.  Modes outside 0..7 give CMS_ERR_ARG.  No reference counterpart. */
+cms_status cms_set_concurrency(cms_ctx* ctx, int32_t mode);
 
 /* Nearest-dot search work the kernels actually did, counted by the kernels
  * themselves in one extra (eager) run of the CMS and SC readouts on the

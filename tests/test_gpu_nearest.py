@@ -163,8 +163,12 @@ def test_concurrent_dot_passes_give_identical_surfaces():
         xyz += [bx, tx]; rad += [br, tr]; nb.append(len(br)); off.append(off[-1] + len(br) + len(tr))
     X, R = np.concatenate(xyz), np.concatenate(rad)
     out = []
-    for conc in (False, True):
+    modes = (0, _lib.CONC_COUNT, _lib.CONC_EMIT, _lib.CONC_READOUT, True)
+    for conc in modes:
         ctx = _lib.Context(0)
+        if conc is True:
+            with pytest.raises(_lib.CmsError):
+                ctx.set_concurrency(8)
         ctx.set_concurrency(conc)
         ctx.set_backward(True, target_side=True)
         ctx.load_batch(np.array(off), np.array(nb), X, R)
@@ -180,10 +184,11 @@ def test_concurrent_dot_passes_give_identical_surfaces():
         sc, sides = ctx.shape_complementarity()
         trimmed = [ctx.export_trimmed(c, m, ctx.info(c)) for c in range(len(names)) for m in (0, 1)]
         out.append((dots, pa, tot, sc, sides, grad, trimmed))
-    for a, b in zip(out[0][0], out[1][0]):
-        for x, y in zip(a, b):
-            assert np.array_equal(x, y, equal_nan=True)
-    for k in (1, 2, 3, 4, 5):
-        assert np.array_equal(out[0][k], out[1][k])
-    for x, y in zip(out[0][6], out[1][6]):
-        assert np.array_equal(x, y)
+    for other in out[1:]:
+        for a, b in zip(out[0][0], other[0]):
+            for x, y in zip(a, b):
+                assert np.array_equal(x, y, equal_nan=True)
+        for k in (1, 2, 3, 4, 5):
+            assert np.array_equal(out[0][k], other[k])
+        for x, y in zip(out[0][6], other[6]):
+            assert np.array_equal(x, y)
