@@ -13,8 +13,10 @@
 
 using namespace cms;
 
-// stage groups run as parallel graph branches unless cms_set_concurrency says otherwise
-#define CMS_CONC_DEFAULT (CMS_CONC_COUNT | CMS_CONC_EMIT | CMS_CONC_READOUT)
+// stage groups run as parallel graph branches unless cms_set_concurrency says otherwise: the emit passes
+// and the readouts (on the 4096-complex batch 231.4 ms a step against 235.5 with every stage in order);
+// the count passes are not (245.4 ms with them alone as branches)
+#define CMS_CONC_DEFAULT (CMS_CONC_EMIT | CMS_CONC_READOUT)
 
 namespace {
 

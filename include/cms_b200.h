@@ -283,9 +283,10 @@ cms_status cms_nn_work(cms_ctx* ctx, int64_t* pairs);
 /* Run independent stages of the captured pipeline concurrently: mode is an
  * OR of CMS_CONC_* bits (0 = every stage in order).  A set bit runs that
  * group on the context's stream and two side streams -- parallel branches of
- * the graph.  The results are the same for every mode; the sizing run, the
- * stage-synchronised path and cms_profile_stages always run the stages in
- * order.  Modes outside 0..7 give CMS_ERR_ARG.  No reference counterpart. */
+ * the graph.  Default: CMS_CONC_EMIT | CMS_CONC_READOUT.  The results are
+ * the same for every mode; the sizing run, the stage-synchronised path and
+ * cms_profile_stages always run the stages in order.  Modes outside 0..7
+ * give CMS_ERR_ARG.  No reference counterpart. */
 cms_status cms_set_concurrency(cms_ctx* ctx, int32_t mode);
 
 /* Nearest-dot search work the kernels actually did, counted by the kernels
