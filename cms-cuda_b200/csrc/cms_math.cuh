@@ -44,12 +44,20 @@ __device__ __forceinline__ V3 xyz_of(double4 a) { return v3(a.x, a.y, a.z); }
 // radius `rad` at `density` points per unit area (the reference's vec_sub_div,
 // _core.py:2429-2486): point i exists iff delta*(i+0.5) <= angle, i < 100,
 // with delta = 1/(sqrt(density)*rad).  NaN angle or infinite delta give 0.
-// For delta > 0 the rounded products delta*(n + 0.5) do not decrease with n
+__device__ __forceinline__ int subdiv_count(double delta, double angle)
+{
+    int n = 0;
+    while (n < CMS_MAX_SUBDIV && delta * ((double)n + 0.5) <= angle) ++n;
+    return n;
+}
+
+// subdiv_count for long circles (latitudes of a sphere: tens of points).  For
+// delta > 0 the rounded products delta*(n + 0.5) do not decrease with n
 // (n + 0.5 is exact and rounding is monotone), so the points that exist are a
 // prefix: start from an FP32 estimate of the quotient and settle the exact
-// boundary with the same FP64 comparisons a point-by-point loop makes.
-// Inputs outside the FP32 range take that loop.
-__device__ __forceinline__ int subdiv_count(double delta, double angle)
+// boundary with the same FP64 comparisons the loop makes.  Inputs outside the
+// FP32 range take the loop.
+__device__ __forceinline__ int subdiv_count_long(double delta, double angle)
 {
     int n = 0;
     if (delta > 1e-30 && delta < 1e30 && fabs(angle) < 1e30) {

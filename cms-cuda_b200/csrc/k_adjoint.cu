@@ -102,7 +102,7 @@ __device__ __forceinline__ ConvexU<T> convex_unit(const Dev& d, int g, const TV3
     }
     const T ang = tarc_angle(eq, n, south, U.ylat);
     U.dl = subdiv_delta(U.dens, ri);
-    U.nl = subdiv_count(U.dl, val(ang));
+    U.nl = subdiv_count_long(U.dl, val(ang));
     U.cs = tsubdiv_ps(ri, ang, U.nl);
     tcircle_frame(n, U.fx, U.fy);
     return U;
@@ -123,7 +123,7 @@ __device__ __forceinline__ LatU<T> convex_lat(const ConvexU<T>& U, int l)
     L.area = lift<T>(0.0);
     if (val(L.rad) > 0.0) {
         L.delta = tsubdiv_delta(U.dens, L.rad);
-        const int nc = subdiv_count(val(L.delta), CMS_TWO_PI);
+        const int nc = subdiv_count_long(val(L.delta), CMS_TWO_PI);
         const T ps = nc > 0 ? (L.rad * CMS_TWO_PI) / (double)nc : lift<T>(0.0);
         L.area = ps * U.cs;
     }
@@ -285,7 +285,7 @@ __device__ __forceinline__ ConcU<T> conc_unit(const Dev& d, const TV3<T>* xa, co
     const TV3<T> axis = tnormalize(tcross(U.vtop, U.south));
     const T ang = tarc_angle(axis, U.vtop, U.south, U.ylat);
     U.dl = subdiv_delta(U.density, rp);
-    U.nl = subdiv_count(U.dl, val(ang));
+    U.nl = subdiv_count_long(U.dl, val(ang));
     U.cs = tsubdiv_ps(rp, ang, U.nl);
     tcircle_frame(U.south, U.fx, U.fy);
     return U;
@@ -305,7 +305,7 @@ __device__ __forceinline__ LatU<T> conc_lat(const Dev& d, const ConcU<T>& U, int
     L.area = lift<T>(0.0);
     if (val(L.rad) > 0.0) {
         L.delta = tsubdiv_delta(U.density, L.rad);
-        const int nc = subdiv_count(val(L.delta), CMS_TWO_PI);
+        const int nc = subdiv_count_long(val(L.delta), CMS_TWO_PI);
         const T ps = nc > 0 ? (L.rad * CMS_TWO_PI) / (double)nc : lift<T>(0.0);
         L.area = ps * U.cs;
     }

@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 10 : 12) k_convex(Dev d)
         V3 ylat;
         const double ang = arc_angle(eq, north, south, ylat);
         const double dl = subdiv_delta(dens, ri);
-        const int nl = subdiv_count(dl, ang);
+        const int nl = subdiv_count_long(dl, ang);
         const double cs = subdiv_ps(ri, ang, nl);
         V3 fx, fy;
         circle_frame(north, fx, fy);
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 10 : 12) k_convex(Dev d)
             double delta = 0.0, ps = 0.0;
             if (rad > 0.0) {
                 delta = subdiv_delta(dens, rad);
-                nc = subdiv_count(delta, CMS_TWO_PI);
+                nc = subdiv_count_long(delta, CMS_TWO_PI);
                 ps = subdiv_ps(rad, CMS_TWO_PI, nc);
             }
             L.dt[l] = dt;
@@ -917,7 +917,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
         V3 ylat;
         const double ang = arc_angle(axis, vtop, south, ylat);
         const double dl = subdiv_delta(density, rp);
-        const int nl = subdiv_count(dl, ang);
+        const int nl = subdiv_count_long(dl, ang);
         const double cs = subdiv_ps(rp, ang, nl);
         V3 fx, fy;
         circle_frame(south, fx, fy);
@@ -930,7 +930,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
             double delta = 0.0, ps = 0.0;
             if (rad > 0.0) {
                 delta = subdiv_delta(density, rad);
-                nc = subdiv_count(delta, CMS_TWO_PI);
+                nc = subdiv_count_long(delta, CMS_TWO_PI);
                 ps = subdiv_ps(rad, CMS_TWO_PI, nc);
             }
             L.dt[l] = dt;
