@@ -641,6 +641,7 @@ __device__ __forceinline__ TripleBase triple_base(const Dev& d, V3 xi, double er
 
 static constexpr int TR_WARPS = 2;
 static constexpr int TR_QCAP = 256;   // queued (pair slot, k slot) triples per warp
+static constexpr int TR_HEAD = 8;     // row slots each lane tests for its own probes before the shared scan
 
 __device__ __forceinline__ void stash_one(const Dev& d, long long e, int a0, int a1, int a2, double h, V3 pt, V3 alt,
                                           int g, unsigned ord)
@@ -884,8 +885,8 @@ __device__ __forceinline__ void triples_flush_c(const Dev& d, int g, V3 xi, doub
     const double rp = d.st.rp;
     for (int e0 = 0; e0 < qn; e0 += 32) {
         const int e = e0 + lane;
-        bool okp = false, okm = false;
-        V3 pp, pm, up;
+        bool okp = false, okm = false, live = false, cp = false, cm = false;
+        V3 pp = v3(0.0, 0.0, 0.0), pm = pp, up;
         double h = 0.0;
         int j = -1, k = -1;
         if (e < qn) {
@@ -915,13 +916,44 @@ __device__ __forceinline__ void triples_flush_c(const Dev& d, int g, V3 xi, doub
                     up = uijk;
                     pp = bijk + uijk * (h * 1.0);
                     pm = bijk + uijk * (h * -1.0);
-                    bool cp, cm;
-                    probe_pair_collides_c(R, K, pp, pm, j, k, rp, cp, cm);
-                    okp = !cp;
-                    okm = !cm;
+                    live = true;
+                    probe_pair_collides_c(R, K < TR_HEAD ? K : TR_HEAD, pp, pm, j, k, rp, cp, cm);
                 }
             }
         }
+        // The rest of the row for the probes still open, one triple at a time with the row over the lanes:
+        // most probes collide with one of the nearest neighbours (the row is in distance order), so a lane
+        // that must scan the whole row would otherwise hold up the warp alone.
+        unsigned open = __ballot_sync(0xffffffffu, live && !(cp && cm));
+        while (open) {
+            const int src = __ffs(open) - 1;
+            open &= open - 1;
+            const V3 qp = v3(__shfl_sync(0xffffffffu, pp.x, src), __shfl_sync(0xffffffffu, pp.y, src),
+                             __shfl_sync(0xffffffffu, pp.z, src));
+            const V3 qm = v3(__shfl_sync(0xffffffffu, pm.x, src), __shfl_sync(0xffffffffu, pm.y, src),
+                             __shfl_sync(0xffffffffu, pm.z, src));
+            const int qj = __shfl_sync(0xffffffffu, j, src), qk = __shfl_sync(0xffffffffu, k, src);
+            bool hp = __shfl_sync(0xffffffffu, cp, src), hm = __shfl_sync(0xffffffffu, cm, src);
+            for (int s0 = TR_HEAD; s0 < K && !(hp && hm); s0 += 32) {
+                const int sl = s0 + lane;
+                bool ap = false, am = false;
+                if (sl < K) {
+                    const int n = R.id[sl];
+                    if (n != qj && n != qk) {
+                        const double t = R.r[sl] + rp;
+                        const double t2 = t * t;
+                        const V3 x = v3(R.x[sl], R.y[sl], R.z[sl]);
+                        ap = sq_alt(qp - x) <= t2;
+                        am = sq_alt(qm - x) <= t2;
+                    }
+                }
+                hp = __any_sync(0xffffffffu, ap) || hp;
+                hm = __any_sync(0xffffffffu, am) || hm;
+            }
+            if (lane == src) { cp = hp; cm = hm; }
+        }
+        okp = live && !cp;
+        okm = live && !cm;
         const unsigned bp = __ballot_sync(0xffffffffu, okp);
         const unsigned bm = __ballot_sync(0xffffffffu, okm);
         if (!EMIT) probe_stash(d, g, j, k, h, pp, pm, up, okp, okm, bp, bm, nplus, nminus);
