@@ -333,6 +333,68 @@ void launch_attention(const Dev& d, cudaStream_t s)
 // ---------------------------------------------------------------------------
 static constexpr int NB_CAP = 256;
 
+// Warp bitonic sort of 32 * E (key, val) pairs into ascending (key, val)
+// order; element i is held by lane i % 32 as its (i / 32)-th entry.  Strides
+// under 32 exchange through shuffles, the others within a lane.  The vals of
+// the real entries are distinct (atom ids or slots); padding is (~0, INT_MAX).
+template <int E>
+__device__ __forceinline__ void warp_bitonic(unsigned long long (&key)[E], int (&val)[E])
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 2; k <= 32 * E; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j >= 32) {
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const int pe = e ^ (j >> 5);
+                    if (pe > e) {
+                        const bool up = ((e * 32 + lane) & k) == 0;
+                        const bool gt = key[e] > key[pe] || (key[e] == key[pe] && val[e] > val[pe]);
+                        if (gt == up) {
+                            const unsigned long long tk = key[e]; key[e] = key[pe]; key[pe] = tk;
+                            const int tv = val[e]; val[e] = val[pe]; val[pe] = tv;
+                        }
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < E; ++e) {
+                    const unsigned long long ok = __shfl_xor_sync(0xffffffffu, key[e], j);
+                    const int ov = __shfl_xor_sync(0xffffffffu, val[e], j);
+                    const bool up = ((e * 32 + lane) & k) == 0;
+                    const bool lower = (lane & j) == 0;
+                    const bool other_less = ok < key[e] || (ok == key[e] && ov < val[e]);
+                    if (lower == up ? other_less : !other_less) { key[e] = ok; val[e] = ov; }
+                }
+            }
+        }
+    }
+}
+
+// write row[i] = the val of rank i for the K (<= 32 * E) entries in sd2 / sid, ranked by (d2, id); d2 >= 0,
+// so its bit pattern orders like the value
+template <int E>
+__device__ __forceinline__ void sort_row(const double* sd2, const int* sid, int K, int* row)
+{
+    const int lane = threadIdx.x & 31;
+    unsigned long long key[E];
+    int val[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int i = e * 32 + lane;
+        key[e] = i < K ? (unsigned long long)__double_as_longlong(sd2[i]) : ~0ULL;
+        val[e] = i < K ? sid[i] : 0x7fffffff;
+    }
+    warp_bitonic<E>(key, val);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int i = e * 32 + lane;
+        if (i < K) row[i] = val[e];
+    }
+}
+
 // every partner of atom g lies within ri + radmax + 2 rp
 __device__ __forceinline__ double nb_range(const Dev& d, int c, double ri)
 {
@@ -480,7 +542,10 @@ __global__ void __launch_bounds__(NB_WARPS * 32) k_nb_emit(Dev d, int* __restric
             });
         }
         __syncwarp();
-        for (int e = lane; e < K; e += 32) {
+        if (K <= 32) sort_row<1>(sd2[w], sid[w], K, d.nb_id + off);
+        else if (K <= 64) sort_row<2>(sd2[w], sid[w], K, d.nb_id + off);
+        else if (K <= 128) sort_row<4>(sd2[w], sid[w], K, d.nb_id + off);
+        else for (int e = lane; e < K; e += 32) {
             const double ke = in_sh ? sd2[w][e] : d.nb_d2[off + e];
             const int je = in_sh ? sid[w][e] : tmp_id[off + e];
             int rank = 0;
