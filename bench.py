@@ -342,20 +342,25 @@ def stage_bytes(name, t, work=None):
 # one launch, ncu on the 256-complex batch of this generator, divided by that
 # batch's units); scaled by the units of the measured batch
 TRAFFIC_PER_UNIT = {
-    "toroidal_emit": (365.19e6 / 5021616, "toroidal"),     # per toroidal dot
-    "toroidal_count": (45.53e6 / 558670, "atoms"),         # per atom
-    "triples_count": (105.68e6 / 558670, "atoms"),         # per atom
+    "neighbor_count": (78.47e6 / 558670, "atoms"),         # per atom
+    "neighbor_emit": (163.85e6 / 558670, "atoms"),
+    "triples_count": (95.88e6 / 558670, "atoms"),
+    "convex_count": (19.10e6 / 558670, "atoms"),
+    "toroidal_count": (46.53e6 / 558670, "atoms"),
+    "concave_count": (20.99e6 / 558670, "atoms"),
     "triples_emit": (19.46e6 / 558670, "atoms"),           # the probe scatter
+    "toroidal_emit": (365.19e6 / 5021616, "toroidal"),     # per toroidal dot
     "cms_nn": (104.73e6 / 2750610, "cms_queries"),         # per query dot
     "sc_band_nn": (405.62e6 / 2750610, "band_queries"),
 }
 
-# FP64 pipe utilisation of the FP64-bound stages (sm__inst_executed_pipe_fp64 active %, ncu --set full on the
+# FP64 pipe utilisation of the FP64-bound stages (sm__pipe_fp64_cycles_active %, ncu --set full on the
 # 256-complex batch; the captures under profiles/)
 FP64_PIPE_PCT = {
-    "triples_count": (21.8, "profiles/k_triples_256_complexes.md"),
-    "toroidal_count": (26.0, "profiles/k_toroidal_256_complexes.md"),
-    "concave_count": (28.0, "profiles/k_concave_256_complexes.md"),
+    "triples_count": (19.6, "profiles/fp64_count_passes_256_complexes.md"),
+    "toroidal_count": (26.5, "profiles/fp64_count_passes_256_complexes.md"),
+    "concave_count": (28.9, "profiles/fp64_count_passes_256_complexes.md"),
+    "convex_count": (37.4, "profiles/fp64_count_passes_256_complexes.md"),
     "cms_backward": (19.6, "profiles/k_adj_units_256_complexes.md"),
 }
 NN_STAGES = {"cms_nn": "cms", "sc_band_nn": "band", "sc_argmin_nn": "sc"}
