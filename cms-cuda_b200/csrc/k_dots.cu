@@ -766,6 +766,19 @@ void launch_toroidal(const Dev& d, long long tor_grid, bool emit, int variant, c
 // ---------------------------------------------------------------------------
 // concave dots: one warp per probe
 // ---------------------------------------------------------------------------
+// subdiv_point with its FP64 sincos as one called copy: the concave kernel calls it from three places, and
+// inlining each copy made a kernel large enough to stall on instruction fetch (concave count 25.1 -> 24.3 ms
+// with the call; the convex and toroidal kernels are faster with it inlined)
+static __device__ __noinline__ void sincos_called(double a, double* s, double* c) { sincos(a, s, c); }
+
+__device__ __forceinline__ V3 subdiv_point_called(V3 cen, double rad, V3 x, V3 y, double delta, int i)
+{
+    const double a = delta * ((double)i + 0.5);
+    double s, c;
+    sincos_called(a, &s, &c);
+    const double rc = rad * c, rs = rad * s;
+    return (cen + x * rc) + y * rs;
+}
 static constexpr int CC_WARPS = 4;
 
 // MINB: CTAs per SM the register allocation must allow -- 4 (128 registers),
@@ -922,7 +935,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
         V3 fx, fy;
         circle_frame(south, fx, fy);
         for (int l = lane; l < nl; l += 32) {
-            V3 lat = subdiv_point(v3(0.0, 0.0, 0.0), rp, vtop, ylat, dl, l);
+            V3 lat = subdiv_point_called(v3(0.0, 0.0, 0.0), rp, vtop, ylat, dl, l);
             double dt = dot_seq(lat, south);
             double rsq = rp2 - dt * dt;
             double rad = sqrt(rsq < 0.0 ? 0.0 : rsq);
@@ -958,7 +971,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
             if (t < total) {
                 l = find_lat(L, nl, t);
                 i = t - L.start[l];
-                V3 pt = subdiv_point(south * L.dt[l], L.rad[l], fx, fy, L.delta[l], i);
+                V3 pt = subdiv_point_called(south * L.dt[l], L.rad[l], fx, fy, L.delta[l], i);
                 keep = !(dot_seq(pt, vec0) >= 0 || dot_seq(pt, vec1) >= 0 || dot_seq(pt, vec2) >= 0);
                 if (keep) {
                     pts = pt + pijk;
@@ -998,7 +1011,7 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
                 for (int e = lane; e < kept; e += 32) {
                     const int sub = ksl[EMIT ? 0 : w][e];
                     const int l = sub >> 16, i = sub & 0xffff;
-                    const V3 pts = subdiv_point(south * L.dt[l], L.rad[l], fx, fy, L.delta[l], i) + pijk;
+                    const V3 pts = subdiv_point_called(south * L.dt[l], L.rad[l], fx, fy, L.delta[l], i) + pijk;
                     double dd[3];
                     for (int k = 0; k < 3; ++k) dd[k] = norm3(pts - xa[k]) - ra[k];
                     int mc = 0;                        // np.argmin: first minimum, NaN wins
