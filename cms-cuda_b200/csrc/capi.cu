@@ -386,7 +386,6 @@ void bind_batch(cms_ctx* x)
     d.dot_off = x->ensure<long long>(cms_ctx::S_DOT_OFF, 2 * B + 1);
     d.tor_last1 = x->ensure<unsigned long long>(cms_ctx::S_TOR_LAST1, N);
     d.tor_last2 = x->ensure<unsigned long long>(cms_ctx::S_TOR_LAST2, N);
-    Rd& r = x->r;
     x->ensure<int>(cms_ctx::S_CM_TMP, 2 * B + 2);
     x->ensure<double>(cms_ctx::S_PER_ATOM_CMS, N);
     x->ensure<double>(cms_ctx::S_TOT_CMS, 2 * B);
