@@ -170,6 +170,7 @@ class Context:
         st = self.lib.cms_ctx_create(ctypes.byref(h), int(device), ctypes.c_void_p(stream) if stream else None)
         self.h = h
         self._check(st)
+        self.device = int(device)
         self.B = 0
         self.N = 0
 
@@ -372,6 +373,10 @@ class Context:
             raise ValueError(f"out must be a C-contiguous float64 array of shape ({self.N}, 3)")
         self._check(self.lib.cms_grad_xyz(self.h, _ptr(out), CMS_HOST))
         return out
+
+    def grad_xyz_device(self, ptr):
+        """The last run's gradient copied to device memory at `ptr` (N x 3 float64)."""
+        self._check(self.lib.cms_grad_xyz(self.h, ctypes.c_void_p(ptr), CMS_DEVICE))
 
     def recompute_dots(self, c, m, info):
         """Dots of complex c, molecule m recomputed by the adjoint's geometry (self-check)."""

@@ -76,6 +76,63 @@ class BatchCalculator:
                     g = grad_out
         return BatchResult(totals, sc, sides, pa if per_atom else None, g)
 
+    def run_stream(self, batches, grad_outs):
+        """
+        Evaluate a sequence of batches of one shape (the same atom_off and
+        n_binder) with the host<->device copies of neighbouring batches
+        overlapped with the pipeline: while batch k runs, batch k+1's
+        coordinates and radii upload on a copy stream, and batch k's gradient
+        downloads while batch k+1 runs.  `batches` is a list of
+        (atom_off, n_binder, xyz, radius) host arrays (pinned xyz / radius
+        make the uploads asynchronous); `grad_outs` one pinned float64 N x 3
+        host array per batch, which receives that batch's d(target-side
+        CMS)/d(xyz).  Returns the BatchResult of every batch; the gradients
+        are in place when it returns.
+        """
+        import torch
+        if len(grad_outs) != len(batches):
+            raise ValueError("one gradient buffer per batch")
+        if not self._grad:
+            self.ctx.set_backward(True, target_side=True)
+            self._grad = True
+        dev = torch.device("cuda", self.ctx.device)
+        n = int(np.asarray(batches[0][0])[-1])
+        stage_x = [torch.empty((n, 3), dtype=torch.float64, device=dev) for _ in range(2)]
+        stage_r = [torch.empty(n, dtype=torch.float64, device=dev) for _ in range(2)]
+        stage_g = [torch.empty((n, 3), dtype=torch.float64, device=dev) for _ in range(2)]
+        copy = torch.cuda.Stream(device=dev)
+        ev_in = [torch.cuda.Event() for _ in range(2)]
+        ev_out = [None, None]
+
+        def upload(k):
+            _, _, x, r = batches[k]
+            with torch.cuda.stream(copy):
+                stage_x[k % 2].copy_(torch.from_numpy(np.asarray(x, np.float64).reshape(-1, 3)), non_blocking=True)
+                stage_r[k % 2].copy_(torch.from_numpy(np.asarray(r, np.float64)), non_blocking=True)
+                ev_in[k % 2].record(copy)
+
+        results = []
+        upload(0)
+        for k in range(len(batches)):
+            off, nb = batches[k][0], batches[k][1]
+            ev_in[k % 2].synchronize()
+            if k + 1 < len(batches):
+                upload(k + 1)            # its staging buffers were last read by batch k - 1's load
+            self.ctx.load_batch_device(off, nb, stage_x[k % 2].data_ptr(), stage_r[k % 2].data_ptr())
+            self.ctx.run_graph()
+            _, totals = self.ctx.contact_ms(per_atom=False)
+            sc, sides = self.ctx.shape_complementarity()
+            if ev_out[k % 2] is not None:
+                ev_out[k % 2].synchronize()      # batch k - 2's download has left this buffer
+            self.ctx.grad_xyz_device(stage_g[k % 2].data_ptr())
+            with torch.cuda.stream(copy):
+                torch.from_numpy(grad_outs[k]).copy_(stage_g[k % 2], non_blocking=True)
+                ev_out[k % 2] = torch.cuda.Event()
+                ev_out[k % 2].record(copy)
+            results.append(BatchResult(totals, sc, sides, None, grad_outs[k]))
+        copy.synchronize()
+        return results
+
     def statuses(self):
         return np.array([self.ctx.info(c).status for c in range(self.ctx.B)], dtype=np.int32)
 

@@ -85,3 +85,37 @@ def test_batch_matches_reference(sample, graph):
         for m in (0, 1):
             side = res.sides[k, m]
             close(f"#{k} surface[{m}]", side[:7], c["surface"][m][:7])
+
+
+def test_stream_of_batches_matches_single_runs(sample):
+    """
+    BatchCalculator.run_stream over three batches of one shape (the sample,
+    then two rigid shifts of its binders) overlaps each batch's uploads and
+    gradient download with its neighbours' pipeline runs; every batch's CMS,
+    SC and gradient equal those of a plain run of that batch, bit for bit.
+    """
+    import torch
+    from cms_cuda.batch import BatchCalculator
+    _, cases = sample
+    off, nb, xyz, rad = _batch(cases)
+    batches = []
+    for shift in (0.0, 0.37, -0.21):
+        x = xyz.copy()
+        for c in range(len(nb)):
+            x[off[c]:off[c] + nb[c]] += shift
+        xp = torch.from_numpy(x).pin_memory().numpy()
+        rp = torch.from_numpy(rad.copy()).pin_memory().numpy()
+        batches.append((off, nb, xp, rp))
+    outs = [torch.empty((len(rad), 3), dtype=torch.float64).pin_memory().numpy() for _ in batches]
+    bc = BatchCalculator(0)
+    bc.load(*batches[0])
+    bc.run(graph=True, grad=True)
+    got = bc.run_stream(batches, outs)
+    for (o, n, x, r), res, g in zip(batches, got, outs):
+        ref = BatchCalculator(0)
+        ref.load(o, n, x, r)
+        want = ref.run(graph=True, grad=True)
+        exact("stream cms", res.cms, want.cms)
+        exact("stream binder cms", res.cms_binder, want.cms_binder)
+        exact("stream sc", res.sc, want.sc)
+        exact("stream gradient", g, want.grad)
