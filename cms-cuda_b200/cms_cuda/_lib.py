@@ -35,7 +35,7 @@ EXPORTED = (
     "cms_nn_evaluated", "cms_set_surface_variants", "cms_get_surface_variants", "cms_set_concurrency",
 )
 
-NN_VARIANT_NAMES = ("q4 r1024", "q4 r512", "q2 r1024", "q2 r512")
+NN_VARIANT_NAMES = ("q4 warp blocks", "q4 r512", "q2 warp blocks", "q2 r512")
 SURFACE_STAGES = ("toroidal_count", "toroidal_emit", "concave_count", "concave_emit", "triples_count")
 SURFACE_VARIANTS = 3
 # cms_set_concurrency bits (CMS_CONC_* of the C header)

@@ -155,9 +155,12 @@ static constexpr int NN_SRB = NN_SR / NN_BLK; // blocks per sub-round
 static constexpr int NN_SORT = 512;           // rounds of a task visited nearest first (more: index order)
 static constexpr int NN_TILE = NN_T * 4;      // queries per tile of the default variant (standalone searches)
 
-// Tunable shapes: queries per thread Q (2 or 4: tiles of 256 or 512 queries)
-// and sub-rounds per staged round (1 or 2: 512 or 1024 references).  Every
-// variant computes the same exact result; the autotuner picks per stage.
+// Tunable shapes: queries per thread Q (2 or 4: tiles of 256 or 512 queries),
+// and either k_nn_w (variants 0 and 2: each warp stages its own blocks in
+// reach) or k_nn with 512-reference rounds staged by the whole CTA (variants 1
+// and 3; k_nn's 1024-reference rounds, nn_var_sub 2, remain for the standalone
+// searches).  Every variant computes the same exact result; the autotuner
+// picks per stage.
 __host__ __device__ constexpr int nn_var_q(int v) { return (v & 2) ? 2 : 4; }
 __host__ __device__ constexpr int nn_var_sub(int v) { return (v & 1) ? 1 : 2; }
 
@@ -651,6 +654,275 @@ __global__ void __launch_bounds__(NN_T, MODE == NN_BAND ? 10 : 8) k_nn(NNArgs a)
     }
 }
 
+// Nearest-dot search with the warps of a tile independent of each other: a
+// warp stages, one 32-reference block at a time in its own shared memory,
+// only the blocks whose box lies within reach of its queries' box (the cull
+// threshold of its open queries), in the FP32 frame of its own queries (the
+// centre of their box).  A CTA-wide staging of whole rounds in reach of the
+// tile's box brings in many references out of reach of a given warp, most of
+// all for the band search's reach of the band width.  The minimum searches
+// visit the sub-round nearest to the warp's box first (its minima set the
+// threshold), then the others in order.  Same FP32 filter, FP64 recheck and
+// error bounds as k_nn (any frame centre bounds |q'| by the box's half
+// diagonal), so the same exact results.
+template <int MODE, int Q>
+__global__ void __launch_bounds__(NN_T, MODE == NN_BAND ? 10 : 8) k_nn_w(NNArgs a)
+{
+    if (a.ovf && *a.ovf) return;
+    constexpr int P = Q / 2;
+    constexpr int WQ = 32 * Q;
+    constexpr int TILE = NN_T * Q;
+    __shared__ float4 wA[NN_W][NN_BLK];       // (x, x, y, y) of the warp's staged block
+    __shared__ float4 wB[NN_W][NN_BLK];       // (z, z, |r|^2, |r|^2)
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float4* const sA = wA[wid];
+    float4* const sB = wB[wid];
+    const long long ntiles = a.tile_off[a.ntask];
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int lo = 0, hi = a.ntask - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (a.tile_off[mid] <= tile) lo = mid; else hi = mid - 1;
+        }
+        const NNTask T = a.task[lo];
+        const long long ro = a.round_off[lo];
+        const int nsr = a.round_cnt[lo];
+        if (ro + nsr > a.round_cap) continue;     // over capacity: the run is flagged and redone
+        const long long qw = (tile - a.tile_off[lo]) * TILE + (long long)wid * WQ;
+        if (qw >= T.qn) continue;
+
+        NNQ q[Q];
+        float qpx[Q], qpy[Q], qpz[Q];
+        float wl[3] = {INFINITY, INFINITY, INFINITY}, wh[3] = {-INFINITY, -INFINITY, -INFINITY};
+#pragma unroll
+        for (int j = 0; j < Q; ++j) {
+            const long long qi = qw + j * 32 + lane;
+            q[j].live = qi < T.qn;
+            qpx[j] = qpy[j] = qpz[j] = 0.f;
+            q[j].dot = 0;
+            if (q[j].live) {
+                const float4 f = a.q_f4[T.q0 + qi];
+                qpx[j] = f.x; qpy[j] = f.y; qpz[j] = f.z;
+                const long long qo = nn_qpos(a, T.q0 + qi);
+                q[j].dot = a.q_idx ? a.q_idx[qo] : (int)qo;
+                wl[0] = fminf(wl[0], f.x); wl[1] = fminf(wl[1], f.y); wl[2] = fminf(wl[2], f.z);
+                wh[0] = fmaxf(wh[0], f.x); wh[1] = fmaxf(wh[1], f.y); wh[2] = fmaxf(wh[2], f.z);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            for (int o = 16; o > 0; o >>= 1) {
+                wl[k] = fminf(wl[k], __shfl_xor_sync(0xffffffffu, wl[k], o));
+                wh[k] = fmaxf(wh[k], __shfl_xor_sync(0xffffffffu, wh[k], o));
+            }
+        }
+        NNTile tl;
+        {
+            const float cx = 0.5f * (wl[0] + wh[0]), cy = 0.5f * (wl[1] + wh[1]), cz = 0.5f * (wl[2] + wh[2]);
+            const double ex = (double)wh[0] - wl[0], ey = (double)wh[1] - wl[1], ez = (double)wh[2] - wl[2];
+            tl = nn_tile(cx, cy, cz, 0.5 * sqrt(ex * ex + ey * ey + ez * ez), T.E);
+        }
+        const double band_th = MODE == NN_BAND ? a.band_thr64 + nn_eps(a.band_thr64, tl.rho, tl.E0) * 1.01 : 0.0;
+        const double band_lo = MODE == NN_BAND ? a.band_thr64 - nn_eps(a.band_thr64, tl.rho, tl.E0) * 1.01 : 0.0;
+        const float band_cth = MODE == NN_BAND ? nn_cull_th(band_th, tl) : 0.f;
+#pragma unroll
+        for (int j = 0; j < Q; ++j) {
+            const float x = qpx[j] - tl.cx, y = qpy[j] - tl.cy, z = qpz[j] - tl.cz;
+            q[j].qx2 = -2.0f * x; q[j].qy2 = -2.0f * y; q[j].qz2 = -2.0f * z;
+            q[j].qq = (double)nn_rr(x, y, z);
+            q[j].ms = INFINITY; q[j].ms2 = INFINITY; q[j].mb = -1;
+            q[j].best = INFINITY; q[j].bidx = -1;
+            q[j].done = !q[j].live;
+            if (MODE == NN_BAND) {
+                q[j].ts = __double2float_ru(band_th - q[j].qq);
+                q[j].tslo = __double2float_rd(band_lo - q[j].qq);
+                q[j].cth = band_cth;
+            } else {
+                q[j].ts = INFINITY;
+                q[j].cth = INFINITY;
+            }
+        }
+        f2_t qxp[P], qyp[P], qzp[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            qxp[p] = pk2(q[2 * p].qx2, q[2 * p + 1].qx2);
+            qyp[p] = pk2(q[2 * p].qy2, q[2 * p + 1].qy2);
+            qzp[p] = pk2(q[2 * p].qz2, q[2 * p + 1].qz2);
+        }
+        // warp cull threshold: the largest over its open queries (-inf: none open)
+        auto warp_cth = [&]() {
+            float c = -INFINITY;
+#pragma unroll
+            for (int j = 0; j < Q; ++j)
+                if (!q[j].done) c = fmaxf(c, q[j].cth);
+            for (int o = 16; o > 0; o >>= 1) c = fmaxf(c, __shfl_xor_sync(0xffffffffu, c, o));
+            return c;
+        };
+        float cthw = warp_cth();
+
+        // one sub-round: its blocks in reach, each staged and scanned
+        auto visit = [&](int g) {
+            const long long rb0 = (long long)g * NN_SR;
+            const int nr = (int)min((long long)NN_SR, T.rn - rb0);
+            bool bn = false;
+            if (lane < NN_SRB && lane * NN_BLK < nr) {
+                const float4 blo = a.box_blk[2 * ((ro + g) * NN_SRB + lane)];
+                const float4 bhi = a.box_blk[2 * ((ro + g) * NN_SRB + lane) + 1];
+                bn = !box_far(box_gap2(wl[0], wl[1], wl[2], wh[0], wh[1], wh[2], blo, bhi), cthw);
+            }
+            unsigned bm = __ballot_sync(0xffffffffu, bn);
+            while (bm && cthw > -INFINITY) {
+                const int b = __ffs(bm) - 1;
+                bm &= bm - 1;
+                const int sb = b * NN_BLK;
+                const int n = min(NN_BLK, nr - sb);
+                const float4 blo = a.box_blk[2 * ((ro + g) * NN_SRB + b)];
+                const float4 bhi = a.box_blk[2 * ((ro + g) * NN_SRB + b) + 1];
+                bool lane_need = false;
+#pragma unroll
+                for (int j = 0; j < Q; ++j)
+                    lane_need |= !q[j].done &&
+                                 !box_far(box_gap2(qpx[j], qpy[j], qpz[j], qpx[j], qpy[j], qpz[j], blo, bhi), q[j].cth);
+                if (!__any_sync(0xffffffffu, lane_need)) continue;
+                __syncwarp();
+                if (lane < n) {
+                    const float4 r = a.r_f4[T.r0 + rb0 + sb + lane];
+                    const float rx = r.x - tl.cx, ry = r.y - tl.cy, rz = r.z - tl.cz;
+                    const float rr = nn_rr(rx, ry, rz);
+                    sA[lane] = make_float4(rx, rx, ry, ry);
+                    sB[lane] = make_float4(rz, rz, rr, rr);
+                }
+                __syncwarp();
+                if (a.pair_count && lane == 0) atomicAdd(a.pair_count, (unsigned long long)n * WQ);
+                float mv[Q];
+#pragma unroll
+                for (int j = 0; j < Q; ++j) mv[j] = INFINITY;
+#pragma unroll 4
+                for (int k = 0; k < n; ++k) {
+                    const float4 ra = sA[k];
+                    const float4 rb4 = sB[k];
+                    const f2_t rxx = pk2(ra.x, ra.y), ryy = pk2(ra.z, ra.w);
+                    const f2_t rzz = pk2(rb4.x, rb4.y), rrr = pk2(rb4.z, rb4.w);
+#pragma unroll
+                    for (int p = 0; p < P; ++p) {
+                        const f2_t sv = fma2(qzp[p], rzz, fma2(qyp[p], ryy, fma2(qxp[p], rxx, rrr)));
+                        float a0, a1;
+                        upk2(sv, a0, a1);
+                        mv[2 * p] = fminf(mv[2 * p], a0);
+                        mv[2 * p + 1] = fminf(mv[2 * p + 1], a1);
+                    }
+                }
+                if (MODE == NN_BAND) {
+#pragma unroll
+                    for (int j = 0; j < Q; ++j) {
+                        // a block minimum within band^2 - eps is a hit without the FP64 recheck
+                        if (!q[j].done && mv[j] <= q[j].tslo) q[j].done = true;
+                        const unsigned nj = __ballot_sync(0xffffffffu, !q[j].done && mv[j] <= q[j].ts);
+                        if (nj) nn_band_warp(a, T, q[j], nj, sA, sB, 0, n, rb0 + sb);
+                    }
+                    cthw = warp_cth();
+                } else {
+                    const int blk = g * NN_SRB + b;
+#pragma unroll
+                    for (int j = 0; j < Q; ++j) {
+                        if (mv[j] < q[j].ms) { q[j].ms2 = q[j].ms; q[j].ms = mv[j]; q[j].mb = blk; }
+                        else q[j].ms2 = fminf(q[j].ms2, mv[j]);
+                    }
+                }
+            }
+            if (MODE != NN_BAND) {
+                // thresholds for the next sub-rounds
+#pragma unroll
+                for (int j = 0; j < Q; ++j)
+                    if (q[j].live && q[j].ms < INFINITY) q[j].cth = nn_cull_th(nn_min_th(q[j].ms, q[j].qq, tl), tl);
+                cthw = warp_cth();
+            }
+        };
+
+        if (nsr > 0 && cthw > -INFINITY) {
+            int gfirst = -1;
+            if (MODE != NN_BAND) {
+                // the sub-round nearest to the warp's box first (smallest gap, then smallest index)
+                float bg = INFINITY;
+                int bi = 0x7fffffff;
+                for (int g0 = 0; g0 < nsr; g0 += 32) {
+                    const int gi = g0 + lane;
+                    if (gi < nsr) {
+                        const float gap = box_gap2(wl[0], wl[1], wl[2], wh[0], wh[1], wh[2], a.box_round[2 * (ro + gi)],
+                                                   a.box_round[2 * (ro + gi) + 1]);
+                        if (gap < bg) { bg = gap; bi = gi; }
+                    }
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    const float g2 = __shfl_xor_sync(0xffffffffu, bg, o);
+                    const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+                    if (g2 < bg || (g2 == bg && i2 < bi)) { bg = g2; bi = i2; }
+                }
+                gfirst = bi < nsr ? bi : 0;
+                visit(gfirst);
+            }
+            for (int g0 = 0; g0 < nsr && cthw > -INFINITY; g0 += 32) {
+                const int gi = g0 + lane;
+                bool near = false;
+                if (gi < nsr && gi != gfirst) {
+                    const float4 rlo = a.box_round[2 * (ro + gi)], rhi = a.box_round[2 * (ro + gi) + 1];
+                    near = !box_far(box_gap2(wl[0], wl[1], wl[2], wh[0], wh[1], wh[2], rlo, rhi), cthw);
+                }
+                unsigned rm = __ballot_sync(0xffffffffu, near);
+                while (rm && cthw > -INFINITY) {
+                    const int g = g0 + __ffs(rm) - 1;
+                    rm &= rm - 1;
+                    if (MODE != NN_BAND) {
+                        // the threshold may have shrunk since the chunk's test
+                        const float gap = box_gap2(wl[0], wl[1], wl[2], wh[0], wh[1], wh[2], a.box_round[2 * (ro + g)],
+                                                   a.box_round[2 * (ro + g) + 1]);
+                        if (box_far(gap, cthw)) continue;
+                    }
+                    visit(g);
+                }
+            }
+        }
+
+        if (MODE != NN_BAND) {
+            // FP64 recheck: the best block alone when no other block can hold a candidate
+            bool full[Q];
+#pragma unroll
+            for (int j = 0; j < Q; ++j) {
+                full[j] = false;
+                if (!q[j].live || !(q[j].ms < INFINITY)) continue;
+                const double th = nn_min_th(q[j].ms, q[j].qq, tl);
+                q[j].ts = __double2float_ru(th - q[j].qq);
+                q[j].cth = nn_cull_th(th, tl);
+                if (q[j].ms2 > q[j].ts) {
+                    const long long k0 = (long long)q[j].mb * NN_BLK;
+                    const long long k1 = min(k0 + NN_BLK, T.rn);
+                    double best = INFINITY;
+                    int bidx = 0x7fffffff;
+                    nn_recheck_block(a, T, tl, q[j].qx2, q[j].qy2, q[j].qz2, q[j].ts, q[j].dot, k0, k1, best, bidx);
+                    q[j].best = best; q[j].bidx = bidx;
+                } else {
+                    full[j] = true;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < Q; ++j) {
+                const unsigned nf = __ballot_sync(0xffffffffu, full[j]);
+                if (nf) nn_full_warp(a, T, tl, ro, nsr, q[j], nf, T.q0 + qw + j * 32);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < Q; ++j) {
+            if (!q[j].live) continue;
+            const long long o = nn_qpos(a, T.q0 + qw + j * 32 + lane);
+            if (MODE == NN_BAND) a.out_flag[o] = q[j].done ? 0 : 1;     // keep iff no reference within the band
+            else {
+                a.out_d2[o] = q[j].best;
+                if (MODE == NN_ARGMIN) a.out_idx[o] = q[j].bidx;
+            }
+        }
+    }
+}
+
 __global__ void k_nn_tiles(NNArgs a)
 {
     if (a.ovf && *a.ovf) return;
@@ -715,9 +987,9 @@ static void nn_dispatch(const NNArgs& a, int variant, unsigned grid, cudaStream_
 {
     switch (variant) {
     case 1: k_nn<MODE, 4, 1><<<grid, NN_T, 0, s>>>(a); break;
-    case 2: k_nn<MODE, 2, 2><<<grid, NN_T, 0, s>>>(a); break;
+    case 2: k_nn_w<MODE, 2><<<grid, NN_T, 0, s>>>(a); break;
     case 3: k_nn<MODE, 2, 1><<<grid, NN_T, 0, s>>>(a); break;
-    default: k_nn<MODE, 4, 2><<<grid, NN_T, 0, s>>>(a); break;
+    default: k_nn_w<MODE, 4><<<grid, NN_T, 0, s>>>(a); break;
     }
 }
 

@@ -249,8 +249,10 @@ cms_status cms_refine_pose(cms_ctx* ctx, double* rot, double* trans, double* xyz
 cms_status cms_refine_end(cms_ctx* ctx);
 
 /* Search shapes of the batched pipeline's three nearest-dot searches (CMS, SC
- * band trim, SC neighbour argmin): variants[3], each 0..3 = (4 queries per
- * thread, 1024-reference rounds), (4, 512), (2, 1024), (2, 512).  Every shape
+ * band trim, SC neighbour argmin): variants[3], each 0..3 = 4 queries per
+ * thread with each warp staging its own reference blocks in reach, 4 queries
+ * per thread with 512-reference rounds staged by the whole CTA, 2 with
+ * per-warp blocks, 2 with 512-reference rounds.  Every shape
  * gives the same results.  By default an autotuner times all shapes on each
  * new batch shape before capturing the graph and keeps the fastest per search
  * (tune_ms[3 x 4]: the times it measured, NULL to skip); cms_set_nn_variants
