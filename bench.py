@@ -352,8 +352,8 @@ TRAFFIC_PER_UNIT = {
     "concave_count": (20.99e6 / 558670, "atoms"),
     "triples_emit": (19.46e6 / 558670, "atoms"),           # the probe scatter
     "toroidal_emit": (365.19e6 / 5021616, "toroidal"),     # per toroidal dot
-    "cms_nn": (104.73e6 / 2750610, "cms_queries"),         # per query dot
-    "sc_band_nn": (405.62e6 / 2750610, "band_queries"),
+    "cms_nn": (273.01e6 / 2750610, "cms_queries"),         # per query dot (k_nn_w, 4 queries per lane)
+    "sc_band_nn": (251.90e6 / 2750610, "band_queries"),
 }
 
 # FP64 pipe utilisation of the FP64-bound stages (sm__pipe_fp64_cycles_active %, ncu --set full on the
