@@ -97,6 +97,12 @@ class BatchCalculator:
             self._grad = True
         dev = torch.device("cuda", self.ctx.device)
         n = int(np.asarray(batches[0][0])[-1])
+        for off, nb, x, r in batches:
+            if int(np.asarray(off)[-1]) != n or np.shape(x) != (n, 3) or np.shape(r) != (n,) or len(nb) != len(off) - 1:
+                raise ValueError("run_stream needs batches of one atom count, with N x 3 coordinates and N radii")
+        for g in grad_outs:
+            if g.dtype != np.float64 or g.shape != (n, 3) or not g.flags.c_contiguous:
+                raise ValueError(f"each gradient buffer must be a C-contiguous float64 array of shape ({n}, 3)")
         stage_x = [torch.empty((n, 3), dtype=torch.float64, device=dev) for _ in range(2)]
         stage_r = [torch.empty(n, dtype=torch.float64, device=dev) for _ in range(2)]
         stage_g = [torch.empty((n, 3), dtype=torch.float64, device=dev) for _ in range(2)]
