@@ -119,3 +119,17 @@ def test_stream_of_batches_matches_single_runs(sample):
         exact("stream binder cms", res.cms_binder, want.cms_binder)
         exact("stream sc", res.sc, want.sc)
         exact("stream gradient", g, want.grad)
+
+
+def test_stream_rejects_other_atom_counts(sample):
+    """run_stream takes batches of one atom count only (its device staging is sized once)."""
+    from cms_cuda.batch import BatchCalculator
+    _, cases = sample
+    off, nb, xyz, rad = _batch(cases)
+    off2, nb2, xyz2, rad2 = _batch(cases[:-1])
+    bc = BatchCalculator(0)
+    g = [np.empty((len(rad), 3)), np.empty((len(rad), 3))]
+    with pytest.raises(ValueError):
+        bc.run_stream([(off, nb, xyz, rad), (off2, nb2, xyz2, rad2)], g)
+    with pytest.raises(ValueError):
+        bc.run_stream([(off, nb, xyz, rad)], [np.empty((len(rad), 2))])
