@@ -24,7 +24,8 @@
 //      adjoint: the unit's geometry in forward-mode duals (6 or 9 tangents,
 //      cms_dual.cuh), the Jacobian-transpose products summed over its dots in
 //      dot order, one 3-vector per atom of the unit;
-//   4. per atom: the unit contributions gathered in a fixed order.
+//   4. per atom: the unit contributions gathered by one warp, lanes over the
+//      atom's row and units, summed in a fixed tree.
 // Every sum has a fixed order, so the gradient is deterministic.
 //
 // The same unit code run on plain doubles recomputes the dots; that recompute
@@ -735,71 +736,6 @@ __device__ __forceinline__ void atom_probe_ranges(const Dev& d, int g, long long
     me = mb + (d.minus_off[g + 1] - d.minus_off[g]);
 }
 
-__device__ __forceinline__ void add_probe_range(const Dev& d, const AdjBuf& a, int atom, long long b, long long e,
-                                                double& x, double& y, double& z)
-{
-    for (long long p = b; p < e && p < d.probe_cap; ++p) {
-        if (!a.act_conc[p]) continue;
-        const int ia[3] = {d.pa0[p], d.pa1[p], d.pa2[p]};
-        for (int s = 0; s < 3; ++s) {
-            if (ia[s] != atom) continue;
-            const double* v = a.gconc + 9 * p + 3 * s;
-            x += v[0]; y += v[1]; z += v[2];
-        }
-    }
-}
-
-// pass 4: per atom of an active unit, in a fixed order: its convex unit,
-// convex units framed by it, its pairs as i, pairs with it as j, probes of
-// its own triples and of its lower-index neighbours' triples
-__global__ void k_adj_gather(Dev d, AdjBuf a, double* grad)
-{
-    CMS_EXIT_ON_OVERFLOW(d);
-    for (long long aa = blockIdx.x * (long long)blockDim.x + threadIdx.x; aa < d.N; aa += (long long)gridDim.x * blockDim.x) {
-        const int at = (int)aa;
-        double x = 0.0, y = 0.0, z = 0.0;
-        if (a.act_atom[at]) {
-            if (a.act_conv[at]) { x = a.gconv[6 * aa]; y = a.gconv[6 * aa + 1]; z = a.gconv[6 * aa + 2]; }
-            const long long off = d.nb_off[at];
-            const int K = d.nnb[at];
-            for (int s = 0; s < K; ++s) {
-                const int g = d.nb_id[off + s];
-                if (a.act_conv[g] && d.nb_id[d.nb_off[g]] == at) {
-                    const double* v = a.gconv + 6LL * g + 3;
-                    x += v[0]; y += v[1]; z += v[2];
-                }
-            }
-            const long long NT = min(d.tor_off[d.N], d.tor_cap);
-            for (long long q = d.tor_off[at]; q < d.tor_off[at + 1] && q < NT; ++q) {
-                if (!a.act_tor[q]) continue;
-                const double* v = a.gtor + 6 * q;
-                x += v[0]; y += v[1]; z += v[2];
-            }
-            for (int s = 0; s < K; ++s) {
-                const int i = d.nb_id[off + s];
-                if (i >= at) continue;
-                for (long long q = d.tor_off[i]; q < d.tor_off[i + 1] && q < NT; ++q) {
-                    if (d.tor_j[q] != at || !a.act_tor[q]) continue;
-                    const double* v = a.gtor + 6 * q + 3;
-                    x += v[0]; y += v[1]; z += v[2];
-                }
-            }
-            long long pb, pe, mb, me;
-            atom_probe_ranges(d, at, pb, pe, mb, me);
-            add_probe_range(d, a, at, pb, pe, x, y, z);
-            add_probe_range(d, a, at, mb, me, x, y, z);
-            for (int s = 0; s < K; ++s) {
-                const int g = d.nb_id[off + s];
-                if (g >= at) continue;
-                atom_probe_ranges(d, g, pb, pe, mb, me);
-                add_probe_range(d, a, at, pb, pe, x, y, z);
-                add_probe_range(d, a, at, mb, me, x, y, z);
-            }
-        }
-        grad[3 * aa] = x; grad[3 * aa + 1] = y; grad[3 * aa + 2] = z;
-    }
-}
-
 // clears the per-dot adjoint of the buried dots (the only ones that get one)
 // and the per-entry and per-unit counters
 __global__ void k_adj_zero(Dev d, Rd r, AdjBuf a, long long dcap)
@@ -818,6 +754,82 @@ __global__ void k_adj_zero(Dev d, Rd r, AdjBuf a, long long dcap)
         if (i < d.tor_cap) a.act_tor[i] = 0;
         if (i < d.probe_cap) a.act_conc[i] = 0;
         if (i < 3) a.nact[i] = 0;
+    }
+}
+
+// pass 4, one warp per active atom: the lanes take the atom's neighbour-row
+// slots (the convex units it frames, the pairs (i, atom) of lower-index
+// neighbours i, their triples' probes) and its own pairs and probes, and the
+// warp sums the lanes' partial sums in a fixed tree; inactive atoms get zeros
+__device__ __forceinline__ void add_probe_range_lanes(const Dev& d, const AdjBuf& a, int atom, long long b, long long e,
+                                                      int start, int step, double& x, double& y, double& z)
+{
+    for (long long p = b + start; p < e && p < d.probe_cap; p += step) {
+        if (!a.act_conc[p]) continue;
+        const int ia[3] = {d.pa0[p], d.pa1[p], d.pa2[p]};
+        for (int s = 0; s < 3; ++s) {
+            if (ia[s] != atom) continue;
+            const double* v = a.gconc + 9 * p + 3 * s;
+            x += v[0]; y += v[1]; z += v[2];
+        }
+    }
+}
+
+__global__ void k_adj_gather_w(Dev d, AdjBuf a, double* grad)
+{
+    CMS_EXIT_ON_OVERFLOW(d);
+    const int lane = threadIdx.x & 31;
+    const long long wid = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long NT = min(d.tor_off[d.N], d.tor_cap);
+    for (long long b0 = wid * 32; b0 < d.N; b0 += nw * 32) {
+        const long long me = b0 + lane;
+        const bool act = me < d.N && a.act_atom[me];
+        if (me < d.N && !act) { grad[3 * me] = 0.0; grad[3 * me + 1] = 0.0; grad[3 * me + 2] = 0.0; }
+        unsigned m = __ballot_sync(0xffffffffu, act);
+        while (m) {
+            const int at = (int)(b0 + __ffs(m) - 1);
+            m &= m - 1;
+            double x = 0.0, y = 0.0, z = 0.0;
+            if (lane == 0 && a.act_conv[at]) {
+                x = a.gconv[6LL * at]; y = a.gconv[6LL * at + 1]; z = a.gconv[6LL * at + 2];
+            }
+            const long long off = d.nb_off[at];
+            const int K = d.nnb[at];
+            for (int s = lane; s < K; s += 32) {
+                const int g = d.nb_id[off + s];
+                if (a.act_conv[g] && d.nb_id[d.nb_off[g]] == at) {
+                    const double* v = a.gconv + 6LL * g + 3;
+                    x += v[0]; y += v[1]; z += v[2];
+                }
+                if (g < at) {
+                    for (long long q = d.tor_off[g]; q < d.tor_off[g + 1] && q < NT; ++q) {
+                        if (d.tor_j[q] != at || !a.act_tor[q]) continue;
+                        const double* v = a.gtor + 6 * q + 3;
+                        x += v[0]; y += v[1]; z += v[2];
+                    }
+                    long long pb, pe, mb, me2;
+                    atom_probe_ranges(d, g, pb, pe, mb, me2);
+                    add_probe_range_lanes(d, a, at, pb, pe, 0, 1, x, y, z);
+                    add_probe_range_lanes(d, a, at, mb, me2, 0, 1, x, y, z);
+                }
+            }
+            for (long long q = d.tor_off[at] + lane; q < d.tor_off[at + 1] && q < NT; q += 32) {
+                if (!a.act_tor[q]) continue;
+                const double* v = a.gtor + 6 * q;
+                x += v[0]; y += v[1]; z += v[2];
+            }
+            long long pb, pe, mb, me2;
+            atom_probe_ranges(d, at, pb, pe, mb, me2);
+            add_probe_range_lanes(d, a, at, pb, pe, lane, 32, x, y, z);
+            add_probe_range_lanes(d, a, at, mb, me2, lane, 32, x, y, z);
+            for (int o = 16; o > 0; o >>= 1) {
+                x += __shfl_xor_sync(0xffffffffu, x, o);
+                y += __shfl_xor_sync(0xffffffffu, y, o);
+                z += __shfl_xor_sync(0xffffffffu, z, o);
+            }
+            if (lane == 0) { grad[3LL * at] = x; grad[3LL * at + 1] = y; grad[3LL * at + 2] = z; }
+        }
     }
 }
 
@@ -840,7 +852,7 @@ void launch_adjoint(const Dev& d, const Rd& r, const AdjBuf& a, const NNTask* cm
     k_adj_units<0, 3><<<grid_adj(d.N, 128), 128, 0, s>>>(d, a);
     k_adj_units<1, 1><<<grid_adj(d.tor_cap, 128), 128, 0, s>>>(d, a);
     k_adj_units<2, 3><<<grid_adj(d.probe_cap, 128), 128, 0, s>>>(d, a);
-    k_adj_gather<<<grid_adj(d.N, 128), 128, 0, s>>>(d, a, grad);
+    k_adj_gather_w<<<grid_adj(d.N, 128), 128, 0, s>>>(d, a, grad);
 }
 
 }  // namespace cms
