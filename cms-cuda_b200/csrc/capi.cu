@@ -840,9 +840,9 @@ AdjBuf bind_adj(cms_ctx* x)
     a.gconc = x->ensure<double>(cms_ctx::S_ADJ_GCONC, 9 * std::max(x->cap_probe, 1LL));
     a.gtot = x->ensure<double>(cms_ctx::S_ADJ_GTOT, x->B);
     const long long T = std::max(x->cap_tor, 1LL), P = std::max(x->cap_probe, 1LL);
-    a.act_conv = x->ensure<int8_t>(cms_ctx::S_ADJ_ACT_CONV, x->N);
-    a.act_tor = x->ensure<int8_t>(cms_ctx::S_ADJ_ACT_TOR, T);
-    a.act_conc = x->ensure<int8_t>(cms_ctx::S_ADJ_ACT_CONC, P);
+    a.act_conv = x->ensure<int>(cms_ctx::S_ADJ_ACT_CONV, x->N);
+    a.act_tor = x->ensure<int>(cms_ctx::S_ADJ_ACT_TOR, T);
+    a.act_conc = x->ensure<int>(cms_ctx::S_ADJ_ACT_CONC, P);
     a.act_atom = x->ensure<int8_t>(cms_ctx::S_ADJ_ACT_ATOM, x->N);
     a.list_conv = x->ensure<int>(cms_ctx::S_ADJ_LIST_CONV, x->N);
     a.list_tor = x->ensure<int>(cms_ctx::S_ADJ_LIST_TOR, T);

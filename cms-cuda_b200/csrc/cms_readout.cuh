@@ -79,7 +79,7 @@ struct AdjBuf {
     double* gconv;         // 6 per atom: convex unit contributions (atom, frame atom)
     double* gtor;          // 6 per toroid pair: (atom 1, atom 2)
     double* gconc;         // 9 per probe: (atom 0, atom 1, atom 2)
-    int8_t* act_conv; int8_t* act_tor; int8_t* act_conc;   // units holding a dot with a non-zero adjoint
+    int* act_conv; int* act_tor; int* act_conc;   // per unit: its dots given an adjoint (> 0: active unit)
     int8_t* act_atom;      // atoms of active units
     int* list_conv; int* list_tor; int* list_conc;         // active units
     int* skey;             // 3 x ADJ_KEYS: active units per work key, then each key's next slot

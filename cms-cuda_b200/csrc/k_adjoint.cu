@@ -354,6 +354,16 @@ struct SeedLane {
     }
 };
 
+// the first dot in [q, e) the consumer wants (e when none): the unit loops step from wanted dot to wanted dot,
+// so the lanes of a warp, whose units hold about as many such dots (the units are ordered by that count), run
+// their k-th wanted dots together
+template <class F>
+__device__ __forceinline__ long long next_wanted(const Dev& d, const F& f, long long q, long long e)
+{
+    while (q < e && (q >= d.dot_cap || !f.want(q))) ++q;
+    return q;
+}
+
 template <class T, class S, class F>
 __device__ __forceinline__ void convex_unit_dots(const Dev& d, int g, const S& seed, F& f)
 {
@@ -363,8 +373,7 @@ __device__ __forceinline__ void convex_unit_dots(const Dev& d, int g, const S& s
     const ConvexU<T> U = convex_unit<T>(d, g, seed.atom(d, g, 0), seed.atom(d, n0, 1), d.xyzr[g].w, d.xyzr[n0].w);
     int cur = -1;
     LatU<T> L;
-    for (long long q = base; q < base + cnt; ++q) {
-        if (q >= d.dot_cap || !f.want(q)) continue;
+    for (long long q = next_wanted(d, f, base, base + cnt); q < base + cnt; q = next_wanted(d, f, q + 1, base + cnt)) {
         const int sub = d.dsub[q];
         const int l = sub >> 16, i = sub & 0xffff;
         if (l != cur) { L = convex_lat(U, l); cur = l; }
@@ -386,8 +395,7 @@ __device__ __forceinline__ void tor_unit_dots(const Dev& d, long long qp, const 
         const int cnt = arc ? d.tor2_cnt[qp] : d.tor1_cnt[qp];
         int cur = -1;
         TorArcU<T> A;
-        for (long long q = base; q < base + cnt; ++q) {
-            if (q >= d.dot_cap || !f.want(q)) continue;
+        for (long long q = next_wanted(d, f, base, base + cnt); q < base + cnt; q = next_wanted(d, f, q + 1, base + cnt)) {
             const int sub = d.dsub[q];
             const int s = sub >> 16, t = sub & 0x7fff;
             if (s != cur) { A = tor_point_arc(d, U, s, arc == 1); cur = s; }
@@ -414,8 +422,7 @@ __device__ __forceinline__ void conc_unit_dots(const Dev& d, long long p, const 
     const int cnt = d.conc_cnt[p];
     int cur = -1;
     LatU<T> L;
-    for (long long q = base; q < base + cnt; ++q) {
-        if (q >= d.dot_cap || !f.want(q)) continue;
+    for (long long q = next_wanted(d, f, base, base + cnt); q < base + cnt; q = next_wanted(d, f, q + 1, base + cnt)) {
         const int sub = d.dsub[q];
         const int l = sub >> 16, i = sub & 0xffff;
         if (l != cur) { L = conc_lat(d, U, l); cur = l; }
@@ -465,13 +472,11 @@ void launch_recompute(const Dev& d, double* xyz, double* area, cudaStream_t s)
 // ---------------------------------------------------------------------------
 // adjoint
 // ---------------------------------------------------------------------------
-// a dot with a non-zero adjoint makes its unit active
+// a dot given an adjoint makes its unit active and counts toward the unit's work
 __device__ __forceinline__ void mark_unit(const Dev& d, const AdjBuf& a, int dot)
 {
     const int t = d.dtype[dot], u = d.dunit[dot];
-    if (t == 1) a.act_conv[u] = 1;
-    else if (t == 2) a.act_tor[u] = 1;
-    else a.act_conc[u] = 1;
+    atomicAdd(t == 1 ? &a.act_conv[u] : (t == 2 ? &a.act_tor[u] : &a.act_conc[u]), 1);
 }
 
 // pass 1: query dots of `side`; A = (d/dp, d/darea) per dot
@@ -572,15 +577,15 @@ __global__ void k_adj_collect(Dev d, AdjBuf a)
     }
 }
 
-// Active units ordered by their dot count, largest first, so the units that
-// share a warp run loops of similar length (a counting sort on the clamped
-// count; the order inside a key does not matter: every unit writes its own
-// slots and the gather sums them in a fixed order).
+// Active units ordered by the number of their dots given an adjoint, largest
+// first, so the units that share a warp run loops of similar length (a
+// counting sort on the clamped count; the order inside a key does not matter:
+// every unit writes its own slots and the gather sums them in a fixed order).
 static constexpr int ADJ_KEYS = 256;
 
-__device__ __forceinline__ int adj_unit_key(const Dev& d, int kind, int u)
+__device__ __forceinline__ int adj_unit_key(const AdjBuf& a, int kind, int u)
 {
-    const int c = kind == 0 ? d.conv_cnt[u] : (kind == 1 ? d.tor1_cnt[u] + d.tor2_cnt[u] : d.conc_cnt[u]);
+    const int c = kind == 0 ? a.act_conv[u] : (kind == 1 ? a.act_tor[u] : a.act_conc[u]);
     return ADJ_KEYS - 1 - min(max(c, 0), ADJ_KEYS - 1);
 }
 
@@ -602,7 +607,7 @@ __global__ void k_adj_key_count(Dev d, AdjBuf a)
     const long long total = (long long)a.nact[0] + a.nact[1] + a.nact[2];
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
         int kind, u;
-        if (adj_entry(a, e, kind, u)) atomicAdd(&h[kind * ADJ_KEYS + adj_unit_key(d, kind, u)], 1);
+        if (adj_entry(a, e, kind, u)) atomicAdd(&h[kind * ADJ_KEYS + adj_unit_key(a, kind, u)], 1);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < 3 * ADJ_KEYS; i += blockDim.x)
@@ -639,7 +644,7 @@ __global__ void k_adj_key_scatter(Dev d, AdjBuf a)
     for (long long e0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); e0 < total; e0 += stride) {
         int kind = 0, u = 0, slot = -1;
         const bool on = adj_entry(a, e0 + lane, kind, u);
-        if (on) slot = kind * ADJ_KEYS + adj_unit_key(d, kind, u);
+        if (on) slot = kind * ADJ_KEYS + adj_unit_key(a, kind, u);
         const unsigned peers = __match_any_sync(0xffffffffu, slot);
         int base = 0;
         if (on && (peers & lt) == 0) base = atomicAdd(&a.skey[slot], __popc(peers));
