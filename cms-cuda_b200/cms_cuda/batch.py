@@ -90,19 +90,11 @@ class BatchCalculator:
         are in place when it returns.
         """
         import torch
-        if len(grad_outs) != len(batches):
-            raise ValueError("one gradient buffer per batch")
         if not self._grad:
             self.ctx.set_backward(True, target_side=True)
             self._grad = True
         dev = torch.device("cuda", self.ctx.device)
-        n = int(np.asarray(batches[0][0])[-1])
-        for off, nb, x, r in batches:
-            if int(np.asarray(off)[-1]) != n or np.shape(x) != (n, 3) or np.shape(r) != (n,) or len(nb) != len(off) - 1:
-                raise ValueError("run_stream needs batches of one atom count, with N x 3 coordinates and N radii")
-        for g in grad_outs:
-            if g.dtype != np.float64 or g.shape != (n, 3) or not g.flags.c_contiguous:
-                raise ValueError(f"each gradient buffer must be a C-contiguous float64 array of shape ({n}, 3)")
+        n = check_stream_args(batches, grad_outs)
         stage_x = [torch.empty((n, 3), dtype=torch.float64, device=dev) for _ in range(2)]
         stage_r = [torch.empty(n, dtype=torch.float64, device=dev) for _ in range(2)]
         stage_g = [torch.empty((n, 3), dtype=torch.float64, device=dev) for _ in range(2)]
@@ -147,6 +139,23 @@ class BatchCalculator:
 
     def profile_stages(self):
         return self.ctx.profile_stages()
+
+
+def check_stream_args(batches, grad_outs):
+    """Atom count N of a run_stream call; ValueError unless every batch has N atoms (N x 3 coordinates, N radii,
+    consistent offsets) and there is one C-contiguous float64 N x 3 gradient buffer per batch."""
+    if not batches:
+        raise ValueError("no batches")
+    if len(grad_outs) != len(batches):
+        raise ValueError("one gradient buffer per batch")
+    n = int(np.asarray(batches[0][0])[-1])
+    for off, nb, x, r in batches:
+        if int(np.asarray(off)[-1]) != n or np.shape(x) != (n, 3) or np.shape(r) != (n,) or len(nb) != len(off) - 1:
+            raise ValueError("run_stream needs batches of one atom count, with N x 3 coordinates and N radii")
+    for g in grad_outs:
+        if g.dtype != np.float64 or g.shape != (n, 3) or not g.flags.c_contiguous:
+            raise ValueError(f"each gradient buffer must be a C-contiguous float64 array of shape ({n}, 3)")
+    return n
 
 
 def pack(complexes):

@@ -105,3 +105,21 @@ def test_gpu_missing_raises_not_falls_back(monkeypatch):
             api.calculate_contact_ms(np.zeros((1, 3)), np.ones(1), np.ones((1, 3)), np.ones(1))
     finally:
         api.gpu_available.cache_clear()
+
+
+def test_stream_arguments_are_checked_before_any_gpu_work():
+    """BatchCalculator.run_stream's argument check: one atom count, one float64 N x 3 buffer per batch."""
+    from cms_cuda.batch import check_stream_args
+    off = np.array([0, 3, 7]); nb = np.array([1, 2])
+    b = (off, nb, np.zeros((7, 3)), np.ones(7))
+    assert check_stream_args([b, b], [np.zeros((7, 3)), np.zeros((7, 3))]) == 7
+    with pytest.raises(ValueError):
+        check_stream_args([b, b], [np.zeros((7, 3))])
+    with pytest.raises(ValueError):
+        check_stream_args([b, (np.array([0, 3, 6]), nb, np.zeros((6, 3)), np.ones(6))], [np.zeros((7, 3))] * 2)
+    with pytest.raises(ValueError):
+        check_stream_args([b], [np.zeros((7, 3), np.float32)])
+    with pytest.raises(ValueError):
+        check_stream_args([b], [np.zeros((3, 7)).T])
+    with pytest.raises(ValueError):
+        check_stream_args([], [])
