@@ -90,11 +90,11 @@ class BatchCalculator:
         are in place when it returns.
         """
         import torch
+        n = check_stream_args(batches, grad_outs)
         if not self._grad:
             self.ctx.set_backward(True, target_side=True)
             self._grad = True
         dev = torch.device("cuda", self.ctx.device)
-        n = check_stream_args(batches, grad_outs)
         stage_x = [torch.empty((n, 3), dtype=torch.float64, device=dev) for _ in range(2)]
         stage_r = [torch.empty(n, dtype=torch.float64, device=dev) for _ in range(2)]
         stage_g = [torch.empty((n, 3), dtype=torch.float64, device=dev) for _ in range(2)]
