@@ -10,6 +10,7 @@
 
 #include "../../include/cms_b200.h"
 #include "cms_readout.cuh"
+#include "cms_circle.cuh"
 
 using namespace cms;
 
@@ -293,7 +294,7 @@ struct cms_ctx {
         S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1, S_KS_TOP, S_KS_BUF, S_CV_SOFF, S_CC_SOFF, S_TOR_SOFF, S_TOR_SN, S_NBS_TOP, S_NBS_BUF, S_NB_SOFF, S_ADJ_SKEY, S_ADJ_SLIST_CONV, S_ADJ_SLIST_TOR, S_ADJ_SLIST_CONC, S_CS_TOP, S_CS_XYZ, S_CS_AREA, S_CS_OWN,
         S_CS_SUB, S_CS_BUR, S_RES_OFF, S_RES_ATOMS, S_RES_SUM, S_RES_FLAG, S_NN_COUNT, S_PLC_CNT, S_PLC_FILL, S_PLC_START,
         S_PLC_ITEM, S_PLC_CELL, S_TILE_CNT2, S_TILE_OFF2, S_ROUND_CNT2, S_ROUND_OFF2, S_BOX_ROUND2,
-        S_BOX_BLK2, S_SCAN_TMP2, S_R_SC_D2,
+        S_BOX_BLK2, S_SCAN_TMP2, S_R_SC_D2, S_TOR_GEO,
         S_COUNT
     };
 
@@ -424,6 +425,7 @@ void bind_caps(cms_ctx* x)
     d.nbs_buf = x->ensure<int>(cms_ctx::S_NBS_BUF, d.nbs_cap);
     d.tor_cap = x->cap_tor;
     d.tor_i = x->ensure<int>(cms_ctx::S_TOR_I, x->cap_tor);
+    d.tor_geo = x->ensure<TorGeo>(cms_ctx::S_TOR_GEO, x->cap_tor);
     d.tor_j = x->ensure<int>(cms_ctx::S_TOR_J, x->cap_tor);
     d.tor1_cnt = x->ensure<int>(cms_ctx::S_TOR1_CNT, x->cap_tor);
     d.tor2_cnt = x->ensure<int>(cms_ctx::S_TOR2_CNT, x->cap_tor);

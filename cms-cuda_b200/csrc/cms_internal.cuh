@@ -87,6 +87,7 @@ struct Dev {
     int* ntor; long long* tor_off;     // N, N+1
     long long tor_cap;
     int* tor_i; int* tor_j;            // tor_cap
+    struct TorGeo* tor_geo;            // tor_cap: each toroid's circle, made after the pair loop (k_tor_geo)
     // probes: per atom counts of + and - probes, per complex layout
     int* nplus; long long* plus_off;   // N, N+1
     int* nminus; long long* minus_off; // N, N+1

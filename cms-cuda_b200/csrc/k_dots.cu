@@ -327,52 +327,6 @@ void launch_convex(const Dev& d, bool emit, cudaStream_t s)
 // NPB * 32 pruned atom ids (past it: the full lists are scanned) and as many
 // kept torus points (past it: the batch is not kept).
 
-struct TorPair {
-    int i, j;
-    V3 xi, xj, uij, tij;
-    double ri, rj, eri, erj, rij, density, ts, dtor, darc;
-    bool between;
-    int ns;
-    V3 fx, fy;
-};
-
-__device__ __forceinline__ TorPair tor_pair(const Dev& d, long long q)
-{
-    TorPair T;
-    const double rp = d.st.rp;
-    T.i = d.tor_i[q]; T.j = d.tor_j[q];
-    double4 a = d.xyzr[T.i], b = d.xyzr[T.j];
-    T.xi = v3(a.x, a.y, a.z); T.xj = v3(b.x, b.y, b.z);
-    T.ri = a.w; T.rj = b.w;
-    // pair geometry, as second_loop computes it (_core.py:1372-1416)
-    V3 diff = T.xj - T.xi;
-    double dij_sq = sq_alt(diff);
-    double dij = sqrt(dij_sq);
-    T.eri = T.ri + rp; T.erj = T.rj + rp;
-    double asymm = (T.eri * T.eri - T.erj * T.erj) / dij;
-    T.between = fabs(asymm) < dij;
-    T.uij = diff / dij;
-    T.tij = ((T.xi + T.xj) * 0.5) + T.uij * (asymm * 0.5);
-    double far_sq = (T.eri + T.erj) * (T.eri + T.erj) - dij_sq;
-    double rd = T.ri - T.rj;
-    double cont_sq = dij_sq - rd * rd;
-    T.rij = ((0.5 * sqrt(far_sq)) * sqrt(cont_sq)) / dij;
-    // torus circle subdivision (_core.py:1863-1885)
-    T.density = (d.dens[T.i] + d.dens[T.j]) * 0.5;
-    double rci = (T.rij * T.ri) / T.eri;
-    double rcj = (T.rij * T.rj) / T.erj;
-    double rbt = T.rij - rp;
-    double rb = rbt < 0.0 ? 0.0 : rbt;                 // np.maximum keeps NaN
-    double rs = ((rci + 2.0 * rb) + rcj) * 0.25;
-    double e = rs / T.rij;
-    double edens = (e * e) * T.density;
-    circle_frame(T.uij, T.fx, T.fy);
-    T.dtor = subdiv_delta(edens, T.rij);
-    T.ns = subdiv_count(T.dtor, CMS_TWO_PI);
-    T.ts = subdiv_ps(T.rij, CMS_TWO_PI, T.ns);
-    T.darc = subdiv_delta(T.density, rp);
-    return T;
-}
 
 // atoms of ids[s, e) other than `skip` that may reach the torus circle of T
 __device__ __forceinline__ int tor_prune(const Dev& d, const TorPair& T, const int* ids, long long s, long long e,
@@ -596,7 +550,7 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_toroidal(Dev d)
         bool kok = true;                           // emit: the pair's torus points with arc dots were kept
         if (lane < np) {
             const long long q = EMIT ? (long long)d.tor_list[q0 + lane] : q0 + lane;
-            const TorPair T = tor_pair(d, q);
+            const TorPair T = tor_pair_load(d, q);
             tp[w][lane] = T;
             tq[w][lane] = (int)q;
             nsv[w][lane] = T.ns;

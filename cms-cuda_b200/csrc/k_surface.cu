@@ -11,6 +11,7 @@
 // cdist / np.sum / norm, dot_alt for einsum) and strictness.
 #include <type_traits>
 
+#include "cms_circle.cuh"
 #include "cms_kernels.cuh"
 
 namespace cms {
@@ -654,10 +655,23 @@ __global__ void k_pairs(Dev d)
     }
 }
 
+// each toroid's circle, one thread per toroid, for the toroidal count and emit passes
+__global__ void k_tor_geo(Dev d)
+{
+    CMS_EXIT_ON_OVERFLOW(d);
+    const long long NT = min(d.tor_off[d.N], d.tor_cap);
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < NT; q += (long long)gridDim.x * blockDim.x)
+        tor_geo_store(d, q, tor_pair_of(d, d.tor_i[q], d.tor_j[q]));
+}
+
 void launch_pairs(const Dev& d, bool emit, cudaStream_t s)
 {
-    if (emit) k_pairs<true><<<grid_for(d.N, 128), 128, 0, s>>>(d);
-    else k_pairs<false><<<grid_for(d.N, 128), 128, 0, s>>>(d);
+    if (emit) {
+        k_pairs<true><<<grid_for(d.N, 128), 128, 0, s>>>(d);
+        k_tor_geo<<<grid_for(d.tor_cap, 128), 128, 0, s>>>(d);
+    } else {
+        k_pairs<false><<<grid_for(d.N, 128), 128, 0, s>>>(d);
+    }
 }
 
 // ---------------------------------------------------------------------------
