@@ -294,7 +294,7 @@ struct cms_ctx {
         S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1, S_KS_TOP, S_KS_BUF, S_CV_SOFF, S_CC_SOFF, S_TOR_SOFF, S_TOR_SN, S_NBS_TOP, S_NBS_BUF, S_NB_SOFF, S_ADJ_SKEY, S_ADJ_SLIST_CONV, S_ADJ_SLIST_TOR, S_ADJ_SLIST_CONC, S_CS_TOP, S_CS_XYZ, S_CS_AREA, S_CS_OWN,
         S_CS_SUB, S_CS_BUR, S_RES_OFF, S_RES_ATOMS, S_RES_SUM, S_RES_FLAG, S_NN_COUNT, S_PLC_CNT, S_PLC_FILL, S_PLC_START,
         S_PLC_ITEM, S_PLC_CELL, S_TILE_CNT2, S_TILE_OFF2, S_ROUND_CNT2, S_ROUND_OFF2, S_BOX_ROUND2,
-        S_BOX_BLK2, S_SCAN_TMP2, S_R_SC_D2, S_TOR_GEO,
+        S_BOX_BLK2, S_SCAN_TMP2, S_R_SC_D2, S_TOR_GEO, S_CC_GEO,
         S_COUNT
     };
 
@@ -460,6 +460,7 @@ void bind_caps(cms_ctx* x)
     d.sp_g = x->ensure<int>(cms_ctx::S_SP_G, x->cap_probe);
     d.sp_ord = x->ensure<unsigned>(cms_ctx::S_SP_ORD, x->cap_probe);
     d.conc_cnt = x->ensure<int>(cms_ctx::S_CONC_CNT, x->cap_probe);
+    d.cc_geo = x->ensure<ConcGeo>(cms_ctx::S_CC_GEO, x->cap_probe);
     d.conc_off = x->ensure<long long>(cms_ctx::S_CONC_OFF, x->cap_probe + 1);
     d.cc_soff = x->ensure<int>(cms_ctx::S_CC_SOFF, x->cap_probe);
     d.cs_cap = x->cap_conc;
@@ -663,6 +664,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
     if (stashed) launch_probe_scatter(d, x->cap_probe, s);
     else launch_triples(d, true, x->sv[4], s);
     launch_low_probes(d, x->cap_probe, tmp, s);
+    launch_probe_geo(d, x->cap_probe, s);
     mark(x, P_TRIPLES_EMIT);
     ck(cudaMemsetAsync(d.tor1_cnt, 0, sizeof(int) * x->cap_tor, s), "memset");
     ck(cudaMemsetAsync(d.tor2_cnt, 0, sizeof(int) * x->cap_tor, s), "memset");

@@ -67,6 +67,15 @@ __device__ __forceinline__ TorPair tor_pair_of(const Dev& d, int i, int j)
     return T;
 }
 
+// a probe's spherical-triangle frame for the concave dots (k_probe_geo): the
+// three plane normals, the top vertex and the latitude arc's second axis, the
+// frame of the latitude circles, the latitude spacing and count, the arc step
+struct ConcGeo {
+    double v0[3], v1[3], v2[3], top[3], ylat[3], fx[3], fy[3];
+    double dl, cs;
+    int nl;
+};
+
 struct TorGeo {
     double ux, uy, uz, tx, ty, tz, fxx, fxy, fxz, fyx, fyy, fyz;
     double rij, ts, dtor, darc;

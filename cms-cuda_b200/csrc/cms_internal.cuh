@@ -113,6 +113,7 @@ struct Dev {
     int* tor_lflag; long long* tor_loff;         // tor_cap, +1: pair has dots, its exclusive scan
     int* tor_list;                               // tor_cap: pairs with dots, in pair order (emit work list)
     int* conc_cnt; long long* conc_off;          // probe_cap, +1
+    struct ConcGeo* cc_geo;                      // probe_cap: each probe's spherical-triangle frame (k_probe_geo)
     // kept candidates of the convex and concave count passes: (latitude << 16 | point) in candidate
     // order per unit, so the emit passes write those alone; cv_soff / cc_soff: first entry (-1: none)
     unsigned long long* ks_top;                  // 1: entries taken

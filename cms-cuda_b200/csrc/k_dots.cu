@@ -863,31 +863,15 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
             }
             __syncwarp();
         }
-        // spherical-triangle frame (_core.py:2140-2164)
-        V3 vp[3];
-        for (int k = 0; k < 3; ++k) vp[k] = normalize3(xa[k] - pijk);
-        const V3 vec0 = normalize3(cross3(vp[0], vp[1]));
-        const V3 vec1 = normalize3(cross3(vp[1], vp[2]));
-        const V3 vec2 = normalize3(cross3(vp[2], vp[0]));
-        double dts[3];
-        for (int k = 0; k < 3; ++k) dts[k] = dot_seq(uijk, vp[k]);
-        int mm = 0;                                   // np.argmax: first maximum, NaN wins
-        if (!isnan(dts[0])) {
-            for (int k = 1; k < 3; ++k) {
-                if (isnan(dts[k])) { mm = k; break; }
-                if (dts[k] > dts[mm]) mm = k;
-            }
-        }
+        // spherical-triangle frame (_core.py:2140-2164), made by k_probe_geo
+        const ConcGeo G = d.cc_geo[p];
+        const V3 vec0 = v3(G.v0[0], G.v0[1], G.v0[2]), vec1 = v3(G.v1[0], G.v1[1], G.v1[2]);
+        const V3 vec2 = v3(G.v2[0], G.v2[1], G.v2[2]);
         const V3 south = -uijk;
-        const V3 vtop = vp[mm];
-        const V3 axis = normalize3(cross3(vtop, south));
-        V3 ylat;
-        const double ang = arc_angle(axis, vtop, south, ylat);
-        const double dl = subdiv_delta(density, rp);
-        const int nl = subdiv_count_long(dl, ang);
-        const double cs = subdiv_ps(rp, ang, nl);
-        V3 fx, fy;
-        circle_frame(south, fx, fy);
+        const V3 vtop = v3(G.top[0], G.top[1], G.top[2]), ylat = v3(G.ylat[0], G.ylat[1], G.ylat[2]);
+        const V3 fx = v3(G.fx[0], G.fx[1], G.fx[2]), fy = v3(G.fy[0], G.fy[1], G.fy[2]);
+        const double dl = G.dl, cs = G.cs;
+        const int nl = G.nl;
         for (int l = lane; l < nl; l += 32) {
             V3 lat = subdiv_point_called(v3(0.0, 0.0, 0.0), rp, vtop, ylat, dl, l);
             double dt = dot_seq(lat, south);
@@ -987,6 +971,62 @@ __global__ void __launch_bounds__(CC_WARPS * 32, MINB) k_concave(Dev d)
         }
         __syncwarp();
     }
+}
+
+// Each probe's spherical-triangle frame, one thread per probe (the concave
+// count and emit passes load it; a warp per probe computing it on every lane
+// spent a long FP64 chain per probe before its points)
+__global__ void k_probe_geo(Dev d)
+{
+    CMS_EXIT_ON_OVERFLOW(d);
+    const double rp = d.st.rp;
+    const long long NP = min(d.plus_off[d.N] + d.minus_off[d.N], d.probe_cap);
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < NP; p += (long long)gridDim.x * blockDim.x) {
+        const int ia[3] = {d.pa0[p], d.pa1[p], d.pa2[p]};
+        V3 xa[3];
+        for (int k = 0; k < 3; ++k) { const double4 a = d.xyzr[ia[k]]; xa[k] = v3(a.x, a.y, a.z); }
+        const double density = ((d.dens[ia[0]] + d.dens[ia[1]]) + d.dens[ia[2]]) / 3.0;
+        const V3 pijk = ld3(d.pxyz + 3 * p);
+        const V3 uijk = ld3(d.palt + 3 * p);
+        V3 vp[3];
+        for (int k = 0; k < 3; ++k) vp[k] = normalize3(xa[k] - pijk);
+        const V3 vec0 = normalize3(cross3(vp[0], vp[1]));
+        const V3 vec1 = normalize3(cross3(vp[1], vp[2]));
+        const V3 vec2 = normalize3(cross3(vp[2], vp[0]));
+        double dts[3];
+        for (int k = 0; k < 3; ++k) dts[k] = dot_seq(uijk, vp[k]);
+        int mm = 0;                                   // np.argmax: first maximum, NaN wins
+        if (!isnan(dts[0])) {
+            for (int k = 1; k < 3; ++k) {
+                if (isnan(dts[k])) { mm = k; break; }
+                if (dts[k] > dts[mm]) mm = k;
+            }
+        }
+        const V3 south = -uijk;
+        const V3 vtop = vp[mm];
+        const V3 axis = normalize3(cross3(vtop, south));
+        V3 ylat;
+        const double ang = arc_angle(axis, vtop, south, ylat);
+        ConcGeo G;
+        G.dl = subdiv_delta(density, rp);
+        G.nl = subdiv_count_long(G.dl, ang);
+        G.cs = subdiv_ps(rp, ang, G.nl);
+        V3 fx, fy;
+        circle_frame(south, fx, fy);
+        G.v0[0] = vec0.x; G.v0[1] = vec0.y; G.v0[2] = vec0.z;
+        G.v1[0] = vec1.x; G.v1[1] = vec1.y; G.v1[2] = vec1.z;
+        G.v2[0] = vec2.x; G.v2[1] = vec2.y; G.v2[2] = vec2.z;
+        G.top[0] = vtop.x; G.top[1] = vtop.y; G.top[2] = vtop.z;
+        G.ylat[0] = ylat.x; G.ylat[1] = ylat.y; G.ylat[2] = ylat.z;
+        G.fx[0] = fx.x; G.fx[1] = fx.y; G.fx[2] = fx.z;
+        G.fy[0] = fy.x; G.fy[1] = fy.y; G.fy[2] = fy.z;
+        d.cc_geo[p] = G;
+    }
+}
+
+void launch_probe_geo(const Dev& d, long long probe_grid, cudaStream_t s)
+{
+    k_probe_geo<<<grid_for(probe_grid, 128), 128, 0, s>>>(d);
 }
 
 void launch_concave(const Dev& d, long long probe_grid, bool emit, int variant, cudaStream_t s)
