@@ -294,7 +294,7 @@ struct cms_ctx {
         S_SO_F4_0, S_SO_F4_1, S_SO_PERM_0, S_SO_PERM_1, S_KS_TOP, S_KS_BUF, S_CV_SOFF, S_CC_SOFF, S_TOR_SOFF, S_TOR_SN, S_NBS_TOP, S_NBS_BUF, S_NB_SOFF, S_ADJ_SKEY, S_ADJ_SLIST_CONV, S_ADJ_SLIST_TOR, S_ADJ_SLIST_CONC, S_CS_TOP, S_CS_XYZ, S_CS_AREA, S_CS_OWN,
         S_CS_SUB, S_CS_BUR, S_RES_OFF, S_RES_ATOMS, S_RES_SUM, S_RES_FLAG, S_NN_COUNT, S_PLC_CNT, S_PLC_FILL, S_PLC_START,
         S_PLC_ITEM, S_PLC_CELL, S_TILE_CNT2, S_TILE_OFF2, S_ROUND_CNT2, S_ROUND_OFF2, S_BOX_ROUND2,
-        S_BOX_BLK2, S_SCAN_TMP2, S_R_SC_D2, S_TOR_GEO, S_CC_GEO,
+        S_BOX_BLK2, S_SCAN_TMP2, S_R_SC_D2, S_TOR_GEO, S_CC_GEO, S_CV_GEO,
         S_COUNT
     };
 
@@ -380,6 +380,7 @@ void bind_batch(cms_ctx* x)
     d.nminus = x->ensure<int>(cms_ctx::S_NMINUS, N);
     d.minus_off = x->ensure<long long>(cms_ctx::S_MINUS_OFF, N + 1);
     d.conv_cnt = x->ensure<int>(cms_ctx::S_CONV_CNT, N);
+    d.cv_geo = x->ensure<CvGeo>(cms_ctx::S_CV_GEO, N);
     d.conv_off = x->ensure<long long>(cms_ctx::S_CONV_OFF, N + 1);
     d.cv_soff = x->ensure<int>(cms_ctx::S_CV_SOFF, N);
     d.ks_top = x->ensure<unsigned long long>(cms_ctx::S_KS_TOP, 1);
@@ -665,6 +666,7 @@ void enqueue_surface(cms_ctx* x, bool sized)
     else launch_triples(d, true, x->sv[4], s);
     launch_low_probes(d, x->cap_probe, tmp, s);
     launch_probe_geo(d, x->cap_probe, s);
+    launch_convex_geo(d, s);
     mark(x, P_TRIPLES_EMIT);
     ck(cudaMemsetAsync(d.tor1_cnt, 0, sizeof(int) * x->cap_tor, s), "memset");
     ck(cudaMemsetAsync(d.tor2_cnt, 0, sizeof(int) * x->cap_tor, s), "memset");

@@ -76,6 +76,14 @@ struct ConcGeo {
     int nl;
 };
 
+// a convex atom's frame (k_convex_geo): the pole, the latitude arc's second
+// axis, the frame of the latitude circles, the latitude spacing, step and count
+struct CvGeo {
+    double north[3], ylat[3], fx[3], fy[3];
+    double dl, cs;
+    int nl;
+};
+
 struct TorGeo {
     double ux, uy, uz, tx, ty, tz, fxx, fxy, fxz, fyx, fyy, fyz;
     double rij, ts, dtor, darc;

@@ -107,6 +107,7 @@ struct Dev {
     int* sp_g; unsigned* sp_ord;               // probe_cap
     // dots
     int* conv_cnt; long long* conv_off;          // N, N+1
+    struct CvGeo* cv_geo;                        // N: each convex atom's frame (k_convex_geo)
     int* tor1_cnt; long long* tor1_off;          // tor_cap, +1
     int* tor2_cnt; long long* tor2_off;          // tor_cap, +1
     int8_t* tor_has;                             // tor_cap (toroidal access)

@@ -22,6 +22,7 @@ void launch_low_probes(const Dev& d, long long probe_cap, long long* scan_tmp, c
 // dots (k_dots.cu)
 void launch_convex(const Dev& d, bool emit, cudaStream_t s);
 void launch_probe_geo(const Dev& d, long long probe_grid, cudaStream_t s);
+void launch_convex_geo(const Dev& d, cudaStream_t s);
 // variant: the autotuned shape (toroidal: 0 = 16 pairs x 4 warps, 1 = 32 pairs x 2 warps per batch / CTA,
 // 2 = 16 x 4 with registers for 6 CTAs per SM; concave: registers for 4, 5 or 6 CTAs per SM)
 static constexpr int SURF_VARIANTS = 3;

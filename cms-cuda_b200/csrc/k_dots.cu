@@ -176,41 +176,12 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 10 : 12) k_convex(Dev d)
         const V3 xi = v3(ai.x, ai.y, ai.z);
         const double ri = ai.w, eri = ri + rp, dens = d.dens[g];
         const long long off = d.nb_off[g];
-        // frame from the nearest neighbour (_core.py:1665-1726)
-        const int n0 = d.nb_id[off];
-        const double4 an = d.xyzr[n0];
-        const V3 xn = v3(an.x, an.y, an.z);
-        const V3 north = normalize3(xi - xn);
-        V3 vt = v3(north.y * north.y + north.z * north.z, north.x * north.x + north.z * north.z,
-                   north.x * north.x + north.y * north.y);
-        vt = normalize3(vt);
-        if (fabs(dot_seq(vt, north)) > 0.99) vt = v3(1.0, 0.0, 0.0);
-        const V3 eq = normalize3(cross3(north, vt));
-        const V3 vql = cross3(eq, north);
-        V3 south = v3(0.0, 0.0, -1.0);
-        {
-            const double rj = an.w, erj = rj + rp;
-            const double dij = norm3(xn - xi);
-            const V3 uij = (xn - xi) / dij;
-            const double asymm = (eri * eri - erj * erj) / dij;
-            const V3 tij = ((xi + xn) * 0.5) + uij * (asymm * 0.5);
-            const double far_sq = (eri + erj) * (eri + erj) - dij * dij;
-            const double rd = ri - rj;
-            const double contain_sq = dij * dij - rd * rd;
-            if (far_sq > 0.0 && contain_sq > 0.0) {
-                const double rij = ((0.5 * sqrt(far_sq)) * sqrt(contain_sq)) / dij;
-                const V3 pij = tij + vql * rij;
-                south = (pij - xi) / eri;
-            }
-        }
-        // latitude arc from north to south in the (north, eq x north) plane
-        V3 ylat;
-        const double ang = arc_angle(eq, north, south, ylat);
-        const double dl = subdiv_delta(dens, ri);
-        const int nl = subdiv_count_long(dl, ang);
-        const double cs = subdiv_ps(ri, ang, nl);
-        V3 fx, fy;
-        circle_frame(north, fx, fy);
+        // frame from the nearest neighbour (_core.py:1665-1726), made by k_convex_geo
+        const CvGeo G = d.cv_geo[g];
+        const V3 north = v3(G.north[0], G.north[1], G.north[2]), ylat = v3(G.ylat[0], G.ylat[1], G.ylat[2]);
+        const V3 fx = v3(G.fx[0], G.fx[1], G.fx[2]), fy = v3(G.fy[0], G.fy[1], G.fy[2]);
+        const double dl = G.dl, cs = G.cs;
+        const int nl = G.nl;
         for (int l = lane; l < nl; l += 32) {
             V3 lat = subdiv_point(v3(0.0, 0.0, 0.0), ri, north, ylat, dl, l);
             double dt = dot_seq(lat, north);
@@ -294,6 +265,71 @@ __global__ void __launch_bounds__(CV_WARPS * 32, EMIT ? 10 : 12) k_convex(Dev d)
         }
         __syncwarp();
     }
+}
+
+// Each convex atom's frame, one thread per atom (the convex count and emit
+// passes load it; a warp per atom computing it on every lane spent a long FP64
+// chain per atom before its points)
+__global__ void k_convex_geo(Dev d)
+{
+    CMS_EXIT_ON_OVERFLOW(d);
+    const double rp = d.st.rp;
+    for (long long gg = blockIdx.x * (long long)blockDim.x + threadIdx.x; gg < d.N; gg += (long long)gridDim.x * blockDim.x) {
+        const int g = (int)gg;
+        const int K = d.nnb[g];
+        if (!(K > 0 && d.access[g] != 0 && d.atten[g] > 1)) continue;
+        const double4 ai = d.xyzr[g];
+        const V3 xi = v3(ai.x, ai.y, ai.z);
+        const double ri = ai.w, eri = ri + rp, dens = d.dens[g];
+        const long long off = d.nb_off[g];
+        // frame from the nearest neighbour (_core.py:1665-1726)
+        const int n0 = d.nb_id[off];
+        const double4 an = d.xyzr[n0];
+        const V3 xn = v3(an.x, an.y, an.z);
+        const V3 north = normalize3(xi - xn);
+        V3 vt = v3(north.y * north.y + north.z * north.z, north.x * north.x + north.z * north.z,
+                   north.x * north.x + north.y * north.y);
+        vt = normalize3(vt);
+        if (fabs(dot_seq(vt, north)) > 0.99) vt = v3(1.0, 0.0, 0.0);
+        const V3 eq = normalize3(cross3(north, vt));
+        const V3 vql = cross3(eq, north);
+        V3 south = v3(0.0, 0.0, -1.0);
+        {
+            const double rj = an.w, erj = rj + rp;
+            const double dij = norm3(xn - xi);
+            const V3 uij = (xn - xi) / dij;
+            const double asymm = (eri * eri - erj * erj) / dij;
+            const V3 tij = ((xi + xn) * 0.5) + uij * (asymm * 0.5);
+            const double far_sq = (eri + erj) * (eri + erj) - dij * dij;
+            const double rd = ri - rj;
+            const double contain_sq = dij * dij - rd * rd;
+            if (far_sq > 0.0 && contain_sq > 0.0) {
+                const double rij = ((0.5 * sqrt(far_sq)) * sqrt(contain_sq)) / dij;
+                const V3 pij = tij + vql * rij;
+                south = (pij - xi) / eri;
+            }
+        }
+        // latitude arc from north to south in the (north, eq x north) plane
+        V3 ylat;
+        const double ang = arc_angle(eq, north, south, ylat);
+        const double dl = subdiv_delta(dens, ri);
+        const int nl = subdiv_count_long(dl, ang);
+        const double cs = subdiv_ps(ri, ang, nl);
+        V3 fx, fy;
+        circle_frame(north, fx, fy);
+        CvGeo G;
+        G.north[0] = north.x; G.north[1] = north.y; G.north[2] = north.z;
+        G.ylat[0] = ylat.x; G.ylat[1] = ylat.y; G.ylat[2] = ylat.z;
+        G.fx[0] = fx.x; G.fx[1] = fx.y; G.fx[2] = fx.z;
+        G.fy[0] = fy.x; G.fy[1] = fy.y; G.fy[2] = fy.z;
+        G.dl = dl; G.cs = cs; G.nl = nl;
+        d.cv_geo[g] = G;
+    }
+}
+
+void launch_convex_geo(const Dev& d, cudaStream_t s)
+{
+    k_convex_geo<<<grid_for(d.N, 128), 128, 0, s>>>(d);
 }
 
 void launch_convex(const Dev& d, bool emit, cudaStream_t s)
