@@ -347,22 +347,14 @@ TRAFFIC_PER_UNIT = {
     "neighbor_count": (78.47e6 / 558670, "atoms"),         # per atom
     "neighbor_emit": (163.85e6 / 558670, "atoms"),
     "triples_count": (95.88e6 / 558670, "atoms"),
-    "convex_count": (19.10e6 / 558670, "atoms"),
-    "toroidal_count": (46.53e6 / 558670, "atoms"),
-    "concave_count": (20.99e6 / 558670, "atoms"),
-    "triples_emit": (19.46e6 / 558670, "atoms"),           # the probe scatter
-    "toroidal_emit": (365.19e6 / 5021616, "toroidal"),     # per toroidal dot
     "cms_nn": (273.01e6 / 2750610, "cms_queries"),         # per query dot (k_nn_w, 4 queries per lane)
     "sc_band_nn": (251.90e6 / 2750610, "band_queries"),
 }
 
 # FP64 pipe utilisation of the FP64-bound stages (sm__pipe_fp64_cycles_active %, ncu --set full on the
-# 256-complex batch; the captures under profiles/)
+# 256-complex batch; the captures under profiles/; stages whose kernels changed since their capture are left out)
 FP64_PIPE_PCT = {
     "triples_count": (19.6, "profiles/fp64_count_passes_256_complexes.md"),
-    "toroidal_count": (26.5, "profiles/fp64_count_passes_256_complexes.md"),
-    "concave_count": (28.9, "profiles/fp64_count_passes_256_complexes.md"),
-    "convex_count": (37.4, "profiles/fp64_count_passes_256_complexes.md"),
     "cms_backward": (19.6, "profiles/k_adj_units_256_complexes.md"),
 }
 NN_STAGES = {"cms_nn": "cms", "sc_band_nn": "band", "sc_argmin_nn": "sc"}
